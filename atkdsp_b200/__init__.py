@@ -1,0 +1,332 @@
+"""atkdsp_b200 -- the atkdsp channelizer path on B200, with atkdsp's Python surface.
+
+This package loads ``lib/libatkdsp_b200.so`` (built in-tree by ``make -C
+atkdsp_b200``), a C-ABI library that exports the reference's
+``atkdsp_pfb_*`` / ``atkdsp_unpack*`` entry points and runs them on the GPU.
+The Python names, arguments, return shapes and errors below mirror the
+reference binding's (python/atkdsp/__init__.py: ``Pfb`` at :4159-4219,
+``unpack`` / ``unpack_dc`` at :337-385, W1/W2 at :4222-4266, identity at
+:285-313), so code and tests written against ``atkdsp`` read the same here.
+
+There is no CPU fallback: if the library is missing or no GPU is usable,
+``load()`` / ``Pfb(...)`` raise ``AtkDspError``.
+
+Every call releases the GIL (ctypes foreign calls) and is synchronous on
+return, like the reference's.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+__all__ = ["ABI_VERSION", "AtkDspError", "load", "available", "lib_path", "version",
+           "build_info", "set_threads", "get_threads", "FMT", "bytes_per_sample",
+           "unpack", "unpack_dc", "Pfb", "pfb_cov_accumulate", "pfb_cov_reset",
+           "pfb_channel_power"]
+
+#: the ABI the library reports (the reference's, include/atkdsp.h:63)
+ABI_VERSION = 26
+
+FMT = {"cu8": 0, "ci8": 1, "ci16": 2, "ci16_le": 2, "cs16": 2,
+       "ci16q11": 3, "cf32": 4, "cf32_le": 4}
+
+_ERRORS = {-1: "bad argument", -2: "out of memory", -3: "output buffer too small",
+           -4: "FFT backend failure"}
+
+HERE = Path(__file__).resolve().parent
+LIB_FILE = HERE / "lib" / "libatkdsp_b200.so"
+
+_lib = None
+_lib_path: Path | None = None
+
+
+class AtkDspError(RuntimeError):
+    pass
+
+
+class _Cf32(C.Structure):
+    _fields_ = [("re", C.c_float), ("im", C.c_float)]
+
+
+def _check(rc: int, what: str) -> int:
+    if rc < 0:
+        raise AtkDspError(f"{what}: {_ERRORS.get(rc, f'error {rc}')}")
+    return rc
+
+
+def _bind(lib) -> None:
+    P = C.POINTER
+    vp, sz, u, d, i64, ssz = C.c_void_p, C.c_size_t, C.c_uint, C.c_double, C.c_int64, C.c_ssize_t
+    pcf, ppcf = P(_Cf32), P(P(_Cf32))
+    sigs = {
+        "atkdsp_abi_version": ([], C.c_int),
+        "atkdsp_version_string": ([], C.c_char_p),
+        "atkdsp_build_info": ([], C.c_char_p),
+        "atkdsp_bytes_per_sample": ([C.c_int], C.c_int),
+        "atkdsp_set_threads": ([C.c_int], C.c_int),
+        "atkdsp_get_threads": ([], C.c_int),
+        "atkdsp_unpack": ([vp, sz, C.c_int, pcf, sz, C.c_float, pcf], ssz),
+        "atkdsp_unpack_dc": ([vp, sz, C.c_int, pcf, sz, C.c_float, C.c_float, P(d), P(d)], ssz),
+        "atkdsp_pfb_create": ([d, u, u, u, d, u], vp),
+        "atkdsp_pfb_destroy": ([vp], None),
+        "atkdsp_pfb_reset": ([vp], None),
+        "atkdsp_pfb_nchan": ([vp], u),
+        "atkdsp_pfb_out_rate": ([vp], d),
+        "atkdsp_pfb_out_hops": ([vp, sz], sz),
+        "atkdsp_pfb_process": ([vp, pcf, sz, pcf, sz], ssz),
+        "atkdsp_pfb_process_n": ([vp, ppcf, u, sz, pcf, sz], ssz),
+        "atkdsp_pfb_block_origin": ([vp, i64], i64),
+        "atkdsp_pfb_group_delay": ([vp], d),
+        "atkdsp_pfb_set_cal": ([vp, pcf, u], C.c_int),
+        "atkdsp_pfb_describe": ([vp, C.c_char_p, sz], C.c_int),
+        "atkdsp_pfb_cov_accumulate": ([pcf, u, u, sz, P(C.c_uint8), pcf, P(C.c_uint32)], None),
+        "atkdsp_pfb_cov_reset": ([pcf, P(C.c_uint32), u, u, P(C.c_uint8)], None),
+        "atkdsp_pfb_channel_power": ([pcf, u, u, sz, P(C.c_float), P(C.c_float)], None),
+        # device-pointer entry points (include/atkdsp_gpu.h)
+        "atkdsp_gpu_pfb_stream": ([vp], vp),
+        "atkdsp_gpu_pfb_sync": ([vp], C.c_int),
+        "atkdsp_gpu_pfb_process_n": ([vp, P(vp), u, sz, vp, sz, vp], ssz),
+        "atkdsp_gpu_unpack_dc": ([vp, sz, C.c_int, vp, sz, C.c_float, C.c_float, vp, vp], ssz),
+        "atkdsp_gpu_unpack": ([vp, sz, C.c_int, vp, sz, C.c_float, vp, vp], ssz),
+        "atkdsp_gpu_pfb_cov_accumulate": ([vp, u, u, sz, vp, vp, vp, vp], C.c_int),
+        "atkdsp_gpu_pfb_cov_reset": ([vp, vp, u, u, vp, vp], C.c_int),
+        "atkdsp_gpu_pfb_channel_power": ([vp, u, u, sz, vp, vp, vp], C.c_int),
+        "atkdsp_gpu_batch_create": ([P(vp), u, C.c_int], vp),
+        "atkdsp_gpu_batch_destroy": ([vp], None),
+        "atkdsp_gpu_batch_process": ([vp, P(vp), P(sz), P(vp), P(ssz), vp], ssz),
+        "atkdsp_gpu_batch_stream": ([vp], vp),
+    }
+    for name, (args, res) in sigs.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+
+
+def load(path: str | os.PathLike | None = None):
+    """Load the library (once). Raises AtkDspError when it is missing."""
+    global _lib, _lib_path
+    if _lib is not None and path is None:
+        return _lib
+    cand = Path(path) if path else Path(os.environ.get("ATKDSP_B200_LIB", str(LIB_FILE)))
+    if not cand.exists():
+        raise AtkDspError(f"could not load {cand}: not built (make -C atkdsp_b200)")
+    try:
+        lib = C.CDLL(str(cand))
+    except OSError as e:
+        raise AtkDspError(f"could not load {cand}: {e}") from None
+    lib.atkdsp_abi_version.restype = C.c_int
+    abi = int(lib.atkdsp_abi_version())
+    if abi != ABI_VERSION:
+        raise AtkDspError(f"{cand}: ABI {abi}, this binding needs {ABI_VERSION}")
+    _bind(lib)
+    _lib, _lib_path = lib, cand
+    return lib
+
+
+def available() -> bool:
+    try:
+        load()
+        return True
+    except AtkDspError:
+        return False
+
+
+def lib_path() -> Path | None:
+    return _lib_path
+
+
+def version() -> str:
+    return load().atkdsp_version_string().decode()
+
+
+def build_info() -> str:
+    return load().atkdsp_build_info().decode()
+
+
+def set_threads(n: int) -> int:
+    return int(load().atkdsp_set_threads(int(n)))
+
+
+def get_threads() -> int:
+    return int(load().atkdsp_get_threads())
+
+
+def _fmt(fmt) -> int:
+    if isinstance(fmt, str):
+        try:
+            return FMT[fmt]
+        except KeyError:
+            raise AtkDspError(f"unknown sample format {fmt!r}") from None
+    return int(fmt)
+
+
+def bytes_per_sample(fmt) -> int:
+    return int(load().atkdsp_bytes_per_sample(_fmt(fmt)))
+
+
+def _cfp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(_Cf32))
+
+
+def _raw_u8(raw) -> np.ndarray:
+    return np.frombuffer(raw, dtype=np.uint8) if not isinstance(raw, np.ndarray) \
+        else np.ascontiguousarray(raw).view(np.uint8).reshape(-1)
+
+
+# -- unpack (reference binding :337-385) -------------------------------------
+def unpack(raw, fmt, dc_alpha: float = 0.0, dc_state: np.ndarray | None = None,
+           out: np.ndarray | None = None) -> np.ndarray:
+    """Raw bytes -> complex64, optional one-pole DC block (state in dc_state)."""
+    lib = load()
+    src = _raw_u8(raw)
+    n = src.size // bytes_per_sample(fmt)
+    if out is None:
+        out = np.empty(n, dtype=np.complex64)
+    elif out.dtype != np.complex64 or not out.flags.c_contiguous:
+        raise AtkDspError("out must be a contiguous complex64 array")
+    st = None
+    if dc_alpha > 0:
+        if dc_state is None or dc_state.dtype != np.complex64 or dc_state.size != 1:
+            raise AtkDspError("dc_state must be a 1-element complex64 array")
+        st = _cfp(dc_state)
+    got = _check(lib.atkdsp_unpack(src.ctypes.data, src.size, _fmt(fmt), _cfp(out), out.size,
+                                   float(dc_alpha), st), "unpack")
+    return out[:got]
+
+
+def unpack_dc(raw, fmt, offset: complex = 0j, out: np.ndarray | None = None,
+              want_mean: bool = True):
+    """Raw bytes -> complex64 with ``offset`` removed; returns ``(x, mean)``,
+    the mean taken BEFORE the offset came out."""
+    lib = load()
+    src = _raw_u8(raw)
+    n = src.size // bytes_per_sample(fmt)
+    if out is None:
+        out = np.empty(n, dtype=np.complex64)
+    elif out.dtype != np.complex64 or not out.flags.c_contiguous:
+        raise AtkDspError("out must be a contiguous complex64 array")
+    mr, mi = C.c_double(0.0), C.c_double(0.0)
+    got = _check(lib.atkdsp_unpack_dc(src.ctypes.data, src.size, _fmt(fmt), _cfp(out), out.size,
+                                      float(offset.real), float(offset.imag),
+                                      C.byref(mr) if want_mean else None,
+                                      C.byref(mi) if want_mean else None), "unpack_dc")
+    return out[:got], complex(mr.value, mi.value)
+
+
+# -- the channelizer (reference binding :4159-4219) ----------------------------
+class Pfb:
+    """Oversampled polyphase filterbank on the GPU (atkdsp_pfb). nchan channels
+    on a uniform grid spaced fs/nchan, ``oversample``x. process_n runs N
+    element streams on one block clock."""
+
+    def __init__(self, fs, nchan, oversample=2, taps_per_poly=12, atten_db=80.0, max_nel=1):
+        self._lib = load()
+        self._p = self._lib.atkdsp_pfb_create(float(fs), int(nchan), int(oversample),
+                                              int(taps_per_poly), float(atten_db), int(max_nel))
+        if not self._p:
+            raise AtkDspError("pfb_create: check fs>0, nchan>=2, nchan%oversample==0, "
+                              "a usable GPU and free device memory")
+        self.nchan = int(nchan)
+        self.max_nel = int(max_nel)
+        self.oversample = int(oversample)
+        self.taps_per_poly = int(taps_per_poly)
+
+    def __del__(self):
+        p = getattr(self, "_p", None)
+        if p:
+            self._lib.atkdsp_pfb_destroy(p)
+            self._p = None
+
+    @property
+    def handle(self):
+        return self._p
+
+    def reset(self):
+        self._lib.atkdsp_pfb_reset(self._p)
+
+    def out_rate(self):
+        return self._lib.atkdsp_pfb_out_rate(self._p)
+
+    def out_hops(self, n):
+        return int(self._lib.atkdsp_pfb_out_hops(self._p, int(n)))
+
+    def group_delay(self):
+        return self._lib.atkdsp_pfb_group_delay(self._p)
+
+    def block_origin(self, hop_index):
+        return int(self._lib.atkdsp_pfb_block_origin(self._p, int(hop_index)))
+
+    def set_cal(self, table, nel):
+        if table is None:
+            _check(self._lib.atkdsp_pfb_set_cal(self._p, None, 0), "pfb_set_cal")
+            return
+        t = np.ascontiguousarray(np.asarray(table, np.complex64)).reshape(int(nel), self.nchan)
+        _check(self._lib.atkdsp_pfb_set_cal(self._p, _cfp(t), int(nel)), "pfb_set_cal")
+
+    def describe(self):
+        buf = C.create_string_buffer(256)
+        n = self._lib.atkdsp_pfb_describe(self._p, buf, 256)
+        return buf.value.decode() if n > 0 else ""
+
+    def process_n(self, ins, nel):
+        nel = int(nel)
+        arrs = [np.ascontiguousarray(np.asarray(ins[e]).ravel(), np.complex64) for e in range(nel)]
+        n = arrs[0].size
+        for a in arrs:
+            if a.size != n:
+                raise AtkDspError("pfb: elements must be equal length")
+        m = self._lib.atkdsp_pfb_out_hops(self._p, n)
+        out = np.zeros(nel * self.nchan * m, np.complex64)
+        inarr = (C.POINTER(_Cf32) * nel)(*[_cfp(a) for a in arrs])
+        got = self._lib.atkdsp_pfb_process_n(self._p, inarr, nel, n, _cfp(out), out.size)
+        _check(int(got), "pfb_process_n")
+        return out[: nel * self.nchan * got].reshape(nel, self.nchan, got)
+
+    def process(self, x):
+        return self.process_n([x], 1)[0]
+
+
+def pfb_cov_accumulate(out, nel, nchan, gate, R, counts):
+    """W1: R[k] += sum_i y_k y_k^H over gated channels; counts[k] += m.
+    out (nel, nchan, m) complex64; R (nchan, nel, nel) complex64 and counts
+    (nchan,) uint32 are updated in place."""
+    lib = load()
+    o = np.ascontiguousarray(out, np.complex64)
+    nel = int(nel); nchan = int(nchan); m = o.shape[2] if o.ndim == 3 else 0
+    if not (R.flags["C_CONTIGUOUS"] and R.dtype == np.complex64):
+        raise AtkDspError("pfb_cov_accumulate: R must be contiguous complex64")
+    if not (counts.flags["C_CONTIGUOUS"] and counts.dtype == np.uint32):
+        raise AtkDspError("pfb_cov_accumulate: counts must be contiguous uint32")
+    gp = None
+    if gate is not None:
+        g = np.ascontiguousarray(gate, np.uint8)
+        gp = g.ctypes.data_as(C.POINTER(C.c_uint8))
+    lib.atkdsp_pfb_cov_accumulate(_cfp(o.reshape(-1)), nel, nchan, m, gp,
+                                  _cfp(R.reshape(-1)), counts.ctypes.data_as(C.POINTER(C.c_uint32)))
+
+
+def pfb_cov_reset(R, counts, nel, nchan, gate=None):
+    lib = load()
+    gp = None
+    if gate is not None:
+        g = np.ascontiguousarray(gate, np.uint8)
+        gp = g.ctypes.data_as(C.POINTER(C.c_uint8))
+    lib.atkdsp_pfb_cov_reset(_cfp(R.reshape(-1)), counts.ctypes.data_as(C.POINTER(C.c_uint32)),
+                             int(nel), int(nchan), gp)
+
+
+def pfb_channel_power(out, nel, nchan):
+    """W2: returns (pwr[nel, nchan], mean_pwr[nchan]) float32."""
+    lib = load()
+    o = np.ascontiguousarray(out, np.complex64)
+    nel = int(nel); nchan = int(nchan); m = o.shape[2] if o.ndim == 3 else 0
+    pwr = np.zeros(nel * nchan, np.float32)
+    meanp = np.zeros(nchan, np.float32)
+    lib.atkdsp_pfb_channel_power(_cfp(o.reshape(-1)), nel, nchan, m,
+                                 pwr.ctypes.data_as(C.POINTER(C.c_float)),
+                                 meanp.ctypes.data_as(C.POINTER(C.c_float)))
+    return pwr.reshape(nel, nchan), meanp

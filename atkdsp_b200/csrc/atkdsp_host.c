@@ -1,0 +1,986 @@
+/* The host layer of the B200 channelizer, in C99.
+ *
+ * It implements the reference's atkdsp_pfb_* / atkdsp_unpack* entry points
+ * (include/atkdsp.h) with the reference's argument checks, return codes and
+ * bookkeeping, designs the prototype filter and the FFT plan on the host,
+ * keeps each handle's streaming state in device memory, and drives the
+ * device through the thin atkb_* shim (internal.h). It includes no CUDA
+ * header and calls no CUDA function directly.
+ *
+ * Layout per handle (allocated once, by atkdsp_pfb_create):
+ *   bank      taps (float, L), rotation table twd (double2, nchan), DFT
+ *             table W (double2, nchan), per-pass twiddles, and a device copy
+ *             of the atkb_bank that points at them
+ *   state     two buffers per element of ov + hop samples (ping-pong): the
+ *             samples s[m*hop, ...) that the next call's windows reach back
+ *             into -- the reference's hist ++ leftover (channelizer.c:56-60)
+ *   staging   per element an input chunk and an output chunk on the device,
+ *             used by the host-pointer calls (long inputs are processed in
+ *             chunks; the output is split-invariant, so this changes nothing)
+ *   tables    job / tile / carry tables (device + pinned host mirror) and
+ *             the persistent kernel's two self-resetting counters
+ */
+#define _POSIX_C_SOURCE 200809L
+#include <math.h>
+#include <pthread.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+#include "atkdsp.h"
+#include "atkdsp_gpu.h"
+#include "internal.h"
+
+#define ATKB_PI 3.14159265358979323846
+#define MAX_NEL_SUPPORTED 32
+#define MAX_POW2_NCHAN 4096
+#define MAX_GENERIC_NCHAN 6400
+
+/* ===================================================================== identity */
+#define STR2(x) #x
+#define STR(x) STR2(x)
+static const char BUILD_INFO[] =
+    ATKDSP_VERSION_STRING " abi " STR(ATKDSP_ABI_VERSION) " b200 cuda sm_100a fp32-fold fp64-fft"
+    " built " __DATE__ " " __TIME__;
+
+ATKDSP_API int atkdsp_abi_version(void) { return ATKDSP_ABI_VERSION; }
+ATKDSP_API const char *atkdsp_version_string(void) { return ATKDSP_VERSION_STRING; }
+ATKDSP_API const char *atkdsp_build_info(void) { return BUILD_INFO; }
+
+/* reference src/atkdsp.c:51-60 */
+ATKDSP_API int atkdsp_bytes_per_sample(int fmt) {
+    switch (fmt) {
+    case ATKDSP_FMT_CU8: return 2;
+    case ATKDSP_FMT_CI8: return 2;
+    case ATKDSP_FMT_CI16: return 4;
+    case ATKDSP_FMT_CI16Q11: return 4;
+    case ATKDSP_FMT_CF32: return 8;
+    default: return 0;
+    }
+}
+
+static int g_threads = 0;
+/* reference src/atkdsp.c:64-80: the count in force; <= 0 restores the
+ * default (the number of online CPUs, what OpenMP would use). */
+ATKDSP_API int atkdsp_set_threads(int n) {
+    g_threads = n > 0 ? n : 0;
+    return atkdsp_get_threads();
+}
+ATKDSP_API int atkdsp_get_threads(void) {
+    if (g_threads > 0) return g_threads;
+    const long c = sysconf(_SC_NPROCESSORS_ONLN);
+    return c > 0 ? (int)c : 1;
+}
+
+static int map_rc(int rc) {
+    switch (rc) {
+    case ATKB_OK: return ATKDSP_OK;
+    case ATKB_E_ARG: return ATKDSP_E_ARG;
+    case ATKB_E_NOMEM: return ATKDSP_E_NOMEM;
+    case ATKB_E_CAP: return ATKDSP_E_CAP;
+    default: return ATKDSP_E_FFT;
+    }
+}
+
+/* =========================================================== prototype design
+ * Kaiser-windowed sinc, cutoff half a channel, unit DC gain times nchan
+ * (reference src/channelizer.c:79-99 with src/design.c:18-22 and the I0
+ * series of src/channelizer.c:33-43). The expressions are evaluated in the
+ * reference's order so the double taps -- and their float rounding, which
+ * the fold multiplies by -- come out bit-identical. */
+static double kaiser_beta(double atten_db) {
+    if (atten_db > 50.0) return 0.1102 * (atten_db - 8.7);
+    if (atten_db >= 21.0) return 0.5842 * pow(atten_db - 21.0, 0.4) + 0.07886 * (atten_db - 21.0);
+    return 0.0;
+}
+
+static double bessel_i0(double x) {
+    const double half = x * 0.5;
+    double acc = 1.0, term = 1.0;
+    int k;
+    for (k = 1; k < 500; ++k) {
+        term *= (half / (double)k);
+        const double sq = term * term;
+        acc += sq;
+        if (sq < acc * 1e-17) break;
+    }
+    return acc;
+}
+
+static double proto_tap(size_t n, double fc, double mid, double beta, double i0b) {
+    const double t = (double)n - mid;
+    const double x = 2.0 * fc * t;
+    const double sinc = (t == 0.0) ? 1.0 : sin(ATKB_PI * x) / (ATKB_PI * x);
+    const double r = (mid > 0.0) ? t / mid : 0.0;
+    const double w = bessel_i0(beta * sqrt(r * r < 1.0 ? 1.0 - r * r : 0.0)) / i0b;
+    return 2.0 * fc * sinc * w;
+}
+
+static void design_prototype(unsigned nchan, unsigned K, double atten_db, double *h) {
+    const size_t L = (size_t)nchan * K;
+    const double fc = 1.0 / (2.0 * (double)nchan);
+    const double mid = (double)(L - 1) * 0.5;
+    const double beta = kaiser_beta(atten_db);
+    const double i0b = bessel_i0(beta);
+    double total = 0.0;
+    size_t n;
+    for (n = 0; n < L; ++n) total += proto_tap(n, fc, mid, beta, i0b);
+    if (total == 0.0) total = 1.0;
+    for (n = 0; n < L; ++n) h[n] = (proto_tap(n, fc, mid, beta, i0b) / total) * (double)nchan;
+}
+
+/* ================================================================== FFT plan */
+static int is_pow2(unsigned v) { return v && !(v & (v - 1)); }
+
+static int plan_fft(unsigned M, atkb_fft_plan *pl) {
+    memset(pl, 0, sizeof *pl);
+    if (is_pow2(M) && M >= 16 && M <= MAX_POW2_NCHAN) {
+        unsigned rem = M / 16;
+        pl->fast = 1;
+        pl->radix[pl->npass++] = 16;
+        while (rem >= 16) { pl->radix[pl->npass++] = 16; rem /= 16; }
+        if (rem > 1) pl->radix[pl->npass++] = (int)rem;
+    } else {
+        unsigned rem = M, p;
+        while (rem % 16 == 0) { pl->radix[pl->npass++] = 16; rem /= 16; }
+        if (rem % 8 == 0) { pl->radix[pl->npass++] = 8; rem /= 8; }
+        if (rem % 4 == 0) { pl->radix[pl->npass++] = 4; rem /= 4; }
+        if (rem % 2 == 0) { pl->radix[pl->npass++] = 2; rem /= 2; }
+        for (p = 3; rem > 1; p += 2) {
+            while (rem % p == 0) {
+                if (pl->npass >= ATKB_MAX_PASS) return -1;
+                pl->radix[pl->npass++] = (int)p;
+                rem /= p;
+            }
+            if (p * p > rem && rem > 1) {
+                if (pl->npass >= ATKB_MAX_PASS) return -1;
+                pl->radix[pl->npass++] = (int)rem;
+                rem = 1;
+            }
+        }
+    }
+    /* per-pass twiddles (fast path): pass p >= 1 holds W_{Ns R}^{r k} at
+     * (r - 1) * Ns + k, r in [1, R), k in [0, Ns) */
+    {
+        int p, Ns = 1, off = 0;
+        for (p = 0; p < pl->npass; ++p) {
+            pl->twoff[p] = off;
+            if (p > 0) off += (pl->radix[p] - 1) * Ns;
+            Ns *= pl->radix[p];
+        }
+        pl->twlen = off > 0 ? off : 1;
+    }
+    return 0;
+}
+
+/* ===================================================================== handle */
+struct atkdsp_pfb {
+    double fs, atten;
+    unsigned nchan, os, K, max_nel, hop;
+    size_t L, ov;
+    int dev;
+    void *stream;
+    void *tbl_event;              /* the last table upload; gates reuse of h_tables */
+    int tbl_event_live;
+    atkb_bank bank;               /* host copy (device pointers inside)       */
+    void *d_bank;
+    void *d_const;                /* taps, twd, W, per-pass twiddles          */
+    void *d_state;                /* 2 * max_nel * cap_state cf32            */
+    size_t cap_state;
+    int cur;
+    unsigned lc;
+    int64_t b;
+    void *d_cal;
+    unsigned cal_nel;
+    size_t chunk, out_ld;         /* host-path chunk (samples) and its output stride */
+    void *d_in_stage, *d_out_stage;
+    void *d_tables, *h_tables;    /* jobs | carries | tile_start              */
+    size_t tbl_bytes;
+    int *d_counters;
+    int grid;
+};
+
+static size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+static size_t tables_bytes(unsigned n) {
+    return align16((size_t)n * sizeof(atkb_job)) + align16((size_t)n * sizeof(atkb_carry)) +
+           align16(((size_t)n + 1) * sizeof(int));
+}
+
+static atkb_job *tbl_jobs(void *base) { return (atkb_job *)base; }
+static atkb_carry *tbl_carry(void *base, unsigned n) {
+    return (atkb_carry *)((char *)base + align16((size_t)n * sizeof(atkb_job)));
+}
+static int *tbl_tiles(void *base, unsigned n) {
+    return (int *)((char *)base + align16((size_t)n * sizeof(atkb_job)) +
+                   align16((size_t)n * sizeof(atkb_carry)));
+}
+
+static atkdsp_cf32 *state_buf(const atkdsp_pfb *p, int which, unsigned e) {
+    return (atkdsp_cf32 *)p->d_state + ((size_t)which * p->max_nel + e) * p->cap_state;
+}
+
+ATKDSP_API void atkdsp_pfb_destroy(atkdsp_pfb *p) {
+    if (!p) return;
+    if (p->dev >= 0) atkb_set_device(p->dev);
+    if (p->stream) atkb_stream_sync(p->stream);
+    atkb_free(p->d_bank);
+    atkb_free(p->d_const);
+    atkb_free(p->d_state);
+    atkb_free(p->d_cal);
+    atkb_free(p->d_in_stage);
+    atkb_free(p->d_out_stage);
+    atkb_free(p->d_tables);
+    atkb_free(p->d_counters);
+    atkb_host_free(p->h_tables);
+    atkb_event_destroy(p->tbl_event);
+    atkb_stream_destroy(p->stream);
+    free(p);
+}
+
+static int upload_bank(atkdsp_pfb *p) {
+    const unsigned M = p->nchan;
+    atkb_fft_plan pl;
+    if (plan_fft(M, &pl) != 0) return ATKB_E_ARG;
+    const size_t taps_b = align16(p->L * sizeof(float));
+    const size_t tab_b = (size_t)M * 2 * sizeof(double);
+    const size_t pass_b = (size_t)pl.twlen * 2 * sizeof(double);
+    const size_t total = taps_b + 2 * tab_b + pass_b;
+    char *h = (char *)calloc(1, total);
+    double *proto = (double *)malloc(p->L * sizeof(double));
+    if (!h || !proto) { free(h); free(proto); return ATKB_E_NOMEM; }
+    design_prototype(M, p->K, p->atten, proto);
+    float *taps = (float *)h;
+    double *twd = (double *)(h + taps_b);
+    double *W = (double *)(h + taps_b + tab_b);
+    double *wp = (double *)(h + taps_b + 2 * tab_b);
+    size_t q;
+    unsigned j;
+    for (q = 0; q < p->L; ++q) taps[q] = (float)proto[q];
+    for (j = 0; j < M; ++j) {
+        /* the reference's rotation table, channelizer.c:164-170 */
+        const double a = 2.0 * ATKB_PI * (double)j / (double)M;
+        twd[2 * j] = cos(a);
+        twd[2 * j + 1] = sin(a);
+        W[2 * j] = cos(a);
+        W[2 * j + 1] = -sin(a);
+    }
+    {
+        int pidx, Ns = 1;
+        for (pidx = 0; pidx < pl.npass; ++pidx) {
+            const int R = pl.radix[pidx];
+            if (pidx > 0) {
+                int r, k;
+                for (r = 1; r < R; ++r)
+                    for (k = 0; k < Ns; ++k) {
+                        const size_t e = (size_t)pl.twoff[pidx] + (size_t)(r - 1) * Ns + k;
+                        const size_t jj = (size_t)r * k * (M / ((size_t)Ns * R));
+                        wp[2 * e] = W[2 * jj];
+                        wp[2 * e + 1] = W[2 * jj + 1];
+                    }
+            }
+            Ns *= R;
+        }
+    }
+    free(proto);
+    int rc = atkb_malloc(&p->d_const, total);
+    if (rc == ATKB_OK) rc = atkb_h2d(p->d_const, h, total, p->stream);
+    if (rc == ATKB_OK) rc = atkb_stream_sync(p->stream);
+    free(h);
+    if (rc != ATKB_OK) return rc;
+    atkb_bank *B = &p->bank;
+    memset(B, 0, sizeof *B);
+    B->nchan = (int)M;
+    B->os = (int)p->os;
+    B->K = (int)p->K;
+    B->hop = (int)p->hop;
+    B->L = (long long)p->L;
+    B->ov = (long long)p->ov;
+    B->taps = (const float *)p->d_const;
+    B->twd = (const char *)p->d_const + taps_b;
+    B->wfull = (const char *)p->d_const + taps_b + tab_b;
+    B->wpass = (const char *)p->d_const + taps_b + 2 * tab_b;
+    B->plan = pl;
+    if (pl.fast) {
+        B->tile_hops = 4096 / (int)M;
+        B->smem_bytes = 4096 * 16;
+    } else {
+        int th = (int)(2048 / M);
+        if (th < 1) th = 1;
+        B->tile_hops = th;
+        B->smem_bytes = 2 * th * (int)M * 16;
+    }
+    rc = atkb_malloc(&p->d_bank, sizeof *B);
+    if (rc == ATKB_OK) rc = atkb_h2d(p->d_bank, B, sizeof *B, p->stream);
+    if (rc == ATKB_OK) rc = atkb_stream_sync(p->stream);
+    return rc;
+}
+
+/* reference src/channelizer.c:138-171 (argument rules and the atten clamp) */
+ATKDSP_API atkdsp_pfb *atkdsp_pfb_create(double fs, unsigned nchan, unsigned oversample,
+                                         unsigned taps_per_poly, double atten_db,
+                                         unsigned max_nel) {
+    if (!(fs > 0.0) || nchan < 2 || oversample < 1 || nchan % oversample != 0) return NULL;
+    if (taps_per_poly < 2 || max_nel < 1) return NULL;
+    if (max_nel > MAX_NEL_SUPPORTED) return NULL;
+    if (is_pow2(nchan) ? nchan > MAX_POW2_NCHAN : nchan > MAX_GENERIC_NCHAN) return NULL;
+    if (atten_db < 20.0) atten_db = 20.0;
+    atkdsp_pfb *p = (atkdsp_pfb *)calloc(1, sizeof *p);
+    if (!p) return NULL;
+    p->dev = -1;
+    p->fs = fs;
+    p->atten = atten_db;
+    p->nchan = nchan;
+    p->os = oversample;
+    p->K = taps_per_poly;
+    p->max_nel = max_nel;
+    p->hop = nchan / oversample;
+    p->L = (size_t)nchan * taps_per_poly;
+    p->ov = p->L - p->hop;
+    if (atkb_get_device(&p->dev) != ATKB_OK || atkb_set_device(p->dev) != ATKB_OK) {
+        p->dev = -1;
+        free(p);
+        return NULL;
+    }
+    int rc = atkb_stream_create(&p->stream);
+    if (rc == ATKB_OK) rc = atkb_event_create(&p->tbl_event);
+    if (rc == ATKB_OK) rc = upload_bank(p);
+    if (rc != ATKB_OK) { atkdsp_pfb_destroy(p); return NULL; }
+    /* state: ov history + up to hop - 1 leftover samples, twice per element */
+    p->cap_state = p->ov + p->hop;
+    rc = atkb_malloc(&p->d_state, 2 * (size_t)max_nel * p->cap_state * sizeof(atkdsp_cf32));
+    if (rc == ATKB_OK)
+        rc = atkb_memset(p->d_state, 0, 2 * (size_t)max_nel * p->cap_state * sizeof(atkdsp_cf32),
+                         p->stream);
+    if (rc == ATKB_OK) rc = atkb_malloc(&p->d_cal, (size_t)max_nel * nchan * sizeof(atkdsp_cf32));
+    /* host-path staging: about 2^20 samples per element, whole hops */
+    if (rc == ATKB_OK) {
+        size_t chunk = ((size_t)1 << 21) / max_nel;
+        if (chunk < (size_t)p->hop * 8) chunk = (size_t)p->hop * 8;
+        chunk = (chunk / p->hop) * p->hop;
+        p->chunk = chunk;
+        p->out_ld = chunk / p->hop + 1;
+        rc = atkb_malloc(&p->d_in_stage, (size_t)max_nel * chunk * sizeof(atkdsp_cf32));
+    }
+    if (rc == ATKB_OK)
+        rc = atkb_malloc(&p->d_out_stage,
+                         (size_t)max_nel * nchan * p->out_ld * sizeof(atkdsp_cf32));
+    if (rc == ATKB_OK) {
+        p->tbl_bytes = tables_bytes(max_nel);
+        rc = atkb_malloc(&p->d_tables, p->tbl_bytes);
+    }
+    if (rc == ATKB_OK) rc = atkb_host_alloc(&p->h_tables, p->tbl_bytes);
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&p->d_counters, 2 * sizeof(int));
+    if (rc == ATKB_OK) rc = atkb_memset(p->d_counters, 0, 2 * sizeof(int), p->stream);
+    if (rc == ATKB_OK) rc = atkb_stream_sync(p->stream);
+    if (rc != ATKB_OK) { atkdsp_pfb_destroy(p); return NULL; }
+    p->grid = atkb_pfb_grid(p->dev, p->bank.smem_bytes);
+    if (p->grid < 1) { atkdsp_pfb_destroy(p); return NULL; }
+    p->lc = 0;
+    p->b = 0;
+    p->cur = 0;
+    return p;
+}
+
+ATKDSP_API void atkdsp_pfb_reset(atkdsp_pfb *p) {
+    if (!p) return;
+    atkb_set_device(p->dev);
+    atkb_memset(p->d_state, 0, 2 * (size_t)p->max_nel * p->cap_state * sizeof(atkdsp_cf32),
+                p->stream);
+    atkb_stream_sync(p->stream);
+    p->lc = 0;
+    p->b = 0;
+    p->cur = 0;
+}
+
+ATKDSP_API unsigned atkdsp_pfb_nchan(const atkdsp_pfb *p) { return p ? p->nchan : 0; }
+ATKDSP_API double atkdsp_pfb_out_rate(const atkdsp_pfb *p) {
+    return p ? (double)p->os * p->fs / (double)p->nchan : 0.0;
+}
+ATKDSP_API size_t atkdsp_pfb_out_hops(const atkdsp_pfb *p, size_t n) {
+    return p ? ((size_t)p->lc + n) / p->hop : 0;
+}
+ATKDSP_API double atkdsp_pfb_group_delay(const atkdsp_pfb *p) {
+    return p ? (double)(p->L - 1) * 0.5 : 0.0;
+}
+ATKDSP_API int64_t atkdsp_pfb_block_origin(const atkdsp_pfb *p, int64_t hop_index) {
+    return p ? hop_index * (int64_t)p->hop - (int64_t)p->ov : 0;
+}
+
+/* reference src/channelizer.c:203-212: the table is copied; NULL clears it */
+ATKDSP_API int atkdsp_pfb_set_cal(atkdsp_pfb *p, const atkdsp_cf32 *table, unsigned nel) {
+    if (!p) return ATKDSP_E_ARG;
+    if (!table) { p->cal_nel = 0; return ATKDSP_OK; }
+    if (nel < 1 || nel > p->max_nel) return ATKDSP_E_ARG;
+    atkb_set_device(p->dev);
+    int rc = atkb_stream_sync(p->stream);       /* earlier work may still read the old table */
+    if (rc == ATKB_OK) rc = atkb_h2d(p->d_cal, table, (size_t)nel * p->nchan * sizeof(atkdsp_cf32), p->stream);
+    if (rc == ATKB_OK) rc = atkb_stream_sync(p->stream);
+    if (rc != ATKB_OK) return map_rc(rc);
+    p->cal_nel = nel;
+    return ATKDSP_OK;
+}
+
+/* reference src/channelizer.c:410-417 (the same description line) */
+ATKDSP_API int atkdsp_pfb_describe(const atkdsp_pfb *p, char *buf, size_t cap) {
+    if (!p || !buf || cap == 0) return ATKDSP_E_ARG;
+    return snprintf(buf, cap,
+                    "PFB %.6g MSPS: %u chan x%u oversample, %.6g kHz spacing, %.6g kHz out, "
+                    "%zu-tap proto (%u/poly), %.0f dB, <=%u el",
+                    p->fs / 1e6, p->nchan, p->os, p->fs / p->nchan / 1e3,
+                    atkdsp_pfb_out_rate(p) / 1e3, p->L, p->K, p->atten, p->max_nel);
+}
+
+/* One step: nel elements, n new samples each at ins[e] (device), m hops
+ * written to outs + e * nchan * ldo (device, row stride ldo). Builds the job
+ * and carry tables, uploads them, launches the tile kernel and the carry,
+ * and advances the host mirror of the state. Asynchronous on `stream`. */
+static int run_step(atkdsp_pfb *p, unsigned nel, const atkdsp_cf32 *const *ins, size_t n,
+                    atkdsp_cf32 *outs, size_t ldo, size_t m, void *stream) {
+    const size_t head = p->ov + p->lc;
+    const unsigned nxt = (unsigned)(p->cur ^ 1);
+    int rc;
+    unsigned e;
+    if (p->tbl_event_live) {
+        rc = atkb_event_sync(p->tbl_event);
+        if (rc != ATKB_OK) return rc;
+    }
+    atkb_job *J = tbl_jobs(p->h_tables);
+    atkb_carry *C = tbl_carry(p->h_tables, p->max_nel);
+    int *T = tbl_tiles(p->h_tables, p->max_nel);
+    const int tiles = (int)((m + (size_t)p->bank.tile_hops - 1) / (size_t)p->bank.tile_hops);
+    for (e = 0; e < nel; ++e) {
+        memset(&J[e], 0, sizeof J[e]);
+        J[e].state = state_buf(p, p->cur, e);
+        J[e].in = ins[e];
+        J[e].out = outs + (size_t)e * p->nchan * ldo;
+        J[e].cal = (p->cal_nel && e < p->cal_nel) ? (const atkdsp_cf32 *)p->d_cal + (size_t)e * p->nchan
+                                                  : NULL;
+        J[e].head = (long long)head;
+        J[e].ldo = (long long)ldo;
+        J[e].out_col = 0;
+        J[e].b0 = (long long)p->b;
+        J[e].hops = (long long)m;
+        J[e].bank = (const atkb_bank *)p->d_bank;
+        J[e].tiles = tiles;
+        T[e] = (int)e * tiles;
+        C[e].state = J[e].state;
+        C[e].in = ins[e];
+        C[e].dst = state_buf(p, (int)nxt, e);
+        C[e].head = (long long)head;
+        C[e].from = (long long)(m * p->hop);
+        C[e].len = (long long)(head + n - m * p->hop);
+    }
+    T[nel] = (int)nel * tiles;
+    /* the tables as laid out for max_nel, uploaded whole (they are small) */
+    rc = atkb_h2d(p->d_tables, p->h_tables, p->tbl_bytes, stream);
+    if (rc == ATKB_OK) rc = atkb_event_record(p->tbl_event, stream);
+    if (rc != ATKB_OK) return rc;
+    p->tbl_event_live = 1;
+    if (tiles > 0) {
+        /* only nel jobs: tile_start[nel] is their total; the kernel reads
+         * tile_start[njobs], so pass the tile table shifted to this nel */
+        rc = atkb_pfb_launch(tbl_jobs(p->d_tables), tbl_tiles(p->d_tables, p->max_nel), (int)nel,
+                             p->d_counters, p->grid < (int)nel * tiles ? p->grid : (int)nel * tiles,
+                             p->bank.smem_bytes, stream);
+        if (rc != ATKB_OK) return rc;
+    }
+    rc = atkb_pfb_carry(tbl_carry(p->d_tables, p->max_nel), (int)nel, (long long)p->cap_state, stream);
+    if (rc != ATKB_OK) return rc;
+    p->cur = (int)nxt;
+    p->lc = (unsigned)(p->lc + n - m * p->hop);
+    p->b += (int64_t)m;
+    return ATKB_OK;
+}
+
+/* reference src/channelizer.c:305-402 */
+ATKDSP_API ptrdiff_t atkdsp_pfb_process_n(atkdsp_pfb *p, const atkdsp_cf32 *const *ins, unsigned nel,
+                                          size_t n, atkdsp_cf32 *out, size_t cap) {
+    if (!p || !ins || nel < 1 || nel > p->max_nel) return ATKDSP_E_ARG;
+    unsigned e;
+    for (e = 0; e < nel && n; ++e)
+        if (!ins[e]) return ATKDSP_E_ARG;
+    const size_t m = ((size_t)p->lc + n) / p->hop;
+    if (m > 0 && (!out || cap < (size_t)nel * p->nchan * m)) return ATKDSP_E_CAP;
+    if (atkb_set_device(p->dev) != ATKB_OK) return ATKDSP_E_FFT;
+    size_t pos = 0, col = 0;
+    int rc = ATKB_OK;
+    const atkdsp_cf32 *dins[MAX_NEL_SUPPORTED];
+    for (e = 0; e < nel; ++e) dins[e] = (const atkdsp_cf32 *)p->d_in_stage + (size_t)e * p->chunk;
+    while (pos < n && rc == ATKB_OK) {
+        const size_t nc = (n - pos < p->chunk) ? n - pos : p->chunk;
+        const size_t mc = ((size_t)p->lc + nc) / p->hop;
+        for (e = 0; e < nel && rc == ATKB_OK; ++e)
+            rc = atkb_h2d((void *)dins[e], ins[e] + pos, nc * sizeof(atkdsp_cf32), p->stream);
+        if (rc != ATKB_OK) break;
+        rc = run_step(p, nel, dins, nc, (atkdsp_cf32 *)p->d_out_stage, p->out_ld, mc, p->stream);
+        if (rc != ATKB_OK) break;
+        if (mc > 0) {
+            /* rows e*nchan + k: out + (e*nchan + k)*m + col  <-  stage + (e*nchan + k)*out_ld */
+            rc = atkb_d2h_2d(out + col, m * sizeof(atkdsp_cf32), p->d_out_stage,
+                             p->out_ld * sizeof(atkdsp_cf32), mc * sizeof(atkdsp_cf32),
+                             (size_t)nel * p->nchan, p->stream);
+        }
+        col += mc;
+        pos += nc;
+    }
+    if (rc == ATKB_OK) rc = atkb_stream_sync(p->stream);
+    if (rc != ATKB_OK) return map_rc(rc);
+    return (ptrdiff_t)m;
+}
+
+ATKDSP_API ptrdiff_t atkdsp_pfb_process(atkdsp_pfb *p, const atkdsp_cf32 *in, size_t n,
+                                        atkdsp_cf32 *out, size_t cap) {
+    const atkdsp_cf32 *ins[1];
+    ins[0] = in;
+    return atkdsp_pfb_process_n(p, ins, 1, n, out, cap);
+}
+
+/* ================================================================ device API */
+ATKDSP_API void *atkdsp_gpu_pfb_stream(atkdsp_pfb *p) { return p ? p->stream : NULL; }
+
+ATKDSP_API int atkdsp_gpu_pfb_sync(atkdsp_pfb *p) {
+    if (!p) return ATKDSP_E_ARG;
+    atkb_set_device(p->dev);
+    return atkb_stream_sync(p->stream) == ATKB_OK ? ATKDSP_OK : ATKDSP_E_FFT;
+}
+
+ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_n(atkdsp_pfb *p, const atkdsp_cf32 *const *d_ins,
+                                              unsigned nel, size_t n, atkdsp_cf32 *d_out,
+                                              size_t cap, void *stream) {
+    if (!p || !d_ins || nel < 1 || nel > p->max_nel) return ATKDSP_E_ARG;
+    unsigned e;
+    for (e = 0; e < nel && n; ++e)
+        if (!d_ins[e]) return ATKDSP_E_ARG;
+    if ((size_t)p->lc + n >= ((size_t)1 << 62)) return ATKDSP_E_ARG;
+    const size_t m = ((size_t)p->lc + n) / p->hop;
+    if (m > 0 && (!d_out || cap < (size_t)nel * p->nchan * m)) return ATKDSP_E_CAP;
+    if (m > (size_t)0x7fffffff / 4 / nel) return ATKDSP_E_ARG;   /* tile indices are int */
+    if (atkb_set_device(p->dev) != ATKB_OK) return ATKDSP_E_FFT;
+    const int rc = run_step(p, nel, d_ins, n, d_out, m, m, stream ? stream : p->stream);
+    return rc == ATKB_OK ? (ptrdiff_t)m : map_rc(rc);
+}
+
+/* ============================================ per-device scratch for host calls
+ * W1/W2 and unpack on HOST buffers stage through device memory. One scratch
+ * area per device, grown when a larger call first needs it and then kept;
+ * calls on one device are serialised by its lock. */
+#define MAX_DEV 16
+typedef struct {
+    pthread_mutex_t lock;
+    void *d;
+    size_t cap;
+    void *stream;
+    int ready;
+} scratch_t;
+static scratch_t g_scr[MAX_DEV];
+static pthread_mutex_t g_scr_init = PTHREAD_MUTEX_INITIALIZER;
+
+static scratch_t *scratch_lock(size_t bytes, int *rc) {
+    int dev = 0;
+    *rc = atkb_get_device(&dev);
+    if (*rc != ATKB_OK) return NULL;
+    if (dev < 0 || dev >= MAX_DEV) { *rc = ATKB_E_NODEV; return NULL; }
+    scratch_t *s = &g_scr[dev];
+    pthread_mutex_lock(&g_scr_init);
+    if (!s->ready) {
+        pthread_mutex_init(&s->lock, NULL);
+        s->ready = 1;
+    }
+    pthread_mutex_unlock(&g_scr_init);
+    pthread_mutex_lock(&s->lock);
+    if (!s->stream && (*rc = atkb_stream_create(&s->stream)) != ATKB_OK) {
+        s->stream = NULL;
+        pthread_mutex_unlock(&s->lock);
+        return NULL;
+    }
+    if (s->cap < bytes) {
+        atkb_free(s->d);
+        s->d = NULL;
+        s->cap = 0;
+        size_t want = bytes + bytes / 4 + 4096;
+        if ((*rc = atkb_malloc(&s->d, want)) != ATKB_OK) {
+            s->d = NULL;
+            pthread_mutex_unlock(&s->lock);
+            return NULL;
+        }
+        s->cap = want;
+    }
+    *rc = ATKB_OK;
+    return s;
+}
+static void scratch_unlock(scratch_t *s) { pthread_mutex_unlock(&s->lock); }
+
+/* ====================================================================== W1/W2 */
+ATKDSP_API void atkdsp_pfb_cov_accumulate(const atkdsp_cf32 *out, unsigned nel, unsigned nchan,
+                                          size_t m, const uint8_t *gate, atkdsp_cf32 *R,
+                                          uint32_t *counts) {
+    if (!out || !R || !counts || nel < 1 || nchan < 1 || nel > MAX_NEL_SUPPORTED) return;
+    const size_t ob = align16((size_t)nel * nchan * m * sizeof(atkdsp_cf32));
+    const size_t rb = align16((size_t)nchan * nel * nel * sizeof(atkdsp_cf32));
+    const size_t cb = align16((size_t)nchan * sizeof(uint32_t));
+    const size_t gb = align16(nchan);
+    int rc;
+    scratch_t *s = scratch_lock(ob + rb + cb + gb, &rc);
+    if (!s) return;
+    char *d = (char *)s->d;
+    rc = atkb_h2d(d, out, (size_t)nel * nchan * m * sizeof(atkdsp_cf32), s->stream);
+    if (rc == ATKB_OK) rc = atkb_h2d(d + ob, R, (size_t)nchan * nel * nel * sizeof(atkdsp_cf32), s->stream);
+    if (rc == ATKB_OK) rc = atkb_h2d(d + ob + rb, counts, nchan * sizeof(uint32_t), s->stream);
+    if (rc == ATKB_OK && gate) rc = atkb_h2d(d + ob + rb + cb, gate, nchan, s->stream);
+    if (rc == ATKB_OK)
+        rc = atkb_w12(d, nel, nchan, m, gate ? (const uint8_t *)(d + ob + rb + cb) : NULL, d + ob,
+                      (uint32_t *)(d + ob + rb), NULL, NULL, s->stream);
+    if (rc == ATKB_OK) rc = atkb_d2h(R, d + ob, (size_t)nchan * nel * nel * sizeof(atkdsp_cf32), s->stream);
+    if (rc == ATKB_OK) rc = atkb_d2h(counts, d + ob + rb, nchan * sizeof(uint32_t), s->stream);
+    atkb_stream_sync(s->stream);
+    scratch_unlock(s);
+}
+
+ATKDSP_API void atkdsp_pfb_cov_reset(atkdsp_cf32 *R, uint32_t *counts, unsigned nel, unsigned nchan,
+                                     const uint8_t *gate) {
+    /* reference src/channelizer.c:442-450: plain memory clearing of the
+     * caller's HOST arrays; there is nothing to compute, so it stays on the
+     * host rather than round-tripping through the device. */
+    unsigned k;
+    if (!R || !counts) return;
+    for (k = 0; k < nchan; ++k) {
+        if (gate && !gate[k]) continue;
+        memset(R + (size_t)k * nel * nel, 0, (size_t)nel * nel * sizeof(atkdsp_cf32));
+        counts[k] = 0;
+    }
+}
+
+ATKDSP_API void atkdsp_pfb_channel_power(const atkdsp_cf32 *out, unsigned nel, unsigned nchan,
+                                         size_t m, float *pwr, float *mean_pwr) {
+    if (!out || nel < 1 || nchan < 1 || nel > MAX_NEL_SUPPORTED) return;
+    const size_t ob = align16((size_t)nel * nchan * m * sizeof(atkdsp_cf32));
+    const size_t pb = align16((size_t)nel * nchan * sizeof(float));
+    const size_t mb = align16((size_t)nchan * sizeof(float));
+    int rc;
+    scratch_t *s = scratch_lock(ob + pb + mb, &rc);
+    if (!s) return;
+    char *d = (char *)s->d;
+    rc = atkb_h2d(d, out, (size_t)nel * nchan * m * sizeof(atkdsp_cf32), s->stream);
+    if (rc == ATKB_OK)
+        rc = atkb_w12(d, nel, nchan, m, NULL, NULL, NULL, pwr ? (float *)(d + ob) : NULL,
+                      mean_pwr ? (float *)(d + ob + pb) : NULL, s->stream);
+    if (rc == ATKB_OK && pwr) rc = atkb_d2h(pwr, d + ob, (size_t)nel * nchan * sizeof(float), s->stream);
+    if (rc == ATKB_OK && mean_pwr) rc = atkb_d2h(mean_pwr, d + ob + pb, nchan * sizeof(float), s->stream);
+    atkb_stream_sync(s->stream);
+    scratch_unlock(s);
+}
+
+ATKDSP_API int atkdsp_gpu_pfb_cov_accumulate(const atkdsp_cf32 *d_out, unsigned nel, unsigned nchan,
+                                             size_t m, const uint8_t *d_gate, atkdsp_cf32 *d_R,
+                                             uint32_t *d_counts, void *stream) {
+    if (!d_out || !d_R || !d_counts || nel < 1 || nchan < 1 || nel > MAX_NEL_SUPPORTED) return ATKDSP_E_ARG;
+    return map_rc(atkb_w12(d_out, nel, nchan, m, d_gate, d_R, d_counts, NULL, NULL, stream));
+}
+
+ATKDSP_API int atkdsp_gpu_pfb_cov_reset(atkdsp_cf32 *d_R, uint32_t *d_counts, unsigned nel,
+                                        unsigned nchan, const uint8_t *d_gate, void *stream) {
+    if (!d_R || !d_counts) return ATKDSP_E_ARG;
+    return map_rc(atkb_cov_reset(d_R, d_counts, nel, nchan, d_gate, stream));
+}
+
+ATKDSP_API int atkdsp_gpu_pfb_channel_power(const atkdsp_cf32 *d_out, unsigned nel, unsigned nchan,
+                                            size_t m, float *d_pwr, float *d_mean_pwr, void *stream) {
+    if (!d_out || nel < 1 || nchan < 1 || nel > MAX_NEL_SUPPORTED) return ATKDSP_E_ARG;
+    return map_rc(atkb_w12(d_out, nel, nchan, m, NULL, NULL, NULL, d_pwr, d_mean_pwr, stream));
+}
+
+/* ===================================================================== unpack
+ * The constants of reference src/convert.c:45-71, computed in float exactly
+ * as the reference does so the device conversion is bit-identical. */
+static int unpack_consts(int fmt, float off_re, float off_im, float *cre, float *cim, float *k) {
+    switch (fmt) {
+    case ATKDSP_FMT_CU8:
+        *k = 1.0f / 127.5f;
+        *cre = 127.5f + off_re / *k;
+        *cim = 127.5f + off_im / *k;
+        return 1;
+    case ATKDSP_FMT_CI8:
+        *k = 1.0f / 128.0f;
+        break;
+    case ATKDSP_FMT_CI16:
+        *k = 1.0f / 32768.0f;
+        break;
+    case ATKDSP_FMT_CI16Q11:
+        *k = 1.0f / 2048.0f;
+        break;
+    case ATKDSP_FMT_CF32:
+        *k = 1.0f;
+        *cre = off_re;
+        *cim = off_im;
+        return 1;
+    default:
+        return 0;
+    }
+    *cre = off_re / *k;
+    *cim = off_im / *k;
+    return 1;
+}
+
+static ptrdiff_t unpack_host(const void *raw, size_t nbytes, int fmt, atkdsp_cf32 *out, size_t cap,
+                             float off_re, float off_im, double *mean_re, double *mean_im,
+                             float dc_alpha, atkdsp_cf32 *dc_state) {
+    if (!raw || !out) return ATKDSP_E_ARG;
+    const int bps = atkdsp_bytes_per_sample(fmt);
+    if (!bps) return ATKDSP_E_ARG;
+    float cre, cim, k;
+    unpack_consts(fmt, off_re, off_im, &cre, &cim, &k);
+    size_t n = nbytes / (size_t)bps;
+    if (n > cap) n = cap;
+    const int want_mean = mean_re || mean_im;
+    const int pole = dc_alpha > 0.0f && dc_state != NULL;
+    if (n == 0) {
+        if (mean_re) *mean_re = (double)off_re;
+        if (mean_im) *mean_im = (double)off_im;
+        return 0;
+    }
+    const size_t rb = align16(n * (size_t)bps);
+    const size_t ob = align16(n * sizeof(atkdsp_cf32));
+    const size_t pb = align16((size_t)atkb_unpack_partials(n) * 2 * sizeof(double));
+    int rc;
+    scratch_t *s = scratch_lock(rb + ob + pb + 64, &rc);
+    if (!s) return map_rc(rc);
+    char *d = (char *)s->d;
+    double *d_mean = (double *)(d + rb + ob + pb);
+    double hm[2] = {0.0, 0.0};
+    rc = atkb_h2d(d, raw, n * (size_t)bps, s->stream);
+    if (rc == ATKB_OK && pole) rc = atkb_h2d(d_mean + 2, dc_state, sizeof(atkdsp_cf32), s->stream);
+    if (rc == ATKB_OK)
+        rc = atkb_unpack(d, fmt, n, d + rb, cre, cim, k, off_re, off_im, want_mean ? d_mean : NULL,
+                         (double *)(d + rb + ob), s->stream);
+    if (rc == ATKB_OK && pole) rc = atkb_dc_pole(d + rb, n, dc_alpha, d_mean + 2, s->stream);
+    if (rc == ATKB_OK) rc = atkb_d2h(out, d + rb, n * sizeof(atkdsp_cf32), s->stream);
+    if (rc == ATKB_OK && want_mean) rc = atkb_d2h(hm, d_mean, sizeof hm, s->stream);
+    if (rc == ATKB_OK && pole) rc = atkb_d2h(dc_state, d_mean + 2, sizeof(atkdsp_cf32), s->stream);
+    if (rc == ATKB_OK) rc = atkb_stream_sync(s->stream);
+    scratch_unlock(s);
+    if (rc != ATKB_OK) return map_rc(rc == ATKB_E_NOMEM ? rc : ATKB_E_KERNEL);
+    if (mean_re) *mean_re = hm[0];
+    if (mean_im) *mean_im = hm[1];
+    return (ptrdiff_t)n;
+}
+
+/* reference src/convert.c:113-120 */
+ATKDSP_API ptrdiff_t atkdsp_unpack(const void *raw, size_t nbytes, int fmt, atkdsp_cf32 *out,
+                                   size_t out_cap, float dc_alpha, atkdsp_cf32 *dc_state) {
+    return unpack_host(raw, nbytes, fmt, out, out_cap, 0.0f, 0.0f, NULL, NULL, dc_alpha, dc_state);
+}
+
+/* reference src/convert.c:122-128 */
+ATKDSP_API ptrdiff_t atkdsp_unpack_dc(const void *raw, size_t nbytes, int fmt, atkdsp_cf32 *out,
+                                      size_t out_cap, float off_re, float off_im, double *mean_re,
+                                      double *mean_im) {
+    return unpack_host(raw, nbytes, fmt, out, out_cap, off_re, off_im, mean_re, mean_im, 0.0f, NULL);
+}
+
+/* device-pointer unpack: a small per-device area holds the mean partials */
+static int gpu_partials(double **d) {
+    int rc;
+    scratch_t *s = scratch_lock(4096 * 2 * sizeof(double), &rc);
+    if (!s) return rc;
+    *d = (double *)s->d;
+    scratch_unlock(s);
+    return ATKB_OK;
+}
+
+static int aligned_for(const void *ptr, int fmt) {
+    const size_t a = fmt == ATKDSP_FMT_CF32 ? 8 : fmt >= ATKDSP_FMT_CI16 ? 4 : 2;
+    return ((size_t)ptr % a) == 0;
+}
+
+ATKDSP_API ptrdiff_t atkdsp_gpu_unpack_dc(const void *d_raw, size_t nbytes, int fmt, atkdsp_cf32 *d_out,
+                                          size_t out_cap, float off_re, float off_im, double *d_mean,
+                                          void *stream) {
+    if (!d_raw || !d_out) return ATKDSP_E_ARG;
+    const int bps = atkdsp_bytes_per_sample(fmt);
+    if (!bps || !aligned_for(d_raw, fmt) || ((size_t)d_out & 7)) return ATKDSP_E_ARG;
+    float cre, cim, k;
+    unpack_consts(fmt, off_re, off_im, &cre, &cim, &k);
+    size_t n = nbytes / (size_t)bps;
+    if (n > out_cap) n = out_cap;
+    double *part = NULL;
+    if (d_mean) {
+        const int rc = gpu_partials(&part);
+        if (rc != ATKB_OK) return map_rc(rc);
+    }
+    const int rc = atkb_unpack(d_raw, fmt, n, d_out, cre, cim, k, off_re, off_im, d_mean, part, stream);
+    return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
+}
+
+ATKDSP_API ptrdiff_t atkdsp_gpu_unpack(const void *d_raw, size_t nbytes, int fmt, atkdsp_cf32 *d_out,
+                                       size_t out_cap, float dc_alpha, atkdsp_cf32 *d_dc_state,
+                                       void *stream) {
+    if (!d_raw || !d_out) return ATKDSP_E_ARG;
+    const int bps = atkdsp_bytes_per_sample(fmt);
+    if (!bps || !aligned_for(d_raw, fmt) || ((size_t)d_out & 7)) return ATKDSP_E_ARG;
+    float cre, cim, k;
+    unpack_consts(fmt, 0.0f, 0.0f, &cre, &cim, &k);
+    size_t n = nbytes / (size_t)bps;
+    if (n > out_cap) n = out_cap;
+    int rc = atkb_unpack(d_raw, fmt, n, d_out, cre, cim, k, 0.0f, 0.0f, NULL, NULL, stream);
+    if (rc == ATKB_OK && dc_alpha > 0.0f && d_dc_state) rc = atkb_dc_pole(d_out, n, dc_alpha, d_dc_state, stream);
+    return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
+}
+
+/* ===================================================================== batches */
+struct atkdsp_gpu_batch {
+    unsigned count;
+    atkdsp_pfb **h;
+    int dev;
+    void *stream;
+    int use_graph;
+    size_t tbl_bytes;
+    void *d_tables;
+    void *h_tables[2];
+    void *ev[2];
+    int ev_live[2];
+    void *graph[2];
+    int slot;
+    int *d_counters;
+    int grid, smem;
+    long long max_carry;
+};
+
+ATKDSP_API void atkdsp_gpu_batch_destroy(atkdsp_gpu_batch *b) {
+    if (!b) return;
+    atkb_set_device(b->dev);
+    if (b->stream) atkb_stream_sync(b->stream);
+    for (int i = 0; i < 2; ++i) {
+        atkb_graph_destroy(b->graph[i]);
+        atkb_event_destroy(b->ev[i]);
+        atkb_host_free(b->h_tables[i]);
+    }
+    atkb_free(b->d_tables);
+    atkb_free(b->d_counters);
+    atkb_stream_destroy(b->stream);
+    free(b->h);
+    free(b);
+}
+
+ATKDSP_API atkdsp_gpu_batch *atkdsp_gpu_batch_create(atkdsp_pfb *const *handles, unsigned count,
+                                                     int use_graph) {
+    if (!handles || count < 1) return NULL;
+    unsigned i;
+    for (i = 0; i < count; ++i)
+        if (!handles[i] || handles[i]->dev != handles[0]->dev) return NULL;
+    atkdsp_gpu_batch *b = (atkdsp_gpu_batch *)calloc(1, sizeof *b);
+    if (!b) return NULL;
+    b->count = count;
+    b->dev = handles[0]->dev;
+    b->use_graph = use_graph;
+    b->h = (atkdsp_pfb **)malloc(count * sizeof *b->h);
+    if (!b->h) { free(b); return NULL; }
+    for (i = 0; i < count; ++i) {
+        b->h[i] = handles[i];
+        if (handles[i]->bank.smem_bytes > b->smem) b->smem = handles[i]->bank.smem_bytes;
+        if ((long long)handles[i]->cap_state > b->max_carry) b->max_carry = (long long)handles[i]->cap_state;
+    }
+    atkb_set_device(b->dev);
+    b->tbl_bytes = tables_bytes(count);
+    int rc = atkb_stream_create(&b->stream);
+    if (rc == ATKB_OK) rc = atkb_malloc(&b->d_tables, b->tbl_bytes);
+    for (i = 0; i < 2 && rc == ATKB_OK; ++i) {
+        rc = atkb_host_alloc(&b->h_tables[i], b->tbl_bytes);
+        if (rc == ATKB_OK) rc = atkb_event_create(&b->ev[i]);
+    }
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&b->d_counters, 2 * sizeof(int));
+    if (rc == ATKB_OK) rc = atkb_memset(b->d_counters, 0, 2 * sizeof(int), b->stream);
+    if (rc == ATKB_OK) rc = atkb_stream_sync(b->stream);
+    if (rc != ATKB_OK) { atkdsp_gpu_batch_destroy(b); return NULL; }
+    b->grid = atkb_pfb_grid(b->dev, b->smem);
+    return b;
+}
+
+ATKDSP_API void *atkdsp_gpu_batch_stream(atkdsp_gpu_batch *b) { return b ? b->stream : NULL; }
+
+static int batch_enqueue(atkdsp_gpu_batch *b, int slot, void *stream) {
+    int rc = atkb_h2d(b->d_tables, b->h_tables[slot], b->tbl_bytes, stream);
+    if (rc == ATKB_OK)
+        rc = atkb_pfb_launch(tbl_jobs(b->d_tables), tbl_tiles(b->d_tables, b->count), (int)b->count,
+                             b->d_counters, b->grid, b->smem, stream);
+    if (rc == ATKB_OK) rc = atkb_pfb_carry(tbl_carry(b->d_tables, b->count), (int)b->count, b->max_carry, stream);
+    return rc;
+}
+
+ATKDSP_API ptrdiff_t atkdsp_gpu_batch_process(atkdsp_gpu_batch *b, const atkdsp_cf32 *const *d_ins,
+                                              const size_t *ns, atkdsp_cf32 *const *d_outs,
+                                              ptrdiff_t *ms, void *stream) {
+    if (!b || !d_ins || !ns || !d_outs) return ATKDSP_E_ARG;
+    if (atkb_set_device(b->dev) != ATKB_OK) return ATKDSP_E_FFT;
+    void *st = stream ? stream : b->stream;
+    const int slot = b->slot;
+    int rc;
+    unsigned i;
+    if (b->ev_live[slot] && atkb_event_sync(b->ev[slot]) != ATKB_OK) return ATKDSP_E_FFT;
+    atkb_job *J = tbl_jobs(b->h_tables[slot]);
+    atkb_carry *C = tbl_carry(b->h_tables[slot], b->count);
+    int *T = tbl_tiles(b->h_tables[slot], b->count);
+    long long total = 0, tiles = 0;
+    for (i = 0; i < b->count; ++i) {
+        atkdsp_pfb *p = b->h[i];
+        const size_t n = ns[i];
+        const size_t head = p->ov + p->lc;
+        const size_t m = ((size_t)p->lc + n) / p->hop;
+        if (n && !d_ins[i]) return ATKDSP_E_ARG;
+        if (m && !d_outs[i]) return ATKDSP_E_ARG;
+        const long long t = (long long)((m + (size_t)p->bank.tile_hops - 1) / (size_t)p->bank.tile_hops);
+        memset(&J[i], 0, sizeof J[i]);
+        J[i].state = state_buf(p, p->cur, 0);
+        J[i].in = d_ins[i];
+        J[i].out = d_outs[i];
+        J[i].cal = p->cal_nel ? p->d_cal : NULL;
+        J[i].head = (long long)head;
+        J[i].ldo = (long long)m;
+        J[i].b0 = (long long)p->b;
+        J[i].hops = (long long)m;
+        J[i].bank = (const atkb_bank *)p->d_bank;
+        J[i].tiles = (int)t;
+        T[i] = (int)tiles;
+        tiles += t;
+        C[i].state = J[i].state;
+        C[i].in = d_ins[i];
+        C[i].dst = state_buf(p, p->cur ^ 1, 0);
+        C[i].head = (long long)head;
+        C[i].from = (long long)(m * p->hop);
+        C[i].len = (long long)(head + n - m * p->hop);
+        total += (long long)m;
+        if (tiles > 0x3fffffff) return ATKDSP_E_ARG;
+    }
+    T[b->count] = (int)tiles;
+    if (b->use_graph && st == b->stream) {
+        if (!b->graph[slot]) {
+            rc = atkb_graph_begin(st);
+            if (rc == ATKB_OK) {
+                rc = batch_enqueue(b, slot, st);
+                void *g = NULL;
+                const int rc2 = atkb_graph_end(st, &g);
+                if (rc == ATKB_OK) rc = rc2;
+                b->graph[slot] = g;
+            }
+            if (rc != ATKB_OK) return map_rc(rc);
+        }
+        rc = atkb_graph_launch(b->graph[slot], st);
+    } else {
+        rc = batch_enqueue(b, slot, st);
+    }
+    if (rc == ATKB_OK) rc = atkb_event_record(b->ev[slot], st);
+    if (rc != ATKB_OK) return map_rc(rc);
+    b->ev_live[slot] = 1;
+    b->slot ^= 1;
+    for (i = 0; i < b->count; ++i) {
+        atkdsp_pfb *p = b->h[i];
+        const size_t n = ns[i];
+        const size_t m = ((size_t)p->lc + n) / p->hop;
+        if (ms) ms[i] = (ptrdiff_t)m;
+        p->cur ^= 1;
+        p->lc = (unsigned)(p->lc + n - m * p->hop);
+        p->b += (int64_t)m;
+    }
+    return (ptrdiff_t)total;
+}

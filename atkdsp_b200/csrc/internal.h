@@ -1,0 +1,144 @@
+/* Internal interface between the C99 host layer (atkdsp_host.c) and the CUDA
+ * shim (*.cu). Not part of the public ABI.
+ *
+ * The host layer owns handles, validation, prototype design and all the
+ * bookkeeping the reference keeps on the CPU; it never includes a CUDA
+ * header. Everything that touches the device goes through the atkb_* calls
+ * below, implemented in shim.cu / pfb.cu / unpack.cu / w12.cu. Device
+ * pointers cross this boundary as void*.
+ */
+#ifndef ATKB_INTERNAL_H
+#define ATKB_INTERNAL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes of the shim (mapped onto ATKDSP_E_* by the host) ------ */
+#define ATKB_OK        0
+#define ATKB_E_ARG    -1
+#define ATKB_E_NOMEM  -2
+#define ATKB_E_CAP    -3
+#define ATKB_E_KERNEL -4   /* a launch or an asynchronous kernel failure */
+#define ATKB_E_NODEV  -8   /* no usable CUDA device */
+
+/* ---- FFT plan --------------------------------------------------------------
+ * nchan = radix[0] * radix[1] * ... * radix[npass-1], Stockham order. For a
+ * power of two >= 16 the fast path is used: radix[0] == 16 and every later
+ * radix is 16, 8, 4 or 2 (16 complex points per thread per pass). */
+#define ATKB_MAX_PASS 24
+typedef struct {
+    int npass;
+    int fast;                     /* 1: power-of-two fast path */
+    int radix[ATKB_MAX_PASS];
+    int twoff[ATKB_MAX_PASS];     /* offset of pass p's twiddles in the table */
+    int twlen;                    /* total twiddle entries (double2)          */
+} atkb_fft_plan;
+
+/* ---- a filterbank's device constants ----------------------------------- */
+typedef struct {
+    int nchan, os, K, hop;
+    long long L, ov;
+    const float *taps;            /* device: L floats, (float)h[q]            */
+    const void *twd;              /* device: nchan double2 (cos, sin)(2 pi j/nchan) */
+    const void *wfull;            /* device: nchan double2 W^j = (cos, -sin)  */
+    const void *wpass;            /* device: per-pass twiddles (fast path)    */
+    atkb_fft_plan plan;
+    int tile_hops;                /* hops per CTA tile                        */
+    int smem_bytes;               /* dynamic shared memory a tile needs       */
+} atkb_bank;
+
+/* ---- one unit of PFB work: a run of hops of one element stream --------- */
+typedef struct {
+    const void *state;            /* device cf32: s[0, head)                   */
+    const void *in;               /* device cf32: s[head, head + n)            */
+    void *out;                    /* device cf32: this element's [nchan][ldo]  */
+    const void *cal;              /* device cf32: nchan factors, or NULL       */
+    long long head;               /* samples held in state                     */
+    long long ldo;                /* output row stride in samples              */
+    long long out_col;            /* column of hop 0 in out                    */
+    long long b0;                 /* global hop index of this call's hop 0     */
+    long long hops;               /* hops in this job                          */
+    const atkb_bank *bank;        /* device copy of the bank                   */
+    int bank_index;               /* unused by kernels; host bookkeeping       */
+    int tiles;                    /* ceil(hops / bank->tile_hops)              */
+} atkb_job;
+
+/* ---- state carry: dst[0, len) = s[from, from + len) -------------------- */
+typedef struct {
+    const void *state;
+    const void *in;
+    void *dst;
+    long long head;
+    long long from;
+    long long len;
+} atkb_carry;
+
+/* device / memory ---------------------------------------------------------- */
+int  atkb_get_device(int *dev);
+int  atkb_set_device(int dev);
+int  atkb_sm_count(int dev);
+int  atkb_stream_create(void **stream);
+void atkb_stream_destroy(void *stream);
+int  atkb_stream_sync(void *stream);
+int  atkb_malloc(void **p, size_t bytes);
+void atkb_free(void *p);
+int  atkb_host_alloc(void **p, size_t bytes);      /* pinned */
+void atkb_host_free(void *p);
+int  atkb_h2d(void *dst, const void *src, size_t bytes, void *stream);
+int  atkb_d2h(void *dst, const void *src, size_t bytes, void *stream);
+int  atkb_d2d(void *dst, const void *src, size_t bytes, void *stream);
+int  atkb_d2h_2d(void *dst, size_t dpitch, const void *src, size_t spitch,
+                 size_t width, size_t height, void *stream);
+int  atkb_memset(void *p, int v, size_t bytes, void *stream);
+int  atkb_mem_info(size_t *free_bytes, size_t *total_bytes);
+int  atkb_event_create(void **ev);
+void atkb_event_destroy(void *ev);
+int  atkb_event_record(void *ev, void *stream);
+int  atkb_event_sync(void *ev);
+int  atkb_stream_wait(void *stream, void *ev);
+/* graphs: capture the work enqueued on `stream` between begin and end */
+int  atkb_graph_begin(void *stream);
+int  atkb_graph_end(void *stream, void **exec);
+int  atkb_graph_launch(void *exec, void *stream);
+void atkb_graph_destroy(void *exec);
+
+/* filterbank --------------------------------------------------------------- */
+/* occupancy-derived number of CTAs for the persistent tile kernel */
+int  atkb_pfb_grid(int dev, int smem_bytes);
+int  atkb_pfb_max_smem(void);
+/* jobs / tile_start / counters are DEVICE arrays; tile_start has njobs + 1
+ * entries, the last one the total tile count, read by the kernel (so a
+ * captured graph can replay with new work). grid CTAs loop over the tiles.
+ * counters: 2 ints, zero before the first launch; the kernel leaves them
+ * zero again. */
+int  atkb_pfb_launch(const atkb_job *d_jobs, const int *d_tile_start, int njobs,
+                     int *d_counters, int grid, int smem_bytes, void *stream);
+int  atkb_pfb_carry(const atkb_carry *d_carry, int ncarry, long long max_len, void *stream);
+
+/* W1 + W2 over a device [nel][nchan][m] block. R, counts, pwr, mean_pwr are
+ * device pointers (any may be NULL to skip that output). */
+int  atkb_w12(const void *out, unsigned nel, unsigned nchan, size_t m, const uint8_t *gate,
+              void *R, uint32_t *counts, float *pwr, float *mean_pwr, void *stream);
+int  atkb_cov_reset(void *R, uint32_t *counts, unsigned nel, unsigned nchan,
+                    const uint8_t *gate, void *stream);
+
+/* unpack ------------------------------------------------------------------- */
+/* device raw -> device cf32, (x - c) * k per component; the means (double,
+ * BEFORE subtraction of the offset, i.e. sum(out)/n + off) go to d_mean[0..1]
+ * when d_mean != NULL, using d_partial (>= 2 * atkb_unpack_partials(n)
+ * doubles) as scratch. */
+int  atkb_unpack_partials(size_t n);
+int  atkb_unpack(const void *raw, int fmt, size_t n, void *out, float cre, float cim, float k,
+                 float off_re, float off_im, double *d_mean, double *d_partial, void *stream);
+/* the one-pole DC block over converted samples, serial per component;
+ * d_state is one cf32 on the device (read and updated). */
+int  atkb_dc_pole(void *out, size_t n, float alpha, void *d_state, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,474 @@
+/* The polyphase filterbank on sm_100a.
+ *
+ * What one hop computes (reference src/channelizer.c:235-292):
+ *   window   w = s[h*hop, h*hop + L),  s = history ++ leftover ++ input
+ *   fold     f[q] = sum_{k ascending} taps[k*M + q] * w[k*M + q]   (float,
+ *            one rounded multiply then one rounded add per tap -- the
+ *            reference's pinned C99 build does exactly this, so the fold is
+ *            bit-identical)
+ *   FFT      X = DFT_M(f) in DOUBLE (the reference runs pocketfft in double;
+ *            a float FFT misses the 1e-5 per-channel bar at M >= 1024)
+ *   rotate   y[k] = X[k] * twd[(-k*shift) mod M], shift = ((b+1)*hop) mod M,
+ *            with the reference's own double table (cos, sin)(2 pi j / M)
+ *   cal      y[k] *= cal[k] (double), then one rounding to float
+ *   out      channel-major: out[k*ldo + h]
+ *
+ * Kernel layout (B200-first):
+ *   - ONE persistent kernel over a device job list. A job is a run of hops of
+ *     one element stream (a handle's element, or one stream of a batch); a
+ *     tile is tile_hops consecutive hops of a job. CTAs take tiles from an
+ *     atomic counter until none are left, so one launch serves one element
+ *     or four thousand uneven streams, and the launch shape is fixed (CUDA
+ *     graph friendly). The counter resets itself when the last CTA leaves.
+ *   - Fast path (M a power of two, 16..4096): a tile is 4096 complex points
+ *     (tile_hops = 4096/M), 256 threads x 16 points. Each thread folds the 16
+ *     branches j + r*M/16 of one hop straight into registers -- exactly the
+ *     inputs of the first radix-16 Stockham butterfly -- so the fold never
+ *     touches shared memory; later radix-16/8/4/2 passes run in place in
+ *     shared memory (register staging between two barriers), per-pass
+ *     twiddle tables are laid out so consecutive lanes read consecutive
+ *     entries. The epilogue rotates, applies cal, rounds, transposes the tile
+ *     hop-major -> channel-major in shared memory and writes runs of
+ *     tile_hops consecutive outputs per channel.
+ *   - Generic path (any M >= 2): ping-pong shared buffers, mixed radix
+ *     (2, 3, 4, 8, 16 butterflies, direct DFT for any other prime factor).
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "internal.h"
+
+#define NT 256
+#define PTS 16
+#define TILE_POINTS (NT * PTS)
+
+namespace {
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+/* multiply by -i */
+__device__ __forceinline__ double2 cmi(double2 a) { return make_double2(a.y, -a.x); }
+
+/* the reference's rotation / cal product: one rounding per multiply and add */
+__device__ __forceinline__ double2 cmul_rn(double2 a, double2 b) {
+    return make_double2(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
+                        __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)));
+}
+
+#define C16_1 0.92387953251128675613   /* cos(pi/8) */
+#define S16_1 0.38268343236508977173   /* sin(pi/8) */
+#define SQH   0.70710678118654752440   /* sqrt(1/2) */
+
+/* forward DFTs, e^{-2 pi i nk/R} */
+__device__ __forceinline__ void dft2(double2 &a, double2 &b) {
+    const double2 t = a;
+    a = cadd(t, b);
+    b = csub(t, b);
+}
+
+__device__ __forceinline__ void dft4(double2 &v0, double2 &v1, double2 &v2, double2 &v3) {
+    const double2 t0 = cadd(v0, v2), t1 = csub(v0, v2);
+    const double2 t2 = cadd(v1, v3), t3 = cmi(csub(v1, v3));
+    v0 = cadd(t0, t2);
+    v2 = csub(t0, t2);
+    v1 = cadd(t1, t3);
+    v3 = csub(t1, t3);
+}
+
+__device__ __forceinline__ void dft8(double2 *v) {
+    /* n = 2 n1 + n2, k = k1 + 4 k2 */
+    double2 a0 = v[0], a1 = v[2], a2 = v[4], a3 = v[6];
+    double2 b0 = v[1], b1 = v[3], b2 = v[5], b3 = v[7];
+    dft4(a0, a1, a2, a3);
+    dft4(b0, b1, b2, b3);
+    b1 = make_double2(SQH * (b1.x + b1.y), SQH * (b1.y - b1.x));      /* W8^1 */
+    b2 = cmi(b2);                                                     /* W8^2 */
+    b3 = make_double2(SQH * (b3.y - b3.x), -SQH * (b3.x + b3.y));     /* W8^3 */
+    v[0] = cadd(a0, b0); v[4] = csub(a0, b0);
+    v[1] = cadd(a1, b1); v[5] = csub(a1, b1);
+    v[2] = cadd(a2, b2); v[6] = csub(a2, b2);
+    v[3] = cadd(a3, b3); v[7] = csub(a3, b3);
+}
+
+__device__ __forceinline__ void dft16(double2 *v) {
+    /* n = 4 n1 + n2, k = k1 + 4 k2: radix-4 columns, W16^(n2 k1), radix-4 rows */
+    double2 z[16];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+        double2 a = v[n2], b = v[4 + n2], c = v[8 + n2], d = v[12 + n2];
+        dft4(a, b, c, d);
+        z[n2 * 4 + 0] = a; z[n2 * 4 + 1] = b; z[n2 * 4 + 2] = c; z[n2 * 4 + 3] = d;
+    }
+    const double2 w1 = make_double2(C16_1, -S16_1), w2 = make_double2(SQH, -SQH);
+    const double2 w3 = make_double2(S16_1, -C16_1), w6 = make_double2(-SQH, -SQH);
+    const double2 w9 = make_double2(-C16_1, S16_1);
+    z[1 * 4 + 1] = cmul(z[1 * 4 + 1], w1);
+    z[1 * 4 + 2] = cmul(z[1 * 4 + 2], w2);
+    z[1 * 4 + 3] = cmul(z[1 * 4 + 3], w3);
+    z[2 * 4 + 1] = cmul(z[2 * 4 + 1], w2);
+    z[2 * 4 + 2] = cmi(z[2 * 4 + 2]);
+    z[2 * 4 + 3] = cmul(z[2 * 4 + 3], w6);
+    z[3 * 4 + 1] = cmul(z[3 * 4 + 1], w3);
+    z[3 * 4 + 2] = cmul(z[3 * 4 + 2], w6);
+    z[3 * 4 + 3] = cmul(z[3 * 4 + 3], w9);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        double2 a = z[0 * 4 + k1], b = z[1 * 4 + k1], c = z[2 * 4 + k1], d = z[3 * 4 + k1];
+        dft4(a, b, c, d);
+        v[k1] = a; v[k1 + 4] = b; v[k1 + 8] = c; v[k1 + 12] = d;
+    }
+}
+
+__device__ __forceinline__ void dft3(double2 &a, double2 &b, double2 &c) {
+    const double S3 = 0.86602540378443864676;   /* sin(2 pi / 3) */
+    const double2 s = cadd(b, c), d = csub(b, c);
+    const double2 m = make_double2(a.x - 0.5 * s.x, a.y - 0.5 * s.y);
+    const double2 r = make_double2(S3 * d.y, -S3 * d.x);  /* -i sin(2pi/3) (b - c) */
+    a = cadd(a, s);
+    b = cadd(m, r);
+    c = csub(m, r);
+}
+
+template <int R>
+__device__ __forceinline__ void dftR(double2 *v) {
+    if (R == 2) dft2(v[0], v[1]);
+    else if (R == 4) dft4(v[0], v[1], v[2], v[3]);
+    else if (R == 8) dft8(v);
+    else if (R == 16) dft16(v);
+}
+
+/* one element of the stream s = state[0, head) ++ in[0, ...) */
+struct Src {
+    const float2 *st;
+    const float2 *in;
+    long long head;
+    __device__ __forceinline__ float2 at(long long i) const {
+        return (i < head) ? __ldg(st + i) : __ldg(in + (i - head));
+    }
+};
+
+/* ---- fast path: nchan = 2^n, 16 <= nchan <= 4096 ------------------------- */
+/* Shared-memory index swizzle for the 16-byte complex doubles: the low four
+ * index bits are XORed with the next four. The first pass stores at a stride
+ * of 16 elements across lanes; swizzled, every 8-lane wavefront lands on 8
+ * distinct 16-byte slots, and the unit-stride accesses of later passes stay
+ * conflict-free too (a XOR with a per-block constant permutes the slots). */
+__device__ __forceinline__ int SW(int i) { return i ^ ((i >> 4) & 15); }
+
+template <int R>
+__device__ __forceinline__ void pass_inplace(double2 *sm, int M, int Ns, const double2 *tw) {
+    constexpr int U = PTS / R;
+    const int MR = M / R;
+    double2 v[U][R];
+    int dst[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int bi = u * NT + threadIdx.x;
+        const int tt = bi / MR;
+        const int j = bi - tt * MR;
+        const int k = j & (Ns - 1);
+        const int base = tt * M + j;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[u][r] = sm[SW(base + r * MR)];
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[u][r] = cmul(v[u][r], __ldg(tw + (r - 1) * Ns + k));
+        dst[u] = tt * M + (j - k) * R + k;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        dftR<R>(v[u]);
+#pragma unroll
+        for (int r = 0; r < R; ++r) sm[SW(dst[u] + r * Ns)] = v[u][r];
+    }
+    __syncthreads();
+}
+
+__device__ void tile_fast(const atkb_job &J, const atkb_bank &B, long long h0, int nvalid,
+                          double2 *sm, float2 *tile_out) {
+    const int M = B.nchan;
+    const int nh = TILE_POINTS / M;
+    const int Mr = M >> 4;
+    const int tid = threadIdx.x;
+    const int tt = tid / Mr;
+    const int j = tid - tt * Mr;
+
+    /* fold: this thread's 16 branches q = j + r*M/16 of hop h0 + tt */
+    double2 v[16];
+    if (tt < nvalid) {
+        const Src src{(const float2 *)J.state, (const float2 *)J.in, J.head};
+        const long long base = (h0 + tt) * (long long)B.hop + j;
+        const float *tp = B.taps + j;
+        float fr[16], fi[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const float h = __ldg(tp + r * Mr);
+            const float2 x = src.at(base + r * Mr);
+            fr[r] = __fmul_rn(h, x.x);
+            fi[r] = __fmul_rn(h, x.y);
+        }
+        for (int k = 1; k < B.K; ++k) {
+            const float *tk = tp + (long long)k * M;
+            const long long sk = base + (long long)k * M;
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                const float h = __ldg(tk + r * Mr);
+                const float2 x = src.at(sk + r * Mr);
+                fr[r] = __fadd_rn(fr[r], __fmul_rn(h, x.x));
+                fi[r] = __fadd_rn(fi[r], __fmul_rn(h, x.y));
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[r] = make_double2((double)fr[r], (double)fi[r]);
+    } else {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[r] = make_double2(0.0, 0.0);
+    }
+    /* first Stockham pass (Ns = 1, radix 16, no twiddles): dst = j*16 + r */
+    dft16(v);
+#pragma unroll
+    for (int r = 0; r < 16; ++r) sm[SW(tt * M + j * 16 + r)] = v[r];
+    __syncthreads();
+
+    const double2 *wp = (const double2 *)B.wpass;
+    int Ns = 16;
+    for (int p = 1; p < B.plan.npass; ++p) {
+        const int R = B.plan.radix[p];
+        const double2 *tw = wp + B.plan.twoff[p];
+        if (R == 16) pass_inplace<16>(sm, M, Ns, tw);
+        else if (R == 8) pass_inplace<8>(sm, M, Ns, tw);
+        else if (R == 4) pass_inplace<4>(sm, M, Ns, tw);
+        else pass_inplace<2>(sm, M, Ns, tw);
+        Ns *= R;
+    }
+
+    /* epilogue: rotate, cal, round; hop-major -> channel-major in smem */
+    const double2 *twd = (const double2 *)B.twd;
+    const float2 *cal = (const float2 *)J.cal;
+    const int os = B.os, hop = B.hop;
+    float2 y[PTS];
+    int ti[PTS];
+#pragma unroll
+    for (int u = 0; u < PTS; ++u) {
+        const int e = u * NT + tid;
+        const int t2 = e / M;
+        const int kb = e - t2 * M;
+        double2 X = sm[SW(e)];
+        const long long b = J.b0 + h0 + t2;
+        const int s = (int)((b + 1) % os);
+        const int jr = (kb * s) % os;
+        X = cmul_rn(X, __ldg(twd + (jr ? M - jr * hop : 0)));
+        if (cal) {
+            const float2 c = __ldg(cal + kb);
+            X = cmul_rn(X, make_double2((double)c.x, (double)c.y));
+        }
+        y[u] = make_float2(__double2float_rn(X.x), __double2float_rn(X.y));
+        ti[u] = kb * (nh + 1) + t2;       /* padded rows: no bank conflicts */
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < PTS; ++u) tile_out[ti[u]] = y[u];
+    __syncthreads();
+    float2 *out = (float2 *)J.out;
+    const long long col = J.out_col + h0;
+#pragma unroll 4
+    for (int u = 0; u < PTS; ++u) {
+        const int e = u * NT + tid;
+        const int kb = e / nh;
+        const int t2 = e - kb * nh;
+        if (t2 < nvalid) out[(long long)kb * J.ldo + col + t2] = tile_out[kb * (nh + 1) + t2];
+    }
+}
+
+/* ---- generic path: any nchan >= 2 ----------------------------------------- */
+__device__ void pass_generic(const double2 *src, double2 *dst, int M, int Ns, int R, int nh,
+                             const double2 *W) {
+    const int MR = M / R;
+    const int NsR = Ns * R;
+    const int stride = M / NsR;
+    for (int bi = threadIdx.x; bi < nh * MR; bi += NT) {
+        const int tt = bi / MR;
+        const int j = bi - tt * MR;
+        const int k = j % Ns;
+        const double2 *s = src + tt * M + j;
+        double2 *d = dst + tt * M + (j - k) * R + k;
+        if (R == 2 || R == 3 || R == 4 || R == 8 || R == 16) {
+            double2 v[16];
+            for (int r = 0; r < R; ++r) {
+                v[r] = s[r * MR];
+                if (r) v[r] = cmul(v[r], __ldg(W + r * k * stride));
+            }
+            if (R == 2) dft2(v[0], v[1]);
+            else if (R == 3) dft3(v[0], v[1], v[2]);
+            else if (R == 4) dft4(v[0], v[1], v[2], v[3]);
+            else if (R == 8) dft8(v);
+            else dft16(v);
+            for (int r = 0; r < R; ++r) d[r * Ns] = v[r];
+        } else {
+            /* direct DFT with the twiddle folded in: W_{NsR}^{r (k + o Ns)} */
+            for (int o = 0; o < R; ++o) {
+                double2 acc = make_double2(0.0, 0.0);
+                for (int r = 0; r < R; ++r) {
+                    const long long e = ((long long)r * (k + o * Ns)) % NsR;
+                    const double2 w = __ldg(W + e * stride);
+                    const double2 x = s[r * MR];
+                    acc.x += x.x * w.x - x.y * w.y;
+                    acc.y += x.x * w.y + x.y * w.x;
+                }
+                d[o * Ns] = acc;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+__device__ void tile_generic(const atkb_job &J, const atkb_bank &B, long long h0, int nvalid,
+                             double2 *sm) {
+    const int M = B.nchan;
+    const int nh = B.tile_hops;
+    double2 *A = sm, *Bf = sm + (size_t)nh * M;
+    const Src src{(const float2 *)J.state, (const float2 *)J.in, J.head};
+    for (int e = threadIdx.x; e < nh * M; e += NT) {
+        const int tt = e / M;
+        const int q = e - tt * M;
+        double2 v = make_double2(0.0, 0.0);
+        if (tt < nvalid) {
+            const long long base = (h0 + tt) * (long long)B.hop + q;
+            float2 x = src.at(base);
+            float h = __ldg(B.taps + q);
+            float fr = __fmul_rn(h, x.x), fi = __fmul_rn(h, x.y);
+            for (int k = 1; k < B.K; ++k) {
+                h = __ldg(B.taps + (long long)k * M + q);
+                x = src.at(base + (long long)k * M);
+                fr = __fadd_rn(fr, __fmul_rn(h, x.x));
+                fi = __fadd_rn(fi, __fmul_rn(h, x.y));
+            }
+            v = make_double2((double)fr, (double)fi);
+        }
+        A[e] = v;
+    }
+    __syncthreads();
+    const double2 *W = (const double2 *)B.wfull;
+    int Ns = 1;
+    double2 *cur = A, *nxt = Bf;
+    for (int p = 0; p < B.plan.npass; ++p) {
+        const int R = B.plan.radix[p];
+        pass_generic(cur, nxt, M, Ns, R, nh, W);
+        Ns *= R;
+        double2 *t = cur; cur = nxt; nxt = t;
+    }
+    const double2 *twd = (const double2 *)B.twd;
+    const float2 *cal = (const float2 *)J.cal;
+    float2 *out = (float2 *)J.out;
+    const int os = B.os, hop = B.hop;
+    for (int e = threadIdx.x; e < nvalid * M; e += NT) {
+        const int kb = e / nvalid;
+        const int tt = e - kb * nvalid;
+        double2 X = cur[tt * M + kb];
+        const long long b = J.b0 + h0 + tt;
+        const int s = (int)((b + 1) % os);
+        const int jr = (int)(((long long)kb * s) % os);
+        X = cmul_rn(X, __ldg(twd + (jr ? M - jr * hop : 0)));
+        if (cal) {
+            const float2 c = __ldg(cal + kb);
+            X = cmul_rn(X, make_double2((double)c.x, (double)c.y));
+        }
+        out[(long long)kb * J.ldo + J.out_col + h0 + tt] =
+            make_float2(__double2float_rn(X.x), __double2float_rn(X.y));
+    }
+}
+
+__global__ void __launch_bounds__(NT)
+pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile_start, int njobs,
+                 int *counters) {
+    extern __shared__ double2 sm[];
+    const int total_tiles = tile_start[njobs];
+    __shared__ int s_tile, s_local;
+    __shared__ atkb_bank s_bank;
+    __shared__ atkb_job s_job;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(&counters[0], 1);
+        __syncthreads();
+        const int tile = s_tile;
+        if (tile >= total_tiles) break;
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = njobs - 1;
+            while (lo < hi) {                   /* last job whose start <= tile */
+                const int mid = (lo + hi + 1) >> 1;
+                if (tile_start[mid] <= tile) lo = mid; else hi = mid - 1;
+            }
+            s_job = jobs[lo];
+            s_bank = *s_job.bank;
+            s_local = tile - tile_start[lo];
+        }
+        __syncthreads();
+        const atkb_job J = s_job;
+        const long long h0 = (long long)s_local * s_bank.tile_hops;
+        const long long left = J.hops - h0;
+        const int nvalid = (int)(left < s_bank.tile_hops ? left : s_bank.tile_hops);
+        if (s_bank.plan.fast)
+            tile_fast(J, s_bank, h0, nvalid, sm, (float2 *)sm);
+        else
+            tile_generic(J, s_bank, h0, nvalid, sm);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const int done = atomicAdd(&counters[1], 1);
+        if (done == (int)gridDim.x - 1) {      /* the last CTA out resets */
+            atomicExch(&counters[0], 0);
+            atomicExch(&counters[1], 0);
+        }
+    }
+}
+
+__global__ void pfb_carry_kernel(const atkb_carry *__restrict__ c, int n) {
+    const int ci = blockIdx.y;
+    if (ci >= n) return;
+    const atkb_carry C = c[ci];
+    const Src src{(const float2 *)C.state, (const float2 *)C.in, C.head};
+    float2 *dst = (float2 *)C.dst;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < C.len;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src.at(C.from + i);
+}
+
+}  // namespace
+
+extern "C" int atkb_pfb_max_smem(void) { return 200 * 1024; }
+
+extern "C" int atkb_pfb_grid(int dev, int smem_bytes) {
+    static int configured[64];
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        if (cudaFuncSetAttribute(pfb_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 atkb_pfb_max_smem()) != cudaSuccess)
+            return -1;
+        configured[dev] = 1;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pfb_tiles_kernel, NT, smem_bytes) !=
+        cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return per_sm * atkb_sm_count(dev);
+}
+
+extern "C" int atkb_pfb_launch(const atkb_job *d_jobs, const int *d_tile_start, int njobs,
+                               int *d_counters, int grid, int smem_bytes, void *stream) {
+    if (njobs <= 0) return ATKB_OK;
+    if (grid < 1) grid = 1;
+    pfb_tiles_kernel<<<grid, NT, smem_bytes, (cudaStream_t)stream>>>(d_jobs, d_tile_start, njobs,
+                                                                    d_counters);
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
+extern "C" int atkb_pfb_carry(const atkb_carry *d_carry, int ncarry, long long max_len,
+                              void *stream) {
+    if (ncarry <= 0 || max_len <= 0) return ATKB_OK;
+    long long bx = (max_len + 255) / 256;
+    if (bx > 1024) bx = 1024;
+    dim3 grid((unsigned)bx, (unsigned)ncarry);
+    pfb_carry_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_carry, ncarry);
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}

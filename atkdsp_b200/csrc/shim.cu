@@ -1,0 +1,110 @@
+/* The thin C-ABI shim between the C99 host layer and the CUDA runtime.
+ * Every function returns an ATKB_* status; no CUDA type crosses into C. */
+#include <cuda_runtime.h>
+#include "internal.h"
+
+static int st(cudaError_t e) {
+    if (e == cudaSuccess) return ATKB_OK;
+    if (e == cudaErrorMemoryAllocation) return ATKB_E_NOMEM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorInvalidDevice)
+        return ATKB_E_NODEV;
+    return ATKB_E_KERNEL;
+}
+
+extern "C" int atkb_get_device(int *dev) { return st(cudaGetDevice(dev)); }
+extern "C" int atkb_set_device(int dev) { return st(cudaSetDevice(dev)); }
+
+extern "C" int atkb_sm_count(int dev) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 1;
+    return n;
+}
+
+extern "C" int atkb_stream_create(void **stream) {
+    cudaStream_t s = nullptr;
+    const int rc = st(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    *stream = (void *)s;
+    return rc;
+}
+extern "C" void atkb_stream_destroy(void *stream) {
+    if (stream) cudaStreamDestroy((cudaStream_t)stream);
+}
+extern "C" int atkb_stream_sync(void *stream) { return st(cudaStreamSynchronize((cudaStream_t)stream)); }
+
+extern "C" int atkb_malloc(void **p, size_t bytes) {
+    *p = nullptr;
+    return st(cudaMalloc(p, bytes ? bytes : 256));
+}
+extern "C" void atkb_free(void *p) {
+    if (p) cudaFree(p);
+}
+extern "C" int atkb_host_alloc(void **p, size_t bytes) {
+    *p = nullptr;
+    return st(cudaMallocHost(p, bytes ? bytes : 256));
+}
+extern "C" void atkb_host_free(void *p) {
+    if (p) cudaFreeHost(p);
+}
+extern "C" int atkb_h2d(void *dst, const void *src, size_t bytes, void *stream) {
+    if (!bytes) return ATKB_OK;
+    return st(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream));
+}
+extern "C" int atkb_d2h(void *dst, const void *src, size_t bytes, void *stream) {
+    if (!bytes) return ATKB_OK;
+    return st(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+}
+extern "C" int atkb_d2d(void *dst, const void *src, size_t bytes, void *stream) {
+    if (!bytes) return ATKB_OK;
+    return st(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+}
+extern "C" int atkb_d2h_2d(void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
+                           size_t height, void *stream) {
+    if (!width || !height) return ATKB_OK;
+    return st(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, cudaMemcpyDeviceToHost,
+                                (cudaStream_t)stream));
+}
+extern "C" int atkb_memset(void *p, int v, size_t bytes, void *stream) {
+    if (!bytes) return ATKB_OK;
+    return st(cudaMemsetAsync(p, v, bytes, (cudaStream_t)stream));
+}
+extern "C" int atkb_mem_info(size_t *free_bytes, size_t *total_bytes) {
+    return st(cudaMemGetInfo(free_bytes, total_bytes));
+}
+
+extern "C" int atkb_event_create(void **ev) {
+    cudaEvent_t e = nullptr;
+    const int rc = st(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    *ev = (void *)e;
+    return rc;
+}
+extern "C" void atkb_event_destroy(void *ev) {
+    if (ev) cudaEventDestroy((cudaEvent_t)ev);
+}
+extern "C" int atkb_event_record(void *ev, void *stream) {
+    return st(cudaEventRecord((cudaEvent_t)ev, (cudaStream_t)stream));
+}
+extern "C" int atkb_event_sync(void *ev) { return st(cudaEventSynchronize((cudaEvent_t)ev)); }
+extern "C" int atkb_stream_wait(void *stream, void *ev) {
+    return st(cudaStreamWaitEvent((cudaStream_t)stream, (cudaEvent_t)ev, 0));
+}
+
+extern "C" int atkb_graph_begin(void *stream) {
+    return st(cudaStreamBeginCapture((cudaStream_t)stream, cudaStreamCaptureModeThreadLocal));
+}
+extern "C" int atkb_graph_end(void *stream, void **exec) {
+    cudaGraph_t g = nullptr;
+    *exec = nullptr;
+    int rc = st(cudaStreamEndCapture((cudaStream_t)stream, &g));
+    if (rc != ATKB_OK) return rc;
+    cudaGraphExec_t x = nullptr;
+    rc = st(cudaGraphInstantiate(&x, g, 0));
+    cudaGraphDestroy(g);
+    *exec = (void *)x;
+    return rc;
+}
+extern "C" int atkb_graph_launch(void *exec, void *stream) {
+    return st(cudaGraphLaunch((cudaGraphExec_t)exec, (cudaStream_t)stream));
+}
+extern "C" void atkb_graph_destroy(void *exec) {
+    if (exec) cudaGraphExecDestroy((cudaGraphExec_t)exec);
+}

@@ -1,0 +1,183 @@
+/* The unpack front end on sm_100a (reference src/convert.c:1-128).
+ *
+ *   out = (float(raw) - c') * k        (c' = c + off/k, precomputed on the
+ *                                       host in float as the reference does)
+ *   cf32: out = raw - off (or a copy when off == 0)
+ *
+ * Subtract and multiply are __fsub_rn / __fmul_rn so nvcc cannot fuse them:
+ * the samples are bit-identical to the reference's. The mean of the samples
+ * BEFORE the offset came out is sum(double(out)) / n + off; the double sum
+ * is a two-stage deterministic reduction (per-block partials, then one
+ * block), so it agrees with the reference's eight-way serial sum to ~1e-16.
+ *
+ * The one-pole DC block (src/convert.c:7-17) is a serial float recurrence;
+ * bit-exactness forbids reassociating it, so one thread per component runs
+ * it in order with rounded operations.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "internal.h"
+
+#define UNPACK_NT 256
+#define UNPACK_PER_THREAD 8
+#define UNPACK_MAX_BLOCKS 2048
+
+namespace {
+
+__device__ __forceinline__ float2 convert_one(const void *raw, int fmt, size_t i, float cre,
+                                              float cim, float k, float offr, float offi) {
+    float a, b;
+    switch (fmt) {
+    case 0: {
+        const uchar2 v = ((const uchar2 *)raw)[i];
+        a = (float)v.x; b = (float)v.y;
+        break;
+    }
+    case 1: {
+        const char2 v = ((const char2 *)raw)[i];
+        a = (float)v.x; b = (float)v.y;
+        break;
+    }
+    case 2:
+    case 3: {
+        const short2 v = ((const short2 *)raw)[i];
+        a = (float)v.x; b = (float)v.y;
+        break;
+    }
+    default: {
+        const float2 v = ((const float2 *)raw)[i];
+        if (offr == 0.0f && offi == 0.0f) return v;       /* the reference copies */
+        return make_float2(__fsub_rn(v.x, offr), __fsub_rn(v.y, offi));
+    }
+    }
+    return make_float2(__fmul_rn(__fsub_rn(a, cre), k), __fmul_rn(__fsub_rn(b, cim), k));
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(UNPACK_NT)
+unpack_kernel(const void *__restrict__ raw, int fmt, size_t n, float2 *__restrict__ out, float cre,
+              float cim, float k, float offr, float offi, double *__restrict__ partial) {
+    double sr = 0.0, si = 0.0;
+    const size_t stride = (size_t)gridDim.x * UNPACK_NT;
+    for (size_t i = (size_t)blockIdx.x * UNPACK_NT + threadIdx.x; i < n; i += stride) {
+        const float2 y = convert_one(raw, fmt, i, cre, cim, k, offr, offi);
+        out[i] = y;
+        sr += (double)y.x;
+        si += (double)y.y;
+    }
+    if (!partial) return;
+    __shared__ double red[2][UNPACK_NT / 32];
+    sr = warp_sum(sr);
+    si = warp_sum(si);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { red[0][w] = sr; red[1][w] = si; }
+    __syncthreads();
+    if (w == 0) {
+        sr = l < UNPACK_NT / 32 ? red[0][l] : 0.0;
+        si = l < UNPACK_NT / 32 ? red[1][l] : 0.0;
+        sr = warp_sum(sr);
+        si = warp_sum(si);
+        if (l == 0) { partial[2 * blockIdx.x] = sr; partial[2 * blockIdx.x + 1] = si; }
+    }
+}
+
+__global__ void __launch_bounds__(UNPACK_NT)
+unpack_mean_kernel(const double *__restrict__ partial, int nblocks, size_t n, float offr, float offi,
+                   double *__restrict__ mean) {
+    double sr = 0.0, si = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += UNPACK_NT) {
+        sr += partial[2 * b];
+        si += partial[2 * b + 1];
+    }
+    __shared__ double red[2][UNPACK_NT / 32];
+    sr = warp_sum(sr);
+    si = warp_sum(si);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { red[0][w] = sr; red[1][w] = si; }
+    __syncthreads();
+    if (w == 0) {
+        sr = l < UNPACK_NT / 32 ? red[0][l] : 0.0;
+        si = l < UNPACK_NT / 32 ? red[1][l] : 0.0;
+        sr = warp_sum(sr);
+        si = warp_sum(si);
+        if (l == 0) {
+            const double inv = n ? 1.0 / (double)n : 0.0;
+            mean[0] = sr * inv + (double)offr;
+            mean[1] = si * inv + (double)offi;
+        }
+    }
+}
+
+/* s += alpha (x - s); y = x - s, in order, one thread per component */
+__global__ void dc_pole_kernel(float *__restrict__ x, size_t n, float alpha, float *__restrict__ state) {
+    const int c = threadIdx.x;
+    if (c > 1) return;
+    float s = state[c];
+    size_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = x[2 * (i + u) + c];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            s = __fadd_rn(s, __fmul_rn(alpha, __fsub_rn(v[u], s)));
+            v[u] = __fsub_rn(v[u], s);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) x[2 * (i + u) + c] = v[u];
+    }
+    for (; i < n; ++i) {
+        const float v = x[2 * i + c];
+        s = __fadd_rn(s, __fmul_rn(alpha, __fsub_rn(v, s)));
+        x[2 * i + c] = __fsub_rn(v, s);
+    }
+    state[c] = s;
+}
+
+}  // namespace
+
+extern "C" int atkb_unpack_partials(size_t n) {
+    size_t b = (n + (size_t)UNPACK_NT * UNPACK_PER_THREAD - 1) / ((size_t)UNPACK_NT * UNPACK_PER_THREAD);
+    if (b < 1) b = 1;
+    if (b > UNPACK_MAX_BLOCKS) b = UNPACK_MAX_BLOCKS;
+    return (int)b;
+}
+
+extern "C" int atkb_unpack(const void *raw, int fmt, size_t n, void *out, float cre, float cim,
+                           float k, float off_re, float off_im, double *d_mean, double *d_partial,
+                           void *stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nb = atkb_unpack_partials(n);
+    if (n) {
+        if (fmt == 4 && off_re == 0.0f && off_im == 0.0f && !d_mean) {
+            if (out != raw && cudaMemcpyAsync(out, raw, n * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+                return ATKB_E_KERNEL;
+        } else {
+            unpack_kernel<<<nb, UNPACK_NT, 0, s>>>(raw, fmt, n, (float2 *)out, cre, cim, k, off_re,
+                                                   off_im, d_mean ? d_partial : nullptr);
+        }
+    }
+    if (d_mean) {
+        if (!n) {
+            /* the reference: inv = 0, so the mean is the offset itself */
+            const double z[2] = {(double)off_re, (double)off_im};
+            if (cudaMemcpyAsync(d_mean, z, sizeof z, cudaMemcpyHostToDevice, s) != cudaSuccess)
+                return ATKB_E_KERNEL;
+            if (cudaStreamSynchronize(s) != cudaSuccess) return ATKB_E_KERNEL;
+        } else {
+            unpack_mean_kernel<<<1, UNPACK_NT, 0, s>>>(d_partial, nb, n, off_re, off_im, d_mean);
+        }
+    }
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
+extern "C" int atkb_dc_pole(void *out, size_t n, float alpha, void *d_state, void *stream) {
+    if (!n) return ATKB_OK;
+    dc_pole_kernel<<<1, 32, 0, (cudaStream_t)stream>>>((float *)out, n, alpha, (float *)d_state);
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}

@@ -1,0 +1,146 @@
+"""Device-pointer front end (include/atkdsp_gpu.h) for torch tensors.
+
+torch is used here only as the owner of device memory and streams: every
+computation runs in the library's own CUDA kernels. Tensors must be
+contiguous and on the handle's device; complex samples are ``torch.complex64``
+(the cf32 layout), raw front-end samples ``torch.uint8`` / ``int8`` /
+``int16`` byte buffers.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import AtkDspError, Pfb, _check, _fmt, bytes_per_sample, load
+
+__all__ = ["process_n", "unpack_dc", "unpack", "cov_accumulate", "channel_power", "Batch",
+           "sync"]
+
+
+def _ptr(t: torch.Tensor | None):
+    if t is None:
+        return None
+    if not t.is_cuda or not t.is_contiguous():
+        raise AtkDspError("device tensors must be contiguous CUDA tensors")
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+def sync(p: Pfb) -> None:
+    _check(load().atkdsp_gpu_pfb_sync(p.handle), "gpu_pfb_sync")
+
+
+def process_n(p: Pfb, ins, nel: int, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """atkdsp_gpu_pfb_process_n: ins are nel complex64 CUDA tensors of equal
+    length; returns (nel, nchan, m) complex64 on the device. Asynchronous on
+    ``stream`` (default: the handle's stream)."""
+    lib = load()
+    nel = int(nel)
+    n = int(ins[0].numel())
+    for t in ins[:nel]:
+        if t.numel() != n or t.dtype != torch.complex64:
+            raise AtkDspError("gpu process_n: inputs must be complex64 of equal length")
+    m = p.out_hops(n)
+    if out is None:
+        out = torch.empty(nel * p.nchan * max(m, 1), dtype=torch.complex64, device=ins[0].device)
+    arr = (C.c_void_p * nel)(*[t.data_ptr() for t in ins[:nel]])
+    got = lib.atkdsp_gpu_pfb_process_n(p.handle, arr, nel, n, _ptr(out), out.numel(), _stream(stream))
+    _check(int(got), "gpu_pfb_process_n")
+    return out[: nel * p.nchan * got].view(nel, p.nchan, got)
+
+
+def unpack_dc(raw: torch.Tensor, fmt, offset: complex = 0j, out: torch.Tensor | None = None,
+              want_mean: bool = True, stream=None):
+    """atkdsp_gpu_unpack_dc: returns (samples, mean) with mean a (2,) float64
+    CUDA tensor (re, im) or None."""
+    lib = load()
+    nbytes = raw.numel() * raw.element_size()
+    n = nbytes // bytes_per_sample(fmt)
+    if out is None:
+        out = torch.empty(max(n, 1), dtype=torch.complex64, device=raw.device)
+    mean = torch.empty(2, dtype=torch.float64, device=raw.device) if want_mean else None
+    got = lib.atkdsp_gpu_unpack_dc(_ptr(raw), nbytes, _fmt(fmt), _ptr(out), out.numel(),
+                                   float(offset.real), float(offset.imag), _ptr(mean),
+                                   _stream(stream))
+    _check(int(got), "gpu_unpack_dc")
+    return out[:got], mean
+
+
+def unpack(raw: torch.Tensor, fmt, dc_alpha: float = 0.0, dc_state: torch.Tensor | None = None,
+           out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    lib = load()
+    nbytes = raw.numel() * raw.element_size()
+    n = nbytes // bytes_per_sample(fmt)
+    if out is None:
+        out = torch.empty(max(n, 1), dtype=torch.complex64, device=raw.device)
+    got = lib.atkdsp_gpu_unpack(_ptr(raw), nbytes, _fmt(fmt), _ptr(out), out.numel(),
+                                float(dc_alpha), _ptr(dc_state), _stream(stream))
+    _check(int(got), "gpu_unpack")
+    return out[:got]
+
+
+def cov_accumulate(out: torch.Tensor, nel: int, nchan: int, gate: torch.Tensor | None,
+                   R: torch.Tensor, counts: torch.Tensor, stream=None) -> None:
+    m = out.shape[-1] if out.dim() == 3 else 0
+    _check(load().atkdsp_gpu_pfb_cov_accumulate(_ptr(out), int(nel), int(nchan), m, _ptr(gate),
+                                                _ptr(R), _ptr(counts), _stream(stream)),
+           "gpu_cov_accumulate")
+
+
+def channel_power(out: torch.Tensor, nel: int, nchan: int, stream=None):
+    m = out.shape[-1] if out.dim() == 3 else 0
+    pwr = torch.zeros(int(nel) * int(nchan), dtype=torch.float32, device=out.device)
+    meanp = torch.zeros(int(nchan), dtype=torch.float32, device=out.device)
+    _check(load().atkdsp_gpu_pfb_channel_power(_ptr(out), int(nel), int(nchan), m, _ptr(pwr),
+                                               _ptr(meanp), _stream(stream)), "gpu_channel_power")
+    return pwr.view(int(nel), int(nchan)), meanp
+
+
+class Batch:
+    """atkdsp_gpu_batch: many single-element handles, one launch per block set."""
+
+    def __init__(self, pfbs, use_graph: bool = True):
+        self._lib = load()
+        self.pfbs = list(pfbs)
+        arr = (C.c_void_p * len(self.pfbs))(*[p.handle for p in self.pfbs])
+        self._b = self._lib.atkdsp_gpu_batch_create(arr, len(self.pfbs), 1 if use_graph else 0)
+        if not self._b:
+            raise AtkDspError("gpu_batch_create failed")
+        n = len(self.pfbs)
+        self._ins = (C.c_void_p * n)()
+        self._outs = (C.c_void_p * n)()
+        self._ns = (C.c_size_t * n)()
+        self._ms = (C.c_ssize_t * n)()
+
+    def __del__(self):
+        b = getattr(self, "_b", None)
+        if b:
+            self._lib.atkdsp_gpu_batch_destroy(b)
+            self._b = None
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(self._lib.atkdsp_gpu_batch_stream(self._b) or 0)
+
+    def out_hops(self, ns) -> list:
+        return [p.out_hops(int(n)) for p, n in zip(self.pfbs, ns)]
+
+    def process(self, ins, outs, stream=None) -> list:
+        """ins[i]: complex64 CUDA tensor (new block of handle i; may be empty);
+        outs[i]: complex64 CUDA tensor of >= nchan_i * out_hops_i samples.
+        Returns the per-handle hop counts. Asynchronous."""
+        for i, (x, o) in enumerate(zip(ins, outs)):
+            self._ins[i] = x.data_ptr() if x.numel() else None
+            self._outs[i] = o.data_ptr() if o is not None and o.numel() else None
+            self._ns[i] = x.numel()
+        got = self._lib.atkdsp_gpu_batch_process(self._b, self._ins, self._ns, self._outs, self._ms,
+                                                 _stream(stream))
+        _check(int(got), "gpu_batch_process")
+        return [int(self._ms[i]) for i in range(len(self.pfbs))]

@@ -1,0 +1,123 @@
+/*
+ * atkdsp.h -- the channelizer slice of atkdsp's C ABI, implemented on B200.
+ *
+ * This header declares exactly the entry points of the reference's ABI
+ * (include/atkdsp.h of atkdsp 0.25.1, ABI 26) that the polyphase-filterbank
+ * path uses: identity, threads, the unpack front end, the atkdsp_pfb_* handle
+ * API and the W1/W2 accumulators. Names, types, argument meaning, return
+ * codes and the channel-major output layout are the reference's, so a caller
+ * of the reference (its ctypes binding, a C program, the in-library survey)
+ * links against this library unchanged for this path. Each declaration cites
+ * the reference declaration it replaces.
+ *
+ * What is different underneath: every *_process / *_unpack call runs on the
+ * GPU (CUDA, sm_100a). Sample buffers are still the caller's host memory and
+ * calls are synchronous on return, as the reference's are. Each handle keeps
+ * its streaming state (FIR history, leftover samples, hop counter) in device
+ * memory, and owns one CUDA stream and the device buffers it needs, all
+ * allocated by *_create; a process call allocates nothing. Device-pointer
+ * entry points for callers that keep samples on the GPU are in atkdsp_gpu.h.
+ *
+ * Threading: one handle is used by one thread at a time; different handles
+ * may be used concurrently from different threads (each has its own stream).
+ */
+#ifndef ATKDSP_H
+#define ATKDSP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(_WIN32) || defined(__CYGWIN__)
+#  define ATKDSP_API __declspec(dllexport)
+#else
+#  define ATKDSP_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* reference include/atkdsp.h:63-64 */
+#define ATKDSP_ABI_VERSION 26
+#define ATKDSP_VERSION_STRING "0.25.1"
+
+/* reference include/atkdsp.h:203-207 */
+#define ATKDSP_OK            0
+#define ATKDSP_E_ARG        -1   /* null pointer, bad size, unknown enum          */
+#define ATKDSP_E_NOMEM      -2   /* allocation failed (host or device)            */
+#define ATKDSP_E_CAP        -3   /* caller's output buffer too small              */
+#define ATKDSP_E_FFT        -4   /* the transform failed: a GPU launch or kernel error */
+
+/* reference include/atkdsp.h:213 -- complex float32, numpy complex64 layout */
+typedef struct { float re, im; } atkdsp_cf32;
+
+/* reference include/atkdsp.h:216-222 */
+enum atkdsp_format {
+    ATKDSP_FMT_CU8     = 0,
+    ATKDSP_FMT_CI8     = 1,
+    ATKDSP_FMT_CI16    = 2,
+    ATKDSP_FMT_CI16Q11 = 3,
+    ATKDSP_FMT_CF32    = 4
+};
+
+/* ---- identity: reference include/atkdsp.h:237-244 ----------------------- */
+ATKDSP_API int         atkdsp_abi_version(void);        /* 26 */
+ATKDSP_API const char *atkdsp_version_string(void);     /* "0.25.1" */
+ATKDSP_API const char *atkdsp_build_info(void);         /* contains "abi 26" */
+ATKDSP_API int         atkdsp_bytes_per_sample(int fmt);
+/* Accepted for compatibility; the GPU path has no host worker threads, so the
+ * count changes nothing but what atkdsp_get_threads reports. */
+ATKDSP_API int         atkdsp_set_threads(int n);
+ATKDSP_API int         atkdsp_get_threads(void);
+
+/* ---- unpack: reference include/atkdsp.h:247-273 ------------------------- */
+ATKDSP_API ptrdiff_t atkdsp_unpack(const void *raw, size_t nbytes, int fmt,
+                                   atkdsp_cf32 *out, size_t out_cap,
+                                   float dc_alpha, atkdsp_cf32 *dc_state);
+ATKDSP_API ptrdiff_t atkdsp_unpack_dc(const void *raw, size_t nbytes, int fmt,
+                                      atkdsp_cf32 *out, size_t out_cap,
+                                      float off_re, float off_im,
+                                      double *mean_re, double *mean_im);
+
+/* ---- the polyphase filterbank: reference include/atkdsp.h:3185-3229 ----- */
+typedef struct atkdsp_pfb atkdsp_pfb;
+/* reference include/atkdsp.h:3191-3193. NULL on bad arguments (fs <= 0,
+ * nchan < 2, nchan % oversample, taps_per_poly < 2, max_nel < 1), when no GPU
+ * is usable, when device memory runs out, or when nchan is beyond what the
+ * device kernels support (power of two up to 4096, any other value up to 6400). */
+ATKDSP_API atkdsp_pfb *atkdsp_pfb_create(double fs, unsigned nchan, unsigned oversample,
+                                         unsigned taps_per_poly, double atten_db,
+                                         unsigned max_nel);
+ATKDSP_API void        atkdsp_pfb_destroy(atkdsp_pfb *p);                  /* :3194 */
+ATKDSP_API void        atkdsp_pfb_reset(atkdsp_pfb *p);                    /* :3195 */
+ATKDSP_API unsigned    atkdsp_pfb_nchan(const atkdsp_pfb *p);              /* :3196 */
+ATKDSP_API double      atkdsp_pfb_out_rate(const atkdsp_pfb *p);           /* :3197 */
+ATKDSP_API size_t      atkdsp_pfb_out_hops(const atkdsp_pfb *p, size_t n); /* :3200 */
+/* reference include/atkdsp.h:3209-3210: out is [nchan][m], channel-major */
+ATKDSP_API ptrdiff_t   atkdsp_pfb_process(atkdsp_pfb *p, const atkdsp_cf32 *in, size_t n,
+                                          atkdsp_cf32 *out, size_t cap);
+/* reference include/atkdsp.h:3218-3220: out is [nel][nchan][m] */
+ATKDSP_API ptrdiff_t   atkdsp_pfb_process_n(atkdsp_pfb *p, const atkdsp_cf32 *const *ins,
+                                            unsigned nel, size_t n,
+                                            atkdsp_cf32 *out, size_t cap);
+ATKDSP_API int64_t     atkdsp_pfb_block_origin(const atkdsp_pfb *p, int64_t hop_index); /* :3223 */
+ATKDSP_API double      atkdsp_pfb_group_delay(const atkdsp_pfb *p);                      /* :3224 */
+ATKDSP_API int         atkdsp_pfb_set_cal(atkdsp_pfb *p, const atkdsp_cf32 *table,
+                                          unsigned nel);                                 /* :3228 */
+ATKDSP_API int         atkdsp_pfb_describe(const atkdsp_pfb *p, char *buf, size_t cap);  /* :3229 */
+
+/* ---- W1 / W2: reference include/atkdsp.h:3239-3251 ---------------------- */
+ATKDSP_API void        atkdsp_pfb_cov_accumulate(const atkdsp_cf32 *out, unsigned nel,
+                                                 unsigned nchan, size_t m,
+                                                 const uint8_t *gate,
+                                                 atkdsp_cf32 *R, uint32_t *counts);
+ATKDSP_API void        atkdsp_pfb_cov_reset(atkdsp_cf32 *R, uint32_t *counts, unsigned nel,
+                                            unsigned nchan, const uint8_t *gate);
+ATKDSP_API void        atkdsp_pfb_channel_power(const atkdsp_cf32 *out, unsigned nel,
+                                                unsigned nchan, size_t m,
+                                                float *pwr, float *mean_pwr);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

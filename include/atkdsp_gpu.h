@@ -1,0 +1,90 @@
+/*
+ * atkdsp_gpu.h -- device-pointer entry points of the B200 channelizer.
+ *
+ * The reference has no device boundary: its atkdsp_pfb_* / atkdsp_unpack*
+ * calls take host memory (include/atkdsp.h:3185-3251, :247-273). These entry
+ * points are the same operations for callers whose samples already live in
+ * GPU memory: every pointer named d_* is a device pointer, work is enqueued
+ * on `stream` (a cudaStream_t passed as void*; NULL means the handle's own
+ * stream for handle calls, the legacy default stream otherwise) and the call
+ * returns without waiting. Results match the host-pointer calls bit for bit.
+ *
+ * State: a handle's streaming state lives on the device and is advanced in
+ * stream order, so successive calls on one handle must be ordered on the
+ * GPU (same stream, or events between streams).
+ */
+#ifndef ATKDSP_GPU_H
+#define ATKDSP_GPU_H
+
+#include "atkdsp.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The handle's own CUDA stream (cudaStream_t as void*). */
+ATKDSP_API void       *atkdsp_gpu_pfb_stream(atkdsp_pfb *p);
+/* Wait for the handle's stream. ATKDSP_OK, or ATKDSP_E_FFT if a kernel failed. */
+ATKDSP_API int         atkdsp_gpu_pfb_sync(atkdsp_pfb *p);
+
+/* atkdsp_pfb_process_n (reference include/atkdsp.h:3218) on device buffers:
+ * d_ins[el] are nel device pointers of n samples each (the array itself is
+ * host memory), d_out is [nel][nchan][m] device memory of cap samples.
+ * Returns m (known on the host before the work runs), or ATKDSP_E_ARG /
+ * ATKDSP_E_CAP (state untouched) / ATKDSP_E_FFT (launch failure). */
+ATKDSP_API ptrdiff_t   atkdsp_gpu_pfb_process_n(atkdsp_pfb *p, const atkdsp_cf32 *const *d_ins,
+                                                unsigned nel, size_t n, atkdsp_cf32 *d_out,
+                                                size_t cap, void *stream);
+
+/* atkdsp_unpack_dc (reference include/atkdsp.h:270) on device buffers. When
+ * d_mean is not NULL it receives the two means (re, im) as doubles on the
+ * device. d_raw must be aligned to the sample's component size. Uses a
+ * per-device scratch area that the library allocates on the first call on
+ * each device; calls on one device must not overlap on the GPU. */
+ATKDSP_API ptrdiff_t   atkdsp_gpu_unpack_dc(const void *d_raw, size_t nbytes, int fmt,
+                                            atkdsp_cf32 *d_out, size_t out_cap,
+                                            float off_re, float off_im, double *d_mean,
+                                            void *stream);
+/* atkdsp_unpack (reference include/atkdsp.h:252) on device buffers;
+ * d_dc_state is one device cf32, read and updated when dc_alpha > 0. */
+ATKDSP_API ptrdiff_t   atkdsp_gpu_unpack(const void *d_raw, size_t nbytes, int fmt,
+                                         atkdsp_cf32 *d_out, size_t out_cap, float dc_alpha,
+                                         atkdsp_cf32 *d_dc_state, void *stream);
+
+/* W1 / W2 (reference include/atkdsp.h:3239-3251) on a device output block. */
+ATKDSP_API int         atkdsp_gpu_pfb_cov_accumulate(const atkdsp_cf32 *d_out, unsigned nel,
+                                                     unsigned nchan, size_t m,
+                                                     const uint8_t *d_gate, atkdsp_cf32 *d_R,
+                                                     uint32_t *d_counts, void *stream);
+ATKDSP_API int         atkdsp_gpu_pfb_cov_reset(atkdsp_cf32 *d_R, uint32_t *d_counts,
+                                                unsigned nel, unsigned nchan,
+                                                const uint8_t *d_gate, void *stream);
+ATKDSP_API int         atkdsp_gpu_pfb_channel_power(const atkdsp_cf32 *d_out, unsigned nel,
+                                                    unsigned nchan, size_t m, float *d_pwr,
+                                                    float *d_mean_pwr, void *stream);
+
+/* ---- batches: many independent handles in one persistent launch --------
+ * A batch groups handles (each single-element, any nchan / taps / oversample)
+ * so that one call channelizes one new block of every handle with a single
+ * kernel launch over all their hops, plus one launch that carries every
+ * handle's state forward. With use_graph != 0 the launch sequence is captured
+ * once in a CUDA graph and replayed; the per-call description of the blocks
+ * travels in a pinned table that the graph copies to the device. */
+typedef struct atkdsp_gpu_batch atkdsp_gpu_batch;
+ATKDSP_API atkdsp_gpu_batch *atkdsp_gpu_batch_create(atkdsp_pfb *const *handles, unsigned count,
+                                                     int use_graph);
+ATKDSP_API void        atkdsp_gpu_batch_destroy(atkdsp_gpu_batch *b);
+/* d_ins[i]: ns[i] new samples of handle i (device); d_outs[i]: its
+ * [nchan][m_i] output (device), at least nchan * out_hops(handle i, ns[i])
+ * samples. ms (host, may be NULL) receives each m_i. ns[i] may be 0. Work runs
+ * on `stream` (NULL: the batch's own stream). Returns the total number of
+ * hops, or ATKDSP_E_*. */
+ATKDSP_API ptrdiff_t   atkdsp_gpu_batch_process(atkdsp_gpu_batch *b, const atkdsp_cf32 *const *d_ins,
+                                                const size_t *ns, atkdsp_cf32 *const *d_outs,
+                                                ptrdiff_t *ms, void *stream);
+ATKDSP_API void       *atkdsp_gpu_batch_stream(atkdsp_gpu_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,229 @@
+"""ctypes front end for the CPU checkers -- TEST INFRASTRUCTURE ONLY.
+
+Two libraries share one Python interface here:
+
+* ``liboracle.so`` -- this repository's C restatement of the reference's
+  channelizer / unpack algorithm (``oracle/pfb_oracle.c``);
+* ``_ref/libatkdsp_ref.so`` -- the reference library itself, compiled from its
+  own sources by ``oracle/Makefile`` (present only where it was built).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module. The product (``atkdsp_b200``) never imports it.
+
+The Python surface mirrors the reference binding (python/atkdsp/__init__.py:
+``Pfb`` at :4159-4219, ``unpack``/``unpack_dc`` at :337-385, W1/W2 at
+:4222-4266) so a parity test reads the same against either side.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_SO = HERE / "_ref" / "libatkdsp_ref.so"
+
+FMT = {"cu8": 0, "ci8": 1, "ci16": 2, "ci16q11": 3, "cf32": 4}
+
+
+class _Cf32(C.Structure):
+    _fields_ = [("re", C.c_float), ("im", C.c_float)]
+
+
+_P = C.POINTER
+_pcf = _P(_Cf32)
+
+
+def _cfp(a: np.ndarray):
+    return a.ctypes.data_as(_pcf)
+
+
+def _fmt(f) -> int:
+    return FMT[f] if isinstance(f, str) else int(f)
+
+
+class CpuLib:
+    """One of the two CPU libraries, behind the reference binding's surface."""
+
+    def __init__(self, path: Path, prefix: str):
+        self.path = Path(path)
+        if not self.path.exists():
+            raise FileNotFoundError(f"{self.path} is not built (make -C oracle)")
+        self.lib = C.CDLL(str(self.path))
+        self.prefix = prefix
+        self._bind()
+
+    def _f(self, name):
+        return getattr(self.lib, self.prefix + name)
+
+    def _bind(self):
+        vp, sz, u, d, i64 = C.c_void_p, C.c_size_t, C.c_uint, C.c_double, C.c_int64
+        f = self._f
+        f("pfb_create").argtypes = [d, u, u, u, d, u]
+        f("pfb_create").restype = vp
+        f("pfb_destroy").argtypes = [vp]
+        f("pfb_destroy").restype = None
+        f("pfb_reset").argtypes = [vp]
+        f("pfb_reset").restype = None
+        f("pfb_out_hops").argtypes = [vp, sz]
+        f("pfb_out_hops").restype = sz
+        f("pfb_process_n").argtypes = [vp, _P(_pcf), u, sz, _pcf, sz]
+        f("pfb_process_n").restype = C.c_ssize_t
+        f("pfb_set_cal").argtypes = [vp, _pcf, u]
+        f("pfb_set_cal").restype = C.c_int
+        f("pfb_cov_accumulate" if self.prefix == "atkdsp_" else "cov_accumulate").argtypes = \
+            [_pcf, u, u, sz, _P(C.c_uint8), _pcf, _P(C.c_uint32)]
+        f("pfb_cov_reset" if self.prefix == "atkdsp_" else "cov_reset").argtypes = \
+            [_pcf, _P(C.c_uint32), u, u, _P(C.c_uint8)]
+        f("pfb_channel_power" if self.prefix == "atkdsp_" else "channel_power").argtypes = \
+            [_pcf, u, u, sz, _P(C.c_float), _P(C.c_float)]
+        f("unpack").argtypes = [C.c_void_p, sz, C.c_int, _pcf, sz, C.c_float, _pcf]
+        f("unpack").restype = C.c_ssize_t
+        f("unpack_dc").argtypes = [C.c_void_p, sz, C.c_int, _pcf, sz, C.c_float, C.c_float,
+                                   _P(C.c_double), _P(C.c_double)]
+        f("unpack_dc").restype = C.c_ssize_t
+        f("bytes_per_sample").argtypes = [C.c_int]
+        f("bytes_per_sample").restype = C.c_int
+        if self.prefix == "orc_":
+            self.lib.orc_pfb_prototype.argtypes = [u, u, d, _P(C.c_double)]
+            self.lib.orc_pfb_prototype.restype = None
+        else:
+            self.lib.atkdsp_set_threads.argtypes = [C.c_int]
+            self.lib.atkdsp_set_threads.restype = C.c_int
+            self.lib.atkdsp_get_threads.restype = C.c_int
+
+    # -- the filterbank -------------------------------------------------------
+    def Pfb(self, fs, nchan, oversample=2, taps_per_poly=12, atten_db=80.0, max_nel=1):
+        return _CpuPfb(self, fs, nchan, oversample, taps_per_poly, atten_db, max_nel)
+
+    def prototype(self, nchan, taps_per_poly, atten_db):
+        h = np.zeros(int(nchan) * int(taps_per_poly), np.float64)
+        self.lib.orc_pfb_prototype(int(nchan), int(taps_per_poly), float(atten_db),
+                                   h.ctypes.data_as(_P(C.c_double)))
+        return h
+
+    # -- W1 / W2 ---------------------------------------------------------------
+    def _w(self, name):
+        return self._f(("pfb_" if self.prefix == "atkdsp_" else "") + name)
+
+    def pfb_cov_accumulate(self, out, nel, nchan, gate, R, counts):
+        o = np.ascontiguousarray(out, np.complex64)
+        m = o.shape[2] if o.ndim == 3 else 0
+        gp = None
+        if gate is not None:
+            g = np.ascontiguousarray(gate, np.uint8)
+            gp = g.ctypes.data_as(_P(C.c_uint8))
+        self._w("cov_accumulate")(_cfp(o.reshape(-1)), int(nel), int(nchan), m, gp,
+                                  _cfp(R.reshape(-1)), counts.ctypes.data_as(_P(C.c_uint32)))
+
+    def pfb_cov_reset(self, R, counts, nel, nchan, gate=None):
+        gp = None
+        if gate is not None:
+            g = np.ascontiguousarray(gate, np.uint8)
+            gp = g.ctypes.data_as(_P(C.c_uint8))
+        self._w("cov_reset")(_cfp(R.reshape(-1)), counts.ctypes.data_as(_P(C.c_uint32)),
+                             int(nel), int(nchan), gp)
+
+    def pfb_channel_power(self, out, nel, nchan):
+        o = np.ascontiguousarray(out, np.complex64)
+        m = o.shape[2] if o.ndim == 3 else 0
+        pwr = np.zeros(int(nel) * int(nchan), np.float32)
+        meanp = np.zeros(int(nchan), np.float32)
+        self._w("channel_power")(_cfp(o.reshape(-1)), int(nel), int(nchan), m,
+                                 pwr.ctypes.data_as(_P(C.c_float)),
+                                 meanp.ctypes.data_as(_P(C.c_float)))
+        return pwr.reshape(int(nel), int(nchan)), meanp
+
+    # -- unpack ----------------------------------------------------------------
+    def bytes_per_sample(self, fmt) -> int:
+        return int(self._f("bytes_per_sample")(_fmt(fmt)))
+
+    def unpack(self, raw, fmt, dc_alpha=0.0, dc_state=None):
+        src = np.frombuffer(raw, np.uint8) if not isinstance(raw, np.ndarray) \
+            else np.ascontiguousarray(raw).view(np.uint8).reshape(-1)
+        bps = self.bytes_per_sample(fmt)
+        out = np.empty(src.size // bps, np.complex64)
+        st = _cfp(dc_state) if (dc_alpha > 0 and dc_state is not None) else None
+        got = self._f("unpack")(src.ctypes.data, src.size, _fmt(fmt), _cfp(out), out.size,
+                                float(dc_alpha), st)
+        if got < 0:
+            raise RuntimeError(f"unpack: {got}")
+        return out[:got]
+
+    def unpack_dc(self, raw, fmt, offset=0j, want_mean=True):
+        src = np.frombuffer(raw, np.uint8) if not isinstance(raw, np.ndarray) \
+            else np.ascontiguousarray(raw).view(np.uint8).reshape(-1)
+        bps = self.bytes_per_sample(fmt)
+        out = np.empty(src.size // bps, np.complex64)
+        mr, mi = C.c_double(0.0), C.c_double(0.0)
+        got = self._f("unpack_dc")(src.ctypes.data, src.size, _fmt(fmt), _cfp(out), out.size,
+                                   float(np.float32(offset.real)), float(np.float32(offset.imag)),
+                                   C.byref(mr) if want_mean else None,
+                                   C.byref(mi) if want_mean else None)
+        if got < 0:
+            raise RuntimeError(f"unpack_dc: {got}")
+        return out[:got], complex(mr.value, mi.value)
+
+
+class _CpuPfb:
+    def __init__(self, owner: CpuLib, fs, nchan, os_, K, atten, max_nel):
+        self._o = owner
+        self._p = owner._f("pfb_create")(float(fs), int(nchan), int(os_), int(K), float(atten),
+                                         int(max_nel))
+        if not self._p:
+            raise ValueError("pfb_create rejected its arguments")
+        self.nchan = int(nchan)
+        self.max_nel = int(max_nel)
+
+    def __del__(self):
+        p = getattr(self, "_p", None)
+        if p:
+            self._o._f("pfb_destroy")(p)
+            self._p = None
+
+    def reset(self):
+        self._o._f("pfb_reset")(self._p)
+
+    def out_hops(self, n):
+        return int(self._o._f("pfb_out_hops")(self._p, int(n)))
+
+    def set_cal(self, table, nel):
+        if table is None:
+            return self._o._f("pfb_set_cal")(self._p, None, 0)
+        t = np.ascontiguousarray(np.asarray(table, np.complex64)).reshape(int(nel), self.nchan)
+        return self._o._f("pfb_set_cal")(self._p, _cfp(t), int(nel))
+
+    def process_n(self, ins, nel):
+        nel = int(nel)
+        arrs = [np.ascontiguousarray(np.asarray(ins[e]).ravel(), np.complex64) for e in range(nel)]
+        n = arrs[0].size
+        m = self.out_hops(n)
+        out = np.zeros(max(nel * self.nchan * m, 1), np.complex64)
+        arr = (_pcf * nel)(*[_cfp(a) for a in arrs])
+        got = self._o._f("pfb_process_n")(self._p, arr, nel, n, _cfp(out), nel * self.nchan * m)
+        if got < 0:
+            raise RuntimeError(f"pfb_process_n: {got}")
+        return out[: nel * self.nchan * got].reshape(nel, self.nchan, got)
+
+    def process(self, x):
+        return self.process_n([x], 1)[0]
+
+
+_cache: dict = {}
+
+
+def oracle() -> CpuLib:
+    """The C restatement (always built by ``make -C oracle``)."""
+    if "orc" not in _cache:
+        _cache["orc"] = CpuLib(ORACLE_SO, "orc_")
+    return _cache["orc"]
+
+
+def reference() -> CpuLib | None:
+    """The reference library built from its own sources, or None if absent."""
+    if "ref" not in _cache:
+        _cache["ref"] = CpuLib(REF_SO, "atkdsp_") if REF_SO.exists() else None
+    return _cache["ref"]

@@ -1,0 +1,155 @@
+"""Unpack front end and W1/W2 accumulators on the GPU, against the reference
+(golden fixtures, bit-exact) and the reference's own tests
+(test_cross_check.py:88-116, 548-587; test_channelizer.py:127-169)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import atkdsp_b200 as ak
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FS = 2.4e6
+NCHAN = 192
+SP = FS / NCHAN
+
+
+def _bits(a):
+    return np.asarray(a).view(np.uint32)
+
+
+@pytest.mark.parametrize("fmt", ["cu8", "ci8", "ci16", "ci16q11", "cf32"])
+def test_unpack_bit_exact_against_golden(golden_unpack, fmt):
+    g = golden_unpack
+    raw = g[f"{fmt}/raw"].tobytes()
+    assert np.array_equal(_bits(ak.unpack(raw, fmt)), _bits(g[f"{fmt}/plain"]))
+    for j in range(3):
+        off = complex(*g[f"{fmt}/off{j}"].astype(np.float64))
+        y, mean = ak.unpack_dc(raw, fmt, off)
+        assert np.array_equal(_bits(y), _bits(g[f"{fmt}/dc{j}"])), (fmt, j)
+        ref_mean = complex(*g[f"{fmt}/mean{j}"])
+        assert abs(mean - ref_mean) <= 1e-12 * max(1.0, abs(ref_mean)), (fmt, j, mean, ref_mean)
+    st = np.zeros(1, np.complex64)
+    bps = ak.bytes_per_sample(fmt)
+    cuts = [0, 40 * bps, 40 * bps + bps, len(raw)]
+    ys = [ak.unpack(raw[a:b], fmt, 0.01, st) for a, b in zip(cuts[:-1], cuts[1:])]
+    assert np.array_equal(_bits(np.concatenate(ys)), _bits(g[f"{fmt}/pole"]))
+    assert np.array_equal(_bits(st), _bits(g[f"{fmt}/pole_state"]))
+
+
+def test_unpack_large_block_bit_exact_and_mean():
+    rng = np.random.default_rng(5)
+    raw = rng.integers(-2048, 2048, 2 * 2_000_000, dtype=np.int64).astype("<i2").tobytes()
+    orc = O.oracle()
+    for off in (0j, 0.0123 - 0.0456j):
+        y, mean = ak.unpack_dc(raw, "ci16q11", off)
+        r, rmean = orc.unpack_dc(raw, "ci16q11", off)
+        assert np.array_equal(_bits(y), _bits(r))
+        assert abs(mean - rmean) < 1e-12
+
+
+def test_unpack_dc_zero_offset_is_unpack_and_torn_tail():
+    raw = np.random.default_rng(3).integers(0, 256, 4097, dtype=np.uint8).tobytes()
+    for f in ("cu8", "ci16q11", "cf32"):
+        a, _ = ak.unpack_dc(raw, f, 0j)
+        b = ak.unpack(raw, f)
+        assert np.array_equal(_bits(a), _bits(b))
+        assert a.size == len(raw) // ak.bytes_per_sample(f)
+
+
+def test_unpack_dc_mean_is_before_subtraction():
+    n = 4096
+    off = 0.25 - 0.1j
+    rng = np.random.default_rng(11)
+    x = (np.full(n, 0.4 + 0.2j) + 0.01 * (rng.standard_normal(n) + 1j * rng.standard_normal(n))).astype(np.complex64)
+    y, mean = ak.unpack_dc(x.tobytes(), "cf32", off)
+    assert abs(mean - complex(np.mean(x, dtype=np.complex128))) < 1e-5
+    assert abs(complex(np.mean(y, dtype=np.complex128)) - (mean - off)) < 1e-5
+
+
+def test_unpack_empty_and_bad_format():
+    y, mean = ak.unpack_dc(b"", "ci16", 0.5 + 0.25j)
+    assert y.size == 0 and mean == 0.5 + 0.25j
+    with pytest.raises(ak.AtkDspError):
+        ak.unpack(b"\x00" * 8, 99)
+
+
+def test_dc_pole_is_continuous_across_blocks():
+    raw = (np.random.default_rng(4).integers(-2048, 2048, 20000, dtype=np.int64) + 300).astype("<i2").tobytes()
+    orc = O.oracle()
+    sa = np.zeros(1, np.complex64)
+    sb = np.zeros(1, np.complex64)
+    outs_a, outs_b = [], []
+    for chunk in (raw[:4000], raw[4000:4004], raw[4004:]):
+        outs_a.append(ak.unpack(chunk, "ci16q11", 0.01, sa))
+        outs_b.append(orc.unpack(chunk, "ci16q11", 0.01, sb))
+    a, b = np.concatenate(outs_a), np.concatenate(outs_b)
+    assert np.array_equal(_bits(a), _bits(b))
+    assert abs(a[-500:].mean()) < 0.01
+
+
+# ---- W1 / W2 ------------------------------------------------------------------
+def test_w1_w2_against_golden(golden_w12):
+    g = golden_w12
+    y = g["y"]
+    nel, M = y.shape[0], y.shape[1]
+    R, c = g["R0"].copy(), g["c0"].copy()
+    ak.pfb_cov_accumulate(y, nel, M, None, R, c)
+    scale = np.max(np.abs(g["R"]))
+    assert np.max(np.abs(R - g["R"])) / scale < 1e-5
+    assert np.array_equal(c, g["counts"])
+    Rg, cg = g["R0"].copy(), g["c0"].copy()
+    ak.pfb_cov_accumulate(y, nel, M, g["gate"], Rg, cg)
+    assert np.max(np.abs(Rg - g["Rg"])) / scale < 1e-5
+    assert np.array_equal(cg, g["cg"])
+    ungated = g["gate"] == 0
+    assert np.array_equal(_bits(Rg[ungated]), _bits(g["R0"][ungated]))
+    ak.pfb_cov_reset(Rg, cg, nel, M, g["gate"])
+    assert np.array_equal(_bits(Rg), _bits(g["Rr"]))
+    assert np.array_equal(cg, g["cr"])
+    pwr, meanp = ak.pfb_channel_power(y, nel, M)
+    assert np.array_equal(_bits(pwr), _bits(g["pwr"]))
+    assert np.array_equal(_bits(meanp), _bits(g["meanp"]))
+
+
+def test_w1_hermitian_and_matches_twin():
+    phi = np.deg2rad(37.0)
+    rng = np.random.default_rng(6)
+    base = (np.exp(2j * np.pi * 40 * SP / FS * np.arange(NCHAN * 80))
+            + 0.05 * (rng.standard_normal(NCHAN * 80) + 1j * rng.standard_normal(NCHAN * 80)))
+    ins = [(base * np.exp(1j * e * phi)).astype(np.complex64) for e in range(5)]
+    oc = ak.Pfb(FS, NCHAN, max_nel=5).process_n(ins, 5)
+    R = np.zeros((NCHAN, 5, 5), np.complex64)
+    cc = np.zeros(NCHAN, np.uint32)
+    ak.pfb_cov_accumulate(oc, 5, NCHAN, None, R, cc)
+    y = oc[:, 40, :].astype(np.complex128)
+    Rt = y @ y.conj().T
+    assert np.max(np.abs(R[40] - Rt)) / np.max(np.abs(Rt)) < 1e-6
+    assert np.array_equal(R[40], R[40].conj().T)
+    assert cc[40] == oc.shape[2]
+
+
+def test_w12_many_elements_and_empty_block():
+    rng = np.random.default_rng(12)
+    nel, M, m = 32, 16, 300
+    y = (rng.standard_normal((nel, M, m)) + 1j * rng.standard_normal((nel, M, m))).astype(np.complex64)
+    R = np.zeros((M, nel, nel), np.complex64)
+    c = np.zeros(M, np.uint32)
+    ak.pfb_cov_accumulate(y, nel, M, None, R, c)
+    for k in (0, 7, 15):
+        yk = y[:, k, :].astype(np.complex128)
+        Rt = yk @ yk.conj().T
+        assert np.max(np.abs(R[k] - Rt)) / np.max(np.abs(Rt)) < 1e-6
+    pwr, meanp = ak.pfb_channel_power(y, nel, M)
+    pt = (np.abs(y.astype(np.complex128)) ** 2).mean(axis=2)
+    assert np.max(np.abs(pwr - pt) / pt) < 1e-6
+    assert np.allclose(meanp, pt.mean(0), rtol=1e-6)
+    empty = np.zeros((nel, M, 0), np.complex64)
+    R0 = R.copy()
+    ak.pfb_cov_accumulate(empty, nel, M, None, R, c)
+    assert np.array_equal(_bits(R), _bits(R0))
+    p0, m0 = ak.pfb_channel_power(empty, nel, M)
+    assert not p0.any() and not m0.any()
