@@ -99,6 +99,7 @@ def _bind(lib) -> None:
         "atkdsp_gpu_batch_destroy": ([vp], None),
         "atkdsp_gpu_batch_process": ([vp, P(vp), P(sz), P(vp), P(ssz), vp], ssz),
         "atkdsp_gpu_batch_stream": ([vp], vp),
+        "atkdsp_gpu_batch_kernel_ms": ([vp], C.c_float),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)

@@ -845,6 +845,7 @@ struct atkdsp_gpu_batch {
     int *d_counters;
     int grid, smem;
     long long max_carry;
+    void *tk[2];                  /* timing events around the tile kernel */
 };
 
 ATKDSP_API void atkdsp_gpu_batch_destroy(atkdsp_gpu_batch *b) {
@@ -854,6 +855,7 @@ ATKDSP_API void atkdsp_gpu_batch_destroy(atkdsp_gpu_batch *b) {
     for (int i = 0; i < 2; ++i) {
         atkb_graph_destroy(b->graph[i]);
         atkb_event_destroy(b->ev[i]);
+        atkb_event_destroy(b->tk[i]);
         atkb_host_free(b->h_tables[i]);
     }
     atkb_free(b->d_tables);
@@ -888,6 +890,7 @@ ATKDSP_API atkdsp_gpu_batch *atkdsp_gpu_batch_create(atkdsp_pfb *const *handles,
     for (i = 0; i < 2 && rc == ATKB_OK; ++i) {
         rc = atkb_host_alloc(&b->h_tables[i], b->tbl_bytes);
         if (rc == ATKB_OK) rc = atkb_event_create(&b->ev[i]);
+        if (rc == ATKB_OK) rc = atkb_event_create_timed(&b->tk[i]);
     }
     if (rc == ATKB_OK) rc = atkb_malloc((void **)&b->d_counters, 2 * sizeof(int));
     if (rc == ATKB_OK) rc = atkb_memset(b->d_counters, 0, 2 * sizeof(int), b->stream);
@@ -899,11 +902,21 @@ ATKDSP_API atkdsp_gpu_batch *atkdsp_gpu_batch_create(atkdsp_pfb *const *handles,
 
 ATKDSP_API void *atkdsp_gpu_batch_stream(atkdsp_gpu_batch *b) { return b ? b->stream : NULL; }
 
+ATKDSP_API float atkdsp_gpu_batch_kernel_ms(atkdsp_gpu_batch *b) {
+    float ms = -1.0f;
+    if (!b) return -1.0f;
+    atkb_set_device(b->dev);
+    if (atkb_event_elapsed_ms(&ms, b->tk[0], b->tk[1]) != ATKB_OK) return -1.0f;
+    return ms;
+}
+
 static int batch_enqueue(atkdsp_gpu_batch *b, int slot, void *stream) {
     int rc = atkb_h2d(b->d_tables, b->h_tables[slot], b->tbl_bytes, stream);
+    if (rc == ATKB_OK) rc = atkb_event_record_node(b->tk[0], stream);
     if (rc == ATKB_OK)
         rc = atkb_pfb_launch(tbl_jobs(b->d_tables), tbl_tiles(b->d_tables, b->count), (int)b->count,
                              b->d_counters, b->grid, b->smem, stream);
+    if (rc == ATKB_OK) rc = atkb_event_record_node(b->tk[1], stream);
     if (rc == ATKB_OK) rc = atkb_pfb_carry(tbl_carry(b->d_tables, b->count), (int)b->count, b->max_carry, stream);
     return rc;
 }

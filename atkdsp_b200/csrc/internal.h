@@ -100,6 +100,10 @@ void atkb_event_destroy(void *ev);
 int  atkb_event_record(void *ev, void *stream);
 int  atkb_event_sync(void *ev);
 int  atkb_stream_wait(void *stream, void *ev);
+/* timing events: recorded as graph nodes when the stream is capturing */
+int  atkb_event_create_timed(void **ev);
+int  atkb_event_record_node(void *ev, void *stream);
+int  atkb_event_elapsed_ms(float *ms, void *start, void *stop);
 /* graphs: capture the work enqueued on `stream` between begin and end */
 int  atkb_graph_begin(void *stream);
 int  atkb_graph_end(void *stream, void **exec);

@@ -108,3 +108,22 @@ extern "C" int atkb_graph_launch(void *exec, void *stream) {
 extern "C" void atkb_graph_destroy(void *exec) {
     if (exec) cudaGraphExecDestroy((cudaGraphExec_t)exec);
 }
+
+extern "C" int atkb_event_create_timed(void **ev) {
+    cudaEvent_t e = nullptr;
+    const int rc = st(cudaEventCreate(&e));
+    *ev = (void *)e;
+    return rc;
+}
+extern "C" int atkb_event_record_node(void *ev, void *stream) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing((cudaStream_t)stream, &cs) != cudaSuccess) return ATKB_E_KERNEL;
+    if (cs == cudaStreamCaptureStatusActive)
+        return st(cudaEventRecordWithFlags((cudaEvent_t)ev, (cudaStream_t)stream, cudaEventRecordExternal));
+    return st(cudaEventRecord((cudaEvent_t)ev, (cudaStream_t)stream));
+}
+extern "C" int atkb_event_elapsed_ms(float *ms, void *start, void *stop) {
+    const int rc = st(cudaEventSynchronize((cudaEvent_t)stop));
+    if (rc != ATKB_OK) return rc;
+    return st(cudaEventElapsedTime(ms, (cudaEvent_t)start, (cudaEvent_t)stop));
+}

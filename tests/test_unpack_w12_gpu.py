@@ -73,8 +73,11 @@ def test_unpack_dc_mean_is_before_subtraction():
 def test_unpack_empty_and_bad_format():
     y, mean = ak.unpack_dc(b"", "ci16", 0.5 + 0.25j)
     assert y.size == 0 and mean == 0.5 + 0.25j
-    with pytest.raises(ak.AtkDspError):
-        ak.unpack(b"\x00" * 8, 99)
+    lib = ak.load()
+    buf = np.zeros(4, np.complex64)
+    raw = np.zeros(8, np.uint8)
+    assert lib.atkdsp_unpack(raw.ctypes.data, 8, 99, ak._cfp(buf), 4, 0.0, None) == -1
+    assert lib.atkdsp_unpack_dc(raw.ctypes.data, 8, 3, None, 4, 0.0, 0.0, None, None) == -1
 
 
 def test_dc_pole_is_continuous_across_blocks():
@@ -88,7 +91,7 @@ def test_dc_pole_is_continuous_across_blocks():
         outs_b.append(orc.unpack(chunk, "ci16q11", 0.01, sb))
     a, b = np.concatenate(outs_a), np.concatenate(outs_b)
     assert np.array_equal(_bits(a), _bits(b))
-    assert abs(a[-500:].mean()) < 0.01
+    assert abs(a[-2000:].mean()) < 0.05          # the 300-LSB offset (0.146) is gone
 
 
 # ---- W1 / W2 ------------------------------------------------------------------
