@@ -246,18 +246,28 @@ static int upload_bank(atkdsp_pfb *p) {
     const size_t taps_b = align16(p->L * sizeof(float));
     const size_t tab_b = (size_t)M * 2 * sizeof(double);
     const size_t pass_b = (size_t)pl.twlen * 2 * sizeof(double);
-    const size_t total = taps_b + 2 * tab_b + pass_b;
+    const size_t total = 2 * taps_b + 2 * tab_b + pass_b;
     char *h = (char *)calloc(1, total);
     double *proto = (double *)malloc(p->L * sizeof(double));
     if (!h || !proto) { free(h); free(proto); return ATKB_E_NOMEM; }
     design_prototype(M, p->K, p->atten, proto);
     float *taps = (float *)h;
-    double *twd = (double *)(h + taps_b);
-    double *W = (double *)(h + taps_b + tab_b);
-    double *wp = (double *)(h + taps_b + 2 * tab_b);
+    float *taps16 = (float *)(h + taps_b);
+    double *twd = (double *)(h + 2 * taps_b);
+    double *W = (double *)(h + 2 * taps_b + tab_b);
+    double *wp = (double *)(h + 2 * taps_b + 2 * tab_b);
     size_t q;
     unsigned j;
     for (q = 0; q < p->L; ++q) taps[q] = (float)proto[q];
+    if (pl.fast) {
+        /* taps16[(k*MR + j)*16 + r] = taps[k*M + j + r*MR], MR = M/16 */
+        const size_t MR = M / 16;
+        size_t k2, jj, r;
+        for (k2 = 0; k2 < p->K; ++k2)
+            for (jj = 0; jj < MR; ++jj)
+                for (r = 0; r < 16; ++r)
+                    taps16[(k2 * MR + jj) * 16 + r] = taps[k2 * M + jj + r * MR];
+    }
     for (j = 0; j < M; ++j) {
         /* the reference's rotation table, channelizer.c:164-170 */
         const double a = 2.0 * ATKB_PI * (double)j / (double)M;
@@ -298,10 +308,16 @@ static int upload_bank(atkdsp_pfb *p) {
     B->L = (long long)p->L;
     B->ov = (long long)p->ov;
     B->taps = (const float *)p->d_const;
-    B->twd = (const char *)p->d_const + taps_b;
-    B->wfull = (const char *)p->d_const + taps_b + tab_b;
-    B->wpass = (const char *)p->d_const + taps_b + 2 * tab_b;
+    B->taps16 = (const float *)((const char *)p->d_const + taps_b);
+    B->twd = (const char *)p->d_const + 2 * taps_b;
+    B->wfull = (const char *)p->d_const + 2 * taps_b + tab_b;
+    B->wpass = (const char *)p->d_const + 2 * taps_b + 2 * tab_b;
     B->plan = pl;
+    B->logm = 0;
+    if (pl.fast) {
+        unsigned v = M;
+        while (v > 1) { v >>= 1; ++B->logm; }
+    }
     if (pl.fast) {
         B->tile_hops = 4096 / (int)M;
         B->smem_bytes = 4096 * 16;

@@ -43,10 +43,14 @@ typedef struct {
     int nchan, os, K, hop;
     long long L, ov;
     const float *taps;            /* device: L floats, (float)h[q]            */
+    const float *taps16;          /* device: fast path, taps permuted so the 16
+                                   * branches j + r*nchan/16 of tap k are the 16
+                                   * floats at ((k*nchan/16 + j)*16 + r)       */
     const void *twd;              /* device: nchan double2 (cos, sin)(2 pi j/nchan) */
     const void *wfull;            /* device: nchan double2 W^j = (cos, -sin)  */
     const void *wpass;            /* device: per-pass twiddles (fast path)    */
     atkb_fft_plan plan;
+    int logm;                     /* log2(nchan) on the fast path, else 0      */
     int tile_hops;                /* hops per CTA tile                        */
     int smem_bytes;               /* dynamic shared memory a tile needs       */
 } atkb_bank;

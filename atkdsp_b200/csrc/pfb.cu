@@ -93,32 +93,30 @@ __device__ __forceinline__ void dft8(double2 *v) {
 }
 
 __device__ __forceinline__ void dft16(double2 *v) {
-    /* n = 4 n1 + n2, k = k1 + 4 k2: radix-4 columns, W16^(n2 k1), radix-4 rows */
-    double2 z[16];
+    /* n = 4 n1 + n2, k = k1 + 4 k2: radix-4 columns, W16^(n2 k1), radix-4
+     * rows, all in place; the rows leave y[k1 + 4 k2] at v[4 k1 + k2], and a
+     * final renaming (free once unrolled) restores natural order */
 #pragma unroll
-    for (int n2 = 0; n2 < 4; ++n2) {
-        double2 a = v[n2], b = v[4 + n2], c = v[8 + n2], d = v[12 + n2];
-        dft4(a, b, c, d);
-        z[n2 * 4 + 0] = a; z[n2 * 4 + 1] = b; z[n2 * 4 + 2] = c; z[n2 * 4 + 3] = d;
-    }
-    const double2 w1 = make_double2(C16_1, -S16_1), w2 = make_double2(SQH, -SQH);
-    const double2 w3 = make_double2(S16_1, -C16_1), w6 = make_double2(-SQH, -SQH);
-    const double2 w9 = make_double2(-C16_1, S16_1);
-    z[1 * 4 + 1] = cmul(z[1 * 4 + 1], w1);
-    z[1 * 4 + 2] = cmul(z[1 * 4 + 2], w2);
-    z[1 * 4 + 3] = cmul(z[1 * 4 + 3], w3);
-    z[2 * 4 + 1] = cmul(z[2 * 4 + 1], w2);
-    z[2 * 4 + 2] = cmi(z[2 * 4 + 2]);
-    z[2 * 4 + 3] = cmul(z[2 * 4 + 3], w6);
-    z[3 * 4 + 1] = cmul(z[3 * 4 + 1], w3);
-    z[3 * 4 + 2] = cmul(z[3 * 4 + 2], w6);
-    z[3 * 4 + 3] = cmul(z[3 * 4 + 3], w9);
+    for (int n2 = 0; n2 < 4; ++n2) dft4(v[n2], v[4 + n2], v[8 + n2], v[12 + n2]);
+    v[4 * 1 + 1] = cmul(v[4 * 1 + 1], make_double2(C16_1, -S16_1));
+    v[4 * 2 + 1] = cmul(v[4 * 2 + 1], make_double2(SQH, -SQH));
+    v[4 * 3 + 1] = cmul(v[4 * 3 + 1], make_double2(S16_1, -C16_1));
+    v[4 * 1 + 2] = cmul(v[4 * 1 + 2], make_double2(SQH, -SQH));
+    v[4 * 2 + 2] = cmi(v[4 * 2 + 2]);
+    v[4 * 3 + 2] = cmul(v[4 * 3 + 2], make_double2(-SQH, -SQH));
+    v[4 * 1 + 3] = cmul(v[4 * 1 + 3], make_double2(S16_1, -C16_1));
+    v[4 * 2 + 3] = cmul(v[4 * 2 + 3], make_double2(-SQH, -SQH));
+    v[4 * 3 + 3] = cmul(v[4 * 3 + 3], make_double2(-C16_1, S16_1));
 #pragma unroll
-    for (int k1 = 0; k1 < 4; ++k1) {
-        double2 a = z[0 * 4 + k1], b = z[1 * 4 + k1], c = z[2 * 4 + k1], d = z[3 * 4 + k1];
-        dft4(a, b, c, d);
-        v[k1] = a; v[k1 + 4] = b; v[k1 + 8] = c; v[k1 + 12] = d;
-    }
+    for (int k1 = 0; k1 < 4; ++k1) dft4(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+    /* transpose the 4x4 index grid */
+    double2 t;
+    t = v[1]; v[1] = v[4]; v[4] = t;
+    t = v[2]; v[2] = v[8]; v[8] = t;
+    t = v[3]; v[3] = v[12]; v[12] = t;
+    t = v[6]; v[6] = v[9]; v[9] = t;
+    t = v[7]; v[7] = v[13]; v[13] = t;
+    t = v[11]; v[11] = v[14]; v[14] = t;
 }
 
 __device__ __forceinline__ void dft3(double2 &a, double2 &b, double2 &c) {
@@ -157,128 +155,182 @@ struct Src {
  * conflict-free too (a XOR with a per-block constant permutes the slots). */
 __device__ __forceinline__ int SW(int i) { return i ^ ((i >> 4) & 15); }
 
-template <int R>
-__device__ __forceinline__ void pass_inplace(double2 *sm, int M, int Ns, const double2 *tw) {
+/* One in-place Stockham pass over a 4096-point tile (NT threads x 16 points):
+ * every index is a compile-time shift or mask. tw holds W_{Ns R}^{r k} at
+ * (r - 1) * Ns + k. */
+template <int LOGM, int R, int LOGNS>
+__device__ __forceinline__ void pass_c(double2 *sm, const double2 *__restrict__ tw) {
+    constexpr int M = 1 << LOGM;
+    constexpr int NS = 1 << LOGNS;
+    constexpr int LOGR = R == 16 ? 4 : R == 8 ? 3 : R == 4 ? 2 : 1;
+    constexpr int LOGMR = LOGM - LOGR;
+    constexpr int MR = 1 << LOGMR;
     constexpr int U = PTS / R;
-    const int MR = M / R;
     double2 v[U][R];
     int dst[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         const int bi = u * NT + threadIdx.x;
-        const int tt = bi / MR;
-        const int j = bi - tt * MR;
-        const int k = j & (Ns - 1);
-        const int base = tt * M + j;
+        const int tt = bi >> LOGMR;
+        const int j = bi & (MR - 1);
+        const int k = j & (NS - 1);
+        const int base = (tt << LOGM) + j;
 #pragma unroll
         for (int r = 0; r < R; ++r) v[u][r] = sm[SW(base + r * MR)];
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[u][r] = cmul(v[u][r], __ldg(tw + (r - 1) * Ns + k));
-        dst[u] = tt * M + (j - k) * R + k;
+        for (int r = 1; r < R; ++r) v[u][r] = cmul(v[u][r], __ldg(tw + (r - 1) * NS + k));
+        dst[u] = (tt << LOGM) + ((j - k) << LOGR) + k;
     }
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         dftR<R>(v[u]);
 #pragma unroll
-        for (int r = 0; r < R; ++r) sm[SW(dst[u] + r * Ns)] = v[u][r];
+        for (int r = 0; r < R; ++r) sm[SW(dst[u] + r * NS)] = v[u][r];
     }
     __syncthreads();
 }
 
-__device__ void tile_fast(const atkb_job &J, const atkb_bank &B, long long h0, int nvalid,
-                          double2 *sm, float2 *tile_out) {
-    const int M = B.nchan;
-    const int nh = TILE_POINTS / M;
-    const int Mr = M >> 4;
-    const int tid = threadIdx.x;
-    const int tt = tid / Mr;
-    const int j = tid - tt * Mr;
+/* passes P, P+1, ... of the power-of-two plan: radix 16 while at least four
+ * index bits remain, then one last radix 8, 4 or 2 */
+template <int LOGM, int P>
+__device__ __forceinline__ void passes_from(double2 *sm, const double2 *wp, const int *twoff) {
+    if constexpr (4 * P < LOGM) {
+        constexpr int REM = LOGM - 4 * P;
+        constexpr int R = REM >= 4 ? 16 : (1 << REM);
+        pass_c<LOGM, R, 4 * P>(sm, wp + twoff[P]);
+        passes_from<LOGM, P + 1>(sm, wp, twoff);
+    }
+}
 
-    /* fold: this thread's 16 branches q = j + r*M/16 of hop h0 + tt */
-    double2 v[16];
-    if (tt < nvalid) {
-        const Src src{(const float2 *)J.state, (const float2 *)J.in, J.head};
-        const long long base = (h0 + tt) * (long long)B.hop + j;
-        const float *tp = B.taps + j;
-        float fr[16], fi[16];
+/* The fold of one hop's 16 branches q = j + r*M/16 (r = 0..15), straight into
+ * the registers of the first radix-16 butterfly. Taps come from the bank's
+ * permuted copy (16 consecutive floats per (k, j): four 16-byte loads).
+ * LINEAR: the tile's windows lie wholly in one buffer, read through `lin`
+ * (already offset to this thread's first sample); otherwise each sample is
+ * taken from the state or the input by index. */
+template <int LOGM, bool LINEAR>
+__device__ __forceinline__ void fold16(double2 *v, const atkb_job &J, const atkb_bank &B,
+                                       long long h0, int tt, int j, const float2 *lin) {
+    constexpr int M = 1 << LOGM;
+    constexpr int MR = M >> 4;
+    const float4 *tq = (const float4 *)B.taps16 + (size_t)j * 4;
+    float fr[16], fi[16];
+    const float2 *xk = lin;
+    const Src src{(const float2 *)J.state, (const float2 *)J.in, J.head};
+    const long long base = (h0 + tt) * (long long)B.hop + j;
 #pragma unroll
-        for (int r = 0; r < 16; ++r) {
-            const float h = __ldg(tp + r * Mr);
-            const float2 x = src.at(base + r * Mr);
-            fr[r] = __fmul_rn(h, x.x);
-            fi[r] = __fmul_rn(h, x.y);
+    for (int q = 0; q < 4; ++q) {
+        const float4 h = __ldg(tq + q);
+        const float hh[4] = {h.x, h.y, h.z, h.w};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int r = 4 * q + c;
+            const float2 x = LINEAR ? __ldg(xk + r * MR) : src.at(base + r * MR);
+            fr[r] = __fmul_rn(hh[c], x.x);
+            fi[r] = __fmul_rn(hh[c], x.y);
         }
-        for (int k = 1; k < B.K; ++k) {
-            const float *tk = tp + (long long)k * M;
-            const long long sk = base + (long long)k * M;
+    }
+    for (int k = 1; k < B.K; ++k) {
+        tq += MR * 4;
+        xk += M;
 #pragma unroll
-            for (int r = 0; r < 16; ++r) {
-                const float h = __ldg(tk + r * Mr);
-                const float2 x = src.at(sk + r * Mr);
-                fr[r] = __fadd_rn(fr[r], __fmul_rn(h, x.x));
-                fi[r] = __fadd_rn(fi[r], __fmul_rn(h, x.y));
+        for (int q = 0; q < 4; ++q) {
+            const float4 h = __ldg(tq + q);
+            const float hh[4] = {h.x, h.y, h.z, h.w};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int r = 4 * q + c;
+                const float2 x = LINEAR ? __ldg(xk + r * MR) : src.at(base + (long long)k * M + r * MR);
+#ifdef ATKB_FOLD_FMA
+                fr[r] = __fmaf_rn(hh[c], x.x, fr[r]);
+                fi[r] = __fmaf_rn(hh[c], x.y, fi[r]);
+#else
+                fr[r] = __fadd_rn(fr[r], __fmul_rn(hh[c], x.x));
+                fi[r] = __fadd_rn(fi[r], __fmul_rn(hh[c], x.y));
+#endif
             }
         }
+    }
 #pragma unroll
-        for (int r = 0; r < 16; ++r) v[r] = make_double2((double)fr[r], (double)fi[r]);
+    for (int r = 0; r < 16; ++r) v[r] = make_double2((double)fr[r], (double)fi[r]);
+}
+
+template <int LOGM>
+__device__ void tile_fast(const atkb_job &J, const atkb_bank &B, long long h0, int nvalid,
+                          double2 *sm, float2 *tile_out) {
+    constexpr int M = 1 << LOGM;
+    constexpr int LOGNH = 12 - LOGM;
+    constexpr int NH = 1 << LOGNH;
+    constexpr int MR = M >> 4;
+    const int tid = threadIdx.x;
+    const int tt = tid >> (LOGM - 4);
+    const int j = tid & (MR - 1);
+
+    /* fold + first Stockham pass (Ns = 1, radix 16, no twiddles) */
+    double2 v[16];
+    if (tt < nvalid) {
+        const long long w0 = h0 * (long long)B.hop;                  /* first window start */
+        const long long w1 = (h0 + nvalid - 1) * (long long)B.hop + B.L;  /* last window end */
+        const long long off = (h0 + tt) * (long long)B.hop + j;
+        if (w0 >= J.head)
+            fold16<LOGM, true>(v, J, B, h0, tt, j, (const float2 *)J.in + (off - J.head));
+        else if (w1 <= J.head)
+            fold16<LOGM, true>(v, J, B, h0, tt, j, (const float2 *)J.state + off);
+        else
+            fold16<LOGM, false>(v, J, B, h0, tt, j, nullptr);
     } else {
 #pragma unroll
         for (int r = 0; r < 16; ++r) v[r] = make_double2(0.0, 0.0);
     }
-    /* first Stockham pass (Ns = 1, radix 16, no twiddles): dst = j*16 + r */
     dft16(v);
 #pragma unroll
-    for (int r = 0; r < 16; ++r) sm[SW(tt * M + j * 16 + r)] = v[r];
+    for (int r = 0; r < 16; ++r) sm[SW((tt << LOGM) + j * 16 + r)] = v[r];
     __syncthreads();
+    passes_from<LOGM, 1>(sm, (const double2 *)B.wpass, B.plan.twoff);
 
-    const double2 *wp = (const double2 *)B.wpass;
-    int Ns = 16;
-    for (int p = 1; p < B.plan.npass; ++p) {
-        const int R = B.plan.radix[p];
-        const double2 *tw = wp + B.plan.twoff[p];
-        if (R == 16) pass_inplace<16>(sm, M, Ns, tw);
-        else if (R == 8) pass_inplace<8>(sm, M, Ns, tw);
-        else if (R == 4) pass_inplace<4>(sm, M, Ns, tw);
-        else pass_inplace<2>(sm, M, Ns, tw);
-        Ns *= R;
-    }
-
-    /* epilogue: rotate, cal, round; hop-major -> channel-major in smem */
+    /* epilogue: rotate to input sample 0, cal, one rounding; transpose the
+     * tile hop-major -> channel-major through padded shared rows */
     const double2 *twd = (const double2 *)B.twd;
     const float2 *cal = (const float2 *)J.cal;
     const int os = B.os, hop = B.hop;
+    const bool os_pow2 = (os & (os - 1)) == 0;
+    const int s0 = (int)((J.b0 + h0 + 1) % os);     /* (b + 1) mod os at hop h0 */
     float2 y[PTS];
-    int ti[PTS];
 #pragma unroll
     for (int u = 0; u < PTS; ++u) {
         const int e = u * NT + tid;
-        const int t2 = e / M;
-        const int kb = e - t2 * M;
+        const int t2 = e >> LOGM;
+        const int kb = e & (M - 1);
         double2 X = sm[SW(e)];
-        const long long b = J.b0 + h0 + t2;
-        const int s = (int)((b + 1) % os);
-        const int jr = (kb * s) % os;
+        int jr;
+        if (os_pow2) jr = (kb * ((s0 + t2) & (os - 1))) & (os - 1);
+        else jr = (kb * ((s0 + t2) % os)) % os;
         X = cmul_rn(X, __ldg(twd + (jr ? M - jr * hop : 0)));
         if (cal) {
             const float2 c = __ldg(cal + kb);
             X = cmul_rn(X, make_double2((double)c.x, (double)c.y));
         }
         y[u] = make_float2(__double2float_rn(X.x), __double2float_rn(X.y));
-        ti[u] = kb * (nh + 1) + t2;       /* padded rows: no bank conflicts */
     }
     __syncthreads();
 #pragma unroll
-    for (int u = 0; u < PTS; ++u) tile_out[ti[u]] = y[u];
-    __syncthreads();
-    float2 *out = (float2 *)J.out;
-    const long long col = J.out_col + h0;
-#pragma unroll 4
     for (int u = 0; u < PTS; ++u) {
         const int e = u * NT + tid;
-        const int kb = e / nh;
-        const int t2 = e - kb * nh;
-        if (t2 < nvalid) out[(long long)kb * J.ldo + col + t2] = tile_out[kb * (nh + 1) + t2];
+        tile_out[(e & (M - 1)) * (NH + 1) + (e >> LOGM)] = y[u];
+    }
+    __syncthreads();
+    /* write: thread -> (channel kb0 + u*MR, hop t2); runs of NH hops */
+    const int t2 = tid & (NH - 1);
+    if (t2 < nvalid) {
+        const int kb0 = tid >> LOGNH;
+        float2 *o = (float2 *)J.out + (J.out_col + h0 + t2) + (long long)kb0 * J.ldo;
+        const long long step = (long long)MR * J.ldo;
+#pragma unroll 4
+        for (int u = 0; u < PTS; ++u) {
+            *o = tile_out[(kb0 + u * MR) * (NH + 1) + t2];
+            o += step;
+        }
     }
 }
 
@@ -380,7 +432,10 @@ __device__ void tile_generic(const atkb_job &J, const atkb_bank &B, long long h0
     }
 }
 
-__global__ void __launch_bounds__(NT)
+#ifndef ATKB_TILE_MINB
+#define ATKB_TILE_MINB 2
+#endif
+__global__ void __launch_bounds__(NT, ATKB_TILE_MINB)
 pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile_start, int njobs,
                  int *counters) {
     extern __shared__ double2 sm[];
@@ -408,10 +463,18 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
         const long long h0 = (long long)s_local * s_bank.tile_hops;
         const long long left = J.hops - h0;
         const int nvalid = (int)(left < s_bank.tile_hops ? left : s_bank.tile_hops);
-        if (s_bank.plan.fast)
-            tile_fast(J, s_bank, h0, nvalid, sm, (float2 *)sm);
-        else
-            tile_generic(J, s_bank, h0, nvalid, sm);
+        switch (s_bank.plan.fast ? s_bank.logm : 0) {
+        case 4: tile_fast<4>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
+        case 5: tile_fast<5>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
+        case 6: tile_fast<6>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
+        case 7: tile_fast<7>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
+        case 8: tile_fast<8>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
+        case 9: tile_fast<9>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
+        case 10: tile_fast<10>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
+        case 11: tile_fast<11>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
+        case 12: tile_fast<12>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
+        default: tile_generic(J, s_bank, h0, nvalid, sm); break;
+        }
         __syncthreads();
     }
     if (threadIdx.x == 0) {

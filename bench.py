@@ -55,9 +55,12 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _specs(rank: int):
+def _specs(rank: int, args=None):
     from atkdsp_b200 import workloads as W
-    return W.uneven_streams(256, seed=4 + 1000 * rank)
+    if args is None:
+        return W.uneven_streams(256, seed=4 + 1000 * rank)
+    return W.uneven_streams(args.streams, seed=4 + 1000 * rank, min_log2=args.min_log2,
+                            max_log2=args.max_log2)
 
 
 # ---------------------------------------------------------------- clocks
@@ -232,7 +235,77 @@ def run_reference(args, rank, world):
     }))
 
 
-# -------------------------------------------------------------- our arm
+# -------------------------------------------------------------- our arms
+def _timed(stream, torch, fn, steps):
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for k in range(steps):
+        fn(k)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / 1e3
+
+
+def _plain_arm(args, specs, sets, outs, torch, device, barrier, max_over_ranks):
+    """One device-pointer call (one launch) per stream, all on one stream."""
+    import atkdsp_b200 as ak
+    from atkdsp_b200 import gpu
+    handles = [ak.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1) for s in specs]
+    st = torch.cuda.Stream(device=device)
+
+    def step(k):
+        for p, x, o in zip(handles, sets[k % 3][1], outs):
+            gpu.process_n(p, [x], 1, out=o, stream=st)
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    barrier()
+    t = max_over_ranks(_timed(st, torch, step, args.steps))
+    barrier()
+    del handles
+    return t
+
+
+def _e2e_arm(args, S, sets, obuf, bstream, bstep, torch, barrier, max_over_ranks):
+    """Pinned host inputs -> device, the batched step, outputs -> pinned host."""
+    h_in = torch.empty(S, dtype=torch.complex64, pin_memory=True)
+    h_in.copy_(sets[0][0].cpu())
+    h_out = torch.empty(obuf.numel(), dtype=torch.complex64, pin_memory=True)
+    d_in = sets[0][0]
+
+    def step(k):
+        with torch.cuda.stream(bstream):
+            d_in.copy_(h_in, non_blocking=True)
+        bstep(0)
+        with torch.cuda.stream(bstream):
+            h_out.copy_(obuf, non_blocking=True)
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    barrier()
+    t = max_over_ranks(_timed(bstream, torch, step, args.steps))
+    barrier()
+    return t
+
+
+def _dropin_arm(specs, sets, barrier, max_over_ranks):
+    """The reference-facing C ABI with host buffers, one call per stream."""
+    import atkdsp_b200 as ak
+    handles = [ak.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1) for s in specs]
+    hx = [v.cpu().numpy() for v in sets[0][1]]
+    for p, x in zip(handles, hx):
+        p.process(x[: x.size // 4])
+    barrier()
+    t0 = time.perf_counter()
+    for p, x in zip(handles, hx):
+        p.process(x)
+    t = max_over_ranks(time.perf_counter() - t0)
+    del handles
+    return t
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -242,8 +315,9 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     device = torch.device("cuda", local_rank)
-    specs = _specs(rank)
+    specs = _specs(rank, args)
     S = sum(s.length for s in specs)
+    arms = set(args.arms.split(","))
     sets = _device_blocks(specs, torch, device, seed=rank)
     obuf, outs = _out_buffers(specs, torch, device)
 
@@ -290,66 +364,14 @@ def run_ours(args, rank, world, local_rank):
         kms.append(batch.kernel_ms())
     k_ms = float(np.mean(kms))
 
-    # ---- plain path: one call per stream ----
-    phandles = [ak.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1) for s in specs]
-    pstream = torch.cuda.Stream(device=device)
-
-    def pstep(k):
-        for p, x, o in zip(phandles, sets[k % 3][1], outs):
-            gpu.process_n(p, [x], 1, out=o, stream=pstream)
-
-    for k in range(args.warmup):
-        pstep(k)
-    torch.cuda.synchronize()
-    barrier()
-    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    p0.record(pstream)
-    for k in range(args.steps):
-        pstep(k)
-    p1.record(pstream)
-    torch.cuda.synchronize()
-    barrier()
-    t_plain = max_over_ranks(p0.elapsed_time(p1) / 1e3)
-    del phandles
-
-    # ---- e2e: pinned host in -> batched path -> pinned host out ----
-    h_in = torch.empty(S, dtype=torch.complex64, pin_memory=True)
-    h_in.copy_(sets[0][0].cpu())
-    h_out = torch.empty(obuf.numel(), dtype=torch.complex64, pin_memory=True)
-    d_in, d_views = sets[0]
-
-    def estep():
-        with torch.cuda.stream(bstream):
-            d_in.copy_(h_in, non_blocking=True)
-        bstep(0)
-        with torch.cuda.stream(bstream):
-            h_out.copy_(obuf, non_blocking=True)
-
-    for _ in range(args.warmup):
-        estep()
-    torch.cuda.synchronize()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(bstream)
-    for _ in range(args.steps):
-        estep()
-    e1.record(bstream)
-    torch.cuda.synchronize()
-    barrier()
-    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    t_plain = t_e2e = t_dropin = None
     out_bytes = 8 * sum(s.nchan * m for s, m in zip(specs, ms_list))
-
-    # ---- drop-in C ABI with host buffers (per stream, synchronous) ----
-    dh = [ak.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1) for s in specs]
-    hx = [v.cpu().numpy() for v in sets[0][1]]
-    for p, x in zip(dh, hx):
-        p.process(x[: x.size // 4])
-    barrier()
-    t0 = time.perf_counter()
-    for p, x in zip(dh, hx):
-        p.process(x)
-    t_dropin = max_over_ranks(time.perf_counter() - t0)
-    del dh
+    if "plain" in arms:
+        t_plain = _plain_arm(args, specs, sets, outs, torch, device, barrier, max_over_ranks)
+    if "e2e" in arms:
+        t_e2e = _e2e_arm(args, S, sets, obuf, bstream, bstep, torch, barrier, max_over_ranks)
+    if "dropin" in arms:
+        t_dropin = _dropin_arm(specs, sets, barrier, max_over_ranks)
 
     del batch, handles, bstream
     torch.cuda.synchronize()
@@ -361,7 +383,7 @@ def run_ours(args, rank, world, local_rank):
     prof = ROOT / "profiles" / "pfb_tiles_uneven256.json"
     if prof.exists():
         traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
-    cpu = _cpu_reference_rate(specs) if not args.no_cpu else None
+    cpu = _cpu_reference_rate(specs) if "cpu" in arms and not args.no_cpu else None
     total = S * world
     value = total * args.steps / t_batch / 1e6
     line = {
@@ -369,17 +391,22 @@ def run_ours(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_batch / args.steps * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 fold + f64 fft", "data": "synthetic (seeded noise + tones, generated on device)",
-        "config": {"workload": WORKLOAD, "streams": 256, "nchan": [64, 256, 1024, 4096],
+        "config": {"workload": WORKLOAD if args.streams == 256 and args.min_log2 == 14 and
+                   args.max_log2 == 22 else f"uneven_streams_{args.streams}_2^{args.min_log2:g}-2^{args.max_log2:g}",
+                   "streams": args.streams, "nchan": [64, 256, 1024, 4096],
                    "taps_per_branch": [8, 12, 16], "oversample": 2, "blocks": 3,
                    "samples_per_step_per_gpu": S, "parallelism": f"replicas x{world} (stream-sharded)",
                    "l2": "inputs larger than L2 (~1.5 GB per step)"},
-        "plain": {"value": round(total * args.steps / t_plain / 1e6, 2), "unit": "MSamples/s",
-                  "what": "one device-pointer call per stream"},
-        "batched_over_plain": round(t_plain / t_batch, 2),
-        "e2e": {"value": round(total * args.steps / t_e2e / 1e6, 2), "unit": "MSamples/s",
-                "h2d_bytes_per_step": 8 * S, "d2h_bytes_per_step": out_bytes},
-        "dropin": {"value": round(total / t_dropin / 1e6, 2), "unit": "MSamples/s",
-                   "what": "atkdsp_pfb_process per stream, pageable host buffers"},
+        "plain": None if t_plain is None else {
+            "value": round(total * args.steps / t_plain / 1e6, 2), "unit": "MSamples/s",
+            "what": "one device-pointer call per stream"},
+        "batched_over_plain": None if t_plain is None else round(t_plain / t_batch, 2),
+        "e2e": None if t_e2e is None else {
+            "value": round(total * args.steps / t_e2e / 1e6, 2), "unit": "MSamples/s",
+            "h2d_bytes_per_step": 8 * S, "d2h_bytes_per_step": out_bytes},
+        "dropin": None if t_dropin is None else {
+            "value": round(total / t_dropin / 1e6, 2), "unit": "MSamples/s",
+            "what": "atkdsp_pfb_process per stream, pageable host buffers"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "kernel": "pfb_tiles_kernel", "kernel_ms": round(k_ms, 4),
@@ -400,6 +427,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--arms", default="batched,plain,e2e,dropin,cpu",
+                    help="comma list of arms to run (the batched arm always runs)")
+    ap.add_argument("--streams", type=int, default=256)
+    ap.add_argument("--min-log2", type=float, default=14.0)
+    ap.add_argument("--max-log2", type=float, default=22.0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
