@@ -829,6 +829,23 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_unpack_dc(const void *d_raw, size_t nbytes, int 
     return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
 }
 
+/* atkdsp_gpu_unpack_dc for callers that cannot allocate device memory: the
+ * mean's scratch is a static device array (unpack.cu), nothing is allocated. */
+ATKDSP_API ptrdiff_t atkdsp_gpu_unpack_dc_noalloc(const void *d_raw, size_t nbytes, int fmt,
+                                                  atkdsp_cf32 *d_out, size_t out_cap, float off_re,
+                                                  float off_im, double *d_mean, void *stream) {
+    if (!d_raw || !d_out) return ATKDSP_E_ARG;
+    const int bps = atkdsp_bytes_per_sample(fmt);
+    if (!bps || !aligned_for(d_raw, fmt) || ((size_t)d_out & 7)) return ATKDSP_E_ARG;
+    float cre, cim, k;
+    unpack_consts(fmt, off_re, off_im, &cre, &cim, &k);
+    size_t n = nbytes / (size_t)bps;
+    if (n > out_cap) n = out_cap;
+    if (n > atkb_unpack_noalloc_max_samples()) return ATKDSP_E_ARG;
+    const int rc = atkb_unpack_noalloc(d_raw, fmt, n, d_out, cre, cim, k, off_re, off_im, d_mean, stream);
+    return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
+}
+
 ATKDSP_API ptrdiff_t atkdsp_gpu_unpack(const void *d_raw, size_t nbytes, int fmt, atkdsp_cf32 *d_out,
                                        size_t out_cap, float dc_alpha, atkdsp_cf32 *d_dc_state,
                                        void *stream) {

@@ -142,6 +142,12 @@ int  atkb_cov_reset(void *R, uint32_t *counts, unsigned nel, unsigned nchan,
 int  atkb_unpack_partials(size_t n);
 int  atkb_unpack(const void *raw, int fmt, size_t n, void *out, float cre, float cim, float k,
                  float off_re, float off_im, double *d_mean, double *d_partial, void *stream);
+/* the same conversion and mean with the partial sums in a static device
+ * array instead of caller scratch; at most atkb_unpack_noalloc_max_samples()
+ * samples per call (ATKB_E_ARG beyond) */
+size_t atkb_unpack_noalloc_max_samples(void);
+int  atkb_unpack_noalloc(const void *raw, int fmt, size_t n, void *out, float cre, float cim, float k,
+                         float off_re, float off_im, double *d_mean, void *stream);
 /* the one-pole DC block over converted samples, serial per component;
  * d_state is one cf32 on the device (read and updated). */
 int  atkb_dc_pole(void *out, size_t n, float alpha, void *d_state, void *stream);

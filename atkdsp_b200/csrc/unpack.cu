@@ -16,6 +16,9 @@
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <mutex>
+
 #include "internal.h"
 
 #define UNPACK_NT 256
@@ -179,5 +182,78 @@ extern "C" int atkb_unpack(const void *raw, int fmt, size_t n, void *out, float 
 extern "C" int atkb_dc_pole(void *out, size_t n, float alpha, void *d_state, void *stream) {
     if (!n) return ATKB_OK;
     dc_pole_kernel<<<1, 32, 0, (cudaStream_t)stream>>>((float *)out, n, alpha, (float *)d_state);
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
+/* ---- the allocation-free variant of the device unpack_dc ------------------
+ * Some callers cannot allocate GPU memory when they call in: a host
+ * application that hands the whole device to its own memory pool and forbids
+ * other allocations, a real-time thread that must not block in the CUDA
+ * allocator, or a plugin whose host gives it buffers but no allocator. For
+ * them the mean's scratch -- two doubles of partial sums per reduction block
+ * -- lives in this file-scope device array instead of memory the library
+ * allocates. It is 32 KiB, on every GPU that loads the library, until the
+ * process exits.
+ *
+ * One block reduces 2048 samples, so the array covers calls of up to
+ * ATKB_NOALLOC_MAX_SAMPLES = 2048 * 2048 = 4,194,304 samples; larger calls are
+ * refused (split the block and combine the means weighted by their lengths).
+ * Up to that size the block count -- and so the order of the double sum --
+ * is exactly the allocating entry point's, and the two give the same bits.
+ *
+ * Every call reuses the same array and leaves its partial sums there. Nothing
+ * in it needs to start at zero: each call writes every entry its mean kernel
+ * reads before reading it. Two calls that overlap on the GPU (different
+ * streams, no ordering between them) race on the array.
+ *
+ * The array's device address is looked up once per device, by the first call
+ * made with that device current; make that first call before any stream
+ * capture begins. */
+#define ATKB_NOALLOC_BLOCKS UNPACK_MAX_BLOCKS
+static __device__ __align__(256) double g_unpack_noalloc_partials[2 * ATKB_NOALLOC_BLOCKS];
+
+static double *g_noalloc_addr[64];
+static std::mutex g_noalloc_lock;
+
+static int noalloc_partials(double **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return ATKB_E_NODEV;
+    std::lock_guard<std::mutex> guard(g_noalloc_lock);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_unpack_noalloc_partials);
+        if (e != cudaSuccess || !p) return ATKB_E_KERNEL;
+        g_noalloc_addr[dev] = (double *)p;
+    }
+    *out = g_noalloc_addr[dev];
+    return ATKB_OK;
+}
+
+extern "C" size_t atkb_unpack_noalloc_max_samples(void) {
+    return (size_t)ATKB_NOALLOC_BLOCKS * UNPACK_NT * UNPACK_PER_THREAD;
+}
+
+extern "C" int atkb_unpack_noalloc(const void *raw, int fmt, size_t n, void *out, float cre, float cim,
+                                   float k, float off_re, float off_im, double *d_mean, void *stream) {
+    if (n > atkb_unpack_noalloc_max_samples()) return ATKB_E_ARG;
+    const int nb = atkb_unpack_partials(n);
+    if (nb > ATKB_NOALLOC_BLOCKS) return ATKB_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    double *part = nullptr;
+    if (d_mean) {
+        const int rc = noalloc_partials(&part);
+        if (rc != ATKB_OK) return rc;
+    }
+    if (n) {
+        if (fmt == 4 && off_re == 0.0f && off_im == 0.0f && !d_mean) {
+            if (out != raw && cudaMemcpyAsync(out, raw, n * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+                return ATKB_E_KERNEL;
+        } else {
+            unpack_kernel<<<nb, UNPACK_NT, 0, s>>>(raw, fmt, n, (float2 *)out, cre, cim, k, off_re,
+                                                   off_im, part);
+        }
+    }
+    /* with n == 0 the mean kernel reads no partial and writes the offset */
+    if (d_mean) unpack_mean_kernel<<<1, UNPACK_NT, 0, s>>>(part, n ? nb : 0, n, off_re, off_im, d_mean);
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }

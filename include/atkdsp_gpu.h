@@ -45,6 +45,22 @@ ATKDSP_API ptrdiff_t   atkdsp_gpu_unpack_dc(const void *d_raw, size_t nbytes, in
                                             atkdsp_cf32 *d_out, size_t out_cap,
                                             float off_re, float off_im, double *d_mean,
                                             void *stream);
+/* atkdsp_gpu_unpack_dc for callers that cannot allocate GPU memory. It has
+ * no counterpart in the reference (whose unpack runs on the CPU and needs no
+ * scratch). Some callers must not allocate device memory when they call in:
+ * a host application that owns all device memory through its own pool, a
+ * real-time thread that cannot block in the CUDA allocator, a plugin given
+ * buffers but no allocator. This entry point allocates nothing: the partial
+ * sums of the mean live in a 32 KiB static device array that every GPU
+ * loading the library holds until exit. Same arguments and results (the same
+ * bits) as atkdsp_gpu_unpack_dc, for at most 4,194,304 samples per call;
+ * larger calls return ATKDSP_E_ARG. The first call on a device looks up the
+ * array's device address, so make it before any stream capture. All calls
+ * share the array: calls that overlap on the GPU race. */
+ATKDSP_API ptrdiff_t   atkdsp_gpu_unpack_dc_noalloc(const void *d_raw, size_t nbytes, int fmt,
+                                                    atkdsp_cf32 *d_out, size_t out_cap,
+                                                    float off_re, float off_im, double *d_mean,
+                                                    void *stream);
 /* atkdsp_unpack (reference include/atkdsp.h:252) on device buffers;
  * d_dc_state is one device cf32, read and updated when dc_alpha > 0. */
 ATKDSP_API ptrdiff_t   atkdsp_gpu_unpack(const void *d_raw, size_t nbytes, int fmt,
