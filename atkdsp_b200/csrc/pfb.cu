@@ -191,16 +191,77 @@ __device__ __forceinline__ void pass_c(double2 *sm, const double2 *__restrict__ 
     __syncthreads();
 }
 
-/* passes P, P+1, ... of the power-of-two plan: radix 16 while at least four
+/* passes P .. PEND-1 of the power-of-two plan: radix 16 while at least four
  * index bits remain, then one last radix 8, 4 or 2 */
-template <int LOGM, int P>
+template <int LOGM, int P, int PEND>
 __device__ __forceinline__ void passes_from(double2 *sm, const double2 *wp, const int *twoff) {
-    if constexpr (4 * P < LOGM) {
+    if constexpr (P < PEND) {
         constexpr int REM = LOGM - 4 * P;
         constexpr int R = REM >= 4 ? 16 : (1 << REM);
         pass_c<LOGM, R, 4 * P>(sm, wp + twoff[P]);
-        passes_from<LOGM, P + 1>(sm, wp, twoff);
+        passes_from<LOGM, P + 1, PEND>(sm, wp, twoff);
     }
+}
+
+/* Rotation to input sample 0 and cal for bin kb of a hop whose (b + 1) mod os
+ * is s, then one rounding to float (reference src/channelizer.c:270-292). */
+__device__ __forceinline__ float2 finish_bin(double2 X, int kb, int s, int M, int os, int hop,
+                                             bool os_pow2, const double2 *twd, const float2 *cal) {
+    const int jr = os_pow2 ? ((kb * s) & (os - 1)) : ((kb * s) % os);
+    X = cmul_rn(X, __ldg(twd + (jr ? M - jr * hop : 0)));
+    if (cal) {
+        const float2 c = __ldg(cal + kb);
+        X = cmul_rn(X, make_double2((double)c.x, (double)c.y));
+    }
+    return make_float2(__double2float_rn(X.x), __double2float_rn(X.y));
+}
+
+/* The last Stockham pass fused with the epilogue: after the butterflies every
+ * output is a final bin (j + r*Ns of hop tt), rotated, calibrated, rounded and
+ * written straight into the padded channel-major tile. */
+template <int LOGM, int R, int LOGNS>
+__device__ __forceinline__ void pass_last(double2 *sm, const double2 *__restrict__ tw,
+                                          float2 *tile_out, const atkb_bank &B, const atkb_job &J,
+                                          long long h0) {
+    constexpr int M = 1 << LOGM;
+    constexpr int NS = 1 << LOGNS;
+    constexpr int LOGR = R == 16 ? 4 : R == 8 ? 3 : R == 4 ? 2 : 1;
+    constexpr int LOGMR = LOGM - LOGR;          /* == LOGNS: Ns * R == M */
+    constexpr int MR = 1 << LOGMR;
+    constexpr int U = PTS / R;
+    constexpr int NH = 1 << (12 - LOGM);
+    double2 v[U][R];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int bi = u * NT + threadIdx.x;
+        const int tt = bi >> LOGMR;
+        const int j = bi & (MR - 1);
+        const int base = (tt << LOGM) + j;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[u][r] = sm[SW(base + r * MR)];
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[u][r] = cmul(v[u][r], __ldg(tw + (r - 1) * NS + j));
+    }
+    __syncthreads();
+    const double2 *twd = (const double2 *)B.twd;
+    const float2 *cal = (const float2 *)J.cal;
+    const int os = B.os, hop = B.hop;
+    const bool os_pow2 = (os & (os - 1)) == 0;
+    const int s0 = (int)((J.b0 + h0 + 1) % os);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int bi = u * NT + threadIdx.x;
+        const int tt = bi >> LOGMR;
+        const int j = bi & (MR - 1);
+        const int s = os_pow2 ? ((s0 + tt) & (os - 1)) : ((s0 + tt) % os);
+        dftR<R>(v[u]);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int kb = j + r * NS;
+            tile_out[kb * (NH + 1) + tt] = finish_bin(v[u][r], kb, s, M, os, hop, os_pow2, twd, cal);
+        }
+    }
+    __syncthreads();
 }
 
 /* The fold of one hop's 16 branches q = j + r*M/16 (r = 0..15), straight into
@@ -242,18 +303,117 @@ __device__ __forceinline__ void fold16(double2 *v, const atkb_job &J, const atkb
             for (int c = 0; c < 4; ++c) {
                 const int r = 4 * q + c;
                 const float2 x = LINEAR ? __ldg(xk + r * MR) : src.at(base + (long long)k * M + r * MR);
-#ifdef ATKB_FOLD_FMA
-                fr[r] = __fmaf_rn(hh[c], x.x, fr[r]);
-                fi[r] = __fmaf_rn(hh[c], x.y, fi[r]);
-#else
                 fr[r] = __fadd_rn(fr[r], __fmul_rn(hh[c], x.x));
                 fi[r] = __fadd_rn(fi[r], __fmul_rn(hh[c], x.y));
-#endif
             }
         }
     }
 #pragma unroll
     for (int r = 0; r < 16; ++r) v[r] = make_double2((double)fr[r], (double)fi[r]);
+}
+
+/* ---- the staged fold for small nchan ----------------------------------------
+ * With nchan <= 512 a tile spans many hops whose windows overlap heavily (each
+ * staged sample is used 6-20 times). The whole tile window is copied once into
+ * shared memory with asynchronous copies (cp.async: no registers held while
+ * the copies fly), then folded from there. Layout: logical sample i of the
+ * window lives at i + (i / hop) * (M/16), a pad of M/16 samples after every
+ * hop-long block, so the lanes of a warp (several hops x M/16 branches) hit
+ * distinct banks. */
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+/* physical size (in samples) of a staged window of W samples */
+__device__ __forceinline__ int staged_size(int W, int logs, int MR) { return W + ((W - 1) >> logs) * MR + MR; }
+
+template <int LOGM, int LOGOS>
+__device__ __forceinline__ void fold16_staged(double2 *v, const atkb_bank &B, int tt, int j,
+                                              const float2 *xs) {
+    constexpr int M = 1 << LOGM;
+    constexpr int MR = M >> 4;
+    constexpr int OS = 1 << LOGOS;
+    constexpr int HOP = M >> LOGOS;
+    /* logical tt*hop + k*M + j + r*MR  ->  physical, with (i / hop) = tt + k*os + (r*os)/16 */
+    const float2 *xb = xs + tt * (HOP + MR) + j;
+    const float4 *tq = (const float4 *)B.taps16 + (size_t)j * 4;
+    float fr[16], fi[16];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float4 h = __ldg(tq + q);
+        const float hh[4] = {h.x, h.y, h.z, h.w};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int r = 4 * q + c;
+            const float2 x = xb[r * MR + ((r * OS) >> 4) * MR];
+            fr[r] = __fmul_rn(hh[c], x.x);
+            fi[r] = __fmul_rn(hh[c], x.y);
+        }
+    }
+    for (int k = 1; k < B.K; ++k) {
+        tq += MR * 4;
+        xb += M + OS * MR;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float4 h = __ldg(tq + q);
+            const float hh[4] = {h.x, h.y, h.z, h.w};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int r = 4 * q + c;
+                const float2 x = xb[r * MR + ((r * OS) >> 4) * MR];
+                fr[r] = __fadd_rn(fr[r], __fmul_rn(hh[c], x.x));
+                fi[r] = __fadd_rn(fi[r], __fmul_rn(hh[c], x.y));
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = make_double2((double)fr[r], (double)fi[r]);
+}
+
+/* copy the tile window s[h0*hop, h0*hop + W) into the padded shared layout */
+__device__ __forceinline__ void stage_window(float2 *xs, const atkb_job &J, long long g0, int W,
+                                             int logs, int MR) {
+    const float2 *st = (const float2 *)J.state;
+    const float2 *in = (const float2 *)J.in;
+    for (int i = threadIdx.x; i < W; i += NT) {
+        const long long g = g0 + i;
+        const float2 *src = g < J.head ? st + g : in + (g - J.head);
+        cp_async8(xs + i + (i >> logs) * MR, src);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+}
+
+template <int LOGM>
+__device__ __forceinline__ bool fold_tile_staged(double2 *v, const atkb_job &J, const atkb_bank &B,
+                                                 long long h0, int nvalid, int tt, int j, double2 *sm) {
+    constexpr int M = 1 << LOGM;
+    constexpr int MR = M >> 4;
+    if constexpr (LOGM > 9) {
+        return false;
+    } else {
+        const int os = B.os;
+        if (os != 1 && os != 2 && os != 4) return false;
+        const int logs = LOGM - (os == 1 ? 0 : os == 2 ? 1 : 2);
+        const long long Wl = (long long)(nvalid - 1) * B.hop + B.L;
+        if (Wl > 8192) return false;
+        const int W = (int)Wl;
+        if (staged_size(W, logs, MR) > 8192) return false;     /* sm holds 8192 float2 */
+        float2 *xs = (float2 *)sm;
+        stage_window(xs, J, h0 * (long long)B.hop, W, logs, MR);
+        if (tt < nvalid) {
+            if (os == 1) fold16_staged<LOGM, 0>(v, B, tt, j, xs);
+            else if (os == 2) fold16_staged<LOGM, 1>(v, B, tt, j, xs);
+            else fold16_staged<LOGM, 2>(v, B, tt, j, xs);
+        } else {
+#pragma unroll
+            for (int r = 0; r < 16; ++r) v[r] = make_double2(0.0, 0.0);
+        }
+        __syncthreads();              /* the window is dead; sm becomes the FFT tile */
+        return true;
+    }
 }
 
 template <int LOGM>
@@ -263,63 +423,64 @@ __device__ void tile_fast(const atkb_job &J, const atkb_bank &B, long long h0, i
     constexpr int LOGNH = 12 - LOGM;
     constexpr int NH = 1 << LOGNH;
     constexpr int MR = M >> 4;
+    constexpr int NPASS = (LOGM + 3) / 4;
     const int tid = threadIdx.x;
     const int tt = tid >> (LOGM - 4);
     const int j = tid & (MR - 1);
 
     /* fold + first Stockham pass (Ns = 1, radix 16, no twiddles) */
     double2 v[16];
-    if (tt < nvalid) {
-        const long long w0 = h0 * (long long)B.hop;                  /* first window start */
-        const long long w1 = (h0 + nvalid - 1) * (long long)B.hop + B.L;  /* last window end */
-        const long long off = (h0 + tt) * (long long)B.hop + j;
-        if (w0 >= J.head)
-            fold16<LOGM, true>(v, J, B, h0, tt, j, (const float2 *)J.in + (off - J.head));
-        else if (w1 <= J.head)
-            fold16<LOGM, true>(v, J, B, h0, tt, j, (const float2 *)J.state + off);
-        else
-            fold16<LOGM, false>(v, J, B, h0, tt, j, nullptr);
-    } else {
+    if (!fold_tile_staged<LOGM>(v, J, B, h0, nvalid, tt, j, sm)) {
+        if (tt < nvalid) {
+            const long long w0 = h0 * (long long)B.hop;                       /* first window start */
+            const long long w1 = (h0 + nvalid - 1) * (long long)B.hop + B.L;  /* last window end */
+            const long long off = (h0 + tt) * (long long)B.hop + j;
+            if (w0 >= J.head)
+                fold16<LOGM, true>(v, J, B, h0, tt, j, (const float2 *)J.in + (off - J.head));
+            else if (w1 <= J.head)
+                fold16<LOGM, true>(v, J, B, h0, tt, j, (const float2 *)J.state + off);
+            else
+                fold16<LOGM, false>(v, J, B, h0, tt, j, nullptr);
+        } else {
 #pragma unroll
-        for (int r = 0; r < 16; ++r) v[r] = make_double2(0.0, 0.0);
+            for (int r = 0; r < 16; ++r) v[r] = make_double2(0.0, 0.0);
+        }
     }
     dft16(v);
 #pragma unroll
     for (int r = 0; r < 16; ++r) sm[SW((tt << LOGM) + j * 16 + r)] = v[r];
     __syncthreads();
-    passes_from<LOGM, 1>(sm, (const double2 *)B.wpass, B.plan.twoff);
 
-    /* epilogue: rotate to input sample 0, cal, one rounding; transpose the
-     * tile hop-major -> channel-major through padded shared rows */
-    const double2 *twd = (const double2 *)B.twd;
-    const float2 *cal = (const float2 *)J.cal;
-    const int os = B.os, hop = B.hop;
-    const bool os_pow2 = (os & (os - 1)) == 0;
-    const int s0 = (int)((J.b0 + h0 + 1) % os);     /* (b + 1) mod os at hop h0 */
-    float2 y[PTS];
+    if constexpr (NPASS == 1) {
+        /* nchan 16: the first pass was the last; a separate epilogue */
+        const double2 *twd = (const double2 *)B.twd;
+        const float2 *cal = (const float2 *)J.cal;
+        const int os = B.os, hop = B.hop;
+        const bool os_pow2 = (os & (os - 1)) == 0;
+        const int s0 = (int)((J.b0 + h0 + 1) % os);
+        float2 y[PTS];
 #pragma unroll
-    for (int u = 0; u < PTS; ++u) {
-        const int e = u * NT + tid;
-        const int t2 = e >> LOGM;
-        const int kb = e & (M - 1);
-        double2 X = sm[SW(e)];
-        int jr;
-        if (os_pow2) jr = (kb * ((s0 + t2) & (os - 1))) & (os - 1);
-        else jr = (kb * ((s0 + t2) % os)) % os;
-        X = cmul_rn(X, __ldg(twd + (jr ? M - jr * hop : 0)));
-        if (cal) {
-            const float2 c = __ldg(cal + kb);
-            X = cmul_rn(X, make_double2((double)c.x, (double)c.y));
+        for (int u = 0; u < PTS; ++u) {
+            const int e = u * NT + tid;
+            const int t2 = e >> LOGM;
+            const int s = os_pow2 ? ((s0 + t2) & (os - 1)) : ((s0 + t2) % os);
+            y[u] = finish_bin(sm[SW(e)], e & (M - 1), s, M, os, hop, os_pow2, twd, cal);
         }
-        y[u] = make_float2(__double2float_rn(X.x), __double2float_rn(X.y));
-    }
-    __syncthreads();
+        __syncthreads();
 #pragma unroll
-    for (int u = 0; u < PTS; ++u) {
-        const int e = u * NT + tid;
-        tile_out[(e & (M - 1)) * (NH + 1) + (e >> LOGM)] = y[u];
+        for (int u = 0; u < PTS; ++u) {
+            const int e = u * NT + tid;
+            tile_out[(e & (M - 1)) * (NH + 1) + (e >> LOGM)] = y[u];
+        }
+        __syncthreads();
+    } else {
+        const double2 *wp = (const double2 *)B.wpass;
+        passes_from<LOGM, 1, NPASS - 1>(sm, wp, B.plan.twoff);
+        constexpr int REM = LOGM - 4 * (NPASS - 1);
+        constexpr int RL = REM >= 4 ? 16 : (1 << REM);
+        pass_last<LOGM, RL, 4 * (NPASS - 1)>(sm, wp + B.plan.twoff[NPASS - 1], tile_out, B, J, h0);
     }
-    __syncthreads();
+
     /* write: thread -> (channel kb0 + u*MR, hop t2); runs of NH hops */
     const int t2 = tid & (NH - 1);
     if (t2 < nvalid) {
