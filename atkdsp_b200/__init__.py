@@ -90,6 +90,9 @@ def _bind(lib) -> None:
         "atkdsp_gpu_pfb_stream": ([vp], vp),
         "atkdsp_gpu_pfb_sync": ([vp], C.c_int),
         "atkdsp_gpu_pfb_process_n": ([vp, P(vp), u, sz, vp, sz, vp], ssz),
+        "atkdsp_gpu_pfb_process_n_raw": ([vp, P(vp), u, sz, C.c_int, C.c_float, C.c_float, vp, sz, vp], ssz),
+        "atkdsp_gpu_batch_process_raw": ([vp, P(vp), P(sz), C.c_int, P(C.c_float), P(vp), P(ssz), vp], ssz),
+        "atkdsp_gpu_unpack_dc_noalloc": ([vp, sz, C.c_int, vp, sz, C.c_float, C.c_float, vp, vp], ssz),
         "atkdsp_gpu_unpack_dc": ([vp, sz, C.c_int, vp, sz, C.c_float, C.c_float, vp, vp], ssz),
         "atkdsp_gpu_unpack": ([vp, sz, C.c_int, vp, sz, C.c_float, vp, vp], ssz),
         "atkdsp_gpu_pfb_cov_accumulate": ([vp, u, u, sz, vp, vp, vp, vp], C.c_int),

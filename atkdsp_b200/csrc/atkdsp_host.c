@@ -28,9 +28,7 @@
 #include <string.h>
 #include <unistd.h>
 
-#include "atkdsp.h"
-#include "atkdsp_gpu.h"
-#include "internal.h"
+#include "host_internal.h"
 
 #define ATKB_PI 3.14159265358979323846
 #define MAX_NEL_SUPPORTED 32
@@ -73,7 +71,8 @@ ATKDSP_API int atkdsp_get_threads(void) {
     return c > 0 ? (int)c : 1;
 }
 
-static int map_rc(int rc) {
+#define map_rc atkb_map_rc
+int atkb_map_rc(int rc) {
     switch (rc) {
     case ATKB_OK: return ATKDSP_OK;
     case ATKB_E_ARG: return ATKDSP_E_ARG;
@@ -174,39 +173,14 @@ static int plan_fft(unsigned M, atkb_fft_plan *pl) {
     return 0;
 }
 
-/* ===================================================================== handle */
-struct atkdsp_pfb {
-    double fs, atten;
-    unsigned nchan, os, K, max_nel, hop;
-    size_t L, ov;
-    int dev;
-    void *stream;
-    void *tbl_event;              /* the last table upload; gates reuse of h_tables */
-    int tbl_event_live;
-    atkb_bank bank;               /* host copy (device pointers inside)       */
-    void *d_bank;
-    void *d_const;                /* taps, twd, W, per-pass twiddles          */
-    void *d_state;                /* 2 * max_nel * cap_state cf32            */
-    size_t cap_state;
-    int cur;
-    unsigned lc;
-    int64_t b;
-    void *d_cal;
-    unsigned cal_nel;
-    size_t chunk, out_ld;         /* host-path chunk (samples) and its output stride */
-    void *d_in_stage, *d_out_stage;
-    void *d_tables, *h_tables;    /* jobs | carries | tile_start              */
-    size_t tbl_bytes;
-    int *d_counters;
-    int grid;
-};
-
 static size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+size_t atkb_align16(size_t v) { return align16(v); }
 
 static size_t tables_bytes(unsigned n) {
     return align16((size_t)n * sizeof(atkb_job)) + align16((size_t)n * sizeof(atkb_carry)) +
            align16(((size_t)n + 1) * sizeof(int));
 }
+size_t atkb_tables_bytes(unsigned n) { return tables_bytes(n); }
 
 static atkb_job *tbl_jobs(void *base) { return (atkb_job *)base; }
 static atkb_carry *tbl_carry(void *base, unsigned n) {
@@ -216,17 +190,45 @@ static int *tbl_tiles(void *base, unsigned n) {
     return (int *)((char *)base + align16((size_t)n * sizeof(atkb_job)) +
                    align16((size_t)n * sizeof(atkb_carry)));
 }
+atkb_job *atkb_tbl_jobs(void *base) { return tbl_jobs(base); }
+atkb_carry *atkb_tbl_carry(void *base, unsigned n) { return tbl_carry(base, n); }
+int *atkb_tbl_tiles(void *base, unsigned n) { return tbl_tiles(base, n); }
 
 static atkdsp_cf32 *state_buf(const atkdsp_pfb *p, int which, unsigned e) {
     return (atkdsp_cf32 *)p->d_state + ((size_t)which * p->max_nel + e) * p->cap_state;
 }
+atkdsp_cf32 *atkb_state_buf(const atkdsp_pfb *p, int which, unsigned e) { return state_buf(p, which, e); }
+
+size_t atkb_stream_footprint(unsigned nchan, unsigned oversample, unsigned taps_per_poly) {
+    const size_t cap = (size_t)nchan * taps_per_poly;          /* ov + hop = L */
+    return 2 * cap * sizeof(atkdsp_cf32) + (size_t)nchan * sizeof(atkdsp_cf32) + 4096;
+    (void)oversample;
+}
+
+/* ================================================================ bank cache
+ * Taps, tables and the device atkb_bank depend only on (device, nchan,
+ * oversample, taps/branch, attenuation). Handles with the same parameters
+ * share one copy: a batch of many streams then keeps a handful of banks hot in
+ * L2 instead of re-reading one copy per stream from HBM. Refcounted. */
+struct bank_entry {
+    int dev;
+    unsigned nchan, os, K;
+    double atten;
+    int refs;
+    void *d_const, *d_bank;
+    atkb_bank bank;
+    bank_entry *next;
+};
+static bank_entry *g_banks;
+static pthread_mutex_t g_bank_lock = PTHREAD_MUTEX_INITIALIZER;
+
+static void bank_release(bank_entry *e);
 
 ATKDSP_API void atkdsp_pfb_destroy(atkdsp_pfb *p) {
     if (!p) return;
     if (p->dev >= 0) atkb_set_device(p->dev);
     if (p->stream) atkb_stream_sync(p->stream);
-    atkb_free(p->d_bank);
-    atkb_free(p->d_const);
+    bank_release(p->be);
     atkb_free(p->d_state);
     atkb_free(p->d_cal);
     atkb_free(p->d_in_stage);
@@ -239,18 +241,19 @@ ATKDSP_API void atkdsp_pfb_destroy(atkdsp_pfb *p) {
     free(p);
 }
 
-static int upload_bank(atkdsp_pfb *p) {
-    const unsigned M = p->nchan;
+static int bank_build(bank_entry *be, void *stream) {
+    const unsigned M = be->nchan;
+    const size_t L = (size_t)M * be->K;
     atkb_fft_plan pl;
     if (plan_fft(M, &pl) != 0) return ATKB_E_ARG;
-    const size_t taps_b = align16(p->L * sizeof(float));
+    const size_t taps_b = align16(L * sizeof(float));
     const size_t tab_b = (size_t)M * 2 * sizeof(double);
     const size_t pass_b = (size_t)pl.twlen * 2 * sizeof(double);
     const size_t total = 2 * taps_b + 2 * tab_b + pass_b;
     char *h = (char *)calloc(1, total);
-    double *proto = (double *)malloc(p->L * sizeof(double));
+    double *proto = (double *)malloc(L * sizeof(double));
     if (!h || !proto) { free(h); free(proto); return ATKB_E_NOMEM; }
-    design_prototype(M, p->K, p->atten, proto);
+    design_prototype(M, be->K, be->atten, proto);
     float *taps = (float *)h;
     float *taps16 = (float *)(h + taps_b);
     double *twd = (double *)(h + 2 * taps_b);
@@ -258,12 +261,12 @@ static int upload_bank(atkdsp_pfb *p) {
     double *wp = (double *)(h + 2 * taps_b + 2 * tab_b);
     size_t q;
     unsigned j;
-    for (q = 0; q < p->L; ++q) taps[q] = (float)proto[q];
+    for (q = 0; q < L; ++q) taps[q] = (float)proto[q];
     if (pl.fast) {
         /* taps16[(k*MR + j)*16 + r] = taps[k*M + j + r*MR], MR = M/16 */
         const size_t MR = M / 16;
         size_t k2, jj, r;
-        for (k2 = 0; k2 < p->K; ++k2)
+        for (k2 = 0; k2 < be->K; ++k2)
             for (jj = 0; jj < MR; ++jj)
                 for (r = 0; r < 16; ++r)
                     taps16[(k2 * MR + jj) * 16 + r] = taps[k2 * M + jj + r * MR];
@@ -294,24 +297,24 @@ static int upload_bank(atkdsp_pfb *p) {
         }
     }
     free(proto);
-    int rc = atkb_malloc(&p->d_const, total);
-    if (rc == ATKB_OK) rc = atkb_h2d(p->d_const, h, total, p->stream);
-    if (rc == ATKB_OK) rc = atkb_stream_sync(p->stream);
+    int rc = atkb_malloc(&be->d_const, total);
+    if (rc == ATKB_OK) rc = atkb_h2d(be->d_const, h, total, stream);
+    if (rc == ATKB_OK) rc = atkb_stream_sync(stream);
     free(h);
     if (rc != ATKB_OK) return rc;
-    atkb_bank *B = &p->bank;
+    atkb_bank *B = &be->bank;
     memset(B, 0, sizeof *B);
     B->nchan = (int)M;
-    B->os = (int)p->os;
-    B->K = (int)p->K;
-    B->hop = (int)p->hop;
-    B->L = (long long)p->L;
-    B->ov = (long long)p->ov;
-    B->taps = (const float *)p->d_const;
-    B->taps16 = (const float *)((const char *)p->d_const + taps_b);
-    B->twd = (const char *)p->d_const + 2 * taps_b;
-    B->wfull = (const char *)p->d_const + 2 * taps_b + tab_b;
-    B->wpass = (const char *)p->d_const + 2 * taps_b + 2 * tab_b;
+    B->os = (int)be->os;
+    B->K = (int)be->K;
+    B->hop = (int)(M / be->os);
+    B->L = (long long)L;
+    B->ov = (long long)(L - M / be->os);
+    B->taps = (const float *)be->d_const;
+    B->taps16 = (const float *)((const char *)be->d_const + taps_b);
+    B->twd = (const char *)be->d_const + 2 * taps_b;
+    B->wfull = (const char *)be->d_const + 2 * taps_b + tab_b;
+    B->wpass = (const char *)be->d_const + 2 * taps_b + 2 * tab_b;
     B->plan = pl;
     B->logm = 0;
     if (pl.fast) {
@@ -327,16 +330,64 @@ static int upload_bank(atkdsp_pfb *p) {
         B->tile_hops = th;
         B->smem_bytes = 2 * th * (int)M * 16;
     }
-    rc = atkb_malloc(&p->d_bank, sizeof *B);
-    if (rc == ATKB_OK) rc = atkb_h2d(p->d_bank, B, sizeof *B, p->stream);
-    if (rc == ATKB_OK) rc = atkb_stream_sync(p->stream);
+    rc = atkb_malloc(&be->d_bank, sizeof *B);
+    if (rc == ATKB_OK) rc = atkb_h2d(be->d_bank, B, sizeof *B, stream);
+    if (rc == ATKB_OK) rc = atkb_stream_sync(stream);
     return rc;
 }
 
-/* reference src/channelizer.c:138-171 (argument rules and the atten clamp) */
-ATKDSP_API atkdsp_pfb *atkdsp_pfb_create(double fs, unsigned nchan, unsigned oversample,
-                                         unsigned taps_per_poly, double atten_db,
-                                         unsigned max_nel) {
+static bank_entry *bank_acquire(int dev, unsigned M, unsigned os, unsigned K, double atten,
+                                void *stream, int *rc) {
+    bank_entry *e;
+    pthread_mutex_lock(&g_bank_lock);
+    for (e = g_banks; e; e = e->next)
+        if (e->dev == dev && e->nchan == M && e->os == os && e->K == K && e->atten == atten) {
+            ++e->refs;
+            pthread_mutex_unlock(&g_bank_lock);
+            *rc = ATKB_OK;
+            return e;
+        }
+    e = (bank_entry *)calloc(1, sizeof *e);
+    if (!e) {
+        pthread_mutex_unlock(&g_bank_lock);
+        *rc = ATKB_E_NOMEM;
+        return NULL;
+    }
+    e->dev = dev; e->nchan = M; e->os = os; e->K = K; e->atten = atten; e->refs = 1;
+    *rc = bank_build(e, stream);
+    if (*rc != ATKB_OK) {
+        atkb_free(e->d_const);
+        atkb_free(e->d_bank);
+        free(e);
+        pthread_mutex_unlock(&g_bank_lock);
+        return NULL;
+    }
+    e->next = g_banks;
+    g_banks = e;
+    pthread_mutex_unlock(&g_bank_lock);
+    return e;
+}
+
+static void bank_release(bank_entry *e) {
+    bank_entry **pp;
+    if (!e) return;
+    pthread_mutex_lock(&g_bank_lock);
+    if (--e->refs == 0) {
+        for (pp = &g_banks; *pp; pp = &(*pp)->next)
+            if (*pp == e) { *pp = e->next; break; }
+        atkb_free(e->d_const);
+        atkb_free(e->d_bank);
+        free(e);
+    }
+    pthread_mutex_unlock(&g_bank_lock);
+}
+
+/* reference src/channelizer.c:138-171 (argument rules and the atten clamp).
+ * lean: a single-element stream for the server, without the host-path
+ * staging and tables (it is driven only through batch launches). */
+atkdsp_pfb *atkb_pfb_create_internal(double fs, unsigned nchan, unsigned oversample,
+                                     unsigned taps_per_poly, double atten_db, unsigned max_nel,
+                                     int lean) {
     if (!(fs > 0.0) || nchan < 2 || oversample < 1 || nchan % oversample != 0) return NULL;
     if (taps_per_poly < 2 || max_nel < 1) return NULL;
     if (max_nel > MAX_NEL_SUPPORTED) return NULL;
@@ -359,9 +410,19 @@ ATKDSP_API atkdsp_pfb *atkdsp_pfb_create(double fs, unsigned nchan, unsigned ove
         free(p);
         return NULL;
     }
-    int rc = atkb_stream_create(&p->stream);
-    if (rc == ATKB_OK) rc = atkb_event_create(&p->tbl_event);
-    if (rc == ATKB_OK) rc = upload_bank(p);
+    p->lean = lean;
+    int rc = lean ? ATKB_OK : atkb_stream_create(&p->stream);
+    if (rc == ATKB_OK && !lean) rc = atkb_event_create(&p->tbl_event);
+    if (rc == ATKB_OK) {
+        void *st = p->stream;
+        if (lean && (rc = atkb_stream_create(&st)) != ATKB_OK) st = NULL;
+        if (rc == ATKB_OK) p->be = bank_acquire(p->dev, nchan, oversample, taps_per_poly, atten_db, st, &rc);
+        if (lean && st) atkb_stream_destroy(st);
+        if (p->be) {
+            p->bank = p->be->bank;
+            p->d_bank = p->be->d_bank;
+        }
+    }
     if (rc != ATKB_OK) { atkdsp_pfb_destroy(p); return NULL; }
     /* state: ov history + up to hop - 1 leftover samples, twice per element */
     p->cap_state = p->ov + p->hop;
@@ -370,6 +431,12 @@ ATKDSP_API atkdsp_pfb *atkdsp_pfb_create(double fs, unsigned nchan, unsigned ove
         rc = atkb_memset(p->d_state, 0, 2 * (size_t)max_nel * p->cap_state * sizeof(atkdsp_cf32),
                          p->stream);
     if (rc == ATKB_OK) rc = atkb_malloc(&p->d_cal, (size_t)max_nel * nchan * sizeof(atkdsp_cf32));
+    if (rc == ATKB_OK && lean) rc = atkb_stream_sync(NULL);
+    if (lean) {
+        if (rc != ATKB_OK) { atkdsp_pfb_destroy(p); return NULL; }
+        p->lc = 0; p->b = 0; p->cur = 0;
+        return p;
+    }
     /* host-path staging: about 2^20 samples per element, whole hops */
     if (rc == ATKB_OK) {
         size_t chunk = ((size_t)1 << 21) / max_nel;
@@ -397,6 +464,12 @@ ATKDSP_API atkdsp_pfb *atkdsp_pfb_create(double fs, unsigned nchan, unsigned ove
     p->b = 0;
     p->cur = 0;
     return p;
+}
+
+ATKDSP_API atkdsp_pfb *atkdsp_pfb_create(double fs, unsigned nchan, unsigned oversample,
+                                         unsigned taps_per_poly, double atten_db,
+                                         unsigned max_nel) {
+    return atkb_pfb_create_internal(fs, nchan, oversample, taps_per_poly, atten_db, max_nel, 0);
 }
 
 ATKDSP_API void atkdsp_pfb_reset(atkdsp_pfb *p) {
@@ -448,12 +521,24 @@ ATKDSP_API int atkdsp_pfb_describe(const atkdsp_pfb *p, char *buf, size_t cap) {
                     atkdsp_pfb_out_rate(p) / 1e3, p->L, p->K, p->atten, p->max_nel);
 }
 
+const conv_t ATKB_CONV_CF32 = {0, 0.0f, 0.0f, 1.0f};
+#define CONV_CF32 ATKB_CONV_CF32
+
+void atkb_job_conv(atkb_job *J, atkb_carry *C, const conv_t *cv);
+#define job_conv atkb_job_conv
+void atkb_job_conv(atkb_job *J, atkb_carry *C, const conv_t *cv) {
+    J->in_kind = C->in_kind = cv->kind;
+    J->cre = C->cre = cv->cre;
+    J->cim = C->cim = cv->cim;
+    J->kscale = C->kscale = cv->k;
+}
+
 /* One step: nel elements, n new samples each at ins[e] (device), m hops
  * written to outs + e * nchan * ldo (device, row stride ldo). Builds the job
  * and carry tables, uploads them, launches the tile kernel and the carry,
  * and advances the host mirror of the state. Asynchronous on `stream`. */
-static int run_step(atkdsp_pfb *p, unsigned nel, const atkdsp_cf32 *const *ins, size_t n,
-                    atkdsp_cf32 *outs, size_t ldo, size_t m, void *stream) {
+static int run_step(atkdsp_pfb *p, unsigned nel, const void *const *ins, size_t n,
+                    atkdsp_cf32 *outs, size_t ldo, size_t m, void *stream, const conv_t *cv) {
     const size_t head = p->ov + p->lc;
     const unsigned nxt = (unsigned)(p->cur ^ 1);
     int rc;
@@ -487,6 +572,7 @@ static int run_step(atkdsp_pfb *p, unsigned nel, const atkdsp_cf32 *const *ins, 
         C[e].head = (long long)head;
         C[e].from = (long long)(m * p->hop);
         C[e].len = (long long)(head + n - m * p->hop);
+        job_conv(&J[e], &C[e], cv);
     }
     T[nel] = (int)nel * tiles;
     /* the tables as laid out for max_nel, uploaded whole (they are small) */
@@ -530,7 +616,8 @@ ATKDSP_API ptrdiff_t atkdsp_pfb_process_n(atkdsp_pfb *p, const atkdsp_cf32 *cons
         for (e = 0; e < nel && rc == ATKB_OK; ++e)
             rc = atkb_h2d((void *)dins[e], ins[e] + pos, nc * sizeof(atkdsp_cf32), p->stream);
         if (rc != ATKB_OK) break;
-        rc = run_step(p, nel, dins, nc, (atkdsp_cf32 *)p->d_out_stage, p->out_ld, mc, p->stream);
+        rc = run_step(p, nel, (const void *const *)dins, nc, (atkdsp_cf32 *)p->d_out_stage, p->out_ld,
+                      mc, p->stream, &CONV_CF32);
         if (rc != ATKB_OK) break;
         if (mc > 0) {
             /* rows e*nchan + k: out + (e*nchan + k)*m + col  <-  stage + (e*nchan + k)*out_ld */
@@ -574,7 +661,38 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_n(atkdsp_pfb *p, const atkdsp_cf32 *
     if (m > 0 && (!d_out || cap < (size_t)nel * p->nchan * m)) return ATKDSP_E_CAP;
     if (m > (size_t)0x7fffffff / 4 / nel) return ATKDSP_E_ARG;   /* tile indices are int */
     if (atkb_set_device(p->dev) != ATKB_OK) return ATKDSP_E_FFT;
-    const int rc = run_step(p, nel, d_ins, n, d_out, m, m, stream ? stream : p->stream);
+    const int rc = run_step(p, nel, (const void *const *)d_ins, n, d_out, m, m,
+                            stream ? stream : p->stream, &CONV_CF32);
+    return rc == ATKB_OK ? (ptrdiff_t)m : map_rc(rc);
+}
+
+static int unpack_consts(int fmt, float off_re, float off_im, float *cre, float *cim, float *k);
+
+/* the int16 formats the filterbank reads directly */
+#define raw_conv atkb_raw_conv
+int atkb_raw_conv(int fmt, float off_re, float off_im, conv_t *cv) {
+    if (fmt != ATKDSP_FMT_CI16 && fmt != ATKDSP_FMT_CI16Q11) return 0;
+    cv->kind = 1;
+    unpack_consts(fmt, off_re, off_im, &cv->cre, &cv->cim, &cv->k);
+    return 1;
+}
+
+ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_n_raw(atkdsp_pfb *p, const void *const *d_raws,
+                                                  unsigned nel, size_t n, int fmt, float off_re,
+                                                  float off_im, atkdsp_cf32 *d_out, size_t cap,
+                                                  void *stream) {
+    conv_t cv;
+    if (!p || !d_raws || nel < 1 || nel > p->max_nel || !raw_conv(fmt, off_re, off_im, &cv))
+        return ATKDSP_E_ARG;
+    unsigned e;
+    for (e = 0; e < nel && n; ++e)
+        if (!d_raws[e] || ((size_t)d_raws[e] & 3)) return ATKDSP_E_ARG;
+    if ((size_t)p->lc + n >= ((size_t)1 << 62)) return ATKDSP_E_ARG;
+    const size_t m = ((size_t)p->lc + n) / p->hop;
+    if (m > 0 && (!d_out || cap < (size_t)nel * p->nchan * m)) return ATKDSP_E_CAP;
+    if (m > (size_t)0x7fffffff / 4 / nel) return ATKDSP_E_ARG;
+    if (atkb_set_device(p->dev) != ATKB_OK) return ATKDSP_E_FFT;
+    const int rc = run_step(p, nel, d_raws, n, d_out, m, m, stream ? stream : p->stream, &cv);
     return rc == ATKB_OK ? (ptrdiff_t)m : map_rc(rc);
 }
 
@@ -954,9 +1072,9 @@ static int batch_enqueue(atkdsp_gpu_batch *b, int slot, void *stream) {
     return rc;
 }
 
-ATKDSP_API ptrdiff_t atkdsp_gpu_batch_process(atkdsp_gpu_batch *b, const atkdsp_cf32 *const *d_ins,
-                                              const size_t *ns, atkdsp_cf32 *const *d_outs,
-                                              ptrdiff_t *ms, void *stream) {
+static ptrdiff_t batch_process(atkdsp_gpu_batch *b, const void *const *d_ins, const size_t *ns,
+                               atkdsp_cf32 *const *d_outs, ptrdiff_t *ms, void *stream, int fmt,
+                               const float *offs) {
     if (!b || !d_ins || !ns || !d_outs) return ATKDSP_E_ARG;
     if (atkb_set_device(b->dev) != ATKB_OK) return ATKDSP_E_FFT;
     void *st = stream ? stream : b->stream;
@@ -975,6 +1093,11 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_batch_process(atkdsp_gpu_batch *b, const atkdsp_
         const size_t m = ((size_t)p->lc + n) / p->hop;
         if (n && !d_ins[i]) return ATKDSP_E_ARG;
         if (m && !d_outs[i]) return ATKDSP_E_ARG;
+        conv_t cv = CONV_CF32;
+        if (fmt >= 0) {
+            if (!raw_conv(fmt, offs ? offs[2 * i] : 0.0f, offs ? offs[2 * i + 1] : 0.0f, &cv)) return ATKDSP_E_ARG;
+            if (n && ((size_t)d_ins[i] & 3)) return ATKDSP_E_ARG;
+        }
         const long long t = (long long)((m + (size_t)p->bank.tile_hops - 1) / (size_t)p->bank.tile_hops);
         memset(&J[i], 0, sizeof J[i]);
         J[i].state = state_buf(p, p->cur, 0);
@@ -995,6 +1118,7 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_batch_process(atkdsp_gpu_batch *b, const atkdsp_
         C[i].head = (long long)head;
         C[i].from = (long long)(m * p->hop);
         C[i].len = (long long)(head + n - m * p->hop);
+        job_conv(&J[i], &C[i], &cv);
         total += (long long)m;
         if (tiles > 0x3fffffff) return ATKDSP_E_ARG;
     }
@@ -1029,4 +1153,18 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_batch_process(atkdsp_gpu_batch *b, const atkdsp_
         p->b += (int64_t)m;
     }
     return (ptrdiff_t)total;
+}
+
+ATKDSP_API ptrdiff_t atkdsp_gpu_batch_process(atkdsp_gpu_batch *b, const atkdsp_cf32 *const *d_ins,
+                                              const size_t *ns, atkdsp_cf32 *const *d_outs,
+                                              ptrdiff_t *ms, void *stream) {
+    return batch_process(b, (const void *const *)d_ins, ns, d_outs, ms, stream, -1, NULL);
+}
+
+ATKDSP_API ptrdiff_t atkdsp_gpu_batch_process_raw(atkdsp_gpu_batch *b, const void *const *d_raws,
+                                                  const size_t *ns, int fmt, const float *offs,
+                                                  atkdsp_cf32 *const *d_outs, ptrdiff_t *ms,
+                                                  void *stream) {
+    if (fmt != ATKDSP_FMT_CI16 && fmt != ATKDSP_FMT_CI16Q11) return ATKDSP_E_ARG;
+    return batch_process(b, d_raws, ns, d_outs, ms, stream, fmt, offs);
 }

@@ -1,0 +1,65 @@
+/* Host-layer internals shared by atkdsp_host.c and serve.c. Not public. */
+#ifndef ATKB_HOST_INTERNAL_H
+#define ATKB_HOST_INTERNAL_H
+
+#include "atkdsp.h"
+#include "atkdsp_gpu.h"
+#include "internal.h"
+
+/* a device bank shared by every handle with the same (device, nchan,
+ * oversample, taps, attenuation): taps, tables and the device atkb_bank */
+typedef struct bank_entry bank_entry;
+
+struct atkdsp_pfb {
+    double fs, atten;
+    unsigned nchan, os, K, max_nel, hop;
+    size_t L, ov;
+    int dev;
+    int lean;                     /* no host-path staging or tables (server streams) */
+    void *stream;
+    void *tbl_event;              /* the last table upload; gates reuse of h_tables */
+    int tbl_event_live;
+    bank_entry *be;
+    atkb_bank bank;               /* host copy (device pointers inside)       */
+    void *d_bank;                 /* the shared device copy                   */
+    void *d_state;                /* 2 * max_nel * cap_state cf32            */
+    size_t cap_state;
+    int cur;
+    unsigned lc;
+    int64_t b;
+    void *d_cal;
+    unsigned cal_nel;
+    size_t chunk, out_ld;         /* host-path chunk (samples) and its output stride */
+    void *d_in_stage, *d_out_stage;
+    void *d_tables, *h_tables;    /* jobs | carries | tile_start              */
+    size_t tbl_bytes;
+    int *d_counters;
+    int grid;
+};
+
+/* How a job's new samples are stored: cf32, or int16 I/Q converted in the
+ * kernels' load path with the unpack constants. */
+typedef struct {
+    int kind;                     /* 0 cf32, 1 int16 pairs */
+    float cre, cim, k;
+} conv_t;
+
+extern const conv_t ATKB_CONV_CF32;
+
+atkdsp_pfb *atkb_pfb_create_internal(double fs, unsigned nchan, unsigned oversample,
+                                     unsigned taps_per_poly, double atten_db, unsigned max_nel,
+                                     int lean);
+size_t atkb_align16(size_t v);
+size_t atkb_tables_bytes(unsigned n);
+atkb_job *atkb_tbl_jobs(void *base);
+atkb_carry *atkb_tbl_carry(void *base, unsigned n);
+int *atkb_tbl_tiles(void *base, unsigned n);
+atkdsp_cf32 *atkb_state_buf(const atkdsp_pfb *p, int which, unsigned e);
+int atkb_raw_conv(int fmt, float off_re, float off_im, conv_t *cv);
+void atkb_job_conv(atkb_job *J, atkb_carry *C, const conv_t *cv);
+int atkb_map_rc(int rc);
+/* bytes of device memory a lean single-element stream of these parameters
+ * needs beyond its (possibly shared) bank */
+size_t atkb_stream_footprint(unsigned nchan, unsigned oversample, unsigned taps_per_poly);
+
+#endif

@@ -67,7 +67,8 @@ typedef struct {
     long long b0;                 /* global hop index of this call's hop 0     */
     long long hops;               /* hops in this job                          */
     const atkb_bank *bank;        /* device copy of the bank                   */
-    int bank_index;               /* unused by kernels; host bookkeeping       */
+    int in_kind;                  /* 0: `in` is cf32; 1: `in` is int16 I/Q     */
+    float cre, cim, kscale;       /* int16 input: sample = (float(v) - c) * k  */
     int tiles;                    /* ceil(hops / bank->tile_hops)              */
 } atkb_job;
 
@@ -79,6 +80,8 @@ typedef struct {
     long long head;
     long long from;
     long long len;
+    int in_kind;                  /* as atkb_job: int16 input is converted   */
+    float cre, cim, kscale;
 } atkb_carry;
 
 /* device / memory ---------------------------------------------------------- */
@@ -126,6 +129,14 @@ int  atkb_pfb_max_smem(void);
 int  atkb_pfb_launch(const atkb_job *d_jobs, const int *d_tile_start, int njobs,
                      int *d_counters, int grid, int smem_bytes, void *stream);
 int  atkb_pfb_carry(const atkb_carry *d_carry, int ncarry, long long max_len, void *stream);
+/* the same with the job / carry count read from device memory (at most the
+ * given maximum): a launch sequence that serves a different set of streams
+ * each time can be captured once */
+int  atkb_pfb_launch_n(const atkb_job *d_jobs, const int *d_tile_start, int njobs_max,
+                       const int *d_njobs, int *d_counters, int grid, int smem_bytes, void *stream);
+int  atkb_pfb_carry_n(const atkb_carry *d_carry, int ncarry_max, const int *d_ncarry,
+                      long long max_len, void *stream);
+int  atkb_event_query(void *ev);        /* ATKB_OK when complete, 1 when pending */
 
 /* W1 + W2 over a device [nel][nchan][m] block. R, counts, pwr, mean_pwr are
  * device pointers (any may be NULL to skip that output). */

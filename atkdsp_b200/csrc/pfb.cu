@@ -138,12 +138,24 @@ __device__ __forceinline__ void dftR(double2 *v) {
 }
 
 /* one element of the stream s = state[0, head) ++ in[0, ...) */
+/* int16 I/Q -> cf32 exactly as the unpack front end does: (float(v) - c) * k
+ * with rounded operations (reference src/convert.c:64-73) */
+__device__ __forceinline__ float2 conv16(short2 v, float cre, float cim, float k) {
+    return make_float2(__fmul_rn(__fsub_rn((float)v.x, cre), k), __fmul_rn(__fsub_rn((float)v.y, cim), k));
+}
+
+/* one element of the stream s = state[0, head) ++ in[0, ...); `in` is cf32 or
+ * raw int16 I/Q converted on the fly */
 struct Src {
     const float2 *st;
-    const float2 *in;
+    const void *in;
     long long head;
+    int kind;
+    float cre, cim, k;
     __device__ __forceinline__ float2 at(long long i) const {
-        return (i < head) ? __ldg(st + i) : __ldg(in + (i - head));
+        if (i < head) return __ldg(st + i);
+        if (kind) return conv16(__ldg((const short2 *)in + (i - head)), cre, cim, k);
+        return __ldg((const float2 *)in + (i - head));
     }
 };
 
@@ -270,15 +282,18 @@ __device__ __forceinline__ void pass_last(double2 *sm, const double2 *__restrict
  * LINEAR: the tile's windows lie wholly in one buffer, read through `lin`
  * (already offset to this thread's first sample); otherwise each sample is
  * taken from the state or the input by index. */
-template <int LOGM, bool LINEAR>
+template <int LOGM, int MODE>
 __device__ __forceinline__ void fold16(double2 *v, const atkb_job &J, const atkb_bank &B,
-                                       long long h0, int tt, int j, const float2 *lin) {
+                                       long long h0, int tt, int j, const void *lin) {
     constexpr int M = 1 << LOGM;
     constexpr int MR = M >> 4;
+    constexpr bool LINEAR = MODE != 2;
     const float4 *tq = (const float4 *)B.taps16 + (size_t)j * 4;
     float fr[16], fi[16];
-    const float2 *xk = lin;
-    const Src src{(const float2 *)J.state, (const float2 *)J.in, J.head};
+    const float2 *xk = (const float2 *)lin;
+    const short2 *xk16 = (const short2 *)lin;
+    const float cre = J.cre, cim = J.cim, ks = J.kscale;
+    const Src src{(const float2 *)J.state, J.in, J.head, J.in_kind, J.cre, J.cim, J.kscale};
     const long long base = (h0 + tt) * (long long)B.hop + j;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -287,7 +302,9 @@ __device__ __forceinline__ void fold16(double2 *v, const atkb_job &J, const atkb
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int r = 4 * q + c;
-            const float2 x = LINEAR ? __ldg(xk + r * MR) : src.at(base + r * MR);
+            const float2 x = MODE == 0 ? __ldg(xk + r * MR)
+                           : MODE == 1 ? conv16(__ldg(xk16 + r * MR), cre, cim, ks)
+                                       : src.at(base + r * MR);
             fr[r] = __fmul_rn(hh[c], x.x);
             fi[r] = __fmul_rn(hh[c], x.y);
         }
@@ -295,6 +312,7 @@ __device__ __forceinline__ void fold16(double2 *v, const atkb_job &J, const atkb
     for (int k = 1; k < B.K; ++k) {
         tq += MR * 4;
         xk += M;
+        xk16 += M;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const float4 h = __ldg(tq + q);
@@ -302,7 +320,9 @@ __device__ __forceinline__ void fold16(double2 *v, const atkb_job &J, const atkb
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int r = 4 * q + c;
-                const float2 x = LINEAR ? __ldg(xk + r * MR) : src.at(base + (long long)k * M + r * MR);
+                const float2 x = MODE == 0 ? __ldg(xk + r * MR)
+                               : MODE == 1 ? conv16(__ldg(xk16 + r * MR), cre, cim, ks)
+                                           : src.at(base + (long long)k * M + r * MR);
                 fr[r] = __fadd_rn(fr[r], __fmul_rn(hh[c], x.x));
                 fi[r] = __fadd_rn(fi[r], __fmul_rn(hh[c], x.y));
             }
@@ -395,7 +415,7 @@ __device__ __forceinline__ bool fold_tile_staged(double2 *v, const atkb_job &J, 
         return false;
     } else {
         const int os = B.os;
-        if (os != 1 && os != 2 && os != 4) return false;
+        if (J.in_kind || (os != 1 && os != 2 && os != 4)) return false;
         const int logs = LOGM - (os == 1 ? 0 : os == 2 ? 1 : 2);
         const long long Wl = (long long)(nvalid - 1) * B.hop + B.L;
         if (Wl > 8192) return false;
@@ -435,12 +455,16 @@ __device__ void tile_fast(const atkb_job &J, const atkb_bank &B, long long h0, i
             const long long w0 = h0 * (long long)B.hop;                       /* first window start */
             const long long w1 = (h0 + nvalid - 1) * (long long)B.hop + B.L;  /* last window end */
             const long long off = (h0 + tt) * (long long)B.hop + j;
-            if (w0 >= J.head)
-                fold16<LOGM, true>(v, J, B, h0, tt, j, (const float2 *)J.in + (off - J.head));
-            else if (w1 <= J.head)
-                fold16<LOGM, true>(v, J, B, h0, tt, j, (const float2 *)J.state + off);
-            else
-                fold16<LOGM, false>(v, J, B, h0, tt, j, nullptr);
+            if (w0 >= J.head) {
+                if (J.in_kind)
+                    fold16<LOGM, 1>(v, J, B, h0, tt, j, (const short2 *)J.in + (off - J.head));
+                else
+                    fold16<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.in + (off - J.head));
+            } else if (w1 <= J.head) {
+                fold16<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.state + off);
+            } else {
+                fold16<LOGM, 2>(v, J, B, h0, tt, j, nullptr);
+            }
         } else {
 #pragma unroll
             for (int r = 0; r < 16; ++r) v[r] = make_double2(0.0, 0.0);
@@ -542,7 +566,7 @@ __device__ void tile_generic(const atkb_job &J, const atkb_bank &B, long long h0
     const int M = B.nchan;
     const int nh = B.tile_hops;
     double2 *A = sm, *Bf = sm + (size_t)nh * M;
-    const Src src{(const float2 *)J.state, (const float2 *)J.in, J.head};
+    const Src src{(const float2 *)J.state, J.in, J.head, J.in_kind, J.cre, J.cim, J.kscale};
     for (int e = threadIdx.x; e < nh * M; e += NT) {
         const int tt = e / M;
         const int q = e - tt * M;
@@ -598,9 +622,10 @@ __device__ void tile_generic(const atkb_job &J, const atkb_bank &B, long long h0
 #endif
 __global__ void __launch_bounds__(NT, ATKB_TILE_MINB)
 pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile_start, int njobs,
-                 int *counters) {
+                 const int *__restrict__ d_njobs, int *counters) {
     extern __shared__ double2 sm[];
-    const int total_tiles = tile_start[njobs];
+    if (d_njobs) njobs = min(njobs, *d_njobs);      /* a server round: count set per launch */
+    const int total_tiles = njobs > 0 ? tile_start[njobs] : 0;
     __shared__ int s_tile, s_local;
     __shared__ atkb_bank s_bank;
     __shared__ atkb_job s_job;
@@ -648,15 +673,16 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
     }
 }
 
-__global__ void pfb_carry_kernel(const atkb_carry *__restrict__ c, int n) {
-    const int ci = blockIdx.y;
-    if (ci >= n) return;
-    const atkb_carry C = c[ci];
-    const Src src{(const float2 *)C.state, (const float2 *)C.in, C.head};
-    float2 *dst = (float2 *)C.dst;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < C.len;
-         i += (long long)gridDim.x * blockDim.x)
-        dst[i] = src.at(C.from + i);
+/* the state carries: CTA b takes carries b, b + gridDim.x, ...; 256 threads
+ * copy one carry's samples */
+__global__ void pfb_carry_kernel(const atkb_carry *__restrict__ c, int n, const int *__restrict__ d_n) {
+    if (d_n) n = min(n, *d_n);
+    for (int ci = blockIdx.x; ci < n; ci += gridDim.x) {
+        const atkb_carry C = c[ci];
+        const Src src{(const float2 *)C.state, C.in, C.head, C.in_kind, C.cre, C.cim, C.kscale};
+        float2 *dst = (float2 *)C.dst;
+        for (long long i = threadIdx.x; i < C.len; i += blockDim.x) dst[i] = src.at(C.from + i);
+    }
 }
 
 }  // namespace
@@ -680,19 +706,28 @@ extern "C" int atkb_pfb_grid(int dev, int smem_bytes) {
 
 extern "C" int atkb_pfb_launch(const atkb_job *d_jobs, const int *d_tile_start, int njobs,
                                int *d_counters, int grid, int smem_bytes, void *stream) {
+    return atkb_pfb_launch_n(d_jobs, d_tile_start, njobs, NULL, d_counters, grid, smem_bytes, stream);
+}
+
+extern "C" int atkb_pfb_launch_n(const atkb_job *d_jobs, const int *d_tile_start, int njobs,
+                                 const int *d_njobs, int *d_counters, int grid, int smem_bytes,
+                                 void *stream) {
     if (njobs <= 0) return ATKB_OK;
     if (grid < 1) grid = 1;
     pfb_tiles_kernel<<<grid, NT, smem_bytes, (cudaStream_t)stream>>>(d_jobs, d_tile_start, njobs,
-                                                                    d_counters);
+                                                                    d_njobs, d_counters);
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }
 
 extern "C" int atkb_pfb_carry(const atkb_carry *d_carry, int ncarry, long long max_len,
                               void *stream) {
+    return atkb_pfb_carry_n(d_carry, ncarry, NULL, max_len, stream);
+}
+
+extern "C" int atkb_pfb_carry_n(const atkb_carry *d_carry, int ncarry, const int *d_ncarry,
+                                long long max_len, void *stream) {
     if (ncarry <= 0 || max_len <= 0) return ATKB_OK;
-    long long bx = (max_len + 255) / 256;
-    if (bx > 1024) bx = 1024;
-    dim3 grid((unsigned)bx, (unsigned)ncarry);
-    pfb_carry_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_carry, ncarry);
+    const int grid = ncarry < 1184 ? ncarry : 1184;
+    pfb_carry_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_carry, ncarry, d_ncarry);
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }

@@ -127,3 +127,10 @@ extern "C" int atkb_event_elapsed_ms(float *ms, void *start, void *stop) {
     if (rc != ATKB_OK) return rc;
     return st(cudaEventElapsedTime(ms, (cudaEvent_t)start, (cudaEvent_t)stop));
 }
+
+extern "C" int atkb_event_query(void *ev) {
+    const cudaError_t e = cudaEventQuery((cudaEvent_t)ev);
+    if (e == cudaSuccess) return ATKB_OK;
+    if (e == cudaErrorNotReady) return 1;
+    return st(e);
+}

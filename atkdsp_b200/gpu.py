@@ -56,6 +56,26 @@ def process_n(p: Pfb, ins, nel: int, out: torch.Tensor | None = None, stream=Non
     return out[: nel * p.nchan * got].view(nel, p.nchan, got)
 
 
+def process_n_raw(p: Pfb, raws, nel: int, fmt, offset: complex = 0j,
+                  out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """atkdsp_gpu_pfb_process_n_raw: unpack_dc(raw, fmt, offset) fused into the
+    filterbank. raws are nel int16 CUDA tensors of 2n values (I, Q pairs)."""
+    lib = load()
+    nel = int(nel)
+    n = int(raws[0].numel()) // 2
+    for t in raws[:nel]:
+        if t.numel() != 2 * n or t.dtype != torch.int16:
+            raise AtkDspError("gpu process_n_raw: inputs must be int16 I/Q of equal length")
+    m = p.out_hops(n)
+    if out is None:
+        out = torch.empty(nel * p.nchan * max(m, 1), dtype=torch.complex64, device=raws[0].device)
+    arr = (C.c_void_p * nel)(*[t.data_ptr() for t in raws[:nel]])
+    got = lib.atkdsp_gpu_pfb_process_n_raw(p.handle, arr, nel, n, _fmt(fmt), float(offset.real),
+                                           float(offset.imag), _ptr(out), out.numel(), _stream(stream))
+    _check(int(got), "gpu_pfb_process_n_raw")
+    return out[: nel * p.nchan * got].view(nel, p.nchan, got)
+
+
 def unpack_dc(raw: torch.Tensor, fmt, offset: complex = 0j, out: torch.Tensor | None = None,
               want_mean: bool = True, stream=None):
     """atkdsp_gpu_unpack_dc: returns (samples, mean) with mean a (2,) float64
@@ -148,3 +168,22 @@ class Batch:
                                                  _stream(stream))
         _check(int(got), "gpu_batch_process")
         return [int(self._ms[i]) for i in range(len(self.pfbs))]
+
+    def process_raw(self, raws, outs, fmt, offs=None, stream=None) -> list:
+        """The same with int16 I/Q blocks (2 values per sample) converted in the
+        filterbank's load path; offs: per-handle complex offsets or None."""
+        n = len(self.pfbs)
+        for i, (x, o) in enumerate(zip(raws, outs)):
+            self._ins[i] = x.data_ptr() if x.numel() else None
+            self._outs[i] = o.data_ptr() if o is not None and o.numel() else None
+            self._ns[i] = x.numel() // 2
+        po = None
+        if offs is not None:
+            fo = (C.c_float * (2 * n))()
+            for i, z in enumerate(offs):
+                fo[2 * i], fo[2 * i + 1] = float(complex(z).real), float(complex(z).imag)
+            po = fo
+        got = self._lib.atkdsp_gpu_batch_process_raw(self._b, self._ins, self._ns, _fmt(fmt), po,
+                                                     self._outs, self._ms, _stream(stream))
+        _check(int(got), "gpu_batch_process_raw")
+        return [int(self._ms[i]) for i in range(n)]

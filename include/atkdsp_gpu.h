@@ -36,6 +36,18 @@ ATKDSP_API ptrdiff_t   atkdsp_gpu_pfb_process_n(atkdsp_pfb *p, const atkdsp_cf32
                                                 unsigned nel, size_t n, atkdsp_cf32 *d_out,
                                                 size_t cap, void *stream);
 
+/* The front end fused into the filterbank: atkdsp_unpack_dc (reference
+ * include/atkdsp.h:270) of int16 I/Q samples (ATKDSP_FMT_CI16 or
+ * ATKDSP_FMT_CI16Q11) with the offset (off_re, off_im), followed by
+ * atkdsp_pfb_process_n (:3218), in one pass: the filterbank reads the raw
+ * samples (4 bytes each instead of 8) and converts them in its load path with
+ * the unpack arithmetic, so the result equals unpacking first, bit for bit.
+ * d_raws[el]: n samples (2n int16) per element, 4-byte aligned. */
+ATKDSP_API ptrdiff_t   atkdsp_gpu_pfb_process_n_raw(atkdsp_pfb *p, const void *const *d_raws,
+                                                    unsigned nel, size_t n, int fmt,
+                                                    float off_re, float off_im,
+                                                    atkdsp_cf32 *d_out, size_t cap, void *stream);
+
 /* atkdsp_unpack_dc (reference include/atkdsp.h:270) on device buffers. When
  * d_mean is not NULL it receives the two means (re, im) as doubles on the
  * device. d_raw must be aligned to the sample's component size. Uses a
@@ -98,6 +110,13 @@ ATKDSP_API void        atkdsp_gpu_batch_destroy(atkdsp_gpu_batch *b);
 ATKDSP_API ptrdiff_t   atkdsp_gpu_batch_process(atkdsp_gpu_batch *b, const atkdsp_cf32 *const *d_ins,
                                                 const size_t *ns, atkdsp_cf32 *const *d_outs,
                                                 ptrdiff_t *ms, void *stream);
+/* The same with int16 I/Q input converted in the load path (see
+ * atkdsp_gpu_pfb_process_n_raw); offs (host, may be NULL) holds each
+ * handle's offset (re, im) as 2 floats per handle. */
+ATKDSP_API ptrdiff_t   atkdsp_gpu_batch_process_raw(atkdsp_gpu_batch *b, const void *const *d_raws,
+                                                    const size_t *ns, int fmt, const float *offs,
+                                                    atkdsp_cf32 *const *d_outs, ptrdiff_t *ms,
+                                                    void *stream);
 ATKDSP_API void       *atkdsp_gpu_batch_stream(atkdsp_gpu_batch *b);
 /* Measurement hook: device time in ms of the filterbank kernel of the most
  * recent atkdsp_gpu_batch_process (CUDA events recorded around that launch,

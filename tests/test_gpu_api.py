@@ -85,3 +85,44 @@ def test_device_unpack_and_w12_equal_host_path():
     p1, m1 = ak.pfb_channel_power(y, 4, 64)
     p2, m2 = gpu.channel_power(_dev(y), 4, 64)
     assert np.array_equal(p1, p2.cpu().numpy()) and np.array_equal(m1, m2.cpu().numpy())
+
+
+def test_fused_front_end_equals_unpack_then_filterbank():
+    """atkdsp_gpu_pfb_process_n_raw == atkdsp_unpack_dc then atkdsp_pfb_process,
+    bit for bit, across uneven blocks with a changing offset (the running DC
+    estimate of the 40 MS/s front end: each block's offset is the previous
+    block's mean)."""
+    from atkdsp_b200 import gpu
+    raw = W.front_end_raw(300_000, seed=7)
+    for M, os_, K, fmt in ((1024, 2, 12, "ci16q11"), (256, 2, 16, "ci16"), (64, 1, 16, "ci16q11")):
+        ph, pd = ak.Pfb(FS, M, os_, K), ak.Pfb(FS, M, os_, K)
+        off, pos = 0j, 0
+        for blk in (100_000, 7, 40_001, 159_992):
+            chunk = raw[pos:pos + blk]
+            x, mean = ak.unpack_dc(chunk.tobytes(), fmt, off)
+            yh = ph.process(x)
+            yd = gpu.process_n_raw(pd, [_dev(chunk.reshape(-1))], 1, fmt, off)[0]
+            gpu.sync(pd)
+            assert np.array_equal(yh, yd.cpu().numpy()), (M, blk)
+            off = complex(np.float32(mean.real), np.float32(mean.imag))
+            pos += blk
+
+
+def test_batch_raw_equals_each_stream_alone():
+    from atkdsp_b200 import gpu
+    specs = W.uneven_streams(12, seed=3, min_log2=11, max_log2=15)
+    alone = [ak.Pfb(FS, s.nchan, s.oversample, s.taps) for s in specs]
+    mixed = [ak.Pfb(FS, s.nchan, s.oversample, s.taps) for s in specs]
+    batch = gpu.Batch(mixed, use_graph=True)
+    offs = [complex(0.01 * i, -0.02 * i) for i in range(len(specs))]
+    for blk in range(3):
+        raws = [W.ci16_block(s.length, s.seed, blk) for s in specs]
+        ms = batch.out_hops([s.length for s in specs])
+        outs = [torch.empty(max(1, s.nchan * m), dtype=torch.complex64, device="cuda")
+                for s, m in zip(specs, ms)]
+        assert batch.process_raw([_dev(r.reshape(-1)) for r in raws], outs, "ci16", offs) == ms
+        torch.cuda.synchronize()
+        for i, s in enumerate(specs):
+            x, _ = ak.unpack_dc(raws[i].tobytes(), "ci16", offs[i])
+            y = alone[i].process(x)
+            assert np.array_equal(y, outs[i][: s.nchan * ms[i]].view(s.nchan, ms[i]).cpu().numpy()), i
