@@ -95,6 +95,8 @@ def _bind(lib) -> None:
         "atkdsp_gpu_unpack_dc_noalloc": ([vp, sz, C.c_int, vp, sz, C.c_float, C.c_float, vp, vp], ssz),
         "atkdsp_gpu_unpack_dc": ([vp, sz, C.c_int, vp, sz, C.c_float, C.c_float, vp, vp], ssz),
         "atkdsp_gpu_unpack": ([vp, sz, C.c_int, vp, sz, C.c_float, vp, vp], ssz),
+        "atkdsp_gpu_block_mean": ([vp, sz, C.c_int, C.c_float, C.c_float, vp, vp], ssz),
+        "atkdsp_gpu_pfb_accumulate": ([vp, u, u, sz, vp, vp, vp, vp, vp, vp], C.c_int),
         "atkdsp_gpu_pfb_cov_accumulate": ([vp, u, u, sz, vp, vp, vp, vp], C.c_int),
         "atkdsp_gpu_pfb_cov_reset": ([vp, vp, u, u, vp, vp], C.c_int),
         "atkdsp_gpu_pfb_channel_power": ([vp, u, u, sz, vp, vp, vp], C.c_int),

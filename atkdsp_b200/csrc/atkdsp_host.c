@@ -135,10 +135,10 @@ static int is_pow2(unsigned v) { return v && !(v & (v - 1)); }
 static int plan_fft(unsigned M, atkb_fft_plan *pl) {
     memset(pl, 0, sizeof *pl);
     if (is_pow2(M) && M >= 16 && M <= MAX_POW2_NCHAN) {
-        unsigned rem = M / 16;
+        unsigned rem = M / ATKB_PTS;
         pl->fast = 1;
-        pl->radix[pl->npass++] = 16;
-        while (rem >= 16) { pl->radix[pl->npass++] = 16; rem /= 16; }
+        pl->radix[pl->npass++] = ATKB_PTS;
+        while (rem >= ATKB_PTS) { pl->radix[pl->npass++] = ATKB_PTS; rem /= ATKB_PTS; }
         if (rem > 1) pl->radix[pl->npass++] = (int)rem;
     } else {
         unsigned rem = M, p;
@@ -255,7 +255,7 @@ static int bank_build(bank_entry *be, void *stream) {
     if (!h || !proto) { free(h); free(proto); return ATKB_E_NOMEM; }
     design_prototype(M, be->K, be->atten, proto);
     float *taps = (float *)h;
-    float *taps16 = (float *)(h + taps_b);
+    float *tapsP = (float *)(h + taps_b);
     double *twd = (double *)(h + 2 * taps_b);
     double *W = (double *)(h + 2 * taps_b + tab_b);
     double *wp = (double *)(h + 2 * taps_b + 2 * tab_b);
@@ -263,13 +263,13 @@ static int bank_build(bank_entry *be, void *stream) {
     unsigned j;
     for (q = 0; q < L; ++q) taps[q] = (float)proto[q];
     if (pl.fast) {
-        /* taps16[(k*MR + j)*16 + r] = taps[k*M + j + r*MR], MR = M/16 */
-        const size_t MR = M / 16;
+        /* tapsP[(k*MP + j)*P + r] = taps[k*M + j + r*MP], MP = M/P */
+        const size_t P = ATKB_PTS, MP = M / ATKB_PTS;
         size_t k2, jj, r;
         for (k2 = 0; k2 < be->K; ++k2)
-            for (jj = 0; jj < MR; ++jj)
-                for (r = 0; r < 16; ++r)
-                    taps16[(k2 * MR + jj) * 16 + r] = taps[k2 * M + jj + r * MR];
+            for (jj = 0; jj < MP; ++jj)
+                for (r = 0; r < P; ++r)
+                    tapsP[(k2 * MP + jj) * P + r] = taps[k2 * M + jj + r * MP];
     }
     for (j = 0; j < M; ++j) {
         /* the reference's rotation table, channelizer.c:164-170 */
@@ -311,7 +311,7 @@ static int bank_build(bank_entry *be, void *stream) {
     B->L = (long long)L;
     B->ov = (long long)(L - M / be->os);
     B->taps = (const float *)be->d_const;
-    B->taps16 = (const float *)((const char *)be->d_const + taps_b);
+    B->tapsP = (const float *)((const char *)be->d_const + taps_b);
     B->twd = (const char *)be->d_const + 2 * taps_b;
     B->wfull = (const char *)be->d_const + 2 * taps_b + tab_b;
     B->wpass = (const char *)be->d_const + 2 * taps_b + 2 * tab_b;
@@ -813,6 +813,15 @@ ATKDSP_API int atkdsp_gpu_pfb_cov_accumulate(const atkdsp_cf32 *d_out, unsigned 
     return map_rc(atkb_w12(d_out, nel, nchan, m, d_gate, d_R, d_counts, NULL, NULL, stream));
 }
 
+ATKDSP_API int atkdsp_gpu_pfb_accumulate(const atkdsp_cf32 *d_out, unsigned nel, unsigned nchan,
+                                         size_t m, const uint8_t *d_gate, atkdsp_cf32 *d_R,
+                                         uint32_t *d_counts, float *d_pwr, float *d_mean_pwr,
+                                         void *stream) {
+    if (!d_out || nel < 1 || nchan < 1 || nel > MAX_NEL_SUPPORTED) return ATKDSP_E_ARG;
+    if ((d_R == NULL) != (d_counts == NULL)) return ATKDSP_E_ARG;
+    return map_rc(atkb_w12(d_out, nel, nchan, m, d_gate, d_R, d_counts, d_pwr, d_mean_pwr, stream));
+}
+
 ATKDSP_API int atkdsp_gpu_pfb_cov_reset(atkdsp_cf32 *d_R, uint32_t *d_counts, unsigned nel,
                                         unsigned nchan, const uint8_t *d_gate, void *stream) {
     if (!d_R || !d_counts) return ATKDSP_E_ARG;
@@ -961,6 +970,20 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_unpack_dc_noalloc(const void *d_raw, size_t nbyt
     if (n > out_cap) n = out_cap;
     if (n > atkb_unpack_noalloc_max_samples()) return ATKDSP_E_ARG;
     const int rc = atkb_unpack_noalloc(d_raw, fmt, n, d_out, cre, cim, k, off_re, off_im, d_mean, stream);
+    return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
+}
+
+ATKDSP_API ptrdiff_t atkdsp_gpu_block_mean(const void *d_raw, size_t nbytes, int fmt, float off_re,
+                                           float off_im, double *d_mean, void *stream) {
+    if (!d_raw || !d_mean) return ATKDSP_E_ARG;
+    const int bps = atkdsp_bytes_per_sample(fmt);
+    if (!bps || !aligned_for(d_raw, fmt)) return ATKDSP_E_ARG;
+    float cre, cim, k;
+    unpack_consts(fmt, off_re, off_im, &cre, &cim, &k);
+    const size_t n = nbytes / (size_t)bps;
+    double *part = NULL;
+    int rc = gpu_partials(&part);
+    if (rc == ATKB_OK) rc = atkb_unpack(d_raw, fmt, n, NULL, cre, cim, k, off_re, off_im, d_mean, part, stream);
     return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
 }
 

@@ -27,9 +27,14 @@ extern "C" {
 
 /* ---- FFT plan --------------------------------------------------------------
  * nchan = radix[0] * radix[1] * ... * radix[npass-1], Stockham order. For a
- * power of two >= 16 the fast path is used: radix[0] == 16 and every later
- * radix is 16, 8, 4 or 2 (16 complex points per thread per pass). */
+ * power of two >= 16 the fast path is used: radix[0] == ATKB_PTS and every
+ * later radix is ATKB_PTS except a smaller last one. */
 #define ATKB_MAX_PASS 24
+/* complex points per thread in the fast path's Stockham passes (8 or 16);
+ * the host's plan and permuted taps follow it */
+#ifndef ATKB_PTS
+#define ATKB_PTS 8
+#endif
 typedef struct {
     int npass;
     int fast;                     /* 1: power-of-two fast path */
@@ -43,9 +48,9 @@ typedef struct {
     int nchan, os, K, hop;
     long long L, ov;
     const float *taps;            /* device: L floats, (float)h[q]            */
-    const float *taps16;          /* device: fast path, taps permuted so the 16
-                                   * branches j + r*nchan/16 of tap k are the 16
-                                   * floats at ((k*nchan/16 + j)*16 + r)       */
+    const float *tapsP;           /* device: fast path, taps permuted so the P
+                                   * branches j + r*nchan/P of tap k are the P
+                                   * floats at ((k*nchan/P + j)*P + r), P = ATKB_PTS */
     const void *twd;              /* device: nchan double2 (cos, sin)(2 pi j/nchan) */
     const void *wfull;            /* device: nchan double2 W^j = (cos, -sin)  */
     const void *wpass;            /* device: per-pass twiddles (fast path)    */
@@ -146,7 +151,7 @@ int  atkb_cov_reset(void *R, uint32_t *counts, unsigned nel, unsigned nchan,
                     const uint8_t *gate, void *stream);
 
 /* unpack ------------------------------------------------------------------- */
-/* device raw -> device cf32, (x - c) * k per component; the means (double,
+/* device raw -> device cf32 (out may be NULL: mean only), (x - c) * k per component; the means (double,
  * BEFORE subtraction of the offset, i.e. sum(out)/n + off) go to d_mean[0..1]
  * when d_mean != NULL, using d_partial (>= 2 * atkb_unpack_partials(n)
  * doubles) as scratch. */

@@ -37,9 +37,12 @@
 #include <stdint.h>
 #include "internal.h"
 
-#define NT 256
-#define PTS 16
-#define TILE_POINTS (NT * PTS)
+/* the fast path's tile: 4096 complex points, PTS per thread (ATKB_PTS in
+ * internal.h: 8 points -> 512 threads at <= 64 registers, 32 warps per SM) */
+#define PTS ATKB_PTS
+#define LOGP (PTS == 16 ? 4 : 3)
+#define TILE_POINTS 4096
+#define NT (TILE_POINTS / PTS)
 
 namespace {
 
@@ -165,7 +168,7 @@ struct Src {
  * of 16 elements across lanes; swizzled, every 8-lane wavefront lands on 8
  * distinct 16-byte slots, and the unit-stride accesses of later passes stay
  * conflict-free too (a XOR with a per-block constant permutes the slots). */
-__device__ __forceinline__ int SW(int i) { return i ^ ((i >> 4) & 15); }
+__device__ __forceinline__ int SW(int i) { return i ^ ((i >> LOGP) & (PTS - 1)); }
 
 /* One in-place Stockham pass over a 4096-point tile (NT threads x 16 points):
  * every index is a compile-time shift or mask. tw holds W_{Ns R}^{r k} at
@@ -203,14 +206,14 @@ __device__ __forceinline__ void pass_c(double2 *sm, const double2 *__restrict__ 
     __syncthreads();
 }
 
-/* passes P .. PEND-1 of the power-of-two plan: radix 16 while at least four
- * index bits remain, then one last radix 8, 4 or 2 */
+/* passes P .. PEND-1 of the power-of-two plan: radix PTS while at least
+ * LOGP index bits remain, then one last smaller radix */
 template <int LOGM, int P, int PEND>
 __device__ __forceinline__ void passes_from(double2 *sm, const double2 *wp, const int *twoff) {
     if constexpr (P < PEND) {
-        constexpr int REM = LOGM - 4 * P;
-        constexpr int R = REM >= 4 ? 16 : (1 << REM);
-        pass_c<LOGM, R, 4 * P>(sm, wp + twoff[P]);
+        constexpr int REM = LOGM - LOGP * P;
+        constexpr int R = REM >= LOGP ? PTS : (1 << REM);
+        pass_c<LOGM, R, LOGP * P>(sm, wp + twoff[P]);
         passes_from<LOGM, P + 1, PEND>(sm, wp, twoff);
     }
 }
@@ -276,60 +279,60 @@ __device__ __forceinline__ void pass_last(double2 *sm, const double2 *__restrict
     __syncthreads();
 }
 
-/* The fold of one hop's 16 branches q = j + r*M/16 (r = 0..15), straight into
- * the registers of the first radix-16 butterfly. Taps come from the bank's
- * permuted copy (16 consecutive floats per (k, j): four 16-byte loads).
- * LINEAR: the tile's windows lie wholly in one buffer, read through `lin`
- * (already offset to this thread's first sample); otherwise each sample is
- * taken from the state or the input by index. */
+/* The fold of one hop's PTS branches q = j + r*M/PTS (r < PTS), straight
+ * into the registers of the first radix-PTS butterfly. Taps come from the
+ * bank's permuted copy (PTS consecutive floats per (k, j): 16-byte loads).
+ * MODE 0: the tile's windows lie wholly in one cf32 buffer, read through
+ * `lin` (offset to this thread's first sample); MODE 1: the same in raw int16
+ * I/Q converted on the fly; MODE 2: each sample from the state or the input
+ * by index. */
 template <int LOGM, int MODE>
-__device__ __forceinline__ void fold16(double2 *v, const atkb_job &J, const atkb_bank &B,
-                                       long long h0, int tt, int j, const void *lin) {
+__device__ __forceinline__ void foldP(double2 *v, const atkb_job &J, const atkb_bank &B,
+                                      long long h0, int tt, int j, const void *lin) {
     constexpr int M = 1 << LOGM;
-    constexpr int MR = M >> 4;
-    constexpr bool LINEAR = MODE != 2;
-    const float4 *tq = (const float4 *)B.taps16 + (size_t)j * 4;
-    float fr[16], fi[16];
+    constexpr int MP = M >> LOGP;
+    const float4 *tq = (const float4 *)B.tapsP + (size_t)j * (PTS / 4);
+    float fr[PTS], fi[PTS];
     const float2 *xk = (const float2 *)lin;
     const short2 *xk16 = (const short2 *)lin;
     const float cre = J.cre, cim = J.cim, ks = J.kscale;
     const Src src{(const float2 *)J.state, J.in, J.head, J.in_kind, J.cre, J.cim, J.kscale};
     const long long base = (h0 + tt) * (long long)B.hop + j;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < PTS / 4; ++q) {
         const float4 h = __ldg(tq + q);
         const float hh[4] = {h.x, h.y, h.z, h.w};
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int r = 4 * q + c;
-            const float2 x = MODE == 0 ? __ldg(xk + r * MR)
-                           : MODE == 1 ? conv16(__ldg(xk16 + r * MR), cre, cim, ks)
-                                       : src.at(base + r * MR);
+            const float2 x = MODE == 0 ? __ldg(xk + r * MP)
+                           : MODE == 1 ? conv16(__ldg(xk16 + r * MP), cre, cim, ks)
+                                       : src.at(base + r * MP);
             fr[r] = __fmul_rn(hh[c], x.x);
             fi[r] = __fmul_rn(hh[c], x.y);
         }
     }
     for (int k = 1; k < B.K; ++k) {
-        tq += MR * 4;
+        tq += MP * (PTS / 4);
         xk += M;
         xk16 += M;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < PTS / 4; ++q) {
             const float4 h = __ldg(tq + q);
             const float hh[4] = {h.x, h.y, h.z, h.w};
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int r = 4 * q + c;
-                const float2 x = MODE == 0 ? __ldg(xk + r * MR)
-                               : MODE == 1 ? conv16(__ldg(xk16 + r * MR), cre, cim, ks)
-                                           : src.at(base + (long long)k * M + r * MR);
+                const float2 x = MODE == 0 ? __ldg(xk + r * MP)
+                               : MODE == 1 ? conv16(__ldg(xk16 + r * MP), cre, cim, ks)
+                                           : src.at(base + (long long)k * M + r * MP);
                 fr[r] = __fadd_rn(fr[r], __fmul_rn(hh[c], x.x));
                 fi[r] = __fadd_rn(fi[r], __fmul_rn(hh[c], x.y));
             }
         }
     }
 #pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = make_double2((double)fr[r], (double)fi[r]);
+    for (int r = 0; r < PTS; ++r) v[r] = make_double2((double)fr[r], (double)fi[r]);
 }
 
 /* ---- the staged fold for small nchan ----------------------------------------
@@ -350,46 +353,46 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 __device__ __forceinline__ int staged_size(int W, int logs, int MR) { return W + ((W - 1) >> logs) * MR + MR; }
 
 template <int LOGM, int LOGOS>
-__device__ __forceinline__ void fold16_staged(double2 *v, const atkb_bank &B, int tt, int j,
-                                              const float2 *xs) {
+__device__ __forceinline__ void foldP_staged(double2 *v, const atkb_bank &B, int tt, int j,
+                                             const float2 *xs) {
     constexpr int M = 1 << LOGM;
-    constexpr int MR = M >> 4;
+    constexpr int MP = M >> LOGP;
     constexpr int OS = 1 << LOGOS;
     constexpr int HOP = M >> LOGOS;
-    /* logical tt*hop + k*M + j + r*MR  ->  physical, with (i / hop) = tt + k*os + (r*os)/16 */
-    const float2 *xb = xs + tt * (HOP + MR) + j;
-    const float4 *tq = (const float4 *)B.taps16 + (size_t)j * 4;
-    float fr[16], fi[16];
+    /* logical tt*hop + k*M + j + r*MP  ->  physical, with (i / hop) = tt + k*os + (r*os)/PTS */
+    const float2 *xb = xs + tt * (HOP + MP) + j;
+    const float4 *tq = (const float4 *)B.tapsP + (size_t)j * (PTS / 4);
+    float fr[PTS], fi[PTS];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < PTS / 4; ++q) {
         const float4 h = __ldg(tq + q);
         const float hh[4] = {h.x, h.y, h.z, h.w};
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int r = 4 * q + c;
-            const float2 x = xb[r * MR + ((r * OS) >> 4) * MR];
+            const float2 x = xb[r * MP + ((r * OS) >> LOGP) * MP];
             fr[r] = __fmul_rn(hh[c], x.x);
             fi[r] = __fmul_rn(hh[c], x.y);
         }
     }
     for (int k = 1; k < B.K; ++k) {
-        tq += MR * 4;
-        xb += M + OS * MR;
+        tq += MP * (PTS / 4);
+        xb += M + OS * MP;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < PTS / 4; ++q) {
             const float4 h = __ldg(tq + q);
             const float hh[4] = {h.x, h.y, h.z, h.w};
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int r = 4 * q + c;
-                const float2 x = xb[r * MR + ((r * OS) >> 4) * MR];
+                const float2 x = xb[r * MP + ((r * OS) >> LOGP) * MP];
                 fr[r] = __fadd_rn(fr[r], __fmul_rn(hh[c], x.x));
                 fi[r] = __fadd_rn(fi[r], __fmul_rn(hh[c], x.y));
             }
         }
     }
 #pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = make_double2((double)fr[r], (double)fi[r]);
+    for (int r = 0; r < PTS; ++r) v[r] = make_double2((double)fr[r], (double)fi[r]);
 }
 
 /* copy the tile window s[h0*hop, h0*hop + W) into the padded shared layout */
@@ -410,7 +413,7 @@ template <int LOGM>
 __device__ __forceinline__ bool fold_tile_staged(double2 *v, const atkb_job &J, const atkb_bank &B,
                                                  long long h0, int nvalid, int tt, int j, double2 *sm) {
     constexpr int M = 1 << LOGM;
-    constexpr int MR = M >> 4;
+    constexpr int MR = M >> LOGP;
     if constexpr (LOGM > 9) {
         return false;
     } else {
@@ -424,12 +427,12 @@ __device__ __forceinline__ bool fold_tile_staged(double2 *v, const atkb_job &J, 
         float2 *xs = (float2 *)sm;
         stage_window(xs, J, h0 * (long long)B.hop, W, logs, MR);
         if (tt < nvalid) {
-            if (os == 1) fold16_staged<LOGM, 0>(v, B, tt, j, xs);
-            else if (os == 2) fold16_staged<LOGM, 1>(v, B, tt, j, xs);
-            else fold16_staged<LOGM, 2>(v, B, tt, j, xs);
+            if (os == 1) foldP_staged<LOGM, 0>(v, B, tt, j, xs);
+            else if (os == 2) foldP_staged<LOGM, 1>(v, B, tt, j, xs);
+            else foldP_staged<LOGM, 2>(v, B, tt, j, xs);
         } else {
 #pragma unroll
-            for (int r = 0; r < 16; ++r) v[r] = make_double2(0.0, 0.0);
+            for (int r = 0; r < PTS; ++r) v[r] = make_double2(0.0, 0.0);
         }
         __syncthreads();              /* the window is dead; sm becomes the FFT tile */
         return true;
@@ -442,14 +445,15 @@ __device__ void tile_fast(const atkb_job &J, const atkb_bank &B, long long h0, i
     constexpr int M = 1 << LOGM;
     constexpr int LOGNH = 12 - LOGM;
     constexpr int NH = 1 << LOGNH;
-    constexpr int MR = M >> 4;
-    constexpr int NPASS = (LOGM + 3) / 4;
+    constexpr int MP = M >> LOGP;
+    constexpr int NPASS = (LOGM + LOGP - 1) / LOGP;
+    static_assert(NPASS >= 2, "the fast path needs nchan > PTS");
     const int tid = threadIdx.x;
-    const int tt = tid >> (LOGM - 4);
-    const int j = tid & (MR - 1);
+    const int tt = tid >> (LOGM - LOGP);
+    const int j = tid & (MP - 1);
 
-    /* fold + first Stockham pass (Ns = 1, radix 16, no twiddles) */
-    double2 v[16];
+    /* fold + first Stockham pass (Ns = 1, radix PTS, no twiddles) */
+    double2 v[PTS];
     if (!fold_tile_staged<LOGM>(v, J, B, h0, nvalid, tt, j, sm)) {
         if (tt < nvalid) {
             const long long w0 = h0 * (long long)B.hop;                       /* first window start */
@@ -457,63 +461,39 @@ __device__ void tile_fast(const atkb_job &J, const atkb_bank &B, long long h0, i
             const long long off = (h0 + tt) * (long long)B.hop + j;
             if (w0 >= J.head) {
                 if (J.in_kind)
-                    fold16<LOGM, 1>(v, J, B, h0, tt, j, (const short2 *)J.in + (off - J.head));
+                    foldP<LOGM, 1>(v, J, B, h0, tt, j, (const short2 *)J.in + (off - J.head));
                 else
-                    fold16<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.in + (off - J.head));
+                    foldP<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.in + (off - J.head));
             } else if (w1 <= J.head) {
-                fold16<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.state + off);
+                foldP<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.state + off);
             } else {
-                fold16<LOGM, 2>(v, J, B, h0, tt, j, nullptr);
+                foldP<LOGM, 2>(v, J, B, h0, tt, j, nullptr);
             }
         } else {
 #pragma unroll
-            for (int r = 0; r < 16; ++r) v[r] = make_double2(0.0, 0.0);
+            for (int r = 0; r < PTS; ++r) v[r] = make_double2(0.0, 0.0);
         }
     }
-    dft16(v);
+    dftR<PTS>(v);
 #pragma unroll
-    for (int r = 0; r < 16; ++r) sm[SW((tt << LOGM) + j * 16 + r)] = v[r];
+    for (int r = 0; r < PTS; ++r) sm[SW((tt << LOGM) + j * PTS + r)] = v[r];
     __syncthreads();
 
-    if constexpr (NPASS == 1) {
-        /* nchan 16: the first pass was the last; a separate epilogue */
-        const double2 *twd = (const double2 *)B.twd;
-        const float2 *cal = (const float2 *)J.cal;
-        const int os = B.os, hop = B.hop;
-        const bool os_pow2 = (os & (os - 1)) == 0;
-        const int s0 = (int)((J.b0 + h0 + 1) % os);
-        float2 y[PTS];
-#pragma unroll
-        for (int u = 0; u < PTS; ++u) {
-            const int e = u * NT + tid;
-            const int t2 = e >> LOGM;
-            const int s = os_pow2 ? ((s0 + t2) & (os - 1)) : ((s0 + t2) % os);
-            y[u] = finish_bin(sm[SW(e)], e & (M - 1), s, M, os, hop, os_pow2, twd, cal);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int u = 0; u < PTS; ++u) {
-            const int e = u * NT + tid;
-            tile_out[(e & (M - 1)) * (NH + 1) + (e >> LOGM)] = y[u];
-        }
-        __syncthreads();
-    } else {
-        const double2 *wp = (const double2 *)B.wpass;
-        passes_from<LOGM, 1, NPASS - 1>(sm, wp, B.plan.twoff);
-        constexpr int REM = LOGM - 4 * (NPASS - 1);
-        constexpr int RL = REM >= 4 ? 16 : (1 << REM);
-        pass_last<LOGM, RL, 4 * (NPASS - 1)>(sm, wp + B.plan.twoff[NPASS - 1], tile_out, B, J, h0);
-    }
+    const double2 *wp = (const double2 *)B.wpass;
+    passes_from<LOGM, 1, NPASS - 1>(sm, wp, B.plan.twoff);
+    constexpr int REM = LOGM - LOGP * (NPASS - 1);
+    constexpr int RL = REM >= LOGP ? PTS : (1 << REM);
+    pass_last<LOGM, RL, LOGP * (NPASS - 1)>(sm, wp + B.plan.twoff[NPASS - 1], tile_out, B, J, h0);
 
-    /* write: thread -> (channel kb0 + u*MR, hop t2); runs of NH hops */
+    /* write: thread -> (channel kb0 + u*MP, hop t2); runs of NH hops */
     const int t2 = tid & (NH - 1);
     if (t2 < nvalid) {
         const int kb0 = tid >> LOGNH;
         float2 *o = (float2 *)J.out + (J.out_col + h0 + t2) + (long long)kb0 * J.ldo;
-        const long long step = (long long)MR * J.ldo;
+        const long long step = (long long)MP * J.ldo;
 #pragma unroll 4
         for (int u = 0; u < PTS; ++u) {
-            *o = tile_out[(kb0 + u * MR) * (NH + 1) + t2];
+            *o = tile_out[(kb0 + u * MP) * (NH + 1) + t2];
             o += step;
         }
     }
@@ -618,7 +598,7 @@ __device__ void tile_generic(const atkb_job &J, const atkb_bank &B, long long h0
 }
 
 #ifndef ATKB_TILE_MINB
-#define ATKB_TILE_MINB 2
+#define ATKB_TILE_MINB (PTS == 8 ? 2 : 2)
 #endif
 __global__ void __launch_bounds__(NT, ATKB_TILE_MINB)
 pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile_start, int njobs,

@@ -69,7 +69,7 @@ unpack_kernel(const void *__restrict__ raw, int fmt, size_t n, float2 *__restric
     const size_t stride = (size_t)gridDim.x * UNPACK_NT;
     for (size_t i = (size_t)blockIdx.x * UNPACK_NT + threadIdx.x; i < n; i += stride) {
         const float2 y = convert_one(raw, fmt, i, cre, cim, k, offr, offi);
-        out[i] = y;
+        if (out) out[i] = y;
         sr += (double)y.x;
         si += (double)y.y;
     }
@@ -158,7 +158,8 @@ extern "C" int atkb_unpack(const void *raw, int fmt, size_t n, void *out, float 
     const int nb = atkb_unpack_partials(n);
     if (n) {
         if (fmt == 4 && off_re == 0.0f && off_im == 0.0f && !d_mean) {
-            if (out != raw && cudaMemcpyAsync(out, raw, n * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            if (out && out != raw &&
+                cudaMemcpyAsync(out, raw, n * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
                 return ATKB_E_KERNEL;
         } else {
             unpack_kernel<<<nb, UNPACK_NT, 0, s>>>(raw, fmt, n, (float2 *)out, cre, cim, k, off_re,

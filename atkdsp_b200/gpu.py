@@ -15,8 +15,8 @@ import torch
 
 from . import AtkDspError, Pfb, _check, _fmt, bytes_per_sample, load
 
-__all__ = ["process_n", "unpack_dc", "unpack", "cov_accumulate", "channel_power", "Batch",
-           "sync"]
+__all__ = ["process_n", "process_n_raw", "unpack_dc", "unpack", "block_mean", "accumulate",
+           "cov_accumulate", "channel_power", "Batch", "sync"]
 
 
 def _ptr(t: torch.Tensor | None):
@@ -104,6 +104,28 @@ def unpack(raw: torch.Tensor, fmt, dc_alpha: float = 0.0, dc_state: torch.Tensor
                                 float(dc_alpha), _ptr(dc_state), _stream(stream))
     _check(int(got), "gpu_unpack")
     return out[:got]
+
+
+def block_mean(raw: torch.Tensor, fmt, offset: complex = 0j, mean: torch.Tensor | None = None,
+               stream=None) -> torch.Tensor:
+    """atkdsp_gpu_block_mean: the unpack_dc mean of a raw block, (2,) float64."""
+    if mean is None:
+        mean = torch.empty(2, dtype=torch.float64, device=raw.device)
+    _check(int(load().atkdsp_gpu_block_mean(_ptr(raw), raw.numel() * raw.element_size(), _fmt(fmt),
+                                            float(offset.real), float(offset.imag), _ptr(mean),
+                                            _stream(stream))), "gpu_block_mean")
+    return mean
+
+
+def accumulate(out: torch.Tensor, nel: int, nchan: int, R: torch.Tensor | None,
+               counts: torch.Tensor | None, pwr: torch.Tensor | None = None,
+               mean_pwr: torch.Tensor | None = None, gate: torch.Tensor | None = None,
+               stream=None) -> None:
+    """atkdsp_gpu_pfb_accumulate: W1 and W2 in one pass over a device block."""
+    m = out.shape[-1] if out.dim() == 3 else 0
+    _check(load().atkdsp_gpu_pfb_accumulate(_ptr(out), int(nel), int(nchan), m, _ptr(gate), _ptr(R),
+                                            _ptr(counts), _ptr(pwr), _ptr(mean_pwr), _stream(stream)),
+           "gpu_pfb_accumulate")
 
 
 def cov_accumulate(out: torch.Tensor, nel: int, nchan: int, gate: torch.Tensor | None,

@@ -65,20 +65,29 @@ def _specs(rank: int, args=None):
 
 # ---------------------------------------------------------------- clocks
 class Clocks:
-    """nvidia-smi sampling during the timed region (200 ms period)."""
+    """nvidia-smi sampling (20 ms period) around the timed region; mark() the
+    region's start and end, summary() keeps the samples taken inside it (or,
+    when the region is shorter than a few periods, the nearest ones)."""
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.lines = []
+        self.t0 = self.t1 = None
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
 
     def __enter__(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -88,7 +97,7 @@ class Clocks:
 
     def _read(self):
         for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
+            self.lines.append((time.time(), ln.strip()))
 
     def __exit__(self, *exc):
         if self.proc:
@@ -102,22 +111,30 @@ class Clocks:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        rows = []
+        for t, ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
-            if len(f) < 8:
-                continue
+            if len(f) >= 9:
+                rows.append((t, f))
+        if self.t0 is not None and self.t1 is not None:
+            inside = [r for r in rows if self.t0 <= r[0] <= self.t1 + 0.02]
+            if len(inside) < 3:           # a short region: the samples nearest to it
+                mid = 0.5 * (self.t0 + self.t1)
+                inside = sorted(rows, key=lambda r: abs(r[0] - mid))[:3]
+            rows = inside
+        for t, f in rows:
             try:
-                sm.append(float(f[0]))
-                mx = float(f[1])
+                sm.append(float(f[1]))
+                mx = float(f[2])
             except ValueError:
                 continue
-            for nm, v in zip(names, f[4:8]):
+            for nm, v in zip(names, f[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "period_ms": 20}
 
 
 # ------------------------------------------------------------ device inputs
@@ -306,6 +323,175 @@ def _dropin_arm(specs, sets, barrier, max_over_ranks):
     return t
 
 
+# --------------------------------------------------- the other configurations
+def _c1_arm(torch):
+    """Single stream, M=64 critically sampled, 16 taps/branch, beta 8, 2^20 cf32
+    samples fed in blocks 1, 999, 4096, 7 (cycling) through the drop-in C ABI
+    with host buffers -- each call is synchronous, so this measures per-call
+    latency as much as the kernel."""
+    import atkdsp_b200 as ak
+    from atkdsp_b200 import workloads as W
+    x = W.single_stream(1 << 20)
+    blocks = W.SINGLE_STREAM_BLOCKS
+    p = ak.Pfb(FS, 64, 1, 16, W.ATTEN_BETA8, 1)
+    p.process(x[:5000])
+    p.reset()
+    t0 = time.perf_counter()
+    pos, i, calls = 0, 0, 0
+    while pos < x.size:
+        b = blocks[i % len(blocks)]
+        p.process(x[pos:pos + b])
+        pos += b
+        i += 1
+        calls += 1
+    dt = time.perf_counter() - t0
+    return {"workload": "single_stream_m64_blocks_1_999_4096_7", "value": round(x.size / dt / 1e6, 2),
+            "unit": "MSamples/s", "calls": calls, "us_per_call": round(dt / calls * 1e6, 2),
+            "path": "atkdsp_pfb_process (host buffers)"}
+
+
+def _c2_arm(torch, device, steps):
+    """40 MS/s front end: ci16q11 with noise + 8 tones + a constant DC offset,
+    2,000,000-sample (50 ms) blocks; per block the running DC estimate (the
+    previous block's mean) is the offset, the filterbank (M=1024, 2x, 12 taps)
+    reads the raw int16 and converts in its load path, W1 and W2 accumulate in
+    one pass. Inputs resident on the device."""
+    import atkdsp_b200 as ak
+    from atkdsp_b200 import gpu
+    from atkdsp_b200 import workloads as W
+    blk = 2_000_000
+    nblk = (1 << 26) // blk
+    g = torch.Generator(device=device)
+    g.manual_seed(2)
+    n = nblk * blk
+    t = torch.arange(n, device=device, dtype=torch.float64)
+    sig = torch.randn(n, dtype=torch.complex128, device=device, generator=g) * 64.0
+    rng = np.random.default_rng(2)
+    for f, ph in zip(rng.uniform(-0.5, 0.5, 8), rng.uniform(0, 2 * math.pi, 8)):
+        sig += 202.0 * torch.exp(1j * (2 * math.pi * f * t + ph))
+    sig += complex(*W.FRONT_END_DC_LSB)
+    raw = torch.stack([sig.real.round(), sig.imag.round()], dim=1).clamp(-2048, 2047).to(torch.int16)
+    del sig, t
+    p = ak.Pfb(FS, 1024, 2, 12, 80.0, 1)
+    m_max = blk // 512 + 1
+    out = torch.empty(1024 * m_max, dtype=torch.complex64, device=device)
+    R = torch.zeros((1024, 1, 1), dtype=torch.complex64, device=device)
+    cnt = torch.zeros(1024, dtype=torch.int32, device=device)
+    pwr = torch.zeros((1, 1024), dtype=torch.float32, device=device)
+    mp = torch.zeros(1024, dtype=torch.float32, device=device)
+    mean = torch.zeros(2, dtype=torch.float64, device=device)
+    st = torch.cuda.ExternalStream(ak.load().atkdsp_gpu_pfb_stream(p.handle), device=device)
+    off = [0j]
+
+    def block(b):
+        r = raw[(b % nblk) * blk:(b % nblk + 1) * blk].reshape(-1)
+        gpu.block_mean(r, "ci16q11", off[0], mean, stream=st)
+        y = gpu.process_n_raw(p, [r], 1, "ci16q11", off[0], out=out, stream=st)
+        gpu.accumulate(y, 1, 1024, R, cnt, pwr, mp, stream=st)
+        mh = mean.cpu().numpy()              # the next block's offset (a 16-byte read)
+        off[0] = complex(np.float32(mh[0]), np.float32(mh[1]))
+
+    for b in range(3):
+        block(b)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(st)
+    nb = max(steps, 1) * nblk
+    for b in range(nb):
+        block(b)
+    ev1.record(st)
+    torch.cuda.synchronize()
+    dt = ev0.elapsed_time(ev1) / 1e3
+    return {"workload": "front_end_ci16q11_m1024_os2_k12_blocks_2e6", "value": round(nb * blk / dt / 1e6, 2),
+            "unit": "MSamples/s", "x_real_time_at_40msps": round(nb * blk / dt / 40e6, 1),
+            "bytes_per_sample": 4 + 4 + 16 + 16,
+            "path": "block_mean + fused unpack/filterbank + one-pass W1/W2, per 50 ms block"}
+
+
+def _c3_arm(torch, device, steps):
+    """Coherent array: 8 cf32 element streams, M=2048, 1x, 16 taps, 2^24 samples
+    each, 4 common tones with per-element phases + noise at 10 dB; one
+    process_n call per step, then W1 (8x8 per channel) and W2 in one pass."""
+    import atkdsp_b200 as ak
+    from atkdsp_b200 import gpu
+    from atkdsp_b200 import workloads as W
+    nel, n = 8, 1 << 24
+    g = torch.Generator(device=device)
+    g.manual_seed(3)
+    rng = np.random.default_rng(3)
+    freqs = rng.uniform(-0.5, 0.5, 4)
+    t = torch.arange(n, device=device, dtype=torch.float64)
+    xs = []
+    for e in range(nel):
+        x = torch.randn(n, dtype=torch.complex64, device=device, generator=g)
+        for f, ph in zip(freqs, rng.uniform(0, 2 * math.pi, 4)):
+            x += (math.sqrt(10.0) * torch.exp(1j * (2 * math.pi * f * t + ph))).to(torch.complex64)
+        xs.append(x)
+    del t
+    p = ak.Pfb(FS, 2048, 1, 16, W.ATTEN_BETA8, nel)
+    m = n // 2048 + 1
+    out = torch.empty(nel * 2048 * m, dtype=torch.complex64, device=device)
+    R = torch.zeros((2048, nel, nel), dtype=torch.complex64, device=device)
+    cnt = torch.zeros(2048, dtype=torch.int32, device=device)
+    pwr = torch.zeros((nel, 2048), dtype=torch.float32, device=device)
+    mp = torch.zeros(2048, dtype=torch.float32, device=device)
+    st = torch.cuda.ExternalStream(ak.load().atkdsp_gpu_pfb_stream(p.handle), device=device)
+
+    def step():
+        y = gpu.process_n(p, xs, nel, out=out, stream=st)
+        gpu.accumulate(y, nel, 2048, R, cnt, pwr, mp, stream=st)
+
+    step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(st)
+    for _ in range(max(steps, 1)):
+        step()
+    ev1.record(st)
+    torch.cuda.synchronize()
+    dt = ev0.elapsed_time(ev1) / 1e3
+    return {"workload": "coherent_8el_m2048_os1_k16_2^24", "value": round(nel * n * max(steps, 1) / dt / 1e6, 2),
+            "unit": "MSamples/s (aggregate over elements)", "path": "process_n (device) + one-pass W1/W2"}
+
+
+def _served_arm(torch, device, duration_s):
+    """Serving: 4096 live streams at {2.4, 10, 40} MS/s delivering 1.6 ms ci16
+    blocks with Poisson arrivals, nchan {256, 1024}, 16 taps, 2x, churn 20/s,
+    admission by free HBM. Then the largest stream count whose p99 block
+    latency stays under 1.6 ms."""
+    from atkdsp_b200.serve import Server, simulate
+    srv = Server(max_streams=4608, hbm_reserve=16 << 30, use_graph=True)
+    raw = torch.randint(-6000, 6000, (2 * (8 << 20),), dtype=torch.int16, device=device)
+    out = torch.empty((2 << 30) // 8, dtype=torch.complex64, device=device)
+    full = simulate(srv, streams=4096, duration_s=duration_s, warmup_s=0.5, raw_pool=raw, out_pool=out)
+    res = {"workload": "served_4096_streams_ci16_m256_1024_k16", "offered_msps": round(full["offered_samples_per_s"] / 1e6, 1),
+           "value": round(full["samples_done"] / full["wall_s"] / 1e6, 2), "unit": "MSamples/s",
+           "p50_ms": round(full["lat_p50_ms"], 3), "p99_ms": round(full["lat_p99_ms"], 3),
+           "blocks_per_round": round(full["blocks_per_round"], 1), "dropped_blocks": int(full["dropped_blocks"]),
+           "denied": int(full["denied"]), "churn_events": int(full["churn_events"])}
+    best = None
+    lo, hi = 64, 4096
+    if full["lat_p99_ms"] < 1.6:
+        best = (4096, full)
+    else:
+        while hi - lo > 64:
+            mid = (lo + hi) // 2
+            srv2 = Server(max_streams=mid + 512, hbm_reserve=16 << 30, use_graph=True)
+            r = simulate(srv2, streams=mid, duration_s=max(1.0, duration_s / 2), warmup_s=0.3, raw_pool=raw,
+                         out_pool=out)
+            del srv2
+            if r["lat_p99_ms"] < 1.6 and r["dropped_blocks"] == 0:
+                lo, best = mid, (mid, r)
+            else:
+                hi = mid
+    if best:
+        n, r = best
+        res["within_p99_1.6ms"] = {"streams": n, "value": round(r["samples_done"] / r["wall_s"] / 1e6, 2),
+                                   "p50_ms": round(r["lat_p50_ms"], 3), "p99_ms": round(r["lat_p99_ms"], 3)}
+    return res
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -346,14 +532,18 @@ def run_ours(args, rank, world, local_rank):
         bstep(k)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    torch.cuda.synchronize()
     with Clocks(local_rank) as clk:
+        time.sleep(0.3)                      # let the sampler start
+        barrier()
+        torch.cuda.synchronize()
+        clk.mark_start()
         ev0.record(bstream)
         for k in range(args.steps):
             bstep(args.warmup + k)
         ev1.record(bstream)
         torch.cuda.synchronize()
+        clk.mark_end()
+        time.sleep(0.05)
     barrier()
     t_batch = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     alg = _alg_bytes(specs, ms_list)
@@ -366,6 +556,7 @@ def run_ours(args, rank, world, local_rank):
 
     t_plain = t_e2e = t_dropin = None
     out_bytes = 8 * sum(s.nchan * m for s, m in zip(specs, ms_list))
+    extra = {}
     if "plain" in arms:
         t_plain = _plain_arm(args, specs, sets, outs, torch, device, barrier, max_over_ranks)
     if "e2e" in arms:
@@ -375,6 +566,18 @@ def run_ours(args, rank, world, local_rank):
 
     del batch, handles, bstream
     torch.cuda.synchronize()
+    if rank == 0:
+        for name, fn in (("single_stream", lambda: _c1_arm(torch)),
+                         ("front_end", lambda: _c2_arm(torch, device, 1)),
+                         ("coherent_array", lambda: _c3_arm(torch, device, args.steps)),
+                         ("served", lambda: _served_arm(torch, device, 3.0))):
+            if name in arms:
+                try:
+                    extra[name] = fn()
+                except Exception as e:                       # report, keep the headline
+                    extra[name] = {"error": f"{type(e).__name__}: {e}"}
+                torch.cuda.synchronize()
+                torch.cuda.empty_cache()
     if rank != 0:
         return
     peak, peak_kind = _peaks()
@@ -411,6 +614,7 @@ def run_ours(args, rank, world, local_rank):
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "kernel": "pfb_tiles_kernel", "kernel_ms": round(k_ms, 4),
                      "alg_bytes_per_launch": alg, "peak_kind": peak_kind},
+        "configs": extra,
         "gpu_launches": 2 * args.steps,
         "clocks": clk.summary(),
     }
@@ -427,7 +631,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--arms", default="batched,plain,e2e,dropin,cpu",
+    ap.add_argument("--arms", default="batched,plain,e2e,dropin,cpu,single_stream,front_end,coherent_array,served",
                     help="comma list of arms to run (the batched arm always runs)")
     ap.add_argument("--streams", type=int, default=256)
     ap.add_argument("--min-log2", type=float, default=14.0)

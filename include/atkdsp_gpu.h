@@ -73,6 +73,13 @@ ATKDSP_API ptrdiff_t   atkdsp_gpu_unpack_dc_noalloc(const void *d_raw, size_t nb
                                                     atkdsp_cf32 *d_out, size_t out_cap,
                                                     float off_re, float off_im, double *d_mean,
                                                     void *stream);
+/* The mean that atkdsp_unpack_dc (reference include/atkdsp.h:270) returns --
+ * of the samples before the offset (off_re, off_im) is taken out -- without
+ * writing the samples: for a caller whose filterbank reads the raw samples
+ * (atkdsp_gpu_pfb_process_n_raw) and who keeps a running DC estimate. d_mean
+ * receives 2 doubles (device). Returns the sample count. */
+ATKDSP_API ptrdiff_t   atkdsp_gpu_block_mean(const void *d_raw, size_t nbytes, int fmt, float off_re,
+                                             float off_im, double *d_mean, void *stream);
 /* atkdsp_unpack (reference include/atkdsp.h:252) on device buffers;
  * d_dc_state is one device cf32, read and updated when dc_alpha > 0. */
 ATKDSP_API ptrdiff_t   atkdsp_gpu_unpack(const void *d_raw, size_t nbytes, int fmt,
@@ -84,6 +91,13 @@ ATKDSP_API int         atkdsp_gpu_pfb_cov_accumulate(const atkdsp_cf32 *d_out, u
                                                      unsigned nchan, size_t m,
                                                      const uint8_t *d_gate, atkdsp_cf32 *d_R,
                                                      uint32_t *d_counts, void *stream);
+/* W1 and W2 (reference include/atkdsp.h:3239-3251) in ONE pass over the
+ * block: R/counts as atkdsp_pfb_cov_accumulate (both NULL to skip W1),
+ * pwr/mean_pwr as atkdsp_pfb_channel_power (either may be NULL). */
+ATKDSP_API int         atkdsp_gpu_pfb_accumulate(const atkdsp_cf32 *d_out, unsigned nel, unsigned nchan,
+                                                 size_t m, const uint8_t *d_gate, atkdsp_cf32 *d_R,
+                                                 uint32_t *d_counts, float *d_pwr, float *d_mean_pwr,
+                                                 void *stream);
 ATKDSP_API int         atkdsp_gpu_pfb_cov_reset(atkdsp_cf32 *d_R, uint32_t *d_counts,
                                                 unsigned nel, unsigned nchan,
                                                 const uint8_t *d_gate, void *stream);

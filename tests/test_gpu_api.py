@@ -126,3 +126,25 @@ def test_batch_raw_equals_each_stream_alone():
             x, _ = ak.unpack_dc(raws[i].tobytes(), "ci16", offs[i])
             y = alone[i].process(x)
             assert np.array_equal(y, outs[i][: s.nchan * ms[i]].view(s.nchan, ms[i]).cpu().numpy()), i
+
+
+def test_block_mean_and_one_pass_accumulate():
+    from atkdsp_b200 import gpu
+    raw = W.front_end_raw(123_457, seed=9)
+    for off in (0j, 0.05 - 0.03j):
+        _, mh = ak.unpack_dc(raw.tobytes(), "ci16q11", off)
+        md = gpu.block_mean(_dev(raw.reshape(-1)), "ci16q11", off).cpu().numpy()
+        assert complex(*md) == mh
+    rng = np.random.default_rng(4)
+    y = (rng.standard_normal((3, 128, 77)) + 1j * rng.standard_normal((3, 128, 77))).astype(np.complex64)
+    R = np.zeros((128, 3, 3), np.complex64)
+    c = np.zeros(128, np.uint32)
+    ak.pfb_cov_accumulate(y, 3, 128, None, R, c)
+    p1, m1 = ak.pfb_channel_power(y, 3, 128)
+    Rd = torch.zeros((128, 3, 3), dtype=torch.complex64, device="cuda")
+    cd = torch.zeros(128, dtype=torch.int32, device="cuda")
+    pd = torch.zeros((3, 128), dtype=torch.float32, device="cuda")
+    md = torch.zeros(128, dtype=torch.float32, device="cuda")
+    gpu.accumulate(_dev(y), 3, 128, Rd, cd, pd, md)
+    assert np.array_equal(R, Rd.cpu().numpy()) and np.array_equal(c.astype(np.int32), cd.cpu().numpy())
+    assert np.array_equal(p1, pd.cpu().numpy()) and np.array_equal(m1, md.cpu().numpy())
