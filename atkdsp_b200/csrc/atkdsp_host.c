@@ -132,12 +132,17 @@ static void design_prototype(unsigned nchan, unsigned K, double atten_db, double
 /* ================================================================== FFT plan */
 static int is_pow2(unsigned v) { return v && !(v & (v - 1)); }
 
-static int plan_fft(unsigned M, atkb_fft_plan *pl) {
+static int plan_fft(unsigned M, unsigned os, atkb_fft_plan *pl) {
     memset(pl, 0, sizeof *pl);
     if (is_pow2(M) && M >= 16 && M <= MAX_POW2_NCHAN) {
-        unsigned rem = M / ATKB_PTS;
+        /* the paired fold: hop b's window is hop a's shifted by 8/os branch
+         * slots, so os must divide 4 (M/os a multiple of 2*M/8); a tile must
+         * hold two hops (M <= 2048) */
+        const int pair = ATKB_PTS == 8 && M <= 2048 && (os == 1 || os == 2 || os == 4);
+        unsigned rem = M / (pair ? 4 : ATKB_PTS);
         pl->fast = 1;
-        pl->radix[pl->npass++] = ATKB_PTS;
+        pl->pair = pair;
+        pl->radix[pl->npass++] = pair ? 4 : ATKB_PTS;
         while (rem >= ATKB_PTS) { pl->radix[pl->npass++] = ATKB_PTS; rem /= ATKB_PTS; }
         if (rem > 1) pl->radix[pl->npass++] = (int)rem;
     } else {
@@ -245,7 +250,7 @@ static int bank_build(bank_entry *be, void *stream) {
     const unsigned M = be->nchan;
     const size_t L = (size_t)M * be->K;
     atkb_fft_plan pl;
-    if (plan_fft(M, &pl) != 0) return ATKB_E_ARG;
+    if (plan_fft(M, be->os, &pl) != 0) return ATKB_E_ARG;
     const size_t taps_b = align16(L * sizeof(float));
     const size_t tab_b = (size_t)M * 2 * sizeof(double);
     const size_t pass_b = (size_t)pl.twlen * 2 * sizeof(double);
@@ -263,13 +268,17 @@ static int bank_build(bank_entry *be, void *stream) {
     unsigned j;
     for (q = 0; q < L; ++q) taps[q] = (float)proto[q];
     if (pl.fast) {
-        /* tapsP[(k*MP + j)*P + r] = taps[k*M + j + r*MP], MP = M/P */
+        /* float4 g = (k*(P/4) + q)*MP + j, component i, holds the tap of
+         * branch j + r*MP, r = 4q + i (paired: r = q + 2i), MP = M/P */
         const size_t P = ATKB_PTS, MP = M / ATKB_PTS;
-        size_t k2, jj, r;
+        size_t k2, q2, jj, i;
         for (k2 = 0; k2 < be->K; ++k2)
-            for (jj = 0; jj < MP; ++jj)
-                for (r = 0; r < P; ++r)
-                    tapsP[(k2 * MP + jj) * P + r] = taps[k2 * M + jj + r * MP];
+            for (q2 = 0; q2 < P / 4; ++q2)
+                for (jj = 0; jj < MP; ++jj)
+                    for (i = 0; i < 4; ++i) {
+                        const size_t r = pl.pair ? q2 + 2 * i : 4 * q2 + i;
+                        tapsP[((k2 * (P / 4) + q2) * MP + jj) * 4 + i] = taps[k2 * M + jj + r * MP];
+                    }
     }
     for (j = 0; j < M; ++j) {
         /* the reference's rotation table, channelizer.c:164-170 */

@@ -27,8 +27,10 @@ extern "C" {
 
 /* ---- FFT plan --------------------------------------------------------------
  * nchan = radix[0] * radix[1] * ... * radix[npass-1], Stockham order. For a
- * power of two >= 16 the fast path is used: radix[0] == ATKB_PTS and every
- * later radix is ATKB_PTS except a smaller last one. */
+ * power of two >= 16 the fast path is used: radix[0] == ATKB_PTS (4 when
+ * `pair` is set) and every later radix is ATKB_PTS except a smaller last one.
+ * `pair`: the paired fold (two consecutive hops per thread, even or odd
+ * branches), used for oversample 1, 2 or 4 and nchan <= 2048. */
 #define ATKB_MAX_PASS 24
 /* complex points per thread in the fast path's Stockham passes (8 or 16);
  * the host's plan and permuted taps follow it */
@@ -38,6 +40,7 @@ extern "C" {
 typedef struct {
     int npass;
     int fast;                     /* 1: power-of-two fast path */
+    int pair;                     /* 1: paired fold, first radix 4             */
     int radix[ATKB_MAX_PASS];
     int twoff[ATKB_MAX_PASS];     /* offset of pass p's twiddles in the table */
     int twlen;                    /* total twiddle entries (double2)          */
@@ -48,9 +51,13 @@ typedef struct {
     int nchan, os, K, hop;
     long long L, ov;
     const float *taps;            /* device: L floats, (float)h[q]            */
-    const float *tapsP;           /* device: fast path, taps permuted so the P
-                                   * branches j + r*nchan/P of tap k are the P
-                                   * floats at ((k*nchan/P + j)*P + r), P = ATKB_PTS */
+    const float *tapsP;           /* device: fast path, taps permuted for float4
+                                   * loads that are contiguous across a warp's
+                                   * branches j (MP = nchan/ATKB_PTS):
+                                   * float4 (k*(P/4) + q)*MP + j holds the taps
+                                   * k*nchan + j + r*MP, r = 4q .. 4q+3; paired:
+                                   * float4 (2k + c)*MP + j holds r = c + 2i,
+                                   * i = 0..3 */
     const void *twd;              /* device: nchan double2 (cos, sin)(2 pi j/nchan) */
     const void *wfull;            /* device: nchan double2 W^j = (cos, -sin)  */
     const void *wpass;            /* device: per-pass twiddles (fast path)    */

@@ -206,18 +206,6 @@ __device__ __forceinline__ void pass_c(double2 *sm, const double2 *__restrict__ 
     __syncthreads();
 }
 
-/* passes P .. PEND-1 of the power-of-two plan: radix PTS while at least
- * LOGP index bits remain, then one last smaller radix */
-template <int LOGM, int P, int PEND>
-__device__ __forceinline__ void passes_from(double2 *sm, const double2 *wp, const int *twoff) {
-    if constexpr (P < PEND) {
-        constexpr int REM = LOGM - LOGP * P;
-        constexpr int R = REM >= LOGP ? PTS : (1 << REM);
-        pass_c<LOGM, R, LOGP * P>(sm, wp + twoff[P]);
-        passes_from<LOGM, P + 1, PEND>(sm, wp, twoff);
-    }
-}
-
 /* Rotation to input sample 0 and cal for bin kb of a hop whose (b + 1) mod os
  * is s, then one rounding to float (reference src/channelizer.c:270-292). */
 __device__ __forceinline__ float2 finish_bin(double2 X, int kb, int s, int M, int os, int hop,
@@ -281,7 +269,8 @@ __device__ __forceinline__ void pass_last(double2 *sm, const double2 *__restrict
 
 /* The fold of one hop's PTS branches q = j + r*M/PTS (r < PTS), straight
  * into the registers of the first radix-PTS butterfly. Taps come from the
- * bank's permuted copy (PTS consecutive floats per (k, j): 16-byte loads).
+ * bank's permuted copy: float4 loads whose addresses are consecutive across
+ * the lanes (branches j) of a warp.
  * MODE 0: the tile's windows lie wholly in one cf32 buffer, read through
  * `lin` (offset to this thread's first sample); MODE 1: the same in raw int16
  * I/Q converted on the fly; MODE 2: each sample from the state or the input
@@ -291,7 +280,7 @@ __device__ __forceinline__ void foldP(double2 *v, const atkb_job &J, const atkb_
                                       long long h0, int tt, int j, const void *lin) {
     constexpr int M = 1 << LOGM;
     constexpr int MP = M >> LOGP;
-    const float4 *tq = (const float4 *)B.tapsP + (size_t)j * (PTS / 4);
+    const float4 *tq = (const float4 *)B.tapsP + j;
     float fr[PTS], fi[PTS];
     const float2 *xk = (const float2 *)lin;
     const short2 *xk16 = (const short2 *)lin;
@@ -300,7 +289,7 @@ __device__ __forceinline__ void foldP(double2 *v, const atkb_job &J, const atkb_
     const long long base = (h0 + tt) * (long long)B.hop + j;
 #pragma unroll
     for (int q = 0; q < PTS / 4; ++q) {
-        const float4 h = __ldg(tq + q);
+        const float4 h = __ldg(tq + q * MP);
         const float hh[4] = {h.x, h.y, h.z, h.w};
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
@@ -318,7 +307,7 @@ __device__ __forceinline__ void foldP(double2 *v, const atkb_job &J, const atkb_
         xk16 += M;
 #pragma unroll
         for (int q = 0; q < PTS / 4; ++q) {
-            const float4 h = __ldg(tq + q);
+            const float4 h = __ldg(tq + q * MP);
             const float hh[4] = {h.x, h.y, h.z, h.w};
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
@@ -361,11 +350,11 @@ __device__ __forceinline__ void foldP_staged(double2 *v, const atkb_bank &B, int
     constexpr int HOP = M >> LOGOS;
     /* logical tt*hop + k*M + j + r*MP  ->  physical, with (i / hop) = tt + k*os + (r*os)/PTS */
     const float2 *xb = xs + tt * (HOP + MP) + j;
-    const float4 *tq = (const float4 *)B.tapsP + (size_t)j * (PTS / 4);
+    const float4 *tq = (const float4 *)B.tapsP + j;
     float fr[PTS], fi[PTS];
 #pragma unroll
     for (int q = 0; q < PTS / 4; ++q) {
-        const float4 h = __ldg(tq + q);
+        const float4 h = __ldg(tq + q * MP);
         const float hh[4] = {h.x, h.y, h.z, h.w};
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
@@ -380,7 +369,7 @@ __device__ __forceinline__ void foldP_staged(double2 *v, const atkb_bank &B, int
         xb += M + OS * MP;
 #pragma unroll
         for (int q = 0; q < PTS / 4; ++q) {
-            const float4 h = __ldg(tq + q);
+            const float4 h = __ldg(tq + q * MP);
             const float hh[4] = {h.x, h.y, h.z, h.w};
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
@@ -439,51 +428,237 @@ __device__ __forceinline__ bool fold_tile_staged(double2 *v, const atkb_job &J, 
     }
 }
 
+/* ---- the paired fold: oversample 1, 2 or 4, nchan <= 2048 -------------------
+ * Thread (pair p, parity c, branch j) folds hops ta = 2p and tb = 2p + 1 of
+ * the tile over the four branches j + r*MP with r = c + 2i, i = 0..3
+ * (MP = M/8). Slot u = 8k + r of hop ta's window (sample u*MP + j, tap
+ * k*M + r*MP + j) is slot u - 8/os of hop tb's: every sample the thread loads
+ * feeds both hops, and each float4 of taps (row k, parity c) serves hop ta in
+ * row k and hop tb in rows k and k + 1. Against one hop and eight branches per
+ * thread this halves the loads of samples and taps per output. Slots stream in
+ * ascending order, so every branch still sums its taps k ascending; the sums
+ * start from -0.0f, and -0 + p == p for every p, so the first product enters
+ * unchanged as in the reference's loop. */
+__device__ __forceinline__ void mac(float2 &a, float h, float2 x) {
+    a.x = __fadd_rn(a.x, __fmul_rn(h, x.x));
+    a.y = __fadd_rn(a.y, __fmul_rn(h, x.y));
+}
+
+/* sample loaders: at(k, i) is slot 8k + c + 2i of hop ta's window */
 template <int LOGM>
+struct PairLin {                       /* cf32, the tile's windows in one buffer */
+    const float2 *p;
+    __device__ __forceinline__ float2 at(int k, int i) const {
+        return __ldg(p + ((long long)k << LOGM) + 2 * i * (1 << (LOGM - LOGP)));
+    }
+};
+template <int LOGM>
+struct PairLin16 {                     /* raw int16 I/Q, converted on the fly */
+    const short2 *p;
+    float cre, cim, ks;
+    __device__ __forceinline__ float2 at(int k, int i) const {
+        return conv16(__ldg(p + ((long long)k << LOGM) + 2 * i * (1 << (LOGM - LOGP))), cre, cim, ks);
+    }
+};
+template <int LOGM>
+struct PairMixed {                     /* state / input by index */
+    Src src;
+    long long g;
+    __device__ __forceinline__ float2 at(int k, int i) const {
+        return src.at(g + ((long long)k << LOGM) + 2 * i * (1 << (LOGM - LOGP)));
+    }
+};
+template <int LOGM, int LOGOS>
+struct PairStaged {                    /* the padded shared-memory window */
+    const float2 *p;                   /* at slot c of hop ta, row 0 */
+    __device__ __forceinline__ float2 at(int k, int i) const {
+        constexpr int MP = 1 << (LOGM - LOGP);
+        constexpr int LOGD = 3 - LOGOS;             /* slot shift 8/os = 2^LOGD */
+        return p[k * ((1 << LOGM) + (MP << LOGOS)) + (2 * i + (i >> (LOGD - 1))) * MP];
+    }
+};
+
+template <int LOGM, int LOGOS, class LD>
+__device__ __forceinline__ void fold_pair(float2 (&a)[4], float2 (&b)[4], const float4 *tq, int K,
+                                          bool tb_ok, const LD &ld) {
+    constexpr int MP = 1 << (LOGM - LOGP);
+    constexpr int D2 = 4 >> LOGOS;     /* hop tb's taps trail hop ta's by D2 entries */
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        a[i] = make_float2(-0.0f, -0.0f);
+        b[i] = make_float2(-0.0f, -0.0f);
+    }
+    float4 pv = __ldg(tq);
+    {
+        const float h[4] = {pv.x, pv.y, pv.z, pv.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 x = ld.at(0, i);
+            mac(a[i], h[i], x);
+            if (i >= D2) mac(b[i - D2], h[i - D2], x);
+        }
+    }
+    for (int k = 1; k < K; ++k) {
+        const float4 cv = __ldg(tq + k * 2 * MP);
+        const float h[4] = {cv.x, cv.y, cv.z, cv.w};
+        const float g[4] = {pv.x, pv.y, pv.z, pv.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 x = ld.at(k, i);
+            mac(a[i], h[i], x);
+            if (i >= D2) mac(b[i - D2], h[i - D2], x);
+            else mac(b[i - D2 + 4], g[i - D2 + 4], x);
+        }
+        pv = cv;
+    }
+    if (tb_ok) {                       /* the slots past hop ta's window */
+        const float g[4] = {pv.x, pv.y, pv.z, pv.w};
+#pragma unroll
+        for (int i = 0; i < D2; ++i) mac(b[i - D2 + 4], g[i - D2 + 4], ld.at(K, i));
+    }
+}
+
+/* radix-4 first pass (Ns = 1) of one hop's four even or odd branches:
+ * branch j + (c + 2i)*MP is point jp + i*M/4 of the hop, jp = j + c*MP */
+template <int LOGM>
+__device__ __forceinline__ void first_pass4(const float2 (&f)[4], double2 *sm, int t, int jp) {
+    double2 v[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = make_double2((double)f[i].x, (double)f[i].y);
+    dft4(v[0], v[1], v[2], v[3]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) sm[SW((t << LOGM) + jp * 4 + i)] = v[i];
+}
+
+template <int LOGM, int LOGOS>
+__device__ __forceinline__ void fold_tile_pair(const atkb_job &J, const atkb_bank &B, long long h0,
+                                               int nvalid, double2 *sm) {
+    constexpr int M = 1 << LOGM;
+    constexpr int LOGMP = LOGM - LOGP;
+    constexpr int MP = 1 << LOGMP;
+    constexpr int HOP = M >> LOGOS;
+    const int tid = threadIdx.x;
+    const int j = tid & (MP - 1);
+    const int c = (tid >> LOGMP) & 1;
+    const int ta = (tid >> (LOGMP + 1)) * 2;
+    const bool ta_ok = ta < nvalid, tb_ok = ta + 1 < nvalid;
+    const float4 *tq = (const float4 *)B.tapsP + c * MP + j;
+    float2 a[4], b[4];
+    if constexpr (LOGM <= 9) {
+        /* small nchan: the whole tile window through shared memory (as in
+         * fold_tile_staged; logical sample i at i + (i / hop) * MP) */
+        const long long Wl = (long long)(nvalid - 1) * HOP + B.L;
+        if (!J.in_kind && Wl <= 8192 && staged_size((int)Wl, LOGM - LOGOS, MP) <= 8192) {
+            float2 *xs = (float2 *)sm;
+            stage_window(xs, J, h0 * (long long)HOP, (int)Wl, LOGM - LOGOS, MP);
+            if (ta_ok) {
+                const PairStaged<LOGM, LOGOS> ld{xs + ta * (HOP + MP) + j + c * MP};
+                fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = b[i] = make_float2(0.0f, 0.0f);
+            }
+            __syncthreads();          /* the window is dead; sm becomes the FFT tile */
+            /* the first pass inside this branch: merging the sums of both
+             * branches ahead of one first pass cost ~1 KB of spills */
+            first_pass4<LOGM>(a, sm, ta, j + c * MP);
+            first_pass4<LOGM>(b, sm, ta + 1, j + c * MP);
+            return;
+        }
+    }
+    if (ta_ok) {
+        const long long w0 = h0 * (long long)HOP;
+        const long long w1 = (h0 + nvalid - 1) * (long long)HOP + B.L;
+        const long long off = (h0 + ta) * (long long)HOP + c * MP + j;
+        if (w0 >= J.head) {
+            if (J.in_kind) {
+                const PairLin16<LOGM> ld{(const short2 *)J.in + (off - J.head), J.cre, J.cim, J.kscale};
+                fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
+            } else {
+                const PairLin<LOGM> ld{(const float2 *)J.in + (off - J.head)};
+                fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
+            }
+        } else if (w1 <= J.head) {
+            const PairLin<LOGM> ld{(const float2 *)J.state + off};
+            fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
+        } else {
+            const PairMixed<LOGM> ld{Src{(const float2 *)J.state, J.in, J.head, J.in_kind, J.cre, J.cim,
+                                         J.kscale},
+                                     off};
+            fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
+        }
+    }
+    if (!ta_ok) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = b[i] = make_float2(0.0f, 0.0f);
+    }
+    first_pass4<LOGM>(a, sm, ta, j + c * MP);
+    first_pass4<LOGM>(b, sm, ta + 1, j + c * MP);
+}
+
+/* the Stockham passes after the first (which left Ns = 2^LOGNS): radix PTS
+ * while more than LOGP index bits remain, then the last pass (radix 2, 4 or
+ * 8) fused with the epilogue; P indexes the plan's twiddle offsets */
+template <int LOGM, int LOGNS, int P>
+__device__ __forceinline__ void fft_rest(double2 *sm, const double2 *wp, const int *twoff,
+                                         float2 *tile_out, const atkb_bank &B, const atkb_job &J,
+                                         long long h0) {
+    if constexpr (LOGM - LOGNS > LOGP) {
+        pass_c<LOGM, PTS, LOGNS>(sm, wp + twoff[P]);
+        fft_rest<LOGM, LOGNS + LOGP, P + 1>(sm, wp, twoff, tile_out, B, J, h0);
+    } else {
+        pass_last<LOGM, (1 << (LOGM - LOGNS)), LOGNS>(sm, wp + twoff[P], tile_out, B, J, h0);
+    }
+}
+
+/* LOGOS < 0: one hop and PTS branches per thread, first pass radix PTS;
+ * LOGOS = log2(os) in 0..2: the paired fold, first pass radix 4 */
+template <int LOGM, int LOGOS>
 __device__ void tile_fast(const atkb_job &J, const atkb_bank &B, long long h0, int nvalid,
                           double2 *sm, float2 *tile_out) {
     constexpr int M = 1 << LOGM;
     constexpr int LOGNH = 12 - LOGM;
     constexpr int NH = 1 << LOGNH;
     constexpr int MP = M >> LOGP;
-    constexpr int NPASS = (LOGM + LOGP - 1) / LOGP;
-    static_assert(NPASS >= 2, "the fast path needs nchan > PTS");
+    static_assert(LOGM > LOGP, "the fast path needs nchan > PTS");
     const int tid = threadIdx.x;
-    const int tt = tid >> (LOGM - LOGP);
-    const int j = tid & (MP - 1);
 
-    /* fold + first Stockham pass (Ns = 1, radix PTS, no twiddles) */
-    double2 v[PTS];
-    if (!fold_tile_staged<LOGM>(v, J, B, h0, nvalid, tt, j, sm)) {
-        if (tt < nvalid) {
-            const long long w0 = h0 * (long long)B.hop;                       /* first window start */
-            const long long w1 = (h0 + nvalid - 1) * (long long)B.hop + B.L;  /* last window end */
-            const long long off = (h0 + tt) * (long long)B.hop + j;
-            if (w0 >= J.head) {
-                if (J.in_kind)
-                    foldP<LOGM, 1>(v, J, B, h0, tt, j, (const short2 *)J.in + (off - J.head));
-                else
-                    foldP<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.in + (off - J.head));
-            } else if (w1 <= J.head) {
-                foldP<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.state + off);
+    if constexpr (LOGOS >= 0) {
+        static_assert(PTS == 8 && LOGM <= 11 && LOGOS <= 2, "paired fold: PTS 8, two hops a tile");
+        fold_tile_pair<LOGM, LOGOS>(J, B, h0, nvalid, sm);
+    } else {
+        const int tt = tid >> (LOGM - LOGP);
+        const int j = tid & (MP - 1);
+        /* fold + first Stockham pass (Ns = 1, radix PTS, no twiddles) */
+        double2 v[PTS];
+        if (!fold_tile_staged<LOGM>(v, J, B, h0, nvalid, tt, j, sm)) {
+            if (tt < nvalid) {
+                const long long w0 = h0 * (long long)B.hop;                       /* first window start */
+                const long long w1 = (h0 + nvalid - 1) * (long long)B.hop + B.L;  /* last window end */
+                const long long off = (h0 + tt) * (long long)B.hop + j;
+                if (w0 >= J.head) {
+                    if (J.in_kind)
+                        foldP<LOGM, 1>(v, J, B, h0, tt, j, (const short2 *)J.in + (off - J.head));
+                    else
+                        foldP<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.in + (off - J.head));
+                } else if (w1 <= J.head) {
+                    foldP<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.state + off);
+                } else {
+                    foldP<LOGM, 2>(v, J, B, h0, tt, j, nullptr);
+                }
             } else {
-                foldP<LOGM, 2>(v, J, B, h0, tt, j, nullptr);
+#pragma unroll
+                for (int r = 0; r < PTS; ++r) v[r] = make_double2(0.0, 0.0);
             }
-        } else {
-#pragma unroll
-            for (int r = 0; r < PTS; ++r) v[r] = make_double2(0.0, 0.0);
         }
-    }
-    dftR<PTS>(v);
+        dftR<PTS>(v);
 #pragma unroll
-    for (int r = 0; r < PTS; ++r) sm[SW((tt << LOGM) + j * PTS + r)] = v[r];
+        for (int r = 0; r < PTS; ++r) sm[SW((tt << LOGM) + j * PTS + r)] = v[r];
+    }
     __syncthreads();
 
-    const double2 *wp = (const double2 *)B.wpass;
-    passes_from<LOGM, 1, NPASS - 1>(sm, wp, B.plan.twoff);
-    constexpr int REM = LOGM - LOGP * (NPASS - 1);
-    constexpr int RL = REM >= LOGP ? PTS : (1 << REM);
-    pass_last<LOGM, RL, LOGP * (NPASS - 1)>(sm, wp + B.plan.twoff[NPASS - 1], tile_out, B, J, h0);
+    fft_rest<LOGM, (LOGOS >= 0 ? 2 : LOGP), 1>(sm, (const double2 *)B.wpass, B.plan.twoff, tile_out, B, J,
+                                                h0);
 
     /* write: thread -> (channel kb0 + u*MP, hop t2); runs of NH hops */
     const int t2 = tid & (NH - 1);
@@ -629,16 +804,20 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
         const long long h0 = (long long)s_local * s_bank.tile_hops;
         const long long left = J.hops - h0;
         const int nvalid = (int)(left < s_bank.tile_hops ? left : s_bank.tile_hops);
-        switch (s_bank.plan.fast ? s_bank.logm : 0) {
-        case 4: tile_fast<4>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
-        case 5: tile_fast<5>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
-        case 6: tile_fast<6>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
-        case 7: tile_fast<7>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
-        case 8: tile_fast<8>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
-        case 9: tile_fast<9>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
-        case 10: tile_fast<10>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
-        case 11: tile_fast<11>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
-        case 12: tile_fast<12>(J, s_bank, h0, nvalid, sm, (float2 *)sm); break;
+        const int lm = s_bank.plan.fast ? s_bank.logm : 0;
+        const int key = s_bank.plan.pair ? 16 * (1 + (s_bank.os == 1 ? 0 : s_bank.os == 2 ? 1 : 2)) + lm : lm;
+        float2 *to = (float2 *)sm;
+        switch (key) {
+#define UNPAIRED(L) case L: tile_fast<L, -1>(J, s_bank, h0, nvalid, sm, to); break;
+#define PAIRED(L)                                                              \
+        case 16 + L: tile_fast<L, 0>(J, s_bank, h0, nvalid, sm, to); break;    \
+        case 32 + L: tile_fast<L, 1>(J, s_bank, h0, nvalid, sm, to); break;    \
+        case 48 + L: tile_fast<L, 2>(J, s_bank, h0, nvalid, sm, to); break;
+        UNPAIRED(4) UNPAIRED(5) UNPAIRED(6) UNPAIRED(7) UNPAIRED(8) UNPAIRED(9) UNPAIRED(10)
+        UNPAIRED(11) UNPAIRED(12)
+        PAIRED(4) PAIRED(5) PAIRED(6) PAIRED(7) PAIRED(8) PAIRED(9) PAIRED(10) PAIRED(11)
+#undef UNPAIRED
+#undef PAIRED
         default: tile_generic(J, s_bank, h0, nvalid, sm); break;
         }
         __syncthreads();
