@@ -6,6 +6,12 @@
 #include "atkdsp_gpu.h"
 #include "internal.h"
 
+/* dynamic shared memory of the largest power-of-two (fast path) tile: the
+ * 4096-point double FFT tile plus, for nchan 4096 paired, hop b's 4096 float2
+ * sums. A launch that may meet any fast-path bank (the server's captured
+ * rounds) reserves this much. */
+#define ATKB_FAST_SMEM_MAX (4096 * 16 + 4096 * 8)
+
 /* a device bank shared by every handle with the same (device, nchan,
  * oversample, taps, attenuation): taps, tables and the device atkb_bank */
 typedef struct bank_entry bank_entry;

@@ -30,7 +30,7 @@ extern "C" {
  * power of two >= 16 the fast path is used: radix[0] == ATKB_PTS (4 when
  * `pair` is set) and every later radix is ATKB_PTS except a smaller last one.
  * `pair`: the paired fold (two consecutive hops per thread, even or odd
- * branches), used for oversample 1, 2 or 4 and nchan <= 2048. */
+ * branches), used for oversample 1, 2 or 4. */
 #define ATKB_MAX_PASS 24
 /* complex points per thread in the fast path's Stockham passes (8 or 16);
  * the host's plan and permuted taps follow it */

@@ -530,6 +530,36 @@ __device__ __forceinline__ void first_pass4(const float2 (&f)[4], double2 *sm, i
     for (int i = 0; i < 4; ++i) sm[SW((t << LOGM) + jp * 4 + i)] = v[i];
 }
 
+/* the paired fold of hops ta, ta + 1 (parity c, branch j) from global memory;
+ * the window source (input, state, or both by index) is chosen per tile */
+template <int LOGM, int LOGOS>
+__device__ __forceinline__ void fold_pair_global(float2 (&a)[4], float2 (&b)[4], const atkb_job &J,
+                                                 const atkb_bank &B, long long h0, int nvalid, int ta,
+                                                 int c, int j, bool tb_ok) {
+    constexpr int MP = 1 << (LOGM - LOGP);
+    constexpr int HOP = (1 << LOGM) >> LOGOS;
+    const float4 *tq = (const float4 *)B.tapsP + c * MP + j;
+    const long long w0 = h0 * (long long)HOP;
+    const long long w1 = (h0 + nvalid - 1) * (long long)HOP + B.L;
+    const long long off = (h0 + ta) * (long long)HOP + c * MP + j;
+    if (w0 >= J.head) {
+        if (J.in_kind) {
+            const PairLin16<LOGM> ld{(const short2 *)J.in + (off - J.head), J.cre, J.cim, J.kscale};
+            fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
+        } else {
+            const PairLin<LOGM> ld{(const float2 *)J.in + (off - J.head)};
+            fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
+        }
+    } else if (w1 <= J.head) {
+        const PairLin<LOGM> ld{(const float2 *)J.state + off};
+        fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
+    } else {
+        const PairMixed<LOGM> ld{Src{(const float2 *)J.state, J.in, J.head, J.in_kind, J.cre, J.cim, J.kscale},
+                                 off};
+        fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
+    }
+}
+
 template <int LOGM, int LOGOS>
 __device__ __forceinline__ void fold_tile_pair(const atkb_job &J, const atkb_bank &B, long long h0,
                                                int nvalid, double2 *sm) {
@@ -566,28 +596,7 @@ __device__ __forceinline__ void fold_tile_pair(const atkb_job &J, const atkb_ban
             return;
         }
     }
-    if (ta_ok) {
-        const long long w0 = h0 * (long long)HOP;
-        const long long w1 = (h0 + nvalid - 1) * (long long)HOP + B.L;
-        const long long off = (h0 + ta) * (long long)HOP + c * MP + j;
-        if (w0 >= J.head) {
-            if (J.in_kind) {
-                const PairLin16<LOGM> ld{(const short2 *)J.in + (off - J.head), J.cre, J.cim, J.kscale};
-                fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
-            } else {
-                const PairLin<LOGM> ld{(const float2 *)J.in + (off - J.head)};
-                fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
-            }
-        } else if (w1 <= J.head) {
-            const PairLin<LOGM> ld{(const float2 *)J.state + off};
-            fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
-        } else {
-            const PairMixed<LOGM> ld{Src{(const float2 *)J.state, J.in, J.head, J.in_kind, J.cre, J.cim,
-                                         J.kscale},
-                                     off};
-            fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
-        }
-    }
+    if (ta_ok) fold_pair_global<LOGM, LOGOS>(a, b, J, B, h0, nvalid, ta, c, j, tb_ok);
     if (!ta_ok) {
 #pragma unroll
         for (int i = 0; i < 4; ++i) a[i] = b[i] = make_float2(0.0f, 0.0f);
@@ -609,6 +618,68 @@ __device__ __forceinline__ void fft_rest(double2 *sm, const double2 *wp, const i
     } else {
         pass_last<LOGM, (1 << (LOGM - LOGNS)), LOGNS>(sm, wp + twoff[P], tile_out, B, J, h0);
     }
+}
+
+/* write a finished tile: thread -> (channel kb0 + u*MP, hop t2), runs of NH
+ * consecutive hops per channel */
+template <int LOGM>
+__device__ __forceinline__ void write_tile(const atkb_job &J, long long h0, int nvalid,
+                                           const float2 *tile_out) {
+    constexpr int LOGNH = 12 - LOGM;
+    constexpr int NH = 1 << LOGNH;
+    constexpr int MP = (1 << LOGM) >> LOGP;
+    const int tid = threadIdx.x;
+    const int t2 = tid & (NH - 1);
+    if (t2 < nvalid) {
+        const int kb0 = tid >> LOGNH;
+        float2 *o = (float2 *)J.out + (J.out_col + h0 + t2) + (long long)kb0 * J.ldo;
+        const long long step = (long long)MP * J.ldo;
+#pragma unroll 4
+        for (int u = 0; u < PTS; ++u) {
+            *o = tile_out[(kb0 + u * MP) * (NH + 1) + t2];
+            o += step;
+        }
+    }
+}
+
+/* nchan 4096, paired: a tile is two hops. Thread j folds both parities in
+ * turn; hop ta's radix-4 outputs go to the FFT tile, hop tb's raw sums to a
+ * side buffer (4096 float2 after the tile, 96 KB in all) until hop ta's FFT
+ * and write are done. */
+template <int LOGOS>
+__device__ void tile_pair_4096(const atkb_job &J, const atkb_bank &B, long long h0, int nvalid,
+                               double2 *sm) {
+    constexpr int M = 4096;
+    constexpr int MP = M >> LOGP;
+    static_assert(PTS == 8 && NT == MP, "one thread per branch j");
+    float2 *side = (float2 *)(sm + M);
+    float2 *to = (float2 *)sm;
+    const int j = threadIdx.x;
+    const bool tb_ok = nvalid > 1;
+#pragma unroll 1
+    for (int c = 0; c < 2; ++c) {
+        float2 a[4], b[4];
+        fold_pair_global<12, LOGOS>(a, b, J, B, h0, nvalid, 0, c, j, tb_ok);
+        first_pass4<12>(a, sm, 0, j + c * MP);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) side[i * (2 * MP) + c * MP + j] = b[i];
+    }
+    __syncthreads();
+    const double2 *wp = (const double2 *)B.wpass;
+    fft_rest<12, 2, 1>(sm, wp, B.plan.twoff, to, B, J, h0);
+    write_tile<12>(J, h0, 1, to);
+    if (!tb_ok) return;                  /* uniform: nvalid is the CTA's */
+    __syncthreads();                     /* tile_out read before the tile is reused */
+#pragma unroll 1
+    for (int c = 0; c < 2; ++c) {
+        float2 b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) b[i] = side[i * (2 * MP) + c * MP + j];
+        first_pass4<12>(b, sm, 0, j + c * MP);
+    }
+    __syncthreads();
+    fft_rest<12, 2, 1>(sm, wp, B.plan.twoff, to, B, J, h0 + 1);
+    write_tile<12>(J, h0 + 1, 1, to);
 }
 
 /* LOGOS < 0: one hop and PTS branches per thread, first pass radix PTS;
@@ -660,18 +731,7 @@ __device__ void tile_fast(const atkb_job &J, const atkb_bank &B, long long h0, i
     fft_rest<LOGM, (LOGOS >= 0 ? 2 : LOGP), 1>(sm, (const double2 *)B.wpass, B.plan.twoff, tile_out, B, J,
                                                 h0);
 
-    /* write: thread -> (channel kb0 + u*MP, hop t2); runs of NH hops */
-    const int t2 = tid & (NH - 1);
-    if (t2 < nvalid) {
-        const int kb0 = tid >> LOGNH;
-        float2 *o = (float2 *)J.out + (J.out_col + h0 + t2) + (long long)kb0 * J.ldo;
-        const long long step = (long long)MP * J.ldo;
-#pragma unroll 4
-        for (int u = 0; u < PTS; ++u) {
-            *o = tile_out[(kb0 + u * MP) * (NH + 1) + t2];
-            o += step;
-        }
-    }
+    write_tile<LOGM>(J, h0, nvalid, tile_out);
 }
 
 /* ---- generic path: any nchan >= 2 ----------------------------------------- */
@@ -780,6 +840,8 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
                  const int *__restrict__ d_njobs, int *counters) {
     extern __shared__ double2 sm[];
     if (d_njobs) njobs = min(njobs, *d_njobs);      /* a server round: count set per launch */
+    unsigned dyn_smem;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_smem));
     const int total_tiles = njobs > 0 ? tile_start[njobs] : 0;
     __shared__ int s_tile, s_local;
     __shared__ atkb_bank s_bank;
@@ -805,7 +867,11 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
         const long long left = J.hops - h0;
         const int nvalid = (int)(left < s_bank.tile_hops ? left : s_bank.tile_hops);
         const int lm = s_bank.plan.fast ? s_bank.logm : 0;
-        const int key = s_bank.plan.pair ? 16 * (1 + (s_bank.os == 1 ? 0 : s_bank.os == 2 ? 1 : 2)) + lm : lm;
+        int key = s_bank.plan.pair ? 16 * (1 + (s_bank.os == 1 ? 0 : s_bank.os == 2 ? 1 : 2)) + lm : lm;
+        /* a launch with less dynamic shared memory than the bank's tile needs
+         * skips the tile (its outputs stay unwritten) instead of running off
+         * the end of shared memory */
+        if ((unsigned)s_bank.smem_bytes > dyn_smem) key = -1;
         float2 *to = (float2 *)sm;
         switch (key) {
 #define UNPAIRED(L) case L: tile_fast<L, -1>(J, s_bank, h0, nvalid, sm, to); break;
@@ -816,8 +882,12 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
         UNPAIRED(4) UNPAIRED(5) UNPAIRED(6) UNPAIRED(7) UNPAIRED(8) UNPAIRED(9) UNPAIRED(10)
         UNPAIRED(11) UNPAIRED(12)
         PAIRED(4) PAIRED(5) PAIRED(6) PAIRED(7) PAIRED(8) PAIRED(9) PAIRED(10) PAIRED(11)
+        case 16 + 12: tile_pair_4096<0>(J, s_bank, h0, nvalid, sm); break;
+        case 32 + 12: tile_pair_4096<1>(J, s_bank, h0, nvalid, sm); break;
+        case 48 + 12: tile_pair_4096<2>(J, s_bank, h0, nvalid, sm); break;
 #undef UNPAIRED
 #undef PAIRED
+        case -1: break;
         default: tile_generic(J, s_bank, h0, nvalid, sm); break;
         }
         __syncthreads();
