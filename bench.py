@@ -492,13 +492,13 @@ def _served_arm(torch, device, duration_s):
     return res
 
 
-def run_ours(args, rank, world, local_rank):
+def run_ours(args, rep):
     import torch
-    import torch.distributed as dist
 
     import atkdsp_b200 as ak
     from atkdsp_b200 import gpu
 
+    rank, world, local_rank = rep.rank, rep.world, rep.local_rank
     torch.cuda.set_device(local_rank)
     device = torch.device("cuda", local_rank)
     specs = _specs(rank, args)
@@ -507,16 +507,8 @@ def run_ours(args, rank, world, local_rank):
     sets = _device_blocks(specs, torch, device, seed=rank)
     obuf, outs = _out_buffers(specs, torch, device)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = rep.barrier
+    max_over_ranks = rep.max
 
     # ---- batched path (the headline) ----
     handles = [ak.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1) for s in specs]
@@ -638,28 +630,17 @@ def main():
     ap.add_argument("--max-log2", type=float, default=22.0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
+    from atkdsp_b200.replicas import Replicas
 
-        import torch.distributed as dist
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        backend = "gloo" if args.impl == "reference" else "nccl"
-        if backend == "nccl":
-            import torch
-            torch.cuda.set_device(local_rank)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    # one process per GPU; the group exists only for the timing reductions
+    rep = Replicas(backend="gloo" if args.impl == "reference" else None, timeout_s=120)
     try:
         if args.impl == "reference":
-            run_reference(args, rank, world)
+            run_reference(args, rep.rank, rep.world)
         else:
-            run_ours(args, rank, world, local_rank)
+            run_ours(args, rep)
     finally:
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        rep.close()
     import gc
     gc.collect()
     if args.impl != "reference":
