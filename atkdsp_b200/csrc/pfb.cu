@@ -170,10 +170,38 @@ struct Src {
  * conflict-free too (a XOR with a per-block constant permutes the slots). */
 __device__ __forceinline__ int SW(int i) { return i ^ ((i >> LOGP) & (PTS - 1)); }
 
-/* One in-place Stockham pass over a 4096-point tile (NT threads x 16 points):
- * every index is a compile-time shift or mask. tw holds W_{Ns R}^{r k} at
- * (r - 1) * Ns + k. */
-template <int LOGM, int R, int LOGNS>
+/* Barrier over the G consecutive threads that share a hop group (G a power of
+ * two): a warp sync up to 32 threads, a named barrier (ids 1..NT/G) up to
+ * the CTA, __syncthreads for the whole CTA. Memory ordering among the
+ * participants is that of bar.sync / bar.warp.sync. */
+template <int G>
+__device__ __forceinline__ void group_sync() {
+    static_assert((G & (G - 1)) == 0 && G <= NT, "group size");
+    if constexpr (G >= NT) {
+        __syncthreads();
+    } else if constexpr (G <= 32) {
+        __syncwarp();
+    } else {
+        static_assert(NT / G <= 15, "named barrier ids 1..15");
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)threadIdx.x / G), "r"(G) : "memory");
+    }
+}
+
+/* Butterfly u of this thread in a pass with U butterflies per thread:
+ * warp w owns butterflies [32 w U, 32 (w + 1) U), lanes consecutive, so a
+ * warp's butterflies are the same hops as its threads' points in a radix-PTS
+ * pass (M/PTS consecutive threads per hop) and lanes read consecutive j. */
+template <int U>
+__device__ __forceinline__ int bfly(int u) {
+    return (((int)threadIdx.x & ~31) * U) + u * 32 + ((int)threadIdx.x & 31);
+}
+
+/* One in-place Stockham pass over a 4096-point tile (NT threads x PTS
+ * points): every index is a compile-time shift or mask. tw holds
+ * W_{Ns R}^{r k} at (r - 1) * Ns + k. G is the group whose barrier
+ * suffices (a multiple of the M/PTS threads of one hop): with bfly's
+ * numbering the pass reads and writes only its group's hops. */
+template <int LOGM, int R, int LOGNS, int G = NT>
 __device__ __forceinline__ void pass_c(double2 *sm, const double2 *__restrict__ tw) {
     constexpr int M = 1 << LOGM;
     constexpr int NS = 1 << LOGNS;
@@ -185,7 +213,7 @@ __device__ __forceinline__ void pass_c(double2 *sm, const double2 *__restrict__ 
     int dst[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-        const int bi = u * NT + threadIdx.x;
+        const int bi = bfly<U>(u);
         const int tt = bi >> LOGMR;
         const int j = bi & (MR - 1);
         const int k = j & (NS - 1);
@@ -196,14 +224,14 @@ __device__ __forceinline__ void pass_c(double2 *sm, const double2 *__restrict__ 
         for (int r = 1; r < R; ++r) v[u][r] = cmul(v[u][r], __ldg(tw + (r - 1) * NS + k));
         dst[u] = (tt << LOGM) + ((j - k) << LOGR) + k;
     }
-    __syncthreads();
+    group_sync<G>();
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         dftR<R>(v[u]);
 #pragma unroll
         for (int r = 0; r < R; ++r) sm[SW(dst[u] + r * NS)] = v[u][r];
     }
-    __syncthreads();
+    group_sync<G>();
 }
 
 /* Rotation to input sample 0 and cal for bin kb of a hop whose (b + 1) mod os
@@ -221,7 +249,10 @@ __device__ __forceinline__ float2 finish_bin(double2 X, int kb, int s, int M, in
 
 /* The last Stockham pass fused with the epilogue: after the butterflies every
  * output is a final bin (j + r*Ns of hop tt), rotated, calibrated, rounded and
- * written straight into the padded channel-major tile. */
+ * written straight into the padded channel-major tile. The loads read only
+ * this thread's group's hops (so the previous pass may end on a group
+ * barrier); the tile_out stores overlap every group's points, hence the
+ * CTA-wide barrier between them. */
 template <int LOGM, int R, int LOGNS>
 __device__ __forceinline__ void pass_last(double2 *sm, const double2 *__restrict__ tw,
                                           float2 *tile_out, const atkb_bank &B, const atkb_job &J,
@@ -236,7 +267,7 @@ __device__ __forceinline__ void pass_last(double2 *sm, const double2 *__restrict
     double2 v[U][R];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-        const int bi = u * NT + threadIdx.x;
+        const int bi = bfly<U>(u);
         const int tt = bi >> LOGMR;
         const int j = bi & (MR - 1);
         const int base = (tt << LOGM) + j;
@@ -253,7 +284,7 @@ __device__ __forceinline__ void pass_last(double2 *sm, const double2 *__restrict
     const int s0 = (int)((J.b0 + h0 + 1) % os);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-        const int bi = u * NT + threadIdx.x;
+        const int bi = bfly<U>(u);
         const int tt = bi >> LOGMR;
         const int j = bi & (MR - 1);
         const int s = os_pow2 ? ((s0 + tt) & (os - 1)) : ((s0 + tt) % os);
@@ -608,13 +639,13 @@ __device__ __forceinline__ void fold_tile_pair(const atkb_job &J, const atkb_ban
 /* the Stockham passes after the first (which left Ns = 2^LOGNS): radix PTS
  * while more than LOGP index bits remain, then the last pass (radix 2, 4 or
  * 8) fused with the epilogue; P indexes the plan's twiddle offsets */
-template <int LOGM, int LOGNS, int P>
+template <int LOGM, int LOGNS, int P, int G = NT>
 __device__ __forceinline__ void fft_rest(double2 *sm, const double2 *wp, const int *twoff,
                                          float2 *tile_out, const atkb_bank &B, const atkb_job &J,
                                          long long h0) {
     if constexpr (LOGM - LOGNS > LOGP) {
-        pass_c<LOGM, PTS, LOGNS>(sm, wp + twoff[P]);
-        fft_rest<LOGM, LOGNS + LOGP, P + 1>(sm, wp, twoff, tile_out, B, J, h0);
+        pass_c<LOGM, PTS, LOGNS, G>(sm, wp + twoff[P]);
+        fft_rest<LOGM, LOGNS + LOGP, P + 1, G>(sm, wp, twoff, tile_out, B, J, h0);
     } else {
         pass_last<LOGM, (1 << (LOGM - LOGNS)), LOGNS>(sm, wp + twoff[P], tile_out, B, J, h0);
     }
@@ -726,10 +757,16 @@ __device__ void tile_fast(const atkb_job &J, const atkb_bank &B, long long h0, i
 #pragma unroll
         for (int r = 0; r < PTS; ++r) sm[SW((tt << LOGM) + j * PTS + r)] = v[r];
     }
-    __syncthreads();
+    /* from here to the last pass each hop group (the threads of a hop pair,
+     * or of one hop) touches only its own points: group barriers suffice.
+     * The region was last used by the previous tile's write, fenced by the
+     * CTA-wide barrier that ends every tile. */
+    constexpr int G0 = (LOGOS >= 0 ? M / 4 : M / PTS);
+    constexpr int G = G0 < 32 ? 32 : G0 > NT ? NT : G0;
+    group_sync<G>();
 
-    fft_rest<LOGM, (LOGOS >= 0 ? 2 : LOGP), 1>(sm, (const double2 *)B.wpass, B.plan.twoff, tile_out, B, J,
-                                                h0);
+    fft_rest<LOGM, (LOGOS >= 0 ? 2 : LOGP), 1, G>(sm, (const double2 *)B.wpass, B.plan.twoff, tile_out, B,
+                                                   J, h0);
 
     write_tile<LOGM>(J, h0, nvalid, tile_out);
 }
