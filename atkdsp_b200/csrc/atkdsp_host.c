@@ -167,13 +167,14 @@ static int plan_fft(unsigned M, unsigned os, atkb_fft_plan *pl) {
             }
         }
     }
-    /* per-pass twiddles (fast path): pass p >= 1 holds W_{Ns R}^{r k} at
-     * (r - 1) * Ns + k, r in [1, R), k in [0, Ns) */
+    /* per-pass twiddles (fast path): pass p >= 1 holds W_{Ns R}^{k} at k,
+     * k in [0, Ns); the kernel forms the powers r = 2 .. R-1 by complex
+     * multiplication */
     {
         int p, Ns = 1, off = 0;
         for (p = 0; p < pl->npass; ++p) {
             pl->twoff[p] = off;
-            if (p > 0) off += (pl->radix[p] - 1) * Ns;
+            if (p > 0) off += Ns;
             Ns *= pl->radix[p];
         }
         pl->twlen = off > 0 ? off : 1;
@@ -295,15 +296,14 @@ static int bank_build(bank_entry *be, void *stream) {
         int pidx, Ns = 1;
         for (pidx = 0; pidx < pl.npass; ++pidx) {
             const int R = pl.radix[pidx];
-            if (pidx > 0) {
-                int r, k;
-                for (r = 1; r < R; ++r)
-                    for (k = 0; k < Ns; ++k) {
-                        const size_t e = (size_t)pl.twoff[pidx] + (size_t)(r - 1) * Ns + k;
-                        const size_t jj = (size_t)r * k * (M / ((size_t)Ns * R));
-                        wp[2 * e] = W[2 * jj];
-                        wp[2 * e + 1] = W[2 * jj + 1];
-                    }
+            if (pidx > 0 && pl.fast) {
+                int k;
+                for (k = 0; k < Ns; ++k) {
+                    const size_t e = (size_t)pl.twoff[pidx] + (size_t)k;
+                    const size_t jj = (size_t)k * (M / ((size_t)Ns * R));
+                    wp[2 * e] = W[2 * jj];
+                    wp[2 * e + 1] = W[2 * jj + 1];
+                }
             }
             Ns *= R;
         }

@@ -170,6 +170,28 @@ struct Src {
  * conflict-free too (a XOR with a per-block constant permutes the slots). */
 __device__ __forceinline__ int SW(int i) { return i ^ ((i >> LOGP) & (PTS - 1)); }
 
+/* the twiddles of one butterfly, w[r] = W^(r k) for r = 1 .. R-1, from the
+ * one table entry w1 = W^k: squares and products (each power carries at most
+ * two double roundings more than a table entry, ~1e-16 relative) instead of
+ * R-1 table loads, so a pass reads Ns table entries, not (R-1)*Ns */
+__device__ __forceinline__ double2 csq(double2 a) {
+    return make_double2(a.x * a.x - a.y * a.y, 2.0 * a.x * a.y);
+}
+template <int R>
+__device__ __forceinline__ void tw_powers(double2 w1, double2 *w) {
+    w[1] = w1;
+    if constexpr (R > 2) {
+        w[2] = csq(w1);
+        w[3] = cmul(w[2], w1);
+    }
+    if constexpr (R > 4) {
+        w[4] = csq(w[2]);
+        w[5] = cmul(w[4], w1);
+        w[6] = csq(w[3]);
+        w[7] = cmul(w[4], w[3]);
+    }
+}
+
 /* Barrier over the G consecutive threads that share a hop group (G a power of
  * two): a warp sync up to 32 threads, a named barrier (ids 1..NT/G) up to
  * the CTA, __syncthreads for the whole CTA. Memory ordering among the
@@ -198,7 +220,7 @@ __device__ __forceinline__ int bfly(int u) {
 
 /* One in-place Stockham pass over a 4096-point tile (NT threads x PTS
  * points): every index is a compile-time shift or mask. tw holds
- * W_{Ns R}^{r k} at (r - 1) * Ns + k. G is the group whose barrier
+ * W_{Ns R}^{k} at k (tw_powers forms the other powers). G is the group whose barrier
  * suffices (a multiple of the M/PTS threads of one hop): with bfly's
  * numbering the pass reads and writes only its group's hops. */
 template <int LOGM, int R, int LOGNS, int G = NT>
@@ -220,8 +242,10 @@ __device__ __forceinline__ void pass_c(double2 *sm, const double2 *__restrict__ 
         const int base = (tt << LOGM) + j;
 #pragma unroll
         for (int r = 0; r < R; ++r) v[u][r] = sm[SW(base + r * MR)];
+        double2 w[R];
+        tw_powers<R>(__ldg(tw + k), w);
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[u][r] = cmul(v[u][r], __ldg(tw + (r - 1) * NS + k));
+        for (int r = 1; r < R; ++r) v[u][r] = cmul(v[u][r], w[r]);
         dst[u] = (tt << LOGM) + ((j - k) << LOGR) + k;
     }
     group_sync<G>();
@@ -273,8 +297,10 @@ __device__ __forceinline__ void pass_last(double2 *sm, const double2 *__restrict
         const int base = (tt << LOGM) + j;
 #pragma unroll
         for (int r = 0; r < R; ++r) v[u][r] = sm[SW(base + r * MR)];
+        double2 w[R];
+        tw_powers<R>(__ldg(tw + j), w);
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[u][r] = cmul(v[u][r], __ldg(tw + (r - 1) * NS + j));
+        for (int r = 1; r < R; ++r) v[u][r] = cmul(v[u][r], w[r]);
     }
     __syncthreads();
     const double2 *twd = (const double2 *)B.twd;
