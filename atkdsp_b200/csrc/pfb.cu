@@ -895,6 +895,44 @@ __device__ void tile_generic(const atkb_job &J, const atkb_bank &B, long long h0
     }
 }
 
+/* The CTA's next tile (warp 0, all lanes): claim it from the counter, find
+ * its job (the last whose first tile <= tile) by a 32-ary search over the
+ * tile prefix table, and copy the job and its bank into shared slot `slot`
+ * with asynchronous copies that land while the CTA works on the current
+ * tile (the caller waits for them before the next barrier). */
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void fetch_tile(const atkb_job *__restrict__ jobs, const int *__restrict__ tile_start,
+                                           int njobs, int total, int *counters, int *s_tile, int *s_local,
+                                           atkb_job *s_job, atkb_bank *s_bank, int slot) {
+    static_assert(sizeof(atkb_job) % 4 == 0 && sizeof(atkb_bank) % 4 == 0, "word copies");
+    const int lane = threadIdx.x & 31;
+    int tile = 0;
+    if (lane == 0) tile = atomicAdd(&counters[0], 1);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (lane == 0) s_tile[slot] = tile;
+    if (tile >= total) return;
+    int lo = 0, hi = njobs - 1;                  /* tile_start[lo] <= tile throughout */
+    while (lo < hi) {
+        const int step = (hi - lo + 32) >> 5;    /* ceil(span / 32) */
+        const int idx = lo + lane * step;
+        const bool ok = idx <= hi && tile_start[idx] <= tile;
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        lo += (31 - __clz(m)) * step;            /* lane 0 is always set */
+        hi = min(hi, lo + step - 1);
+    }
+    const int *js = (const int *)(jobs + lo);
+    int *jd = (int *)(s_job + slot);
+    for (int w = lane; w < (int)(sizeof(atkb_job) / 4); w += 32) cp_async4(jd + w, js + w);
+    const int *bs = (const int *)jobs[lo].bank;
+    int *bd = (int *)(s_bank + slot);
+    for (int w = lane; w < (int)(sizeof(atkb_bank) / 4); w += 32) cp_async4(bd + w, bs + w);
+    if (lane == 0) s_local[slot] = tile - tile_start[lo];
+}
+
 #ifndef ATKB_TILE_MINB
 #define ATKB_TILE_MINB (PTS == 8 ? 2 : 2)
 #endif
@@ -906,54 +944,50 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
     unsigned dyn_smem;
     asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_smem));
     const int total_tiles = njobs > 0 ? tile_start[njobs] : 0;
-    __shared__ int s_tile, s_local;
-    __shared__ atkb_bank s_bank;
-    __shared__ atkb_job s_job;
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(&counters[0], 1);
+    /* two slots: warp 0 fetches tile i+1 into one while the CTA works on
+     * tile i from the other */
+    __shared__ int s_tile[2], s_local[2];
+    __shared__ atkb_bank s_bank[2];
+    __shared__ atkb_job s_job[2];
+    if (threadIdx.x < 32) fetch_tile(jobs, tile_start, njobs, total_tiles, counters, s_tile, s_local, s_job, s_bank, 0);
+    for (int slot = 0;; slot ^= 1) {
+        if (threadIdx.x < 32) cp_async_wait_all();  /* this slot's copies, issued by warp 0 */
         __syncthreads();
-        const int tile = s_tile;
+        const int tile = s_tile[slot];
         if (tile >= total_tiles) break;
-        if (threadIdx.x == 0) {
-            int lo = 0, hi = njobs - 1;
-            while (lo < hi) {                   /* last job whose start <= tile */
-                const int mid = (lo + hi + 1) >> 1;
-                if (tile_start[mid] <= tile) lo = mid; else hi = mid - 1;
-            }
-            s_job = jobs[lo];
-            s_bank = *s_job.bank;
-            s_local = tile - tile_start[lo];
-        }
-        __syncthreads();
-        const atkb_job J = s_job;
-        const long long h0 = (long long)s_local * s_bank.tile_hops;
+        if (threadIdx.x < 32)
+            fetch_tile(jobs, tile_start, njobs, total_tiles, counters, s_tile, s_local, s_job, s_bank, slot ^ 1);
+        const atkb_job J = s_job[slot];
+        const atkb_bank &SB = s_bank[slot];
+        const long long h0 = (long long)s_local[slot] * SB.tile_hops;
         const long long left = J.hops - h0;
-        const int nvalid = (int)(left < s_bank.tile_hops ? left : s_bank.tile_hops);
-        const int lm = s_bank.plan.fast ? s_bank.logm : 0;
-        int key = s_bank.plan.pair ? 16 * (1 + (s_bank.os == 1 ? 0 : s_bank.os == 2 ? 1 : 2)) + lm : lm;
+        const int nvalid = (int)(left < SB.tile_hops ? left : SB.tile_hops);
+        const int lm = SB.plan.fast ? SB.logm : 0;
+        int key = SB.plan.pair ? 16 * (1 + (SB.os == 1 ? 0 : SB.os == 2 ? 1 : 2)) + lm : lm;
         /* a launch with less dynamic shared memory than the bank's tile needs
          * skips the tile (its outputs stay unwritten) instead of running off
          * the end of shared memory */
-        if ((unsigned)s_bank.smem_bytes > dyn_smem) key = -1;
+        if ((unsigned)SB.smem_bytes > dyn_smem) key = -1;
         float2 *to = (float2 *)sm;
         switch (key) {
-#define UNPAIRED(L) case L: tile_fast<L, -1>(J, s_bank, h0, nvalid, sm, to); break;
+#define UNPAIRED(L) case L: tile_fast<L, -1>(J, SB, h0, nvalid, sm, to); break;
 #define PAIRED(L)                                                              \
-        case 16 + L: tile_fast<L, 0>(J, s_bank, h0, nvalid, sm, to); break;    \
-        case 32 + L: tile_fast<L, 1>(J, s_bank, h0, nvalid, sm, to); break;    \
-        case 48 + L: tile_fast<L, 2>(J, s_bank, h0, nvalid, sm, to); break;
+        case 16 + L: tile_fast<L, 0>(J, SB, h0, nvalid, sm, to); break;    \
+        case 32 + L: tile_fast<L, 1>(J, SB, h0, nvalid, sm, to); break;    \
+        case 48 + L: tile_fast<L, 2>(J, SB, h0, nvalid, sm, to); break;
         UNPAIRED(4) UNPAIRED(5) UNPAIRED(6) UNPAIRED(7) UNPAIRED(8) UNPAIRED(9) UNPAIRED(10)
         UNPAIRED(11) UNPAIRED(12)
         PAIRED(4) PAIRED(5) PAIRED(6) PAIRED(7) PAIRED(8) PAIRED(9) PAIRED(10) PAIRED(11)
-        case 16 + 12: tile_pair_4096<0>(J, s_bank, h0, nvalid, sm); break;
-        case 32 + 12: tile_pair_4096<1>(J, s_bank, h0, nvalid, sm); break;
-        case 48 + 12: tile_pair_4096<2>(J, s_bank, h0, nvalid, sm); break;
+        case 16 + 12: tile_pair_4096<0>(J, SB, h0, nvalid, sm); break;
+        case 32 + 12: tile_pair_4096<1>(J, SB, h0, nvalid, sm); break;
+        case 48 + 12: tile_pair_4096<2>(J, SB, h0, nvalid, sm); break;
 #undef UNPAIRED
 #undef PAIRED
         case -1: break;
-        default: tile_generic(J, s_bank, h0, nvalid, sm); break;
+        default: tile_generic(J, SB, h0, nvalid, sm); break;
         }
-        __syncthreads();
+        /* the barrier at the top of the loop fences this tile's reads of sm
+         * and of its slot from the next tile's writes */
     }
     if (threadIdx.x == 0) {
         __threadfence();
