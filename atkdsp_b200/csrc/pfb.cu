@@ -957,7 +957,7 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
         if (tile >= total_tiles) break;
         if (threadIdx.x < 32)
             fetch_tile(jobs, tile_start, njobs, total_tiles, counters, s_tile, s_local, s_job, s_bank, slot ^ 1);
-        const atkb_job J = s_job[slot];
+        const atkb_job &J = s_job[slot];
         const atkb_bank &SB = s_bank[slot];
         const long long h0 = (long long)s_local[slot] * SB.tile_hops;
         const long long left = J.hops - h0;
