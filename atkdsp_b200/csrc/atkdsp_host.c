@@ -245,6 +245,9 @@ ATKDSP_API void atkdsp_pfb_destroy(atkdsp_pfb *p) {
     atkb_free(p->d_tables);
     atkb_free(p->d_counters);
     atkb_host_free(p->h_tables);
+    atkb_host_free(p->h_small_in);
+    atkb_host_free(p->h_small_out);
+    atkb_event_destroy(p->small_ev);
     atkb_event_destroy(p->tbl_event);
     atkb_stream_destroy(p->stream);
     free(p);
@@ -470,8 +473,15 @@ atkdsp_pfb *atkb_pfb_create_internal(double fs, unsigned nchan, unsigned oversam
         rc = atkb_malloc(&p->d_tables, p->tbl_bytes);
     }
     if (rc == ATKB_OK) rc = atkb_host_alloc(&p->h_tables, p->tbl_bytes);
-    if (rc == ATKB_OK) rc = atkb_malloc((void **)&p->d_counters, 2 * sizeof(int));
-    if (rc == ATKB_OK) rc = atkb_memset(p->d_counters, 0, 2 * sizeof(int), p->stream);
+    if (rc == ATKB_OK && p->chunk >= ATKB_SMALL_N) {
+        const size_t m_small = (p->hop - 1 + ATKB_SMALL_N) / p->hop;
+        rc = atkb_host_alloc(&p->h_small_in, (size_t)max_nel * ATKB_SMALL_N * sizeof(atkdsp_cf32));
+        if (rc == ATKB_OK)
+            rc = atkb_host_alloc(&p->h_small_out, (size_t)max_nel * nchan * m_small * sizeof(atkdsp_cf32));
+        if (rc == ATKB_OK) rc = atkb_event_create(&p->small_ev);
+    }
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&p->d_counters, ATKB_NCOUNTERS * sizeof(int));
+    if (rc == ATKB_OK) rc = atkb_memset(p->d_counters, 0, ATKB_NCOUNTERS * sizeof(int), p->stream);
     if (rc == ATKB_OK) rc = atkb_stream_sync(p->stream);
     if (rc != ATKB_OK) { atkdsp_pfb_destroy(p); return NULL; }
     p->grid = atkb_pfb_grid(p->dev, p->bank.smem_bytes);
@@ -494,6 +504,7 @@ ATKDSP_API void atkdsp_pfb_reset(atkdsp_pfb *p) {
     atkb_memset(p->d_state, 0, 2 * (size_t)p->max_nel * p->cap_state * sizeof(atkdsp_cf32),
                 p->stream);
     atkb_stream_sync(p->stream);
+    p->small_live = 0;
     p->lc = 0;
     p->b = 0;
     p->cur = 0;
@@ -596,20 +607,72 @@ static int run_step(atkdsp_pfb *p, unsigned nel, const void *const *ins, size_t 
     if (rc == ATKB_OK) rc = atkb_event_record(p->tbl_event, stream);
     if (rc != ATKB_OK) return rc;
     p->tbl_event_live = 1;
-    if (tiles > 0) {
-        /* only nel jobs: tile_start[nel] is their total; the kernel reads
-         * tile_start[njobs], so pass the tile table shifted to this nel */
-        rc = atkb_pfb_launch(tbl_jobs(p->d_tables), tbl_tiles(p->d_tables, p->max_nel), (int)nel,
-                             p->d_counters, p->grid < (int)nel * tiles ? p->grid : (int)nel * tiles,
-                             p->bank.smem_bytes, stream);
+    {
+        /* nel jobs: tile_start[nel] is their total (the kernel reads
+         * tile_start[njobs]); the same launch copies the nel carries */
+        const int work = (int)nel * tiles + (int)nel;
+        rc = atkb_pfb_launch(tbl_jobs(p->d_tables), tbl_tiles(p->d_tables, p->max_nel),
+                             tbl_carry(p->d_tables, p->max_nel), (int)nel, p->d_counters,
+                             p->grid < work ? p->grid : work, p->bank.smem_bytes, stream);
         if (rc != ATKB_OK) return rc;
     }
-    rc = atkb_pfb_carry(tbl_carry(p->d_tables, p->max_nel), (int)nel, (long long)p->cap_state, stream);
-    if (rc != ATKB_OK) return rc;
     p->cur = (int)nxt;
     p->lc = (unsigned)(p->lc + n - m * p->hop);
     p->b += (int64_t)m;
     return ATKB_OK;
+}
+
+/* A small host call through the handle's pinned staging: one memcpy in, one
+ * DMA each way, one memcpy out. A block that completes no hop only extends
+ * the state (s = state ++ in): one copy into the current state buffer, left
+ * in flight -- the call returns 0 at once, and every later use of the handle
+ * is ordered after that copy (same stream, or atkb_pfb_order_after_small). */
+static ptrdiff_t process_small(atkdsp_pfb *p, const atkdsp_cf32 *const *ins, unsigned nel, size_t n,
+                               atkdsp_cf32 *out, size_t m) {
+    int rc = ATKB_OK;
+    unsigned e;
+    if (p->small_live) {                 /* h_small_in may still feed that copy */
+        rc = atkb_event_sync(p->small_ev);
+        if (rc != ATKB_OK) return map_rc(rc);
+        p->small_live = 0;
+    }
+    atkdsp_cf32 *hin = (atkdsp_cf32 *)p->h_small_in;
+    if (n)
+        for (e = 0; e < nel; ++e) memcpy(hin + (size_t)e * ATKB_SMALL_N, ins[e], n * sizeof(atkdsp_cf32));
+    if (m == 0) {
+        const size_t head = p->ov + p->lc;      /* head + n < ov + hop: within the buffer */
+        for (e = 0; e < nel && n && rc == ATKB_OK; ++e)
+            rc = atkb_h2d(state_buf(p, p->cur, e) + head, hin + (size_t)e * ATKB_SMALL_N,
+                          n * sizeof(atkdsp_cf32), p->stream);
+        if (rc == ATKB_OK && n) {
+            rc = atkb_event_record(p->small_ev, p->stream);
+            if (rc == ATKB_OK) p->small_live = 1;
+        }
+        if (rc != ATKB_OK) return map_rc(rc);
+        p->lc = (unsigned)(p->lc + n);
+        return 0;
+    }
+    const void *dins[MAX_NEL_SUPPORTED];
+    for (e = 0; e < nel && rc == ATKB_OK; ++e) {
+        dins[e] = (const atkdsp_cf32 *)p->d_in_stage + (size_t)e * p->chunk;
+        if (n) rc = atkb_h2d((void *)dins[e], hin + (size_t)e * ATKB_SMALL_N, n * sizeof(atkdsp_cf32), p->stream);
+    }
+    /* outputs packed with stride m: [nel * nchan][m], the caller's layout */
+    const size_t out_n = (size_t)nel * p->nchan * m;
+    if (rc == ATKB_OK)
+        rc = run_step(p, nel, dins, n, (atkdsp_cf32 *)p->d_out_stage, m, m, p->stream, &CONV_CF32);
+    if (rc == ATKB_OK)
+        rc = atkb_d2h(p->h_small_out, p->d_out_stage, out_n * sizeof(atkdsp_cf32), p->stream);
+    if (rc == ATKB_OK) rc = atkb_stream_sync(p->stream);
+    if (rc != ATKB_OK) return map_rc(rc);
+    memcpy(out, p->h_small_out, out_n * sizeof(atkdsp_cf32));
+    return (ptrdiff_t)m;
+}
+
+int atkb_pfb_order_after_small(atkdsp_pfb *p, void *stream) {
+    if (!p->small_live) return ATKB_OK;
+    if (!stream || stream == p->stream) return ATKB_OK;
+    return atkb_stream_wait(stream, p->small_ev);
 }
 
 /* reference src/channelizer.c:305-402 */
@@ -622,6 +685,12 @@ ATKDSP_API ptrdiff_t atkdsp_pfb_process_n(atkdsp_pfb *p, const atkdsp_cf32 *cons
     const size_t m = ((size_t)p->lc + n) / p->hop;
     if (m > 0 && (!out || cap < (size_t)nel * p->nchan * m)) return ATKDSP_E_CAP;
     if (atkb_set_device(p->dev) != ATKB_OK) return ATKDSP_E_FFT;
+    if (p->h_small_in && n <= ATKB_SMALL_N) return process_small(p, ins, nel, n, out, m);
+    if (p->small_live) {
+        const int rs = atkb_event_sync(p->small_ev);
+        if (rs != ATKB_OK) return map_rc(rs);
+        p->small_live = 0;
+    }
     size_t pos = 0, col = 0;
     int rc = ATKB_OK;
     const atkdsp_cf32 *dins[MAX_NEL_SUPPORTED];
@@ -677,6 +746,7 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_n(atkdsp_pfb *p, const atkdsp_cf32 *
     if (m > 0 && (!d_out || cap < (size_t)nel * p->nchan * m)) return ATKDSP_E_CAP;
     if (m > (size_t)0x7fffffff / 4 / nel) return ATKDSP_E_ARG;   /* tile indices are int */
     if (atkb_set_device(p->dev) != ATKB_OK) return ATKDSP_E_FFT;
+    if (atkb_pfb_order_after_small(p, stream) != ATKB_OK) return ATKDSP_E_FFT;
     const int rc = run_step(p, nel, (const void *const *)d_ins, n, d_out, m, m,
                             stream ? stream : p->stream, &CONV_CF32);
     return rc == ATKB_OK ? (ptrdiff_t)m : map_rc(rc);
@@ -708,6 +778,7 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_n_raw(atkdsp_pfb *p, const void *con
     if (m > 0 && (!d_out || cap < (size_t)nel * p->nchan * m)) return ATKDSP_E_CAP;
     if (m > (size_t)0x7fffffff / 4 / nel) return ATKDSP_E_ARG;
     if (atkb_set_device(p->dev) != ATKB_OK) return ATKDSP_E_FFT;
+    if (atkb_pfb_order_after_small(p, stream) != ATKB_OK) return ATKDSP_E_FFT;
     const int rc = run_step(p, nel, d_raws, n, d_out, m, m, stream ? stream : p->stream, &cv);
     return rc == ATKB_OK ? (ptrdiff_t)m : map_rc(rc);
 }
@@ -1034,7 +1105,6 @@ struct atkdsp_gpu_batch {
     int slot;
     int *d_counters;
     int grid, smem;
-    long long max_carry;
     void *tk[2];                  /* timing events around the tile kernel */
 };
 
@@ -1071,7 +1141,6 @@ ATKDSP_API atkdsp_gpu_batch *atkdsp_gpu_batch_create(atkdsp_pfb *const *handles,
     for (i = 0; i < count; ++i) {
         b->h[i] = handles[i];
         if (handles[i]->bank.smem_bytes > b->smem) b->smem = handles[i]->bank.smem_bytes;
-        if ((long long)handles[i]->cap_state > b->max_carry) b->max_carry = (long long)handles[i]->cap_state;
     }
     atkb_set_device(b->dev);
     b->tbl_bytes = tables_bytes(count);
@@ -1082,8 +1151,8 @@ ATKDSP_API atkdsp_gpu_batch *atkdsp_gpu_batch_create(atkdsp_pfb *const *handles,
         if (rc == ATKB_OK) rc = atkb_event_create(&b->ev[i]);
         if (rc == ATKB_OK) rc = atkb_event_create_timed(&b->tk[i]);
     }
-    if (rc == ATKB_OK) rc = atkb_malloc((void **)&b->d_counters, 2 * sizeof(int));
-    if (rc == ATKB_OK) rc = atkb_memset(b->d_counters, 0, 2 * sizeof(int), b->stream);
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&b->d_counters, ATKB_NCOUNTERS * sizeof(int));
+    if (rc == ATKB_OK) rc = atkb_memset(b->d_counters, 0, ATKB_NCOUNTERS * sizeof(int), b->stream);
     if (rc == ATKB_OK) rc = atkb_stream_sync(b->stream);
     if (rc != ATKB_OK) { atkdsp_gpu_batch_destroy(b); return NULL; }
     b->grid = atkb_pfb_grid(b->dev, b->smem);
@@ -1104,10 +1173,10 @@ static int batch_enqueue(atkdsp_gpu_batch *b, int slot, void *stream) {
     int rc = atkb_h2d(b->d_tables, b->h_tables[slot], b->tbl_bytes, stream);
     if (rc == ATKB_OK) rc = atkb_event_record_node(b->tk[0], stream);
     if (rc == ATKB_OK)
-        rc = atkb_pfb_launch(tbl_jobs(b->d_tables), tbl_tiles(b->d_tables, b->count), (int)b->count,
-                             b->d_counters, b->grid, b->smem, stream);
+        rc = atkb_pfb_launch(tbl_jobs(b->d_tables), tbl_tiles(b->d_tables, b->count),
+                             tbl_carry(b->d_tables, b->count), (int)b->count, b->d_counters, b->grid,
+                             b->smem, stream);
     if (rc == ATKB_OK) rc = atkb_event_record_node(b->tk[1], stream);
-    if (rc == ATKB_OK) rc = atkb_pfb_carry(tbl_carry(b->d_tables, b->count), (int)b->count, b->max_carry, stream);
     return rc;
 }
 
@@ -1121,6 +1190,13 @@ static ptrdiff_t batch_process(atkdsp_gpu_batch *b, const void *const *d_ins, co
     int rc;
     unsigned i;
     if (b->ev_live[slot] && atkb_event_sync(b->ev[slot]) != ATKB_OK) return ATKDSP_E_FFT;
+    for (i = 0; i < b->count; ++i) {     /* a handle's pending small-call copy lands first */
+        atkdsp_pfb *h = b->h[i];
+        if (h->small_live) {
+            if (atkb_event_sync(h->small_ev) != ATKB_OK) return ATKDSP_E_FFT;
+            h->small_live = 0;
+        }
+    }
     atkb_job *J = tbl_jobs(b->h_tables[slot]);
     atkb_carry *C = tbl_carry(b->h_tables[slot], b->count);
     int *T = tbl_tiles(b->h_tables[slot], b->count);

@@ -12,6 +12,14 @@
  * rounds) reserves this much. */
 #define ATKB_FAST_SMEM_MAX (4096 * 16 + 4096 * 8)
 
+/* host calls of at most this many samples per element stage through pinned
+ * memory owned by the handle */
+#define ATKB_SMALL_N ((size_t)1 << 15)
+
+/* order `stream` (NULL: the handle's) after the handle's pending small-call
+ * copy, if any; the device-pointer and batch paths call it first */
+int atkb_pfb_order_after_small(atkdsp_pfb *p, void *stream);
+
 /* a device bank shared by every handle with the same (device, nchan,
  * oversample, taps, attenuation): taps, tables and the device atkb_bank */
 typedef struct bank_entry bank_entry;
@@ -38,6 +46,12 @@ struct atkdsp_pfb {
     size_t chunk, out_ld;         /* host-path chunk (samples) and its output stride */
     void *d_in_stage, *d_out_stage;
     void *d_tables, *h_tables;    /* jobs | carries | tile_start              */
+    /* small host calls (n <= ATKB_SMALL_N): pinned staging for the block and
+     * its output; `small_ev` marks the last copy out of h_small_in, which a
+     * call that completes no hop leaves in flight (small_live) */
+    void *h_small_in, *h_small_out;
+    void *small_ev;
+    int small_live;
     size_t tbl_bytes;
     int *d_counters;
     int grid;

@@ -133,21 +133,22 @@ void atkb_graph_destroy(void *exec);
 /* occupancy-derived number of CTAs for the persistent tile kernel */
 int  atkb_pfb_grid(int dev, int smem_bytes);
 int  atkb_pfb_max_smem(void);
-/* jobs / tile_start / counters are DEVICE arrays; tile_start has njobs + 1
- * entries, the last one the total tile count, read by the kernel (so a
- * captured graph can replay with new work). grid CTAs loop over the tiles.
- * counters: 2 ints, zero before the first launch; the kernel leaves them
- * zero again. */
-int  atkb_pfb_launch(const atkb_job *d_jobs, const int *d_tile_start, int njobs,
-                     int *d_counters, int grid, int smem_bytes, void *stream);
-int  atkb_pfb_carry(const atkb_carry *d_carry, int ncarry, long long max_len, void *stream);
-/* the same with the job / carry count read from device memory (at most the
- * given maximum): a launch sequence that serves a different set of streams
- * each time can be captured once */
-int  atkb_pfb_launch_n(const atkb_job *d_jobs, const int *d_tile_start, int njobs_max,
-                       const int *d_njobs, int *d_counters, int grid, int smem_bytes, void *stream);
-int  atkb_pfb_carry_n(const atkb_carry *d_carry, int ncarry_max, const int *d_ncarry,
-                      long long max_len, void *stream);
+/* jobs / tile_start / carries / counters are DEVICE arrays; tile_start has
+ * njobs + 1 entries, the last one the total tile count, read by the kernel
+ * (so a captured graph can replay with new work). grid CTAs loop over the
+ * tiles, then over the carries (one per job: it writes only the other state
+ * buffer, which no tile reads, so it needs no ordering against the tiles).
+ * counters: ATKB_NCOUNTERS ints, zero before the first launch; the kernel
+ * leaves them zero again. */
+#define ATKB_NCOUNTERS 4
+int  atkb_pfb_launch(const atkb_job *d_jobs, const int *d_tile_start, const atkb_carry *d_carry,
+                     int njobs, int *d_counters, int grid, int smem_bytes, void *stream);
+/* the same with the job count read from device memory (at most the given
+ * maximum): a launch that serves a different set of streams each time can
+ * be captured once */
+int  atkb_pfb_launch_n(const atkb_job *d_jobs, const int *d_tile_start, const atkb_carry *d_carry,
+                       int njobs_max, const int *d_njobs, int *d_counters, int grid, int smem_bytes,
+                       void *stream);
 int  atkb_event_query(void *ev);        /* ATKB_OK when complete, 1 when pending */
 
 /* W1 + W2 over a device [nel][nchan][m] block. R, counts, pwr, mean_pwr are

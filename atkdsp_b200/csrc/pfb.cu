@@ -937,8 +937,9 @@ __device__ __forceinline__ void fetch_tile(const atkb_job *__restrict__ jobs, co
 #define ATKB_TILE_MINB (PTS == 8 ? 2 : 2)
 #endif
 __global__ void __launch_bounds__(NT, ATKB_TILE_MINB)
-pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile_start, int njobs,
-                 const int *__restrict__ d_njobs, int *counters) {
+pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile_start,
+                 const atkb_carry *__restrict__ carries, int njobs, const int *__restrict__ d_njobs,
+                 int *counters) {
     extern __shared__ double2 sm[];
     if (d_njobs) njobs = min(njobs, *d_njobs);      /* a server round: count set per launch */
     unsigned dyn_smem;
@@ -989,25 +990,29 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
         /* the barrier at the top of the loop fences this tile's reads of sm
          * and of its slot from the next tile's writes */
     }
+    /* then the state carries, one job's per claim, the CTA's threads copying
+     * s[from, from + len) into the other state buffer (no tile reads it) */
+    __shared__ int s_carry;
+    for (;;) {
+        if (threadIdx.x == 0) s_carry = atomicAdd(&counters[2], 1);
+        __syncthreads();
+        const int ci = s_carry;
+        __syncthreads();                  /* read before thread 0 claims again */
+        if (ci >= njobs) break;
+        const atkb_carry &C = carries[ci];
+        const Src src{(const float2 *)C.state, C.in, C.head, C.in_kind, C.cre, C.cim, C.kscale};
+        float2 *dst = (float2 *)C.dst;
+        const long long from = C.from, len = C.len;
+        for (long long i = threadIdx.x; i < len; i += NT) dst[i] = src.at(from + i);
+    }
     if (threadIdx.x == 0) {
         __threadfence();
         const int done = atomicAdd(&counters[1], 1);
         if (done == (int)gridDim.x - 1) {      /* the last CTA out resets */
             atomicExch(&counters[0], 0);
+            atomicExch(&counters[2], 0);
             atomicExch(&counters[1], 0);
         }
-    }
-}
-
-/* the state carries: CTA b takes carries b, b + gridDim.x, ...; 256 threads
- * copy one carry's samples */
-__global__ void pfb_carry_kernel(const atkb_carry *__restrict__ c, int n, const int *__restrict__ d_n) {
-    if (d_n) n = min(n, *d_n);
-    for (int ci = blockIdx.x; ci < n; ci += gridDim.x) {
-        const atkb_carry C = c[ci];
-        const Src src{(const float2 *)C.state, C.in, C.head, C.in_kind, C.cre, C.cim, C.kscale};
-        float2 *dst = (float2 *)C.dst;
-        for (long long i = threadIdx.x; i < C.len; i += blockDim.x) dst[i] = src.at(C.from + i);
     }
 }
 
@@ -1030,30 +1035,18 @@ extern "C" int atkb_pfb_grid(int dev, int smem_bytes) {
     return per_sm * atkb_sm_count(dev);
 }
 
-extern "C" int atkb_pfb_launch(const atkb_job *d_jobs, const int *d_tile_start, int njobs,
-                               int *d_counters, int grid, int smem_bytes, void *stream) {
-    return atkb_pfb_launch_n(d_jobs, d_tile_start, njobs, NULL, d_counters, grid, smem_bytes, stream);
+extern "C" int atkb_pfb_launch(const atkb_job *d_jobs, const int *d_tile_start, const atkb_carry *d_carry,
+                               int njobs, int *d_counters, int grid, int smem_bytes, void *stream) {
+    return atkb_pfb_launch_n(d_jobs, d_tile_start, d_carry, njobs, NULL, d_counters, grid, smem_bytes,
+                             stream);
 }
 
-extern "C" int atkb_pfb_launch_n(const atkb_job *d_jobs, const int *d_tile_start, int njobs,
-                                 const int *d_njobs, int *d_counters, int grid, int smem_bytes,
+extern "C" int atkb_pfb_launch_n(const atkb_job *d_jobs, const int *d_tile_start, const atkb_carry *d_carry,
+                                 int njobs, const int *d_njobs, int *d_counters, int grid, int smem_bytes,
                                  void *stream) {
     if (njobs <= 0) return ATKB_OK;
     if (grid < 1) grid = 1;
-    pfb_tiles_kernel<<<grid, NT, smem_bytes, (cudaStream_t)stream>>>(d_jobs, d_tile_start, njobs,
+    pfb_tiles_kernel<<<grid, NT, smem_bytes, (cudaStream_t)stream>>>(d_jobs, d_tile_start, d_carry, njobs,
                                                                     d_njobs, d_counters);
-    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
-}
-
-extern "C" int atkb_pfb_carry(const atkb_carry *d_carry, int ncarry, long long max_len,
-                              void *stream) {
-    return atkb_pfb_carry_n(d_carry, ncarry, NULL, max_len, stream);
-}
-
-extern "C" int atkb_pfb_carry_n(const atkb_carry *d_carry, int ncarry, const int *d_ncarry,
-                                long long max_len, void *stream) {
-    if (ncarry <= 0 || max_len <= 0) return ATKB_OK;
-    const int grid = ncarry < 1184 ? ncarry : 1184;
-    pfb_carry_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_carry, ncarry, d_ncarry);
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }

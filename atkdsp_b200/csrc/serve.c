@@ -131,8 +131,8 @@ ATKDSP_API atkdsp_server *atkdsp_server_create(unsigned max_streams, size_t hbm_
         s->rounds[r].rec = (atkdsp_server_done *)malloc(max_streams * sizeof(atkdsp_server_done));
         if (rc == ATKB_OK && !s->rounds[r].rec) rc = ATKB_E_NOMEM;
     }
-    if (rc == ATKB_OK) rc = atkb_malloc((void **)&s->d_counters, 2 * sizeof(int));
-    if (rc == ATKB_OK) rc = atkb_memset(s->d_counters, 0, 2 * sizeof(int), s->stream);
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&s->d_counters, ATKB_NCOUNTERS * sizeof(int));
+    if (rc == ATKB_OK) rc = atkb_memset(s->d_counters, 0, ATKB_NCOUNTERS * sizeof(int), s->stream);
     if (rc == ATKB_OK) rc = atkb_stream_sync(s->stream);
     if (rc != ATKB_OK) { atkdsp_server_destroy(s); return NULL; }
     s->grid = atkb_pfb_grid(s->dev, ATKB_FAST_SMEM_MAX);
@@ -217,11 +217,9 @@ static int enqueue_round(atkdsp_server *s, int slot) {
     void *st = s->stream;
     int rc = atkb_h2d(s->d_tables, s->h_tables[slot], s->tbl_bytes, st);
     if (rc == ATKB_OK)
-        rc = atkb_pfb_launch_n(atkb_tbl_jobs(s->d_tables), atkb_tbl_tiles(s->d_tables, s->cap), (int)s->cap,
-                               tbl_count(s->d_tables, s->cap), s->d_counters, s->grid, ATKB_FAST_SMEM_MAX, st);
-    if (rc == ATKB_OK)
-        rc = atkb_pfb_carry_n(atkb_tbl_carry(s->d_tables, s->cap), (int)s->cap, tbl_count(s->d_tables, s->cap),
-                              1, st);
+        rc = atkb_pfb_launch_n(atkb_tbl_jobs(s->d_tables), atkb_tbl_tiles(s->d_tables, s->cap),
+                               atkb_tbl_carry(s->d_tables, s->cap), (int)s->cap, tbl_count(s->d_tables, s->cap),
+                               s->d_counters, s->grid, ATKB_FAST_SMEM_MAX, st);
     return rc;
 }
 

@@ -664,7 +664,7 @@ def run_ours(args, rep):
                      "kernel": "pfb_tiles_kernel", "kernel_ms": round(k_ms, 4),
                      "alg_bytes_per_launch": alg, "peak_kind": peak_kind},
         "configs": extra,
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": args.steps,
         "clocks": clk.summary(),
     }
     if cpu:
