@@ -74,6 +74,12 @@ struct atkdsp_server {
     round_t rounds[NROUNDS];
     int r_head, r_len;
     atkdsp_server_stats stats;
+    /* handles of closed streams, kept for the next open with the same filter
+     * (nchan, oversample, taps, attenuation): closing and reopening then
+     * allocate and free nothing -- a device free would wait for every round
+     * in flight */
+    atkdsp_pfb **parked;
+    unsigned nparked;
 };
 
 static double now_s(void) {
@@ -92,6 +98,8 @@ ATKDSP_API void atkdsp_server_destroy(atkdsp_server *s) {
     atkb_set_device(s->dev);
     if (s->stream) atkb_stream_sync(s->stream);
     for (i = 0; s->st && i < s->cap; ++i) atkdsp_pfb_destroy(s->st[i].p);
+    for (i = 0; i < s->nparked; ++i) atkdsp_pfb_destroy(s->parked[i]);
+    free(s->parked);
     for (r = 0; r < NROUNDS; ++r) {
         atkb_event_destroy(s->rounds[r].ev);
         free(s->rounds[r].rec);
@@ -117,7 +125,8 @@ ATKDSP_API atkdsp_server *atkdsp_server_create(unsigned max_streams, size_t hbm_
     s->reserve = hbm_reserve;
     s->use_graph = use_graph;
     s->st = (sstream *)calloc(max_streams, sizeof *s->st);
-    int rc = s->st ? atkb_get_device(&s->dev) : ATKB_E_NOMEM;
+    s->parked = (atkdsp_pfb **)calloc(max_streams, sizeof *s->parked);
+    int rc = (s->st && s->parked) ? atkb_get_device(&s->dev) : ATKB_E_NOMEM;
     if (rc == ATKB_OK) rc = atkb_set_device(s->dev);
     if (rc == ATKB_OK) rc = atkb_stream_create(&s->stream);
     s->tbl_bytes = atkb_tables_bytes(max_streams) + 16;
@@ -139,6 +148,27 @@ ATKDSP_API atkdsp_server *atkdsp_server_create(unsigned max_streams, size_t hbm_
     return s;
 }
 
+/* a parked handle for this filter, its state cleared on the server's stream
+ * (ordered before any round that uses it), or NULL */
+static atkdsp_pfb *unpark(atkdsp_server *s, double fs, unsigned nchan, unsigned os, unsigned K, double atten) {
+    unsigned k;
+    if (atten < 20.0) atten = 20.0;                 /* as create clamps it */
+    for (k = 0; k < s->nparked; ++k) {
+        atkdsp_pfb *p = s->parked[k];
+        if (p->nchan != nchan || p->os != os || p->K != K || p->atten != atten) continue;
+        if (atkb_memset(p->d_state, 0, 2 * (size_t)p->max_nel * p->cap_state * sizeof(atkdsp_cf32), s->stream) !=
+            ATKB_OK)
+            return NULL;
+        s->parked[k] = s->parked[--s->nparked];
+        p->fs = fs;
+        p->lc = 0;
+        p->b = 0;
+        p->cur = 0;
+        return p;
+    }
+    return NULL;
+}
+
 ATKDSP_API int atkdsp_server_open(atkdsp_server *s, double fs, unsigned nchan, unsigned oversample,
                                   unsigned taps_per_poly, double atten_db, int fmt) {
     unsigned i;
@@ -151,14 +181,24 @@ ATKDSP_API int atkdsp_server_open(atkdsp_server *s, double fs, unsigned nchan, u
     /* only power-of-two channel counts up to 4096 fit the server's 64 KB tile */
     if ((nchan & (nchan - 1)) || nchan < 16 || nchan > 4096) return ATKDSP_E_ARG;
     atkb_set_device(s->dev);
-    size_t fr = 0, tot = 0;
-    if (atkb_mem_info(&fr, &tot) != ATKB_OK) return ATKDSP_E_FFT;
-    if (fr < s->reserve + atkb_stream_footprint(nchan, oversample, taps_per_poly)) {
-        ++s->stats.denied;
-        return ATKDSP_E_NOMEM;
+    atkdsp_pfb *p = unpark(s, fs, nchan, oversample, taps_per_poly, atten_db);
+    if (!p) {
+        size_t fr = 0, tot = 0;
+        const size_t need = s->reserve + atkb_stream_footprint(nchan, oversample, taps_per_poly);
+        if (atkb_mem_info(&fr, &tot) != ATKB_OK) return ATKDSP_E_FFT;
+        if (fr < need && s->nparked) {              /* parked handles of other shapes give way */
+            unsigned k;
+            for (k = 0; k < s->nparked; ++k) atkdsp_pfb_destroy(s->parked[k]);
+            s->nparked = 0;
+            if (atkb_mem_info(&fr, &tot) != ATKB_OK) return ATKDSP_E_FFT;
+        }
+        if (fr < need) {
+            ++s->stats.denied;
+            return ATKDSP_E_NOMEM;
+        }
+        p = atkb_pfb_create_internal(fs, nchan, oversample, taps_per_poly, atten_db, 1, 1);
+        if (!p) { ++s->stats.denied; return ATKDSP_E_NOMEM; }
     }
-    atkdsp_pfb *p = atkb_pfb_create_internal(fs, nchan, oversample, taps_per_poly, atten_db, 1, 1);
-    if (!p) { ++s->stats.denied; return ATKDSP_E_NOMEM; }
     memset(&s->st[i], 0, sizeof s->st[i]);
     s->st[i].p = p;
     s->st[i].state = 1;
@@ -168,7 +208,8 @@ ATKDSP_API int atkdsp_server_open(atkdsp_server *s, double fs, unsigned nchan, u
 }
 
 static void stream_free(atkdsp_server *s, unsigned i) {
-    atkdsp_pfb_destroy(s->st[i].p);
+    if (s->parked && s->nparked < s->cap) s->parked[s->nparked++] = s->st[i].p;
+    else atkdsp_pfb_destroy(s->st[i].p);
     s->st[i].p = NULL;
     s->st[i].state = 0;
     ++s->stats.closed;
