@@ -238,7 +238,8 @@ ATKDSP_API void atkdsp_pfb_destroy(atkdsp_pfb *p) {
     if (p->dev >= 0) atkb_set_device(p->dev);
     if (p->stream) atkb_stream_sync(p->stream);
     bank_release(p->be);
-    atkb_free(p->d_state);
+    if (p->pool_stream) atkb_free_async(p->d_state, p->pool_stream);
+    else atkb_free(p->d_state);
     atkb_free(p->d_cal);
     atkb_free(p->d_in_stage);
     atkb_free(p->d_out_stage);
@@ -489,6 +490,41 @@ atkdsp_pfb *atkb_pfb_create_internal(double fs, unsigned nchan, unsigned oversam
     p->lc = 0;
     p->b = 0;
     p->cur = 0;
+    return p;
+}
+
+atkdsp_pfb *atkb_pfb_create_served(double fs, unsigned nchan, unsigned oversample, unsigned taps_per_poly,
+                                   double atten_db, void *pool, void *stream) {
+    if (!(fs > 0.0) || nchan < 2 || oversample < 1 || nchan % oversample != 0 || taps_per_poly < 2) return NULL;
+    if (is_pow2(nchan) ? nchan > MAX_POW2_NCHAN : nchan > MAX_GENERIC_NCHAN) return NULL;
+    if (atten_db < 20.0) atten_db = 20.0;
+    atkdsp_pfb *p = (atkdsp_pfb *)calloc(1, sizeof *p);
+    if (!p) return NULL;
+    p->fs = fs;
+    p->atten = atten_db;
+    p->nchan = nchan;
+    p->os = oversample;
+    p->K = taps_per_poly;
+    p->max_nel = 1;
+    p->hop = nchan / oversample;
+    p->L = (size_t)nchan * taps_per_poly;
+    p->ov = p->L - p->hop;
+    p->lean = 1;
+    if (atkb_get_device(&p->dev) != ATKB_OK) { free(p); return NULL; }
+    int rc = ATKB_OK;
+    /* a bank already in the cache costs nothing; a new one is built (and
+     * waited for) on the server's stream */
+    p->be = bank_acquire(p->dev, nchan, oversample, taps_per_poly, atten_db, stream, &rc);
+    if (p->be) {
+        p->bank = p->be->bank;
+        p->d_bank = p->be->d_bank;
+    }
+    p->cap_state = p->ov + p->hop;
+    const size_t sb = 2 * p->cap_state * sizeof(atkdsp_cf32);
+    if (rc == ATKB_OK) rc = atkb_malloc_pool(&p->d_state, sb, pool, stream);
+    if (rc == ATKB_OK) p->pool_stream = stream;
+    if (rc == ATKB_OK) rc = atkb_memset(p->d_state, 0, sb, stream);
+    if (rc != ATKB_OK) { atkdsp_pfb_destroy(p); return NULL; }
     return p;
 }
 

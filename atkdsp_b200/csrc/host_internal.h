@@ -12,6 +12,11 @@
  * rounds) reserves this much. */
 #define ATKB_FAST_SMEM_MAX (4096 * 16 + 4096 * 8)
 
+/* a server stream's handle: lean, its state from `pool` on `stream`
+ * (stream-ordered, cleared there), no cal table, no synchronisation */
+atkdsp_pfb *atkb_pfb_create_served(double fs, unsigned nchan, unsigned oversample, unsigned taps_per_poly,
+                                   double atten_db, void *pool, void *stream);
+
 /* host calls of at most this many samples per element stage through pinned
  * memory owned by the handle */
 #define ATKB_SMALL_N ((size_t)1 << 15)
@@ -30,6 +35,8 @@ struct atkdsp_pfb {
     size_t L, ov;
     int dev;
     int lean;                     /* no host-path staging or tables (server streams) */
+    void *pool_stream;            /* server streams: d_state came from the server's
+                                   * pool on this stream and is freed on it */
     void *stream;
     void *tbl_event;              /* the last table upload; gates reuse of h_tables */
     int tbl_event_live;

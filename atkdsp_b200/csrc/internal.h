@@ -105,6 +105,11 @@ void atkb_stream_destroy(void *stream);
 int  atkb_stream_sync(void *stream);
 int  atkb_malloc(void **p, size_t bytes);
 void atkb_free(void *p);
+int  atkb_pool_create(int dev, void **pool);       /* stream-ordered device pool */
+void atkb_pool_destroy(void *pool);
+size_t atkb_pool_idle_bytes(void *pool);
+int  atkb_malloc_pool(void **p, size_t bytes, void *pool, void *stream);
+void atkb_free_async(void *p, void *stream);
 int  atkb_host_alloc(void **p, size_t bytes);      /* pinned */
 void atkb_host_free(void *p);
 int  atkb_h2d(void *dst, const void *src, size_t bytes, void *stream);

@@ -76,10 +76,10 @@ struct atkdsp_server {
     atkdsp_server_stats stats;
     /* handles of closed streams, kept for the next open with the same filter
      * (nchan, oversample, taps, attenuation): closing and reopening then
-     * allocate and free nothing -- a device free would wait for every round
-     * in flight */
+     * allocate and free nothing */
     atkdsp_pfb **parked;
     unsigned nparked;
+    void *pool;                   /* stream-ordered pool for the streams' state */
 };
 
 static double now_s(void) {
@@ -100,6 +100,8 @@ ATKDSP_API void atkdsp_server_destroy(atkdsp_server *s) {
     for (i = 0; s->st && i < s->cap; ++i) atkdsp_pfb_destroy(s->st[i].p);
     for (i = 0; i < s->nparked; ++i) atkdsp_pfb_destroy(s->parked[i]);
     free(s->parked);
+    if (s->stream) atkb_stream_sync(s->stream);
+    atkb_pool_destroy(s->pool);
     for (r = 0; r < NROUNDS; ++r) {
         atkb_event_destroy(s->rounds[r].ev);
         free(s->rounds[r].rec);
@@ -129,6 +131,7 @@ ATKDSP_API atkdsp_server *atkdsp_server_create(unsigned max_streams, size_t hbm_
     int rc = (s->st && s->parked) ? atkb_get_device(&s->dev) : ATKB_E_NOMEM;
     if (rc == ATKB_OK) rc = atkb_set_device(s->dev);
     if (rc == ATKB_OK) rc = atkb_stream_create(&s->stream);
+    if (rc == ATKB_OK) rc = atkb_pool_create(s->dev, &s->pool);
     s->tbl_bytes = atkb_tables_bytes(max_streams) + 16;
     if (rc == ATKB_OK) rc = atkb_malloc(&s->d_tables, s->tbl_bytes);
     for (r = 0; r < 2 && rc == ATKB_OK; ++r) {
@@ -183,20 +186,24 @@ ATKDSP_API int atkdsp_server_open(atkdsp_server *s, double fs, unsigned nchan, u
     atkb_set_device(s->dev);
     atkdsp_pfb *p = unpark(s, fs, nchan, oversample, taps_per_poly, atten_db);
     if (!p) {
+        /* free HBM plus what the pool holds unused must cover the reserve and
+         * the stream's footprint */
         size_t fr = 0, tot = 0;
         const size_t need = s->reserve + atkb_stream_footprint(nchan, oversample, taps_per_poly);
         if (atkb_mem_info(&fr, &tot) != ATKB_OK) return ATKDSP_E_FFT;
+        fr += atkb_pool_idle_bytes(s->pool);
         if (fr < need && s->nparked) {              /* parked handles of other shapes give way */
             unsigned k;
             for (k = 0; k < s->nparked; ++k) atkdsp_pfb_destroy(s->parked[k]);
             s->nparked = 0;
             if (atkb_mem_info(&fr, &tot) != ATKB_OK) return ATKDSP_E_FFT;
+            fr += atkb_pool_idle_bytes(s->pool);
         }
         if (fr < need) {
             ++s->stats.denied;
             return ATKDSP_E_NOMEM;
         }
-        p = atkb_pfb_create_internal(fs, nchan, oversample, taps_per_poly, atten_db, 1, 1);
+        p = atkb_pfb_create_served(fs, nchan, oversample, taps_per_poly, atten_db, s->pool, s->stream);
         if (!p) { ++s->stats.denied; return ATKDSP_E_NOMEM; }
     }
     memset(&s->st[i], 0, sizeof s->st[i]);
@@ -208,17 +215,26 @@ ATKDSP_API int atkdsp_server_open(atkdsp_server *s, double fs, unsigned nchan, u
 }
 
 static void stream_free(atkdsp_server *s, unsigned i) {
-    if (s->parked && s->nparked < s->cap) s->parked[s->nparked++] = s->st[i].p;
-    else atkdsp_pfb_destroy(s->st[i].p);
-    s->st[i].p = NULL;
     s->st[i].state = 0;
     ++s->stats.closed;
+}
+
+/* A closed stream's handle is parked at once, rounds in flight or not: every
+ * later use of it -- the memset that clears it for a new stream, that
+ * stream's rounds, or an asynchronous free -- is queued on the server's
+ * stream behind those rounds. */
+static void park(atkdsp_server *s, atkdsp_pfb *p) {
+    if (!p) return;
+    if (s->nparked < s->cap) s->parked[s->nparked++] = p;
+    else atkdsp_pfb_destroy(p);
 }
 
 ATKDSP_API int atkdsp_server_close(atkdsp_server *s, int id) {
     if (!s || id < 0 || (unsigned)id >= s->cap || s->st[id].state != 1) return ATKDSP_E_ARG;
     s->st[id].state = 2;
     s->st[id].qlen = 0;                      /* blocks not yet launched are dropped */
+    park(s, s->st[id].p);
+    s->st[id].p = NULL;
     if (!s->st[id].inflight) stream_free(s, (unsigned)id);
     return ATKDSP_OK;
 }
@@ -502,6 +518,7 @@ ATKDSP_API int atkdsp_server_simulate(atkdsp_server *s, const atkdsp_sim_config 
         double next_churn = cfg->churn_per_s > 0 ? t0 + rng_exp(&seed, 1.0 / cfg->churn_per_s) : 1e300;
         const double t_end = t0 + cfg->duration_s;
         const double t_warm = t0 + cfg->warmup_s;
+        double t_prev = 0.0;
         for (;;) {
             const double t = now_s();
             if (t >= t_end && s->r_len == 0) break;
@@ -525,9 +542,14 @@ ATKDSP_API int atkdsp_server_simulate(atkdsp_server *s, const atkdsp_sim_config 
                 if (t >= next_churn) {
                     /* one stream leaves and a new one asks to join */
                     const unsigned k = (unsigned)(rng_next(&seed) % ns);
+                    double c0 = now_s();
                     if (sid[k] >= 0) atkdsp_server_close(s, sid[k]);
+                    double c1 = now_s();
                     sid[k] = atkdsp_server_open(s, rate[k], nch[k], cfg->oversample, cfg->taps, cfg->atten_db,
                                                 cfg->fmt);
+                    const double c2 = now_s();
+                    if ((c1 - c0) * 1e3 > res->max_close_ms) res->max_close_ms = (c1 - c0) * 1e3;
+                    if ((c2 - c1) * 1e3 > res->max_open_ms) res->max_open_ms = (c2 - c1) * 1e3;
                     if (sid[k] < 0) ++res->denied;
                     else ++res->admitted;
                     res->churn_events += 1;
@@ -536,11 +558,21 @@ ATKDSP_API int atkdsp_server_simulate(atkdsp_server *s, const atkdsp_sim_config 
             }
             /* continuous batching: a new round whenever fewer than two are on the GPU */
             if (s->r_len < 2) {
+                const double l0 = now_s();
                 const int got = atkdsp_server_launch(s);
                 if (got < 0) { rc = got; goto out; }
+                const double dl = (now_s() - l0) * 1e3;
+                if (dl > res->max_launch_ms) res->max_launch_ms = dl;
             }
+            const double p0 = now_s();
             const int nd = atkdsp_server_poll(s, done, dcap, 0);
             if (nd < 0) { rc = nd; goto out; }
+            {
+                const double p1 = now_s();
+                if ((p1 - p0) * 1e3 > res->max_poll_ms) res->max_poll_ms = (p1 - p0) * 1e3;
+                if (t_prev > 0.0 && (p1 - t_prev) * 1e3 > res->max_loop_ms) res->max_loop_ms = (p1 - t_prev) * 1e3;
+                t_prev = p1;
+            }
             for (int k2 = 0; k2 < nd; ++k2) {
                 if (done[k2].t_arrival < t_warm) continue;       /* warm-up blocks not counted */
                 res->samples_done += (uint64_t)done[k2].n;

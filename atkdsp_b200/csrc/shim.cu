@@ -1,6 +1,7 @@
 /* The thin C-ABI shim between the C99 host layer and the CUDA runtime.
  * Every function returns an ATKB_* status; no CUDA type crosses into C. */
 #include <cuda_runtime.h>
+#include <stdint.h>
 #include "internal.h"
 
 static int st(cudaError_t e) {
@@ -37,6 +38,43 @@ extern "C" int atkb_malloc(void **p, size_t bytes) {
 }
 extern "C" void atkb_free(void *p) {
     if (p) cudaFree(p);
+}
+/* a stream-ordered pool on `dev` that keeps freed memory for reuse (release
+ * threshold at its maximum): allocations from it in steady state map nothing
+ * and wait for nothing */
+extern "C" int atkb_pool_create(int dev, void **pool) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t mp = nullptr;
+    *pool = nullptr;
+    int rc = st(cudaMemPoolCreate(&mp, &props));
+    if (rc != ATKB_OK) return rc;
+    uint64_t thr = ~(uint64_t)0;
+    rc = st(cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr));
+    if (rc != ATKB_OK) { cudaMemPoolDestroy(mp); return rc; }
+    *pool = (void *)mp;
+    return ATKB_OK;
+}
+extern "C" void atkb_pool_destroy(void *pool) {
+    if (pool) cudaMemPoolDestroy((cudaMemPool_t)pool);
+}
+/* bytes the pool holds but no allocation uses */
+extern "C" size_t atkb_pool_idle_bytes(void *pool) {
+    uint64_t res = 0, used = 0;
+    if (!pool) return 0;
+    if (cudaMemPoolGetAttribute((cudaMemPool_t)pool, cudaMemPoolAttrReservedMemCurrent, &res) != cudaSuccess ||
+        cudaMemPoolGetAttribute((cudaMemPool_t)pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess)
+        return 0;
+    return res > used ? (size_t)(res - used) : 0;
+}
+extern "C" int atkb_malloc_pool(void **p, size_t bytes, void *pool, void *stream) {
+    *p = nullptr;
+    return st(cudaMallocFromPoolAsync(p, bytes ? bytes : 256, (cudaMemPool_t)pool, (cudaStream_t)stream));
+}
+extern "C" void atkb_free_async(void *p, void *stream) {
+    if (p) cudaFreeAsync(p, (cudaStream_t)stream);
 }
 extern "C" int atkb_host_alloc(void **p, size_t bytes) {
     *p = nullptr;

@@ -43,7 +43,9 @@ class SimResult(C.Structure):
                 ("samples_done", C.c_uint64), ("churn_events", C.c_uint64), ("admitted", C.c_uint64),
                 ("denied", C.c_uint64), ("rounds", C.c_uint64), ("blocks_per_round", C.c_double),
                 ("wall_s", C.c_double), ("lat_p50_ms", C.c_double), ("lat_p90_ms", C.c_double),
-                ("lat_p99_ms", C.c_double), ("lat_max_ms", C.c_double)]
+                ("lat_p99_ms", C.c_double), ("lat_max_ms", C.c_double), ("max_open_ms", C.c_double),
+                ("max_close_ms", C.c_double), ("max_launch_ms", C.c_double), ("max_poll_ms", C.c_double),
+                ("max_loop_ms", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

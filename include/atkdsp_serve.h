@@ -93,6 +93,9 @@ typedef struct {
         rounds;
     double blocks_per_round, wall_s;
     double lat_p50_ms, lat_p90_ms, lat_p99_ms, lat_max_ms;
+    /* the longest single host call of each kind during the run, and the
+     * longest pass of the driver loop (where a stall on the host shows) */
+    double max_open_ms, max_close_ms, max_launch_ms, max_poll_ms, max_loop_ms;
 } atkdsp_sim_result;
 
 ATKDSP_API int           atkdsp_server_simulate(atkdsp_server *s, const atkdsp_sim_config *cfg,
