@@ -136,11 +136,8 @@ static int plan_fft(unsigned M, unsigned os, atkb_fft_plan *pl) {
     memset(pl, 0, sizeof *pl);
     if (is_pow2(M) && M >= 16 && M <= MAX_POW2_NCHAN) {
         /* the paired fold: hop b's window is hop a's shifted by 8/os branch
-         * slots, so os must divide 4 (M/os a multiple of 2*M/8). At nchan
-         * 4096 (two-hop tiles with a 32 KB side buffer) it measured no faster
-         * on B200 (22.5 vs 22.4 GS/s at K=16, os=2) while its 96 KB of shared
-         * memory per CTA shrank L1 for every other tile in a mixed launch, so
-         * it stays off there */
+         * slots, so os must divide 4 (M/os a multiple of 2*M/8), and a tile
+         * must hold two hops (nchan <= 2048) */
         const int pair = ATKB_PTS == 8 && M <= 2048 && (os == 1 || os == 2 || os == 4);
         unsigned rem = M / (pair ? 4 : ATKB_PTS);
         pl->fast = 1;
@@ -337,11 +334,7 @@ static int bank_build(bank_entry *be, void *stream) {
         unsigned v = M;
         while (v > 1) { v >>= 1; ++B->logm; }
     }
-    if (pl.fast && pl.pair && M == 4096) {
-        /* two hops a tile: the FFT tile plus hop b's sums (4096 float2) */
-        B->tile_hops = 2;
-        B->smem_bytes = ATKB_FAST_SMEM_MAX;
-    } else if (pl.fast) {
+    if (pl.fast) {
         B->tile_hops = 4096 / (int)M;
         B->smem_bytes = 4096 * 16;
     } else {

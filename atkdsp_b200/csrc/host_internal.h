@@ -6,11 +6,10 @@
 #include "atkdsp_gpu.h"
 #include "internal.h"
 
-/* dynamic shared memory of the largest power-of-two (fast path) tile: the
- * 4096-point double FFT tile plus, for nchan 4096 paired, hop b's 4096 float2
- * sums. A launch that may meet any fast-path bank (the server's captured
- * rounds) reserves this much. */
-#define ATKB_FAST_SMEM_MAX (4096 * 16 + 4096 * 8)
+/* dynamic shared memory of the largest power-of-two (fast path) tile, the
+ * 4096-point double FFT tile: a launch that may meet any fast-path bank (the
+ * server's captured rounds) reserves this much */
+#define ATKB_FAST_SMEM_MAX (4096 * 16)
 
 /* a server stream's handle: lean, its state from `pool` on `stream`
  * (stream-ordered, cleared there), no cal table, no synchronisation */

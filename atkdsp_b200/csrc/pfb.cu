@@ -15,21 +15,25 @@
  *
  * Kernel layout (B200-first):
  *   - ONE persistent kernel over a device job list. A job is a run of hops of
- *     one element stream (a handle's element, or one stream of a batch); a
- *     tile is tile_hops consecutive hops of a job. CTAs take tiles from an
- *     atomic counter until none are left, so one launch serves one element
- *     or four thousand uneven streams, and the launch shape is fixed (CUDA
- *     graph friendly). The counter resets itself when the last CTA leaves.
+ *     one element stream (a handle's element, one stream of a batch, or one
+ *     served block); a tile is tile_hops consecutive hops of a job. CTAs
+ *     (512 threads, 2 per SM) claim tiles from an atomic counter; warp 0
+ *     claims and looks up the next tile while the CTA works on the current
+ *     one. CTAs out of tiles copy the state carries (each job's tail into
+ *     its other state buffer, which no tile reads). The launch shape is
+ *     fixed (CUDA graph friendly) and the counters reset themselves when the
+ *     last CTA leaves.
  *   - Fast path (M a power of two, 16..4096): a tile is 4096 complex points
- *     (tile_hops = 4096/M), 256 threads x 16 points. Each thread folds the 16
- *     branches j + r*M/16 of one hop straight into registers -- exactly the
- *     inputs of the first radix-16 Stockham butterfly -- so the fold never
- *     touches shared memory; later radix-16/8/4/2 passes run in place in
- *     shared memory (register staging between two barriers), per-pass
- *     twiddle tables are laid out so consecutive lanes read consecutive
- *     entries. The epilogue rotates, applies cal, rounds, transposes the tile
- *     hop-major -> channel-major in shared memory and writes runs of
- *     tile_hops consecutive outputs per channel.
+ *     (tile_hops = 4096/M), 512 threads x 8 points. For oversample 1/2/4 and
+ *     M <= 2048 each thread folds two consecutive hops over the even or odd
+ *     branches (the paired fold: every sample and tap load serves both
+ *     hops) into a radix-4 first Stockham pass in registers; otherwise one
+ *     hop's 8 branches into a radix-8 first pass. Small M stages the tile
+ *     window in shared memory with cp.async first. The FFT runs in double,
+ *     radix-8 passes in place in shared memory (XOR swizzle, one twiddle
+ *     load per butterfly, group barriers), the last pass fused with the
+ *     rotation, cal, rounding and the transpose to channel-major; each
+ *     channel gets a run of tile_hops consecutive outputs.
  *   - Generic path (any M >= 2): ping-pong shared buffers, mixed radix
  *     (2, 3, 4, 8, 16 butterflies, direct DFT for any other prime factor).
  */
@@ -163,11 +167,12 @@ struct Src {
 };
 
 /* ---- fast path: nchan = 2^n, 16 <= nchan <= 4096 ------------------------- */
-/* Shared-memory index swizzle for the 16-byte complex doubles: the low four
- * index bits are XORed with the next four. The first pass stores at a stride
- * of 16 elements across lanes; swizzled, every 8-lane wavefront lands on 8
- * distinct 16-byte slots, and the unit-stride accesses of later passes stay
- * conflict-free too (a XOR with a per-block constant permutes the slots). */
+/* Shared-memory index swizzle for the 16-byte complex doubles: the low LOGP
+ * index bits are XORed with the next LOGP. The first pass stores at a stride
+ * of PTS (or 4) elements across lanes; swizzled, every 8-lane wavefront lands
+ * on 8 distinct 16-byte slots, and the unit-stride accesses of later passes
+ * stay conflict-free too (a XOR with a per-block constant permutes the
+ * slots). */
 __device__ __forceinline__ int SW(int i) { return i ^ ((i >> LOGP) & (PTS - 1)); }
 
 /* the twiddles of one butterfly, w[r] = W^(r k) for r = 1 .. R-1, from the
@@ -699,46 +704,6 @@ __device__ __forceinline__ void write_tile(const atkb_job &J, long long h0, int 
     }
 }
 
-/* nchan 4096, paired: a tile is two hops. Thread j folds both parities in
- * turn; hop ta's radix-4 outputs go to the FFT tile, hop tb's raw sums to a
- * side buffer (4096 float2 after the tile, 96 KB in all) until hop ta's FFT
- * and write are done. */
-template <int LOGOS>
-__device__ void tile_pair_4096(const atkb_job &J, const atkb_bank &B, long long h0, int nvalid,
-                               double2 *sm) {
-    constexpr int M = 4096;
-    constexpr int MP = M >> LOGP;
-    static_assert(PTS == 8 && NT == MP, "one thread per branch j");
-    float2 *side = (float2 *)(sm + M);
-    float2 *to = (float2 *)sm;
-    const int j = threadIdx.x;
-    const bool tb_ok = nvalid > 1;
-#pragma unroll 1
-    for (int c = 0; c < 2; ++c) {
-        float2 a[4], b[4];
-        fold_pair_global<12, LOGOS>(a, b, J, B, h0, nvalid, 0, c, j, tb_ok);
-        first_pass4<12>(a, sm, 0, j + c * MP);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) side[i * (2 * MP) + c * MP + j] = b[i];
-    }
-    __syncthreads();
-    const double2 *wp = (const double2 *)B.wpass;
-    fft_rest<12, 2, 1>(sm, wp, B.plan.twoff, to, B, J, h0);
-    write_tile<12>(J, h0, 1, to);
-    if (!tb_ok) return;                  /* uniform: nvalid is the CTA's */
-    __syncthreads();                     /* tile_out read before the tile is reused */
-#pragma unroll 1
-    for (int c = 0; c < 2; ++c) {
-        float2 b[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) b[i] = side[i * (2 * MP) + c * MP + j];
-        first_pass4<12>(b, sm, 0, j + c * MP);
-    }
-    __syncthreads();
-    fft_rest<12, 2, 1>(sm, wp, B.plan.twoff, to, B, J, h0 + 1);
-    write_tile<12>(J, h0 + 1, 1, to);
-}
-
 /* LOGOS < 0: one hop and PTS branches per thread, first pass radix PTS;
  * LOGOS = log2(os) in 0..2: the paired fold, first pass radix 4 */
 template <int LOGM, int LOGOS>
@@ -979,9 +944,6 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
         UNPAIRED(4) UNPAIRED(5) UNPAIRED(6) UNPAIRED(7) UNPAIRED(8) UNPAIRED(9) UNPAIRED(10)
         UNPAIRED(11) UNPAIRED(12)
         PAIRED(4) PAIRED(5) PAIRED(6) PAIRED(7) PAIRED(8) PAIRED(9) PAIRED(10) PAIRED(11)
-        case 16 + 12: tile_pair_4096<0>(J, SB, h0, nvalid, sm); break;
-        case 32 + 12: tile_pair_4096<1>(J, SB, h0, nvalid, sm); break;
-        case 48 + 12: tile_pair_4096<2>(J, SB, h0, nvalid, sm); break;
 #undef UNPAIRED
 #undef PAIRED
         case -1: break;
