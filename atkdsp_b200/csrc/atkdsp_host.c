@@ -334,7 +334,12 @@ static int bank_build(bank_entry *be, void *stream) {
         unsigned v = M;
         while (v > 1) { v >>= 1; ++B->logm; }
     }
-    if (pl.fast) {
+    if (pl.fast && M == 4096) {
+        /* two hops a tile, computed in turn: the FFT tile plus the first
+         * hop's 4096 outputs (so the write covers two hops per channel) */
+        B->tile_hops = 2;
+        B->smem_bytes = ATKB_FAST_SMEM_MAX;
+    } else if (pl.fast) {
         B->tile_hops = 4096 / (int)M;
         B->smem_bytes = 4096 * 16;
     } else {

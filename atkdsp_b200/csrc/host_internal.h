@@ -6,10 +6,11 @@
 #include "atkdsp_gpu.h"
 #include "internal.h"
 
-/* dynamic shared memory of the largest power-of-two (fast path) tile, the
- * 4096-point double FFT tile: a launch that may meet any fast-path bank (the
- * server's captured rounds) reserves this much */
-#define ATKB_FAST_SMEM_MAX (4096 * 16)
+/* dynamic shared memory of the largest power-of-two (fast path) tile: the
+ * 4096-point double FFT tile plus, at nchan 4096, one hop's 4096 outputs. A
+ * launch that may meet any fast-path bank (the server's captured rounds)
+ * reserves this much. */
+#define ATKB_FAST_SMEM_MAX (4096 * 16 + 4096 * 8)
 
 /* a server stream's handle: lean, its state from `pool` on `stream`
  * (stream-ordered, cleared there), no cal table, no synchronisation */

@@ -704,6 +704,80 @@ __device__ __forceinline__ void write_tile(const atkb_job &J, long long h0, int 
     }
 }
 
+/* fold + first Stockham pass (Ns = 1, radix PTS, no twiddles) of one hop
+ * and PTS branches per thread, into the tile's shared points */
+template <int LOGM>
+__device__ __forceinline__ void fold_first_unpaired(const atkb_job &J, const atkb_bank &B, long long h0,
+                                                    int nvalid, double2 *sm) {
+    constexpr int MP = (1 << LOGM) >> LOGP;
+    const int tid = threadIdx.x;
+    const int tt = tid >> (LOGM - LOGP);
+    const int j = tid & (MP - 1);
+    double2 v[PTS];
+    if (!fold_tile_staged<LOGM>(v, J, B, h0, nvalid, tt, j, sm)) {
+        if (tt < nvalid) {
+            const long long w0 = h0 * (long long)B.hop;                       /* first window start */
+            const long long w1 = (h0 + nvalid - 1) * (long long)B.hop + B.L;  /* last window end */
+            const long long off = (h0 + tt) * (long long)B.hop + j;
+            if (w0 >= J.head) {
+                if (J.in_kind)
+                    foldP<LOGM, 1>(v, J, B, h0, tt, j, (const short2 *)J.in + (off - J.head));
+                else
+                    foldP<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.in + (off - J.head));
+            } else if (w1 <= J.head) {
+                foldP<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.state + off);
+            } else {
+                foldP<LOGM, 2>(v, J, B, h0, tt, j, nullptr);
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < PTS; ++r) v[r] = make_double2(0.0, 0.0);
+        }
+    }
+    dftR<PTS>(v);
+#pragma unroll
+    for (int r = 0; r < PTS; ++r) sm[SW((tt << LOGM) + j * PTS + r)] = v[r];
+}
+
+/* nchan 4096: a tile is two hops, computed in turn. Hop a's outputs wait in
+ * a side buffer (4096 float2 after the FFT tile, 96 KB in all) while hop b
+ * is computed, so the write covers two hops per channel: lanes 2l and 2l+1
+ * write the two adjacent outputs of one channel, half the sectors of
+ * single-hop writes (a single hop's 4096 outputs land in 4096 rows). */
+__device__ void tile_4096x2(const atkb_job &J, const atkb_bank &B, long long h0, int nvalid, double2 *sm) {
+    constexpr int LOGM = 12;
+    constexpr int M = 1 << LOGM;
+    constexpr int MP = M >> LOGP;
+    static_assert(NT == MP, "one thread per branch group");
+    float2 *tile_out = (float2 *)sm;       /* pass_last: hop at tile_out[kb * 2] */
+    float2 *side = (float2 *)(sm + M);
+    const double2 *wp = (const double2 *)B.wpass;
+    const int tid = threadIdx.x;
+#pragma unroll 1
+    for (int sub = 0; sub < 2 && sub < nvalid; ++sub) {
+        fold_first_unpaired<LOGM>(J, B, h0 + sub, 1, sm);
+        __syncthreads();
+        fft_rest<LOGM, LOGP, 1, NT>(sm, wp, B.plan.twoff, tile_out, B, J, h0 + sub);
+        if (sub == 0) {
+#pragma unroll
+            for (int u = 0; u < PTS; ++u) side[tid + u * MP] = tile_out[(tid + u * MP) * 2];
+            __syncthreads();                 /* read before hop b's first pass */
+        }
+    }
+    const int t2 = tid & 1;
+    if (t2 < nvalid) {
+        const int kb0 = tid >> 1;
+        float2 *o = (float2 *)J.out + (J.out_col + h0 + t2) + (long long)kb0 * J.ldo;
+        const long long step = (long long)(NT / 2) * J.ldo;
+#pragma unroll 4
+        for (int u = 0; u < 2 * PTS; ++u) {
+            const int kb = kb0 + u * (NT / 2);
+            *o = t2 ? tile_out[kb * 2] : side[kb];
+            o += step;
+        }
+    }
+}
+
 /* LOGOS < 0: one hop and PTS branches per thread, first pass radix PTS;
  * LOGOS = log2(os) in 0..2: the paired fold, first pass radix 4 */
 template <int LOGM, int LOGOS>
@@ -720,33 +794,7 @@ __device__ void tile_fast(const atkb_job &J, const atkb_bank &B, long long h0, i
         static_assert(PTS == 8 && LOGM <= 11 && LOGOS <= 2, "paired fold: PTS 8, two hops a tile");
         fold_tile_pair<LOGM, LOGOS>(J, B, h0, nvalid, sm);
     } else {
-        const int tt = tid >> (LOGM - LOGP);
-        const int j = tid & (MP - 1);
-        /* fold + first Stockham pass (Ns = 1, radix PTS, no twiddles) */
-        double2 v[PTS];
-        if (!fold_tile_staged<LOGM>(v, J, B, h0, nvalid, tt, j, sm)) {
-            if (tt < nvalid) {
-                const long long w0 = h0 * (long long)B.hop;                       /* first window start */
-                const long long w1 = (h0 + nvalid - 1) * (long long)B.hop + B.L;  /* last window end */
-                const long long off = (h0 + tt) * (long long)B.hop + j;
-                if (w0 >= J.head) {
-                    if (J.in_kind)
-                        foldP<LOGM, 1>(v, J, B, h0, tt, j, (const short2 *)J.in + (off - J.head));
-                    else
-                        foldP<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.in + (off - J.head));
-                } else if (w1 <= J.head) {
-                    foldP<LOGM, 0>(v, J, B, h0, tt, j, (const float2 *)J.state + off);
-                } else {
-                    foldP<LOGM, 2>(v, J, B, h0, tt, j, nullptr);
-                }
-            } else {
-#pragma unroll
-                for (int r = 0; r < PTS; ++r) v[r] = make_double2(0.0, 0.0);
-            }
-        }
-        dftR<PTS>(v);
-#pragma unroll
-        for (int r = 0; r < PTS; ++r) sm[SW((tt << LOGM) + j * PTS + r)] = v[r];
+        fold_first_unpaired<LOGM>(J, B, h0, nvalid, sm);
     }
     /* from here to the last pass each hop group (the threads of a hop pair,
      * or of one hop) touches only its own points: group barriers suffice.
@@ -942,7 +990,8 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
         case 32 + L: tile_fast<L, 1>(J, SB, h0, nvalid, sm, to); break;    \
         case 48 + L: tile_fast<L, 2>(J, SB, h0, nvalid, sm, to); break;
         UNPAIRED(4) UNPAIRED(5) UNPAIRED(6) UNPAIRED(7) UNPAIRED(8) UNPAIRED(9) UNPAIRED(10)
-        UNPAIRED(11) UNPAIRED(12)
+        UNPAIRED(11)
+        case 12: tile_4096x2(J, SB, h0, nvalid, sm); break;
         PAIRED(4) PAIRED(5) PAIRED(6) PAIRED(7) PAIRED(8) PAIRED(9) PAIRED(10) PAIRED(11)
 #undef UNPAIRED
 #undef PAIRED
