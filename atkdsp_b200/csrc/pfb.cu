@@ -310,20 +310,20 @@ __device__ __forceinline__ void pass_last(double2 *sm, const double2 *__restrict
     __syncthreads();
     const double2 *twd = (const double2 *)B.twd;
     const float2 *cal = (const float2 *)J.cal;
-    const int os = B.os, hop = B.hop;
-    const bool os_pow2 = (os & (os - 1)) == 0;
-    const int s0 = (int)((J.b0 + h0 + 1) % os);
+    /* os divides M, a power of two here: every "mod os" is a mask */
+    const int osm = B.os - 1, hop = B.hop;
+    const int s0 = (int)(J.b0 + h0 + 1) & osm;
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         const int bi = bfly<U>(u);
         const int tt = bi >> LOGMR;
         const int j = bi & (MR - 1);
-        const int s = os_pow2 ? ((s0 + tt) & (os - 1)) : ((s0 + tt) % os);
+        const int s = (s0 + tt) & osm;
         dftR<R>(v[u]);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int kb = j + r * NS;
-            tile_out[kb * (NH + 1) + tt] = finish_bin(v[u][r], kb, s, M, os, hop, os_pow2, twd, cal);
+            tile_out[kb * (NH + 1) + tt] = finish_bin(v[u][r], kb, s, M, osm + 1, hop, true, twd, cal);
         }
     }
     __syncthreads();
