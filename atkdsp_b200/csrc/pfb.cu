@@ -523,11 +523,23 @@ struct PairLin16 {                     /* raw int16 I/Q, converted on the fly */
     }
 };
 template <int LOGM>
-struct PairMixed {                     /* state / input by index */
-    Src src;
-    long long g;
+struct PairMixed {                     /* cf32 state / input by index */
+    const float2 *st, *in;
+    long long g, head;
     __device__ __forceinline__ float2 at(int k, int i) const {
-        return src.at(g + ((long long)k << LOGM) + 2 * i * (1 << (LOGM - LOGP)));
+        const long long pos = g + ((long long)k << LOGM) + 2 * i * (1 << (LOGM - LOGP));
+        return __ldg(pos < head ? st + pos : in + (pos - head));
+    }
+};
+template <int LOGM>
+struct PairMixed16 {                   /* cf32 state / raw int16 input by index */
+    const float2 *st;
+    const short2 *in;
+    long long g, head;
+    float cre, cim, ks;
+    __device__ __forceinline__ float2 at(int k, int i) const {
+        const long long pos = g + ((long long)k << LOGM) + 2 * i * (1 << (LOGM - LOGP));
+        return pos < head ? __ldg(st + pos) : conv16(__ldg(in + (pos - head)), cre, cim, ks);
     }
 };
 template <int LOGM, int LOGOS>
@@ -616,9 +628,14 @@ __device__ __forceinline__ void fold_pair_global(float2 (&a)[4], float2 (&b)[4],
         const PairLin<LOGM> ld{(const float2 *)J.state + off};
         fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
     } else {
-        const PairMixed<LOGM> ld{Src{(const float2 *)J.state, J.in, J.head, J.in_kind, J.cre, J.cim, J.kscale},
-                                 off};
-        fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
+        if (J.in_kind) {
+            const PairMixed16<LOGM> ld{(const float2 *)J.state, (const short2 *)J.in, off, J.head,
+                                       J.cre, J.cim, J.kscale};
+            fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
+        } else {
+            const PairMixed<LOGM> ld{(const float2 *)J.state, (const float2 *)J.in, off, J.head};
+            fold_pair<LOGM, LOGOS>(a, b, tq, B.K, tb_ok, ld);
+        }
     }
 }
 
