@@ -105,6 +105,8 @@ def _bind(lib) -> None:
         "atkdsp_gpu_batch_process": ([vp, P(vp), P(sz), P(vp), P(ssz), vp], ssz),
         "atkdsp_gpu_batch_stream": ([vp], vp),
         "atkdsp_gpu_batch_kernel_ms": ([vp], C.c_float),
+        "atkdsp_gpu_tune_set": ([u, u, u, C.c_int], C.c_int),
+        "atkdsp_gpu_tune_get": ([u, u, u], C.c_int),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)

@@ -132,13 +132,72 @@ static void design_prototype(unsigned nchan, unsigned K, double atten_db, double
 /* ================================================================== FFT plan */
 static int is_pow2(unsigned v) { return v && !(v & (v - 1)); }
 
-static int plan_fft(unsigned M, unsigned os, atkb_fft_plan *pl) {
+/* ---- the tile-shape choice -----------------------------------------------
+ * Where both exist (can_pair), a bank uses the paired fold (two hops per
+ * thread over even or odd branches: half the loads, one more FFT pass) or
+ * one hop and 8 branches per thread. The choice comes from a runtime
+ * override (atkdsp_gpu_tune_set), else from the table the autotuner wrote
+ * (tune_table.h, measured on B200), else the paired fold. */
+typedef struct { unsigned nchan, os, K; int pair; } tune_entry;
+#include "tune_table.h"
+#define MAX_TUNE_OVERRIDES 256
+static tune_entry g_tune_ovr[MAX_TUNE_OVERRIDES];
+static unsigned g_tune_novr;
+static pthread_mutex_t g_tune_lock = PTHREAD_MUTEX_INITIALIZER;
+
+/* the paired fold: hop b's window is hop a's shifted by 8/os branch slots,
+ * so os must divide 4 (M/os a multiple of 2*M/8), and a tile must hold two
+ * hops (nchan <= 2048) */
+static int can_pair(unsigned M, unsigned os) {
+    return ATKB_PTS == 8 && is_pow2(M) && M >= 16 && M <= 2048 && (os == 1 || os == 2 || os == 4);
+}
+
+static int tune_choice(unsigned M, unsigned os, unsigned K) {
+    unsigned i;
+    int c = -1;
+    if (!can_pair(M, os)) return 0;
+    pthread_mutex_lock(&g_tune_lock);
+    for (i = 0; i < g_tune_novr; ++i)
+        if (g_tune_ovr[i].nchan == M && g_tune_ovr[i].os == os && g_tune_ovr[i].K == K) c = g_tune_ovr[i].pair;
+    pthread_mutex_unlock(&g_tune_lock);
+    if (c >= 0) return c;
+    for (i = 0; i < sizeof k_tune_table / sizeof k_tune_table[0]; ++i)
+        if (k_tune_table[i].nchan == M && k_tune_table[i].os == os && k_tune_table[i].K == K)
+            return k_tune_table[i].pair;
+    return 1;
+}
+
+ATKDSP_API int atkdsp_gpu_tune_set(unsigned nchan, unsigned oversample, unsigned taps_per_poly, int choice) {
+    unsigned i;
+    int rc = ATKDSP_OK;
+    if (!can_pair(nchan, oversample) || choice < -1 || choice > 1) return ATKDSP_E_ARG;
+    pthread_mutex_lock(&g_tune_lock);
+    for (i = 0; i < g_tune_novr; ++i)
+        if (g_tune_ovr[i].nchan == nchan && g_tune_ovr[i].os == oversample && g_tune_ovr[i].K == taps_per_poly)
+            break;
+    if (choice < 0) {                                      /* back to the table */
+        if (i < g_tune_novr) g_tune_ovr[i] = g_tune_ovr[--g_tune_novr];
+    } else if (i < g_tune_novr) {
+        g_tune_ovr[i].pair = choice;
+    } else if (g_tune_novr < MAX_TUNE_OVERRIDES) {
+        tune_entry t = {nchan, oversample, taps_per_poly, choice};
+        g_tune_ovr[g_tune_novr++] = t;
+    } else {
+        rc = ATKDSP_E_NOMEM;
+    }
+    pthread_mutex_unlock(&g_tune_lock);
+    return rc;
+}
+
+ATKDSP_API int atkdsp_gpu_tune_get(unsigned nchan, unsigned oversample, unsigned taps_per_poly) {
+    if (!can_pair(nchan, oversample)) return ATKDSP_E_ARG;
+    return tune_choice(nchan, oversample, taps_per_poly);
+}
+
+static int plan_fft(unsigned M, unsigned os, int want_pair, atkb_fft_plan *pl) {
     memset(pl, 0, sizeof *pl);
     if (is_pow2(M) && M >= 16 && M <= MAX_POW2_NCHAN) {
-        /* the paired fold: hop b's window is hop a's shifted by 8/os branch
-         * slots, so os must divide 4 (M/os a multiple of 2*M/8), and a tile
-         * must hold two hops (nchan <= 2048) */
-        const int pair = ATKB_PTS == 8 && M <= 2048 && (os == 1 || os == 2 || os == 4);
+        const int pair = want_pair && can_pair(M, os);
         unsigned rem = M / (pair ? 4 : ATKB_PTS);
         pl->fast = 1;
         pl->pair = pair;
@@ -220,6 +279,7 @@ struct bank_entry {
     int dev;
     unsigned nchan, os, K;
     double atten;
+    int pair;                     /* the tile-shape choice it was built with */
     int refs;
     void *d_const, *d_bank;
     atkb_bank bank;
@@ -255,7 +315,7 @@ static int bank_build(bank_entry *be, void *stream) {
     const unsigned M = be->nchan;
     const size_t L = (size_t)M * be->K;
     atkb_fft_plan pl;
-    if (plan_fft(M, be->os, &pl) != 0) return ATKB_E_ARG;
+    if (plan_fft(M, be->os, be->pair, &pl) != 0) return ATKB_E_ARG;
     const size_t taps_b = align16(L * sizeof(float));
     const size_t tab_b = (size_t)M * 2 * sizeof(double);
     const size_t pass_b = (size_t)pl.twlen * 2 * sizeof(double);
@@ -357,9 +417,10 @@ static int bank_build(bank_entry *be, void *stream) {
 static bank_entry *bank_acquire(int dev, unsigned M, unsigned os, unsigned K, double atten,
                                 void *stream, int *rc) {
     bank_entry *e;
+    const int pair = tune_choice(M, os, K);
     pthread_mutex_lock(&g_bank_lock);
     for (e = g_banks; e; e = e->next)
-        if (e->dev == dev && e->nchan == M && e->os == os && e->K == K && e->atten == atten) {
+        if (e->dev == dev && e->nchan == M && e->os == os && e->K == K && e->atten == atten && e->pair == pair) {
             ++e->refs;
             pthread_mutex_unlock(&g_bank_lock);
             *rc = ATKB_OK;
@@ -371,7 +432,7 @@ static bank_entry *bank_acquire(int dev, unsigned M, unsigned os, unsigned K, do
         *rc = ATKB_E_NOMEM;
         return NULL;
     }
-    e->dev = dev; e->nchan = M; e->os = os; e->K = K; e->atten = atten; e->refs = 1;
+    e->dev = dev; e->nchan = M; e->os = os; e->K = K; e->atten = atten; e->pair = pair; e->refs = 1;
     *rc = bank_build(e, stream);
     if (*rc != ATKB_OK) {
         atkb_free(e->d_const);

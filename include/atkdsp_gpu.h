@@ -105,13 +105,30 @@ ATKDSP_API int         atkdsp_gpu_pfb_channel_power(const atkdsp_cf32 *d_out, un
                                                     unsigned nchan, size_t m, float *d_pwr,
                                                     float *d_mean_pwr, void *stream);
 
+/* ---- tile shape (no reference counterpart) ------------------------------
+ * For a power-of-two nchan <= 2048 at oversample 1, 2 or 4 the kernel has two
+ * tile shapes: the paired fold (each thread folds two consecutive hops over
+ * the even or odd branches: half the sample and tap loads, one more FFT pass)
+ * or one hop and 8 branches per thread. Filterbanks take the choice for their
+ * (nchan, oversample, taps/branch) from the table compiled into the library
+ * (written by `python -m atkdsp_b200.autotune --write` from measurements on
+ * the device), else the paired fold. atkdsp_gpu_tune_set overrides it for
+ * filterbanks created afterwards in this process (choice 1: paired, 0: one
+ * hop per thread, -1: back to the table); ATKDSP_E_ARG for a shape with only
+ * one tile shape. atkdsp_gpu_tune_get returns the choice such a filterbank
+ * gets now (1 or 0), or ATKDSP_E_ARG. Outputs are the same either way. */
+ATKDSP_API int         atkdsp_gpu_tune_set(unsigned nchan, unsigned oversample,
+                                           unsigned taps_per_poly, int choice);
+ATKDSP_API int         atkdsp_gpu_tune_get(unsigned nchan, unsigned oversample,
+                                           unsigned taps_per_poly);
+
 /* ---- batches: many independent handles in one persistent launch --------
  * A batch groups handles (each single-element, any nchan / taps / oversample)
  * so that one call channelizes one new block of every handle with a single
- * kernel launch over all their hops, plus one launch that carries every
- * handle's state forward. With use_graph != 0 the launch sequence is captured
- * once in a CUDA graph and replayed; the per-call description of the blocks
- * travels in a pinned table that the graph copies to the device. */
+ * kernel launch over all their hops (CTAs out of hops then carry every
+ * handle's state forward). With use_graph != 0 the launch sequence is
+ * captured once in a CUDA graph and replayed; the per-call description of the
+ * blocks travels in a pinned table that the graph copies to the device. */
 typedef struct atkdsp_gpu_batch atkdsp_gpu_batch;
 ATKDSP_API atkdsp_gpu_batch *atkdsp_gpu_batch_create(atkdsp_pfb *const *handles, unsigned count,
                                                      int use_graph);
