@@ -107,3 +107,44 @@ def test_load_generator_runs():
     assert r["blocks_done"] > 0 and r["admitted"] >= 64
     assert 0 < r["lat_p50_ms"] <= r["lat_p99_ms"] <= r["lat_max_ms"]
     assert r["blocks_per_round"] >= 1.0
+
+
+def test_reopened_stream_reuses_a_parked_handle_with_clean_state():
+    """A closed stream's handle is parked and handed to the next open of the
+    same filter -- here while the closed stream's last round may still be on
+    the GPU. The new stream must behave exactly like a fresh handle: its
+    state cleared, its hop counter at zero."""
+    from atkdsp_b200.serve import Server
+    srv = Server(max_streams=4, hbm_reserve=1 << 30)
+    rng = np.random.default_rng(11)
+    M, os_, K = 256, 2, 16
+    a = srv.open(FS, M, os_, K)
+    keep = []
+    for _ in range(3):                                   # give stream a some history
+        x = torch.from_numpy(W.tones_noise(5000, 3, 15.0, rng)).cuda()
+        out = torch.zeros(M * 40, dtype=torch.complex64, device="cuda")
+        keep.append((x, out))
+        assert srv.submit(a, x, out) == 0
+    srv.launch()                                         # in flight when closed
+    assert srv.close(a) == 0
+    b = srv.open(FS, M, os_, K)                          # takes the parked handle
+    assert b >= 0
+    fresh = ak.Pfb(FS, M, os_, K)
+    got, want = [], []
+    for blk in (3000, 7, 12000):
+        x = W.tones_noise(blk, 2, 15.0, rng)
+        d = torch.from_numpy(x).cuda()
+        hop = M // os_
+        out = torch.zeros(M * ((hop - 1 + blk) // hop) + M, dtype=torch.complex64, device="cuda")
+        keep.append((d, out))
+        assert srv.submit(b, d, out, tag=blk) == 0
+        want.append(fresh.process(x))
+    done = srv.drain()
+    for sid, tag, m, n, ta, td in done:
+        if sid == b:
+            out = [o for (d, o) in keep if d.numel() == n][-1]
+            got.append((tag, out[: M * m].view(M, m).cpu().numpy()))
+    got = [y for _, y in sorted(got, key=lambda t: [3000, 7, 12000].index(t[0]))]
+    assert len(got) == 3
+    for y, r in zip(got, want):
+        assert y.shape == r.shape and np.array_equal(y, r)
