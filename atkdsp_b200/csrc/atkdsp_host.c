@@ -201,6 +201,10 @@ static int plan_fft(unsigned M, unsigned os, int want_pair, atkb_fft_plan *pl) {
         unsigned rem = M / (pair ? 4 : ATKB_PTS);
         pl->fast = 1;
         pl->pair = pair;
+        /* nchan 4096 at oversample 1/2/4: one thread folds both parities of
+         * both hops of its two-hop tile (paired loads), then radix-8 first
+         * passes: the paired tap layout with the radix-8 plan */
+        pl->ptaps = pair || (M == 4096 && (os == 1 || os == 2 || os == 4));
         pl->radix[pl->npass++] = pair ? 4 : ATKB_PTS;
         while (rem >= ATKB_PTS) { pl->radix[pl->npass++] = ATKB_PTS; rem /= ATKB_PTS; }
         if (rem > 1) pl->radix[pl->npass++] = (int)rem;
@@ -341,7 +345,7 @@ static int bank_build(bank_entry *be, void *stream) {
             for (q2 = 0; q2 < P / 4; ++q2)
                 for (jj = 0; jj < MP; ++jj)
                     for (i = 0; i < 4; ++i) {
-                        const size_t r = pl.pair ? q2 + 2 * i : 4 * q2 + i;
+                        const size_t r = pl.ptaps ? q2 + 2 * i : 4 * q2 + i;
                         tapsP[((k2 * (P / 4) + q2) * MP + jj) * 4 + i] = taps[k2 * M + jj + r * MP];
                     }
     }

@@ -41,6 +41,8 @@ typedef struct {
     int npass;
     int fast;                     /* 1: power-of-two fast path */
     int pair;                     /* 1: paired fold, first radix 4             */
+    int ptaps;                    /* taps in the paired layout (pair, or the
+                                   * nchan-4096 two-hop tile's paired fold) */
     int radix[ATKB_MAX_PASS];
     int twoff[ATKB_MAX_PASS];     /* offset of pass p's twiddles in the table */
     int twlen;                    /* total twiddle entries (double2)          */

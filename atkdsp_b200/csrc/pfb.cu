@@ -795,6 +795,83 @@ __device__ void tile_4096x2(const atkb_job &J, const atkb_bank &B, long long h0,
     }
 }
 
+/* nchan 4096 at oversample 1/2/4: the same two-hop tile with the paired
+ * fold. Thread j folds both hops over the even branches, then over the odd
+ * ones (each sample and tap loaded once for the two hops); the even sums
+ * wait in the side buffer, so each hop's 8 branches meet in registers for a
+ * radix-8 first pass (the 4-pass plan). Hop b's sums wait in the side
+ * buffer while hop a is transformed; then hop a's outputs take their place. */
+template <int LOGOS>
+__device__ void tile_4096x2_pair(const atkb_job &J, const atkb_bank &B, long long h0, int nvalid,
+                                 double2 *sm) {
+    constexpr int LOGM = 12;
+    constexpr int M = 1 << LOGM;
+    constexpr int MP = M >> LOGP;
+    static_assert(NT == MP && PTS == 8, "one thread per branch group");
+    float2 *tile_out = (float2 *)sm;       /* pass_last: hop at tile_out[kb * 2] */
+    float2 *side = (float2 *)(sm + M);     /* [8][MP] float2, slot (row, j) owned by thread j */
+    const double2 *wp = (const double2 *)B.wpass;
+    const int j = threadIdx.x;
+    const bool tb_ok = nvalid > 1;
+    float2 a[4], b[4];
+    fold_pair_global<LOGM, LOGOS>(a, b, J, B, h0, nvalid, 0, 0, j, tb_ok);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        side[i * MP + j] = a[i];           /* rows 0-3: hop a, even branches */
+        side[(4 + i) * MP + j] = b[i];     /* rows 4-7: hop b, even branches */
+    }
+    fold_pair_global<LOGM, LOGOS>(a, b, J, B, h0, nvalid, 0, 1, j, tb_ok);
+    {
+        double2 v[PTS];                    /* branch r = c + 2i of hop a */
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 e = side[i * MP + j];
+            v[2 * i] = make_double2((double)e.x, (double)e.y);
+            v[2 * i + 1] = make_double2((double)a[i].x, (double)a[i].y);
+            side[i * MP + j] = b[i];       /* rows 0-3 now: hop b, odd branches */
+        }
+        dftR<PTS>(v);
+#pragma unroll
+        for (int r = 0; r < PTS; ++r) sm[SW(j * PTS + r)] = v[r];
+    }
+    __syncthreads();
+    fft_rest<LOGM, LOGP, 1, NT>(sm, wp, B.plan.twoff, tile_out, B, J, h0);
+    if (tb_ok) {
+        double2 v[PTS];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 e = side[(4 + i) * MP + j], o = side[i * MP + j];
+            v[2 * i] = make_double2((double)e.x, (double)e.y);
+            v[2 * i + 1] = make_double2((double)o.x, (double)o.y);
+        }
+#pragma unroll
+        for (int u = 0; u < PTS; ++u) side[u * MP + j] = tile_out[(j + u * MP) * 2];   /* hop a's outputs */
+        __syncthreads();                   /* tile_out read before hop b's first pass */
+        dftR<PTS>(v);
+#pragma unroll
+        for (int r = 0; r < PTS; ++r) sm[SW(j * PTS + r)] = v[r];
+        __syncthreads();
+        fft_rest<LOGM, LOGP, 1, NT>(sm, wp, B.plan.twoff, tile_out, B, J, h0 + 1);
+    } else {
+#pragma unroll
+        for (int u = 0; u < PTS; ++u) side[u * MP + j] = tile_out[(j + u * MP) * 2];
+        __syncthreads();
+    }
+    const int tid = threadIdx.x;
+    const int t2 = tid & 1;
+    if (t2 < nvalid) {
+        const int kb0 = tid >> 1;
+        float2 *o = (float2 *)J.out + (J.out_col + h0 + t2) + (long long)kb0 * J.ldo;
+        const long long step = (long long)(NT / 2) * J.ldo;
+#pragma unroll 4
+        for (int u = 0; u < 2 * PTS; ++u) {
+            const int kb = kb0 + u * (NT / 2);
+            *o = t2 ? tile_out[kb * 2] : side[kb];
+            o += step;
+        }
+    }
+}
+
 /* LOGOS < 0: one hop and PTS branches per thread, first pass radix PTS;
  * LOGOS = log2(os) in 0..2: the paired fold, first pass radix 4 */
 template <int LOGM, int LOGOS>
@@ -1008,7 +1085,12 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
         case 48 + L: tile_fast<L, 2>(J, SB, h0, nvalid, sm, to); break;
         UNPAIRED(4) UNPAIRED(5) UNPAIRED(6) UNPAIRED(7) UNPAIRED(8) UNPAIRED(9) UNPAIRED(10)
         UNPAIRED(11)
-        case 12: tile_4096x2(J, SB, h0, nvalid, sm); break;
+        case 12:
+            if (!SB.plan.ptaps) tile_4096x2(J, SB, h0, nvalid, sm);
+            else if (SB.os == 1) tile_4096x2_pair<0>(J, SB, h0, nvalid, sm);
+            else if (SB.os == 2) tile_4096x2_pair<1>(J, SB, h0, nvalid, sm);
+            else tile_4096x2_pair<2>(J, SB, h0, nvalid, sm);
+            break;
         PAIRED(4) PAIRED(5) PAIRED(6) PAIRED(7) PAIRED(8) PAIRED(9) PAIRED(10) PAIRED(11)
 #undef UNPAIRED
 #undef PAIRED
