@@ -306,8 +306,7 @@ ATKDSP_API void atkdsp_pfb_destroy(atkdsp_pfb *p) {
     atkb_free(p->d_out_stage);
     atkb_free(p->d_tables);
     atkb_free(p->d_counters);
-    atkb_host_free(p->h_tables);
-    atkb_host_free(p->h_small_in);
+    atkb_host_free(p->h_tables);           /* h_small_in lives inside it */
     atkb_host_free(p->h_small_out);
     atkb_event_destroy(p->small_ev);
     atkb_event_destroy(p->tbl_event);
@@ -534,15 +533,21 @@ atkdsp_pfb *atkb_pfb_create_internal(double fs, unsigned nchan, unsigned oversam
                          (size_t)max_nel * nchan * p->out_ld * sizeof(atkdsp_cf32));
     if (rc == ATKB_OK) {
         p->tbl_bytes = tables_bytes(max_nel);
-        rc = atkb_malloc(&p->d_tables, p->tbl_bytes);
     }
-    if (rc == ATKB_OK) rc = atkb_host_alloc(&p->h_tables, p->tbl_bytes);
-    if (rc == ATKB_OK && p->chunk >= ATKB_SMALL_N) {
-        const size_t m_small = (p->hop - 1 + ATKB_SMALL_N) / p->hop;
-        rc = atkb_host_alloc(&p->h_small_in, (size_t)max_nel * ATKB_SMALL_N * sizeof(atkdsp_cf32));
-        if (rc == ATKB_OK)
+    {
+        /* small calls: their blocks travel right after the tables, in the
+         * same pinned buffer and the same host->device copy */
+        const int small = p->chunk >= ATKB_SMALL_N;
+        const size_t in_b = small ? (size_t)max_nel * ATKB_SMALL_N * sizeof(atkdsp_cf32) : 0;
+        if (rc == ATKB_OK) rc = atkb_malloc(&p->d_tables, p->tbl_bytes + in_b);
+        if (rc == ATKB_OK) rc = atkb_host_alloc(&p->h_tables, p->tbl_bytes + in_b);
+        if (rc == ATKB_OK && small) {
+            const size_t m_small = (p->hop - 1 + ATKB_SMALL_N) / p->hop;
+            p->h_small_in = (char *)p->h_tables + p->tbl_bytes;
+            p->d_small_in = (char *)p->d_tables + p->tbl_bytes;
             rc = atkb_host_alloc(&p->h_small_out, (size_t)max_nel * nchan * m_small * sizeof(atkdsp_cf32));
-        if (rc == ATKB_OK) rc = atkb_event_create(&p->small_ev);
+            if (rc == ATKB_OK) rc = atkb_event_create(&p->small_ev);
+        }
     }
     if (rc == ATKB_OK) rc = atkb_malloc((void **)&p->d_counters, ATKB_NCOUNTERS * sizeof(int));
     if (rc == ATKB_OK) rc = atkb_memset(p->d_counters, 0, ATKB_NCOUNTERS * sizeof(int), p->stream);
@@ -663,8 +668,17 @@ void atkb_job_conv(atkb_job *J, atkb_carry *C, const conv_t *cv) {
  * written to outs + e * nchan * ldo (device, row stride ldo). Builds the job
  * and carry tables, uploads them, launches the tile kernel and the carry,
  * and advances the host mirror of the state. Asynchronous on `stream`. */
+static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size_t n, atkdsp_cf32 *outs,
+                       size_t ldo, size_t m, void *stream, const conv_t *cv, size_t up_extra);
+
 static int run_step(atkdsp_pfb *p, unsigned nel, const void *const *ins, size_t n,
                     atkdsp_cf32 *outs, size_t ldo, size_t m, void *stream, const conv_t *cv) {
+    return run_step_up(p, nel, ins, n, outs, ldo, m, stream, cv, 0);
+}
+
+/* up_extra: bytes after the tables (a small call's block) in the same upload */
+static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size_t n, atkdsp_cf32 *outs,
+                       size_t ldo, size_t m, void *stream, const conv_t *cv, size_t up_extra) {
     const size_t head = p->ov + p->lc;
     const unsigned nxt = (unsigned)(p->cur ^ 1);
     int rc;
@@ -702,7 +716,7 @@ static int run_step(atkdsp_pfb *p, unsigned nel, const void *const *ins, size_t 
     }
     T[nel] = (int)nel * tiles;
     /* the tables as laid out for max_nel, uploaded whole (they are small) */
-    rc = atkb_h2d(p->d_tables, p->h_tables, p->tbl_bytes, stream);
+    rc = atkb_h2d(p->d_tables, p->h_tables, p->tbl_bytes + up_extra, stream);
     if (rc == ATKB_OK) rc = atkb_event_record(p->tbl_event, stream);
     if (rc != ATKB_OK) return rc;
     p->tbl_event_live = 1;
@@ -735,6 +749,10 @@ static ptrdiff_t process_small(atkdsp_pfb *p, const atkdsp_cf32 *const *ins, uns
         if (rc != ATKB_OK) return map_rc(rc);
         p->small_live = 0;
     }
+    if (p->tbl_event_live) {             /* ... or the last table upload */
+        rc = atkb_event_sync(p->tbl_event);
+        if (rc != ATKB_OK) return map_rc(rc);
+    }
     atkdsp_cf32 *hin = (atkdsp_cf32 *)p->h_small_in;
     if (n)
         for (e = 0; e < nel; ++e) memcpy(hin + (size_t)e * ATKB_SMALL_N, ins[e], n * sizeof(atkdsp_cf32));
@@ -752,14 +770,11 @@ static ptrdiff_t process_small(atkdsp_pfb *p, const atkdsp_cf32 *const *ins, uns
         return 0;
     }
     const void *dins[MAX_NEL_SUPPORTED];
-    for (e = 0; e < nel && rc == ATKB_OK; ++e) {
-        dins[e] = (const atkdsp_cf32 *)p->d_in_stage + (size_t)e * p->chunk;
-        if (n) rc = atkb_h2d((void *)dins[e], hin + (size_t)e * ATKB_SMALL_N, n * sizeof(atkdsp_cf32), p->stream);
-    }
+    for (e = 0; e < nel; ++e) dins[e] = (const atkdsp_cf32 *)p->d_small_in + (size_t)e * ATKB_SMALL_N;
     /* outputs packed with stride m: [nel * nchan][m], the caller's layout */
     const size_t out_n = (size_t)nel * p->nchan * m;
-    if (rc == ATKB_OK)
-        rc = run_step(p, nel, dins, n, (atkdsp_cf32 *)p->d_out_stage, m, m, p->stream, &CONV_CF32);
+    const size_t up = ((size_t)(nel - 1) * ATKB_SMALL_N + n) * sizeof(atkdsp_cf32);
+    rc = run_step_up(p, nel, dins, n, (atkdsp_cf32 *)p->d_out_stage, m, m, p->stream, &CONV_CF32, up);
     if (rc == ATKB_OK)
         rc = atkb_d2h(p->h_small_out, p->d_out_stage, out_n * sizeof(atkdsp_cf32), p->stream);
     if (rc == ATKB_OK) rc = atkb_stream_sync(p->stream);

@@ -56,7 +56,9 @@ struct atkdsp_pfb {
     /* small host calls (n <= ATKB_SMALL_N): pinned staging for the block and
      * its output; `small_ev` marks the last copy out of h_small_in, which a
      * call that completes no hop leaves in flight (small_live) */
-    void *h_small_in, *h_small_out;
+    void *h_small_in, *h_small_out;  /* h_small_in: right after the pinned tables */
+    void *d_small_in;                 /* right after the device tables: one copy
+                                       * carries a small call's tables and block */
     void *small_ev;
     int small_live;
     size_t tbl_bytes;
