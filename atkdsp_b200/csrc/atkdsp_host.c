@@ -657,11 +657,21 @@ const conv_t ATKB_CONV_CF32 = {0, 0.0f, 0.0f, 1.0f};
 
 void atkb_job_conv(atkb_job *J, atkb_carry *C, const conv_t *cv);
 #define job_conv atkb_job_conv
+/* int16 input reaches the kernel as fma(float(v), k, -(c*k)): k is a power of
+ * two for both int16 formats, so c*k and v*k are exact and the fused form
+ * rounds exactly like the reference's (float(v) - c) * k (scaling by 2^-e
+ * commutes with rounding; where c*k would be subnormal, c is below half an
+ * ulp of every nonzero v and both forms give v*k, or -(c*k) for v = 0) */
 void atkb_job_conv(atkb_job *J, atkb_carry *C, const conv_t *cv) {
     J->in_kind = C->in_kind = cv->kind;
-    J->cre = C->cre = cv->cre;
-    J->cim = C->cim = cv->cim;
     J->kscale = C->kscale = cv->k;
+    if (cv->kind) {
+        J->cre = C->cre = -(cv->cre * cv->k);
+        J->cim = C->cim = -(cv->cim * cv->k);
+    } else {
+        J->cre = C->cre = cv->cre;
+        J->cim = C->cim = cv->cim;
+    }
 }
 
 /* One step: nel elements, n new samples each at ins[e] (device), m hops

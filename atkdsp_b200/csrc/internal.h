@@ -82,7 +82,9 @@ typedef struct {
     long long hops;               /* hops in this job                          */
     const atkb_bank *bank;        /* device copy of the bank                   */
     int in_kind;                  /* 0: `in` is cf32; 1: `in` is int16 I/Q     */
-    float cre, cim, kscale;       /* int16 input: sample = (float(v) - c) * k  */
+    float cre, cim, kscale;       /* int16 input: sample = (float(v) - c) * k,
+                                   * held as cre/cim = -(c * k), kscale = k (a
+                                   * power of two): fma(float(v), k, cre) */
     int tiles;                    /* ceil(hops / bank->tile_hops)              */
 } atkb_job;
 

@@ -145,10 +145,11 @@ __device__ __forceinline__ void dftR(double2 *v) {
 }
 
 /* one element of the stream s = state[0, head) ++ in[0, ...) */
-/* int16 I/Q -> cf32 exactly as the unpack front end does: (float(v) - c) * k
- * with rounded operations (reference src/convert.c:64-73) */
-__device__ __forceinline__ float2 conv16(short2 v, float cre, float cim, float k) {
-    return make_float2(__fmul_rn(__fsub_rn((float)v.x, cre), k), __fmul_rn(__fsub_rn((float)v.y, cim), k));
+/* int16 I/Q -> cf32 exactly as the unpack front end does, (float(v) - c) * k
+ * with rounded operations (reference src/convert.c:64-73), in the fused form
+ * the host prepares: nc = -(c * k) with k a power of two, one rounding */
+__device__ __forceinline__ float2 conv16(short2 v, float ncre, float ncim, float k) {
+    return make_float2(__fmaf_rn((float)v.x, k, ncre), __fmaf_rn((float)v.y, k, ncim));
 }
 
 /* one element of the stream s = state[0, head) ++ in[0, ...); `in` is cf32 or
