@@ -87,6 +87,28 @@ class CpuLib:
         f("unpack_dc").restype = C.c_ssize_t
         f("bytes_per_sample").argtypes = [C.c_int]
         f("bytes_per_sample").restype = C.c_int
+        f("osx_create").argtypes = [d, sz, d, u]
+        f("osx_create").restype = vp
+        f("osx_destroy").argtypes = [vp]
+        f("osx_destroy").restype = None
+        f("osx_reset").argtypes = [vp]
+        f("osx_reset").restype = None
+        f("osx_add").argtypes = [vp, d, d, d]
+        f("osx_add").restype = C.c_int
+        f("osx_retune").argtypes = [vp, C.c_int, d]
+        f("osx_retune").restype = C.c_int
+        f("osx_remove").argtypes = [vp, C.c_int]
+        f("osx_remove").restype = C.c_int
+        f("osx_channels").argtypes = [vp]
+        f("osx_channels").restype = C.c_int
+        f("osx_chan_rate").argtypes = [vp, C.c_int]
+        f("osx_chan_rate").restype = d
+        f("osx_out_max").argtypes = [vp, C.c_int, sz]
+        f("osx_out_max").restype = sz
+        f("osx_process_n").argtypes = [vp, _P(_pcf), u, sz, _P(_pcf), _P(sz), sz]
+        f("osx_process_n").restype = C.c_ssize_t
+        f("osx_describe").argtypes = [vp, C.c_char_p, sz]
+        f("osx_describe").restype = C.c_int
         if self.prefix == "orc_":
             self.lib.orc_pfb_prototype.argtypes = [u, u, d, _P(C.c_double)]
             self.lib.orc_pfb_prototype.restype = None
@@ -104,6 +126,10 @@ class CpuLib:
         self.lib.orc_pfb_prototype(int(nchan), int(taps_per_poly), float(atten_db),
                                    h.ctypes.data_as(_P(C.c_double)))
         return h
+
+    # -- the overlap-save extractor ----------------------------------------------
+    def Osx(self, fs, nfft=4096, atten_db=80.0, max_nel=1):
+        return _CpuOsx(self, fs, nfft, atten_db, max_nel)
 
     # -- W1 / W2 ---------------------------------------------------------------
     def _w(self, name):
@@ -210,6 +236,90 @@ class _CpuPfb:
 
     def process(self, x):
         return self.process_n([x], 1)[0]
+
+
+class _CpuOsx:
+    """The binding's ``Osx`` (python/atkdsp/__init__.py:4269-4342) over a CPU library."""
+
+    def __init__(self, owner: CpuLib, fs, nfft, atten, max_nel):
+        self._o = owner
+        self._p = owner._f("osx_create")(float(fs), int(nfft), float(atten), int(max_nel))
+        if not self._p:
+            raise ValueError("osx_create rejected its arguments")
+        self.max_nel = int(max_nel)
+
+    def __del__(self):
+        p = getattr(self, "_p", None)
+        if p:
+            self._o._f("osx_destroy")(p)
+            self._p = None
+
+    def reset(self):
+        self._o._f("osx_reset")(self._p)
+
+    def add(self, offset_hz, bw_hz, out_rate):
+        ch = self._o._f("osx_add")(self._p, float(offset_hz), float(bw_hz), float(out_rate))
+        if ch < 0:
+            raise RuntimeError(f"osx_add: {ch}")
+        return ch
+
+    def retune(self, ch, offset_hz):
+        rc = self._o._f("osx_retune")(self._p, int(ch), float(offset_hz))
+        if rc < 0:
+            raise RuntimeError(f"osx_retune: {rc}")
+
+    def remove(self, ch):
+        rc = self._o._f("osx_remove")(self._p, int(ch))
+        if rc < 0:
+            raise RuntimeError(f"osx_remove: {rc}")
+
+    def channels(self):
+        return int(self._o._f("osx_channels")(self._p))
+
+    def chan_rate(self, ch):
+        return float(self._o._f("osx_chan_rate")(self._p, int(ch)))
+
+    def out_max(self, ch, n):
+        return int(self._o._f("osx_out_max")(self._p, int(ch), int(n)))
+
+    def describe(self):
+        buf = C.create_string_buffer(256)
+        n = self._o._f("osx_describe")(self._p, buf, 256)
+        return buf.value.decode() if n > 0 else ""
+
+    def process_n(self, ins, nel, cap=None):
+        """cap: the per-channel capacity passed as cap_each (default the
+        binding's, the largest out_max; a larger one admits calls whose
+        carried samples complete more hops than out_max allows for)."""
+        nel = int(nel)
+        arrs = [np.ascontiguousarray(np.asarray(ins[e]).ravel(), np.complex64) for e in range(nel)]
+        n = arrs[0].size
+        ns = self.channels()
+        active = [self.chan_rate(ci) > 0 for ci in range(ns)]
+        if cap is None:
+            cap = max([self.out_max(ci, n) for ci in range(ns) if active[ci]], default=0)
+        bufs = [[np.zeros(cap, np.complex64) if active[ci] else None for ci in range(ns)]
+                for _ in range(nel)]
+        ptrs = (_pcf * max(nel * ns, 1))()
+        for e in range(nel):
+            for ci in range(ns):
+                ptrs[e * ns + ci] = _cfp(bufs[e][ci]) if active[ci] else None
+        counts = (C.c_size_t * max(ns, 1))()
+        inarr = (_pcf * nel)(*[_cfp(a) for a in arrs])
+        got = self._o._f("osx_process_n")(self._p, inarr, nel, n, ptrs, counts, cap)
+        if got < 0:
+            raise RuntimeError(f"osx_process_n: {got}")
+        cnts = [int(counts[ci]) for ci in range(ns)]
+        outs = [None] * ns
+        for ci in range(ns):
+            if active[ci]:
+                outs[ci] = np.array([bufs[e][ci][:cnts[ci]] for e in range(nel)], np.complex64) \
+                    if cnts[ci] else np.zeros((nel, 0), np.complex64)
+        return outs, cnts
+
+    def process(self, x, cap=None):
+        outs, cnts = self.process_n([x], 1, cap)
+        return [o[0] if o is not None else None for o in outs], cnts
 
 
 _cache: dict = {}

@@ -70,3 +70,8 @@ def golden_unpack():
 @pytest.fixture(scope="session")
 def golden_proto():
     return load_golden("proto.npz")
+
+
+@pytest.fixture(scope="session")
+def golden_osx():
+    return load_golden("osx.npz")

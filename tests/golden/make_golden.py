@@ -4,7 +4,7 @@ Run in a container that has the reference sources (it reads them; nothing on
 the GPU machine does):
 
     make -C oracle            # builds oracle/_ref/libatkdsp_ref.so from the sources
-    python tests/golden/make_golden.py [REF_ROOT]
+    python tests/golden/make_golden.py [REF_ROOT] [--only NAME ...]
 
 Every output here is produced by the REFERENCE: its C library (compiled from
 its own sources by oracle/Makefile) for float32 results, and its numpy twin
@@ -20,6 +20,8 @@ Fixture files (tests/golden/*.npz):
   unpack.npz        unpack / unpack_dc / DC pole on all five formats
   proto.npz         prototype taps: the twin's (numpy), the C restatement's,
                     and hashes of the C restatement's for long prototypes
+  osx.npz           overlap-save extractor outputs per channel slot for the
+                    cases of tests/osx_cases.py (reference C library)
 """
 
 from __future__ import annotations
@@ -37,7 +39,13 @@ sys.path.insert(0, str(REPO))
 from oracle import oracle as O                 # noqa: E402
 from atkdsp_b200 import workloads as W         # noqa: E402
 
-REF_ROOT = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+sys.path.insert(0, str(HERE.parent))
+from osx_cases import OSX_CASES, run_case      # noqa: E402
+
+_ARGS = [a for a in sys.argv[1:] if not a.startswith("--")]
+ONLY = sys.argv[sys.argv.index("--only") + 1:] if "--only" in sys.argv else None
+REF_ROOT = Path(_ARGS[0]) if _ARGS and (ONLY is None or sys.argv.index(_ARGS[0]) < sys.argv.index("--only")) \
+    else Path("/root/reference")
 sys.path.insert(0, str(REF_ROOT / "python"))
 from atkdsp import reference as twin           # noqa: E402
 
@@ -172,16 +180,34 @@ def make_proto():
     return out
 
 
+def make_osx(ref):
+    out = {}
+    for name in OSX_CASES:
+        ys, xs = run_case(lambda fs, nfft, nel: ref.Osx(fs, nfft, 80.0, nel), name)
+        out[f"{name}/in"] = np.stack(xs)
+        for ci, y in ys.items():
+            out[f"{name}/out{ci}"] = y.astype(np.complex64)
+        print(f"{name}: " + ", ".join(f"slot {ci}: {y.shape}" for ci, y in ys.items()))
+    return out
+
+
 def main():
     ref = O.reference()
     if ref is None:
         raise SystemExit("oracle/_ref/libatkdsp_ref.so is not built: run make -C oracle")
-    data, tw = make_pfb(ref)
-    np.savez_compressed(HERE / "pfb_cases.npz", **data)
-    np.savez_compressed(HERE / "pfb_twin.npz", **tw)
-    np.savez_compressed(HERE / "w12.npz", **make_w12(ref))
-    np.savez_compressed(HERE / "unpack.npz", **make_unpack(ref))
-    np.savez_compressed(HERE / "proto.npz", **make_proto())
+    want = (lambda k: ONLY is None or k in ONLY)
+    if want("pfb"):
+        data, tw = make_pfb(ref)
+        np.savez_compressed(HERE / "pfb_cases.npz", **data)
+        np.savez_compressed(HERE / "pfb_twin.npz", **tw)
+    if want("w12"):
+        np.savez_compressed(HERE / "w12.npz", **make_w12(ref))
+    if want("unpack"):
+        np.savez_compressed(HERE / "unpack.npz", **make_unpack(ref))
+    if want("proto"):
+        np.savez_compressed(HERE / "proto.npz", **make_proto())
+    if want("osx"):
+        np.savez_compressed(HERE / "osx.npz", **make_osx(ref))
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

@@ -140,3 +140,44 @@ def test_oracle_against_reference_library_directly():
         b = run_blocks(ref.Pfb(FS, M, os_, K, 80.0, nel), xs, blocks)
         u = _ulp_diff(a, b)
         assert u.max() <= 1 and np.mean(u > 0) < 1e-2
+
+
+# ---- the overlap-save extractor (oracle/osx_oracle.c) ----------------------
+def _osx_max_rel(a: np.ndarray, b: np.ndarray) -> float:
+    """max |a - b| over the slot's largest reference magnitude"""
+    return float(np.max(np.abs(a - b), initial=0.0) / (np.max(np.abs(b), initial=0.0) + 1e-30))
+
+
+@pytest.mark.parametrize("name", sorted(__import__("osx_cases").OSX_CASES))
+def test_osx_oracle_matches_reference_golden(golden_osx, name):
+    """Every slot's output, same length; bit-identical where the two FFTs
+    round alike, and within 1e-5 of the slot's peak everywhere."""
+    from osx_cases import run_case
+    xs = list(golden_osx[f"{name}/in"])
+    ys, _ = run_case(lambda fs, nfft, nel: _orc().Osx(fs, nfft, 80.0, nel), name, xs)
+    want = sorted(int(k.split("/out")[1]) for k in golden_osx if k.startswith(f"{name}/out"))
+    assert sorted(ys) == want
+    for ci in want:
+        g = golden_osx[f"{name}/out{ci}"]
+        assert ys[ci].shape == g.shape
+        assert _osx_max_rel(ys[ci], g) < 1e-5, (name, ci)
+
+
+def test_osx_oracle_bookkeeping_matches_reference_semantics():
+    orc = _orc()
+    assert orc.lib.orc_osx_create(FS, 100, 80.0, 1) is None       # not a power of two
+    assert orc.lib.orc_osx_create(FS, 32, 80.0, 1) is None        # below 64
+    assert orc.lib.orc_osx_create(0.0, 4096, 80.0, 1) is None
+    o = orc.Osx(FS, 4096)
+    assert o.add(300e3, 50e3, 50e3) == 0
+    assert o.add(-300e3, 50e3, 75e3) == 1
+    assert o.chan_rate(0) == 50e3 and o.chan_rate(1) == 75e3
+    assert o.out_max(0, 240000) == 5000 + 64
+    o.remove(0)
+    assert o.chan_rate(0) == 0.0 and o.channels() == 2
+    assert o.add(100e3, 50e3, 50e3) == 0                          # the hole is reused
+    with pytest.raises(RuntimeError):
+        o.add(0.0, -1.0, 50e3)
+    with pytest.raises(RuntimeError):
+        o.retune(5, 0.0)
+    assert "2 channel(s)" in o.describe()
