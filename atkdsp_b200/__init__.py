@@ -5,8 +5,8 @@ atkdsp_b200``), a C-ABI library that exports the reference's
 ``atkdsp_pfb_*`` / ``atkdsp_unpack*`` entry points and runs them on the GPU.
 The Python names, arguments, return shapes and errors below mirror the
 reference binding's (python/atkdsp/__init__.py: ``Pfb`` at :4159-4219,
-``unpack`` / ``unpack_dc`` at :337-385, W1/W2 at :4222-4266, identity at
-:285-313), so code and tests written against ``atkdsp`` read the same here.
+``unpack`` / ``unpack_dc`` at :337-385, W1/W2 at :4222-4266, ``Osx`` at
+:4269-4342, identity at :285-313), so code and tests written against ``atkdsp`` read the same here.
 
 There is no CPU fallback: if the library is missing or no GPU is usable,
 ``load()`` / ``Pfb(...)`` raise ``AtkDspError``.
@@ -26,7 +26,7 @@ import numpy as np
 __all__ = ["ABI_VERSION", "AtkDspError", "load", "available", "lib_path", "version",
            "build_info", "set_threads", "get_threads", "FMT", "bytes_per_sample",
            "unpack", "unpack_dc", "Pfb", "pfb_cov_accumulate", "pfb_cov_reset",
-           "pfb_channel_power"]
+           "pfb_channel_power", "Osx"]
 
 #: the ABI the library reports (the reference's, include/atkdsp.h:63)
 ABI_VERSION = 26
@@ -105,6 +105,21 @@ def _bind(lib) -> None:
         "atkdsp_gpu_batch_process": ([vp, P(vp), P(sz), P(vp), P(ssz), vp], ssz),
         "atkdsp_gpu_batch_stream": ([vp], vp),
         "atkdsp_gpu_batch_kernel_ms": ([vp], C.c_float),
+        "atkdsp_osx_create": ([d, sz, d, u], vp),
+        "atkdsp_osx_destroy": ([vp], None),
+        "atkdsp_osx_reset": ([vp], None),
+        "atkdsp_osx_add": ([vp, d, d, d], C.c_int),
+        "atkdsp_osx_retune": ([vp, C.c_int, d], C.c_int),
+        "atkdsp_osx_remove": ([vp, C.c_int], C.c_int),
+        "atkdsp_osx_channels": ([vp], C.c_int),
+        "atkdsp_osx_chan_rate": ([vp, C.c_int], d),
+        "atkdsp_osx_out_max": ([vp, C.c_int, sz], sz),
+        "atkdsp_osx_process": ([vp, pcf, sz, ppcf, P(sz), sz], ssz),
+        "atkdsp_osx_process_n": ([vp, ppcf, u, sz, ppcf, P(sz), sz], ssz),
+        "atkdsp_osx_describe": ([vp, C.c_char_p, sz], C.c_int),
+        "atkdsp_gpu_osx_process_n": ([vp, P(vp), u, sz, P(vp), P(sz), sz], ssz),
+        "atkdsp_gpu_osx_stream": ([vp], vp),
+        "atkdsp_gpu_osx_sync": ([vp], C.c_int),
         "atkdsp_gpu_tune_set": ([u, u, u, C.c_int], C.c_int),
         "atkdsp_gpu_tune_get": ([u, u, u], C.c_int),
     }
@@ -296,6 +311,95 @@ class Pfb:
 
     def process(self, x):
         return self.process_n([x], 1)[0]
+
+
+class Osx:
+    """Overlap-save extractor on the GPU (atkdsp_osx): arbitrary channels at
+    arbitrary centres from one forward FFT per block, each landed on its own
+    out_rate. add/retune/remove between calls without disturbing the others;
+    process_n runs N elements phase-coherently."""
+
+    def __init__(self, fs, nfft=4096, atten_db=80.0, max_nel=1):
+        self._lib = load()
+        self._p = self._lib.atkdsp_osx_create(float(fs), int(nfft), float(atten_db), int(max_nel))
+        if not self._p:
+            raise AtkDspError("osx_create: check fs>0, nfft a power of two >= 64, "
+                              "a usable GPU and free device memory")
+        self.max_nel = int(max_nel)
+        self.nfft = int(nfft)
+
+    def __del__(self):
+        p = getattr(self, "_p", None)
+        if p:
+            self._lib.atkdsp_osx_destroy(p)
+            self._p = None
+
+    @property
+    def handle(self):
+        return self._p
+
+    def reset(self):
+        self._lib.atkdsp_osx_reset(self._p)
+
+    def add(self, offset_hz, bw_hz, out_rate):
+        ch = self._lib.atkdsp_osx_add(self._p, float(offset_hz), float(bw_hz), float(out_rate))
+        return _check(int(ch), "osx_add")
+
+    def retune(self, ch, offset_hz):
+        _check(self._lib.atkdsp_osx_retune(self._p, int(ch), float(offset_hz)), "osx_retune")
+
+    def remove(self, ch):
+        _check(self._lib.atkdsp_osx_remove(self._p, int(ch)), "osx_remove")
+
+    def channels(self):
+        return int(self._lib.atkdsp_osx_channels(self._p))
+
+    def chan_rate(self, ch):
+        return float(self._lib.atkdsp_osx_chan_rate(self._p, int(ch)))
+
+    def out_max(self, ch, n):
+        return int(self._lib.atkdsp_osx_out_max(self._p, int(ch), int(n)))
+
+    def describe(self):
+        buf = C.create_string_buffer(256)
+        n = self._lib.atkdsp_osx_describe(self._p, buf, 256)
+        return buf.value.decode() if n > 0 else ""
+
+    def process_n(self, ins, nel, cap=None):
+        """(outs, counts): outs[slot] is an (nel, count) array or None for a
+        free slot. cap: cap_each (default the binding's, the largest
+        out_max over the active slots)."""
+        nel = int(nel)
+        arrs = [np.ascontiguousarray(np.asarray(ins[e]).ravel(), np.complex64) for e in range(nel)]
+        n = arrs[0].size
+        for a in arrs:
+            if a.size != n:
+                raise AtkDspError("osx: elements must be equal length")
+        ns = self.channels()
+        active = [self.chan_rate(ci) > 0 for ci in range(ns)]
+        if cap is None:
+            cap = max([self.out_max(ci, n) for ci in range(ns) if active[ci]], default=0)
+        bufs = [[np.zeros(cap, np.complex64) if active[ci] else None for ci in range(ns)]
+                for _ in range(nel)]
+        ptrs = (C.POINTER(_Cf32) * max(nel * ns, 1))()
+        for e in range(nel):
+            for ci in range(ns):
+                ptrs[e * ns + ci] = _cfp(bufs[e][ci]) if active[ci] else None
+        counts = (C.c_size_t * max(ns, 1))()
+        inarr = (C.POINTER(_Cf32) * nel)(*[_cfp(a) for a in arrs])
+        got = self._lib.atkdsp_osx_process_n(self._p, inarr, nel, n, ptrs, counts, int(cap))
+        _check(int(got), "osx_process_n")
+        cnts = [int(counts[ci]) for ci in range(ns)]
+        outs = [None] * ns
+        for ci in range(ns):
+            if active[ci]:
+                outs[ci] = np.array([bufs[e][ci][:cnts[ci]] for e in range(nel)], np.complex64) \
+                    if cnts[ci] else np.zeros((nel, 0), np.complex64)
+        return outs, cnts
+
+    def process(self, x, cap=None):
+        outs, cnts = self.process_n([x], 1, cap)
+        return [o[0] if o is not None else None for o in outs], cnts
 
 
 def pfb_cov_accumulate(out, nel, nchan, gate, R, counts):

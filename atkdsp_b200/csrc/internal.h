@@ -167,6 +167,69 @@ int  atkb_w12(const void *out, unsigned nel, unsigned nchan, size_t m, const uin
 int  atkb_cov_reset(void *R, uint32_t *counts, unsigned nel, unsigned nchan,
                     const uint8_t *gate, void *stream);
 
+/* overlap-save extractor ----------------------------------------------------
+ * One run = m consecutive blocks (hops) of nel element streams. Block i of
+ * element e is s[i*hop, i*hop + nfft) of s = state[e][0, head) ++
+ * ins[e][in_off, ...).
+ * Each block is forward-transformed (double, rounded to float like the
+ * reference's spectrum), then every channel folds it to M bins, inverts them
+ * and writes its nvalid = hop/decim samples of block i, rolled to absolute
+ * time: to dsts[e] + (hop_base + i)*nvalid when dsts is set (the caller's
+ * device buffers), else to the channel's staging
+ * stage + par*par_stride + e*stage_stride + lead + i*nvalid. */
+typedef struct {
+    const void *H;                /* device cf32, nfft: the channel filter's spectrum */
+    void *const *dsts;            /* device array of nel device pointers, or NULL */
+    void *stage;                  /* device cf32 [2][max_nel][stage_stride]       */
+    long long stage_stride, par_stride, lead;
+    double delta;                 /* residual offset (Hz) after the integer roll  */
+    int M, logm, ovd, nvalid, decim, shift;
+} atkb_osx_chan;
+
+typedef struct {
+    const void *state;            /* device cf32 [nel][state_stride]              */
+    const void *const *ins;       /* device array of nel device cf32 pointers     */
+    long long state_stride, in_off, head;
+    long long blk0;               /* absolute index of block 0                    */
+    const void *tw;               /* device double2 [nfft]: (cos, -sin)(2 pi j/nfft) */
+    const atkb_osx_chan *chans;   /* device, nchans: nsmall channels with
+                                   * M <= ATKB_OSX_SMALL_M, then nmid with
+                                   * M <= 4096, then those with M > 4096       */
+    const atkb_osx_chan *h_chans; /* the same table in host memory (launcher)   */
+    double fs;
+    long long hop_base;           /* blocks of this call before this run          */
+    int par;                      /* which half of the channels' staging          */
+    int nfft, lognfft, hop, ov, nchans, nsmall, nmid;
+    void *X;                      /* device cf32 [nel][m][nfft]: nfft > fused max */
+    void *T, *Y;                  /* device double2 scratch, same shape           */
+} atkb_osx_run;
+/* channels of at most this many bins run one warp each */
+#define ATKB_OSX_SMALL_M 64
+/* dynamic shared memory of the fused kernel for one nfft */
+size_t atkb_osx_group_smem(int nfft);
+
+/* the largest nfft whose whole chain runs in one CTA's shared memory */
+#define ATKB_OSX_FUSED_MAX 4096
+/* the largest nfft at all (two passes of at most 4096 points) */
+#define ATKB_OSX_NFFT_MAX (1 << 24)
+int  atkb_osx_launch(const atkb_osx_run *run, int m, int nel, void *stream);
+/* the arbitrary resampler over one channel's sample stream, per element
+ * e < nel: v + e*v_stride holds hist (Q) ++ nv new samples. Outputs K0 + k,
+ * k < count, at input position base + K*step - inoff (the reference's
+ * formula) go to outs[e] + out_off (outs: a device array of nel device
+ * pointers) or, when outs is NULL, to stage + e*stage_stride + k. The new
+ * history, the last Q of hist ++ new, goes to v_next + e*v_stride. pd = P*Q
+ * prototype taps then P*Q forward differences. */
+int  atkb_osx_resample(const void *v, void *v_next, long long v_stride, long long nv, int Q, int P,
+                       const float *pd, double base, double step, double inoff, unsigned long long K0,
+                       long long count, void *const *outs, long long out_off, void *stage,
+                       long long stage_stride, int nel, void *stream);
+/* dst[e][0, len) = s[from, from + len) of s = state[e][0, head) ++
+ * ins[e][in_off, ...), ins a device array of nel device pointers */
+int  atkb_osx_carry(const void *state, long long state_stride, const void *const *ins, long long in_off,
+                    long long head, long long from, long long len, void *dst, long long dst_stride,
+                    int nel, void *stream);
+
 /* unpack ------------------------------------------------------------------- */
 /* device raw -> device cf32 (out may be NULL: mean only), (x - c) * k per component; the means (double,
  * BEFORE subtraction of the offset, i.e. sum(out)/n + off) go to d_mean[0..1]

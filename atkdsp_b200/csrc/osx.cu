@@ -1,0 +1,466 @@
+/* The overlap-save extractor on sm_100a (reference src/channelizer.c:473-788).
+ *
+ * One CTA per (block, element). For nfft <= ATKB_OSX_FUSED_MAX the whole chain
+ * stays in shared memory: the block's nfft samples are gathered from the
+ * element's state and input, transformed in double (Stockham, radix 4 with
+ * one radix-2 pass when log2 nfft is odd), and rounded to a float spectrum X
+ * as the reference stores it. Then, per channel: the decimating fold of X
+ * against the channel filter's spectrum into M bins (float, the reference's
+ * expression order with rounded operations: src/channelizer.c:707-716), the
+ * M-point inverse (double, scaled by 1/M and rounded to float like
+ * pocketfft's backward transform), and the roll to absolute time with the
+ * residual offset removed per sample (double, :721-737), one rounding to
+ * float. X never leaves the SM. Larger transforms run as two passes of at
+ * most 4096 points over a double scratch in HBM (the four-step form), then
+ * the same per-channel code reads X from HBM.
+ *
+ * The arbitrary resampler (src/resample.c:194-260) computes every output
+ * independently: output K sits at input position base + K*step - in_off,
+ * which the reference made blocking-invariant, so one thread per output
+ * reproduces the reference's per-block loop bit for bit.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "internal.h"
+
+#define OSX_NT 512
+#define OSX_WARPS (OSX_NT / 32)
+#define OSX_G 4                              /* blocks per CTA */
+#define OSX_WREG 256                         /* double2 per warp's region */
+#define OSX_WORK (OSX_WARPS * OSX_WREG)      /* 4096 double2: the work area */
+static_assert(OSX_G * ATKB_OSX_SMALL_M <= OSX_WREG, "a small channel's blocks fit its warp's region");
+static_assert(OSX_WORK >= ATKB_OSX_FUSED_MAX, "the work area holds one fused transform");
+#define OSX_PI2 6.283185307179586476925286766559
+
+namespace {
+
+__device__ __forceinline__ double2 d2add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 d2sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 d2mul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+/* W^j of the nfft-point table, read at stride 2^sh for a shorter transform;
+ * conjugated for the inverse */
+__device__ __forceinline__ double2 tw_at(const double2 *tw, int j, int sh, bool inv) {
+    double2 w = __ldg(tw + ((size_t)j << sh));
+    if (inv) w.y = -w.y;
+    return w;
+}
+
+/* 4-point DFT in place; the inverse swaps the roles of -i and +i */
+__device__ __forceinline__ void dft4(double2 *v, bool inv) {
+    const double2 s02 = d2add(v[0], v[2]), d02 = d2sub(v[0], v[2]);
+    const double2 s13 = d2add(v[1], v[3]), d13 = d2sub(v[1], v[3]);
+    const double2 r = inv ? make_double2(-d13.y, d13.x) : make_double2(d13.y, -d13.x);  /* -+i d13 */
+    v[0] = d2add(s02, s13);
+    v[2] = d2sub(s02, s13);
+    v[1] = d2add(d02, r);
+    v[3] = d2sub(d02, r);
+}
+
+/* Batched in-place Stockham transforms by NTH threads (a warp or the CTA):
+ * nb transforms of n = 2^logn points at sm + b*n, natural order in and out,
+ * nb*n <= 8*NTH. Each pass reads every value a thread needs into registers,
+ * then all write after a barrier (radix 4, after one radix-2 pass when
+ * log2 n is odd). Twiddles come from the nfft-point table (lognfft) at the
+ * stride that gives this length's roots. Ends with a barrier. */
+template <int NTH>
+__device__ __forceinline__ void osx_sync() {
+    if (NTH == 32) __syncwarp();
+    else __syncthreads();
+}
+
+template <int NTH>
+__device__ void fft_b(double2 *sm, int logn, int nb, const double2 *__restrict__ tw, int lognfft, bool inv,
+                      int tid) {
+    const int n = 1 << logn;
+    int lg = 0;                                /* log2 of the finished sub-length Ns */
+    if (logn & 1) {                            /* radix 2 with Ns = 1: no twiddles */
+        const int h = n >> 1, tot = nb * h;
+        double2 a[4], c[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int T = tid + u * NTH;
+            if (T < tot) {
+                const int base = (T >> (logn - 1)) << logn, t = T & (h - 1);
+                a[u] = sm[base + t];
+                c[u] = sm[base + t + h];
+            }
+        }
+        osx_sync<NTH>();
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int T = tid + u * NTH;
+            if (T < tot) {
+                const int base = (T >> (logn - 1)) << logn, t = T & (h - 1);
+                sm[base + 2 * t] = d2add(a[u], c[u]);
+                sm[base + 2 * t + 1] = d2sub(a[u], c[u]);
+            }
+        }
+        osx_sync<NTH>();
+        lg = 1;
+    }
+    const int q = n >> 2, totq = nb * q;
+    for (; lg < logn; lg += 2) {
+        const int Ns = 1 << lg;
+        const int sh = lognfft - lg - 2;       /* W_{4 Ns}^j = W_nfft^(j << sh) */
+        double2 v[2][4];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int T = tid + u * NTH;
+            if (T < totq) {
+                const int base = (T >> (logn - 2)) << logn, t = T & (q - 1), k = t & (Ns - 1);
+#pragma unroll
+                for (int r = 0; r < 4; ++r) v[u][r] = sm[base + t + r * q];
+                if (lg) {
+#pragma unroll
+                    for (int r = 1; r < 4; ++r) v[u][r] = d2mul(v[u][r], tw_at(tw, r * k, sh, inv));
+                }
+                dft4(v[u], inv);
+            }
+        }
+        osx_sync<NTH>();
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int T = tid + u * NTH;
+            if (T < totq) {
+                const int base = (T >> (logn - 2)) << logn, t = T & (q - 1), k = t & (Ns - 1);
+                const int o = base + ((t >> lg) << (lg + 2)) + k;
+#pragma unroll
+                for (int r = 0; r < 4; ++r) sm[o + r * Ns] = v[u][r];
+            }
+        }
+        osx_sync<NTH>();
+    }
+}
+
+/* bin k of a channel's decimating fold of one spectrum row (float, j
+ * ascending, the reference's rounded expression, src/channelizer.c:707-716) */
+__device__ __forceinline__ double2 fold_bin(const float2 *X, const float2 *__restrict__ H, int k, int M, int decim,
+                                            int shift, int mask) {
+    float ar = 0.0f, ai = 0.0f;
+    int bin = k;
+#pragma unroll 4
+    for (int j = 0; j < decim; ++j, bin += M) {
+        const float2 xv = X[(bin + shift) & mask];
+        const float2 hv = __ldg(H + bin);
+        ar = __fadd_rn(ar, __fsub_rn(__fmul_rn(xv.x, hv.x), __fmul_rn(xv.y, hv.y)));
+        ai = __fadd_rn(ai, __fadd_rn(__fmul_rn(xv.x, hv.y), __fmul_rn(xv.y, hv.x)));
+    }
+    return make_double2((double)ar, (double)ai);
+}
+
+/* output k of block bi from the channel's unscaled inverse y (the float
+ * output pocketfft's 1/M scaling gives, then the roll to absolute time with
+ * the residual removed: src/channelizer.c:721-737, one rounding per step) */
+__device__ __forceinline__ float2 roll_out(double2 y, const atkb_osx_chan &C, long long bi, int k, int hop,
+                                           int ov, int nfft, double fs) {
+    const long long start = bi * hop - ov;
+    long long smod = ((long long)C.shift * start) % nfft;
+    if (smod < 0) smod += nfft;
+    const double a0 = (double)smod / (double)nfft;
+    const double invm = 1.0 / (double)C.M, invd = 1.0 / (double)C.decim;
+    const float ysr = __double2float_rn(__dmul_rn(y.x, invm));
+    const float ysi = __double2float_rn(__dmul_rn(y.y, invm));
+    const double yr = __dmul_rn((double)ysr, invd), yi = __dmul_rn((double)ysi, invd);
+    const long long nabs = bi * hop + (long long)k * C.decim;
+    const double ph = __dmul_rn(-OSX_PI2, __dadd_rn(a0, __ddiv_rn(__dmul_rn(C.delta, (double)nabs), fs)));
+    double s, c;
+    sincos(ph, &s, &c);
+    return make_float2(__double2float_rn(__dsub_rn(__dmul_rn(yr, c), __dmul_rn(yi, s))),
+                       __double2float_rn(__dadd_rn(__dmul_rn(yr, s), __dmul_rn(yi, c))));
+}
+
+/* where element e's samples of block 0 of this run go */
+__device__ __forceinline__ float2 *osx_dst(const atkb_osx_chan &C, const atkb_osx_run &R, int e) {
+    if (C.dsts) return (float2 *)C.dsts[e] + R.hop_base * C.nvalid;
+    return (float2 *)C.stage + R.par * C.par_stride + e * C.stage_stride + C.lead;
+}
+
+/* One channel over nb consecutive blocks (spectrum rows X + g*xs, blocks
+ * i0 + g) by NTH threads in `buf` (nb*M <= 8*NTH double2): folds, batched
+ * inverse, rolled outputs. Ends with a barrier of the NTH threads. */
+template <int NTH>
+__device__ void osx_channel(const float2 *X, int xs, int nb, const atkb_osx_chan &C, double2 *buf,
+                            const atkb_osx_run &R, int e, int i0, int tid) {
+    const float2 *H = (const float2 *)C.H;
+    const int logm = C.logm, M = C.M, mask = R.nfft - 1;
+    for (int it = tid; it < (nb << logm); it += NTH)
+        buf[it] = fold_bin(X + (it >> logm) * xs, H, it & (M - 1), M, C.decim, C.shift, mask);
+    osx_sync<NTH>();
+    fft_b<NTH>(buf, logm, nb, (const double2 *)R.tw, R.lognfft, true, tid);
+    float2 *dst = osx_dst(C, R, e);
+    const int lv = logm - 1;                   /* nvalid = M / 2 */
+    for (int it = tid; it < (nb << lv); it += NTH) {
+        const int g = it >> lv, k = it & ((1 << lv) - 1);
+        const int i = i0 + g;
+        dst[(long long)i * C.nvalid + k] =
+            roll_out(buf[(g << logm) + C.ovd + k], C, R.blk0 + i, k, R.hop, R.ov, R.nfft, R.fs);
+    }
+    osx_sync<NTH>();
+}
+
+/* the channels of nb blocks whose float spectra are rows X + g*xs: the
+ * small ones (M * OSX_G <= OSX_WREG) one warp each in its own region of
+ * `work`, then the others by the whole CTA in batches of blocks */
+__device__ void osx_channels(const float2 *X, int xs, int nb, double2 *work, const atkb_osx_run &R, int e,
+                             int i0) {
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    for (int c = w; c < R.nsmall; c += OSX_WARPS) {
+        const atkb_osx_chan C = R.chans[c];
+        osx_channel<32>(X, xs, nb, C, work + w * OSX_WREG, R, e, i0, lane);
+    }
+    __syncthreads();
+    for (int c = R.nsmall; c < R.nsmall + R.nmid; ++c) {
+        const atkb_osx_chan C = R.chans[c];
+        const int per = ATKB_OSX_FUSED_MAX >> C.logm;     /* blocks per batch */
+        for (int g0 = 0; g0 < nb; g0 += per) {
+            const int cnt = min(per, nb - g0);
+            osx_channel<OSX_NT>(X + g0 * xs, xs, cnt, C, work, R, e, i0 + g0, tid);
+        }
+    }
+}
+
+/* sample g of element e's stream state ++ in (in: the element's input, at
+ * the run's offset) */
+__device__ __forceinline__ float2 osx_sample(const atkb_osx_run &R, const float2 *in, int e, long long g) {
+    if (g < R.head) return __ldg((const float2 *)R.state + e * R.state_stride + g);
+    return __ldg(in + (g - R.head));
+}
+__device__ __forceinline__ const float2 *osx_in(const atkb_osx_run &R, int e) {
+    return (const float2 *)R.ins[e] + R.in_off;
+}
+
+/* nfft <= ATKB_OSX_FUSED_MAX: grid (ceil(m / OSX_G), nel). Shared memory:
+ * the work area (OSX_WORK double2: each forward transform, then the
+ * channels' folds and inverses) and OSX_G float spectrum rows of nfft + 1
+ * (the pad staggers the rows across banks). */
+__global__ void __launch_bounds__(OSX_NT, 1) osx_group_kernel(const atkb_osx_run R, int m) {
+    extern __shared__ double2 smem[];
+    double2 *work = smem;
+    const int nfft = R.nfft, xs = nfft + 1;
+    float2 *X = (float2 *)(smem + OSX_WORK);
+    const int i0 = blockIdx.x * OSX_G, e = blockIdx.y, nb = min(OSX_G, m - i0);
+    const float2 *in = osx_in(R, e);
+    const double2 *tw = (const double2 *)R.tw;
+    for (int g = 0; g < nb; ++g) {
+        const long long g0 = (long long)(i0 + g) * R.hop;
+        for (int p = threadIdx.x; p < nfft; p += OSX_NT) {
+            const float2 v = osx_sample(R, in, e, g0 + p);
+            work[p] = make_double2((double)v.x, (double)v.y);
+        }
+        __syncthreads();
+        fft_b<OSX_NT>(work, R.lognfft, 1, tw, R.lognfft, false, threadIdx.x);
+        for (int p = threadIdx.x; p < nfft; p += OSX_NT)
+            X[g * xs + p] = make_float2(__double2float_rn(work[p].x), __double2float_rn(work[p].y));
+        __syncthreads();
+    }
+    osx_channels(X, xs, nb, work, R, e, i0);
+}
+
+/* nfft > ATKB_OSX_FUSED_MAX: the channels read the spectra from HBM */
+__global__ void __launch_bounds__(OSX_NT, 1) osx_group_chan_kernel(const atkb_osx_run R, int m) {
+    extern __shared__ double2 smem[];
+    const int i0 = blockIdx.x * OSX_G, e = blockIdx.y, nb = min(OSX_G, m - i0);
+    const float2 *X = (const float2 *)R.X + ((long long)e * m + i0) * R.nfft;
+    osx_channels(X, R.nfft, nb, smem, R, e, i0);
+}
+
+/* Transforms longer than 4096 points: n = n1 * n2 in the four-step form,
+ * X[k1 + n1 k2] = sum_q W_n2^(q k2) W_n^(q k1) sum_r x[q + n2 r] W_n1^(r k1).
+ * Pass A, grid (n2, m, nel): column q's n1-point transform, times
+ * W_n^(q k1), to T[item][k1 n2 + q]. The source is the block of the stream
+ * (SRC 0, a forward transform of nfft points) or a double buffer of n-point
+ * items (SRC 1). */
+template <int SRC>
+__global__ void __launch_bounds__(OSX_NT) osx_four_a(const atkb_osx_run R, const double2 *__restrict__ src, int logn1,
+                                                     int logn2, bool inv, double2 *__restrict__ T, int m) {
+    extern __shared__ double2 sm[];
+    const int q = blockIdx.x, i = blockIdx.y, e = blockIdx.z;
+    const int n1 = 1 << logn1, logn = logn1 + logn2;
+    const double2 *tw = (const double2 *)R.tw;
+    const long long item = (long long)e * m + i;
+    if (SRC == 0) {
+        const float2 *in = osx_in(R, e);
+        const long long g0 = (long long)i * R.hop + q;
+        for (int r = threadIdx.x; r < n1; r += OSX_NT) {
+            const float2 v = osx_sample(R, in, e, g0 + ((long long)r << logn2));
+            sm[r] = make_double2((double)v.x, (double)v.y);
+        }
+    } else {
+        const double2 *s = src + (item << logn) + q;
+        for (int r = threadIdx.x; r < n1; r += OSX_NT) sm[r] = s[(long long)r << logn2];
+    }
+    __syncthreads();
+    fft_b<OSX_NT>(sm, logn1, 1, tw, R.lognfft, inv, threadIdx.x);
+    double2 *t = T + (item << logn);
+    const int sh = R.lognfft - logn, mask = (1 << logn) - 1;
+    for (int k1 = threadIdx.x; k1 < n1; k1 += OSX_NT)
+        t[((long long)k1 << logn2) + q] = q ? d2mul(sm[k1], tw_at(tw, (q * k1) & mask, sh, inv)) : sm[k1];
+}
+
+/* Pass B, grid (n1, m, nel): row k1's n2-point transform, to a float
+ * spectrum (DST 0) or a double buffer (DST 1), natural order */
+template <int DST>
+__global__ void __launch_bounds__(OSX_NT) osx_four_b(const atkb_osx_run R, const double2 *__restrict__ T, int logn1,
+                                                     int logn2, bool inv, void *out, int m) {
+    extern __shared__ double2 sm[];
+    const int k1 = blockIdx.x, i = blockIdx.y, e = blockIdx.z;
+    const int n2 = 1 << logn2, logn = logn1 + logn2;
+    const long long item = (long long)e * m + i;
+    const double2 *t = T + (item << logn) + ((long long)k1 << logn2);
+    for (int q = threadIdx.x; q < n2; q += OSX_NT) sm[q] = t[q];
+    __syncthreads();
+    fft_b<OSX_NT>(sm, logn2, 1, (const double2 *)R.tw, R.lognfft, inv, threadIdx.x);
+    for (int k2 = threadIdx.x; k2 < n2; k2 += OSX_NT) {
+        const long long o = (item << logn) + k1 + ((long long)k2 << logn1);
+        if (DST == 0) ((float2 *)out)[o] = make_float2(__double2float_rn(sm[k2].x), __double2float_rn(sm[k2].y));
+        else ((double2 *)out)[o] = sm[k2];
+    }
+}
+
+/* a channel with M > 4096 (nfft > 4096, small decimation): its folds to a
+ * double buffer Y[item][M], grid (ceil(M / 256), m, nel) */
+__global__ void osx_fold_big(const atkb_osx_run R, int c, double2 *__restrict__ Y, int m) {
+    const atkb_osx_chan C = R.chans[c];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y, e = blockIdx.z;
+    if (k >= C.M) return;
+    const long long item = (long long)e * m + i;
+    Y[(item << C.logm) + k] = fold_bin((const float2 *)R.X + item * R.nfft, (const float2 *)C.H, k, C.M,
+                                       C.decim, C.shift, R.nfft - 1);
+}
+
+/* ... and its rolled outputs from the inverse in Y, grid (ceil(nvalid / 256), m, nel) */
+__global__ void osx_roll_big(const atkb_osx_run R, int c, const double2 *__restrict__ Y, int m) {
+    const atkb_osx_chan C = R.chans[c];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y, e = blockIdx.z;
+    if (k >= C.nvalid) return;
+    const long long item = (long long)e * m + i;
+    float2 *dst = osx_dst(C, R, e);
+    dst[(long long)i * C.nvalid + k] = roll_out(Y[(item << C.logm) + C.ovd + k], C, R.blk0 + i, k, R.hop, R.ov,
+                                                R.nfft, R.fs);
+}
+
+__global__ void osx_resample_kernel(const float2 *__restrict__ v, float2 *__restrict__ v_next, long long v_stride,
+                                    long long nv, int Q, int P, const float *__restrict__ pp,
+                                    const float *__restrict__ dd, double base, double step, double inoff,
+                                    unsigned long long K0, long long count, void *const *__restrict__ outs,
+                                    long long out_off, float2 *__restrict__ stage, long long stage_stride) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = blockIdx.y;
+    const float2 *x = v + (long long)e * v_stride + Q;       /* x[m], m >= -Q */
+    if (k < Q) v_next[(long long)e * v_stride + k] = x[nv - Q + k];
+    if (k >= count) return;
+    const double local = __dsub_rn(__dadd_rn(base, __dmul_rn((double)(K0 + (unsigned long long)k), step)), inoff);
+    const long long i = (long long)floor(local);
+    const double frac = __dsub_rn(local, (double)i);
+    const double ph = __dmul_rn(frac, (double)P);
+    int b = (int)ph;
+    if (b >= P) b = P - 1;
+    const float mu = __double2float_rn(__dsub_rn(ph, (double)b));
+    float ar = 0.0f, ai = 0.0f;
+    for (int q = 0; q < Q; ++q) {
+        const long long mm = i - q;
+        if (mm < -(long long)Q) break;                          /* older than the kept history */
+        const float2 xv = __ldg(x + mm);
+        const float c = __fadd_rn(__ldg(pp + b + q * P), __fmul_rn(mu, __ldg(dd + b + q * P)));
+        ar = __fadd_rn(ar, __fmul_rn(c, xv.x));
+        ai = __fadd_rn(ai, __fmul_rn(c, xv.y));
+    }
+    float2 *o = outs ? (float2 *)outs[e] + out_off : stage + (long long)e * stage_stride;
+    o[k] = make_float2(ar, ai);
+}
+
+__global__ void osx_carry_kernel(const float2 *__restrict__ state, long long state_stride,
+                                 const void *const *__restrict__ ins, long long in_off, long long head,
+                                 long long from, long long len, float2 *__restrict__ dst, long long dst_stride) {
+    const int e = blockIdx.y;
+    const float2 *in = (const float2 *)ins[e] + in_off;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < len;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long g = from + t;
+        dst[e * dst_stride + t] = g < head ? state[e * state_stride + g] : in[g - head];
+    }
+}
+
+bool g_configured[64];
+
+int set_smem(const void *fn, int bytes) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" size_t atkb_osx_group_smem(int nfft) {
+    return (size_t)OSX_WORK * 16 + (size_t)OSX_G * (nfft + 1) * 8;
+}
+
+extern "C" int atkb_osx_launch(const atkb_osx_run *run, int m, int nel, void *stream) {
+    if (m <= 0 || nel <= 0) return ATKB_OK;
+    const atkb_osx_run &R = *run;
+    cudaStream_t s = (cudaStream_t)stream;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !g_configured[dev]) {
+        const int big = (int)atkb_osx_group_smem(ATKB_OSX_FUSED_MAX);
+        if (!set_smem((const void *)osx_group_kernel, big) || !set_smem((const void *)osx_group_chan_kernel, OSX_WORK * 16) ||
+            !set_smem((const void *)osx_four_a<0>, 4096 * 16) || !set_smem((const void *)osx_four_a<1>, 4096 * 16) ||
+            !set_smem((const void *)osx_four_b<0>, 4096 * 16) || !set_smem((const void *)osx_four_b<1>, 4096 * 16))
+            return ATKB_E_KERNEL;
+        g_configured[dev] = true;
+    }
+    const dim3 groups((m + OSX_G - 1) / OSX_G, nel);
+    if (R.nfft <= ATKB_OSX_FUSED_MAX) {
+        osx_group_kernel<<<groups, OSX_NT, atkb_osx_group_smem(R.nfft), s>>>(R, m);
+        return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+    }
+    int logn2 = R.lognfft / 2, logn1 = R.lognfft - logn2;
+    if (logn1 > 12) return ATKB_E_ARG;
+    osx_four_a<0><<<dim3(1 << logn2, m, nel), OSX_NT, (size_t)16 << logn1, s>>>(R, nullptr, logn1, logn2, false,
+                                                                                (double2 *)R.T, m);
+    osx_four_b<0><<<dim3(1 << logn1, m, nel), OSX_NT, (size_t)16 << logn2, s>>>(R, (const double2 *)R.T, logn1,
+                                                                                logn2, false, R.X, m);
+    if (R.nsmall + R.nmid > 0) osx_group_chan_kernel<<<groups, OSX_NT, OSX_WORK * 16, s>>>(R, m);
+    for (int c = R.nsmall + R.nmid; c < R.nchans; ++c) {
+        /* M > 4096: fold to Y, four-step inverse through T back into Y, roll */
+        const int logm = R.h_chans[c].logm;
+        const int M = 1 << logm, nv = M >> 1;
+        double2 *Y = (double2 *)R.Y, *T = (double2 *)R.T;
+        logn2 = logm / 2;
+        logn1 = logm - logn2;
+        osx_fold_big<<<dim3((M + 255) / 256, m, nel), 256, 0, s>>>(R, c, Y, m);
+        osx_four_a<1><<<dim3(1 << logn2, m, nel), OSX_NT, (size_t)16 << logn1, s>>>(R, Y, logn1, logn2, true, T, m);
+        osx_four_b<1><<<dim3(1 << logn1, m, nel), OSX_NT, (size_t)16 << logn2, s>>>(R, T, logn1, logn2, true, Y, m);
+        osx_roll_big<<<dim3((nv + 255) / 256, m, nel), 256, 0, s>>>(R, c, Y, m);
+    }
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
+extern "C" int atkb_osx_resample(const void *v, void *v_next, long long v_stride, long long nv, int Q, int P,
+                                 const float *pd, double base, double step, double inoff, unsigned long long K0,
+                                 long long count, void *const *outs, long long out_off, void *stage,
+                                 long long stage_stride, int nel, void *stream) {
+    if (nel <= 0) return ATKB_OK;
+    const int nt = 128;
+    const long long work = count > Q ? count : Q;
+    if (work <= 0) return ATKB_OK;
+    const long long blocks = (work + nt - 1) / nt;
+    osx_resample_kernel<<<dim3((unsigned)blocks, nel), nt, 0, (cudaStream_t)stream>>>(
+        (const float2 *)v, (float2 *)v_next, v_stride, nv, Q, P, pd, pd + (size_t)P * Q, base, step, inoff, K0,
+        count, outs, out_off, (float2 *)stage, stage_stride);
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
+extern "C" int atkb_osx_carry(const void *state, long long state_stride, const void *const *ins,
+                              long long in_off, long long head, long long from, long long len, void *dst,
+                              long long dst_stride, int nel, void *stream) {
+    if (len <= 0 || nel <= 0) return ATKB_OK;
+    const int nt = 256;
+    long long blocks = (len + nt - 1) / nt;
+    if (blocks > 1024) blocks = 1024;
+    osx_carry_kernel<<<dim3((unsigned)blocks, nel), nt, 0, (cudaStream_t)stream>>>(
+        (const float2 *)state, state_stride, ins, in_off, head, from, len, (float2 *)dst, dst_stride);
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}

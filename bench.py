@@ -22,6 +22,10 @@ Arms printed in ONE JSON line (rank 0):
               8*oversample B out per input sample) / its CUDA-event duration
   cpu_baseline the reference's own C library (built from its sources) on this
               host's cores over a bounded sample of the same workload
+  configs     the other configurations, each with its own rate: single
+              stream (C ABI, uneven blocks), the unpack front end, the
+              coherent array, the overlap-save extractor (64 channels from
+              one 61.44 MS/s stream), the serving loop
 
 --impl reference runs only the reference's CPU channelizer (all host threads)
 on the same workload and prints its line.
@@ -504,6 +508,109 @@ def _c3_arm(torch, device, steps):
             "unit": "MSamples/s (aggregate over elements)", "path": "process_n (device) + one-pass W1/W2"}
 
 
+OSX_FS = 61.44e6
+OSX_NFFT = 4096
+OSX_N = 1 << 24
+
+
+def osx_channels(nch: int = 64, seed: int = 9):
+    """The extractor workload's channel plan: nch channels at seeded offsets
+    across +-0.45 fs, bandwidths cycling 12.5 / 25 / 50 / 200 kHz, half landed
+    at 1.25 x bw (their decimated rate: no resampling), half at 1.0 x bw
+    (resampled)."""
+    rng = np.random.default_rng(seed)
+    bws = (12.5e3, 25e3, 50e3, 200e3)
+    return [(float(rng.uniform(-0.45, 0.45) * OSX_FS), bws[i % 4], bws[i % 4] * (1.25 if i % 2 else 1.0))
+            for i in range(nch)]
+
+
+def _osx_arm(torch, device, steps, cpu: bool):
+    """The overlap-save extractor: one 61.44 MS/s cf32 stream (noise + tones),
+    nfft 4096, 64 channels (osx_channels). value: atkdsp_gpu_osx_process_n on
+    2^24 samples resident in HBM per step (CUDA events on the handle's stream,
+    every kernel of the call inside); e2e: atkdsp_osx_process with host
+    buffers; cpu: the reference library on 2^20 samples of the same stream."""
+    import ctypes as C
+    import atkdsp_b200 as ak
+    lib = ak.load()
+    chans = osx_channels()
+    g = torch.Generator(device=device)
+    g.manual_seed(9)
+    x = torch.randn(OSX_N, dtype=torch.complex64, device=device, generator=g) * 0.5
+    t = torch.arange(OSX_N, device=device, dtype=torch.float64)
+    for f in (0.013, -0.21, 0.377):
+        x += torch.exp(2j * math.pi * f * t).to(torch.complex64)
+    del t
+    o = ak.Osx(OSX_FS, OSX_NFFT)
+    slots = [o.add(*c) for c in chans]
+    cap = OSX_N // 64
+    ys = [torch.empty(cap, dtype=torch.complex64, device=device) for _ in slots]
+    ins = (C.c_void_p * 1)(x.data_ptr())
+    outs = (C.c_void_p * len(slots))(*[y.data_ptr() for y in ys])
+    counts = (C.c_size_t * len(slots))()
+    st = torch.cuda.ExternalStream(lib.atkdsp_gpu_osx_stream(o.handle), device=device)
+
+    def step():
+        rc = lib.atkdsp_gpu_osx_process_n(o.handle, ins, 1, OSX_N, outs, counts, cap)
+        if rc < 0:
+            raise RuntimeError(f"osx: {rc}")
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k = max(steps, 1)
+    ev0.record(st)
+    for _ in range(k):
+        step()
+    ev1.record(st)
+    torch.cuda.synchronize()
+    dt = ev0.elapsed_time(ev1) / 1e3
+    out_samples = int(sum(counts))
+    alg = 8 * OSX_N + 8 * out_samples
+    achieved = alg / (dt / k) / 1e9
+    peak, peak_kind = _peaks()
+    # e2e: the C ABI with host buffers, copies inside the timed region
+    xh = x.cpu().numpy()
+    oh = ak.Osx(OSX_FS, OSX_NFFT)
+    for c in chans:
+        oh.add(*c)
+    hb = [np.zeros(cap, np.complex64) for _ in slots]
+    hptr = (C.POINTER(ak._Cf32) * len(slots))(*[ak._cfp(b) for b in hb])
+    hcnt = (C.c_size_t * len(slots))()
+    ke = max(1, min(k, 3))
+    lib.atkdsp_osx_process(oh.handle, ak._cfp(xh), OSX_N, hptr, hcnt, cap)
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        lib.atkdsp_osx_process(oh.handle, ak._cfp(xh), OSX_N, hptr, hcnt, cap)
+    te = (time.perf_counter() - t0) / ke
+    res = {"workload": f"extractor_nfft{OSX_NFFT}_64ch_61.44msps_2^24", "value": round(OSX_N * k / dt / 1e6, 2),
+           "unit": "MSamples/s", "ms_per_step": round(dt / k * 1e3, 3),
+           "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(achieved / peak, 4), "alg_bytes_per_step": alg, "peak_kind": peak_kind},
+           "e2e": {"value": round(OSX_N / te / 1e6, 2), "unit": "MSamples/s", "h2d_bytes_per_step": 8 * OSX_N,
+                   "d2h_bytes_per_step": 8 * int(sum(hcnt)), "path": "atkdsp_osx_process, pageable host buffers"},
+           "out_samples_per_step": out_samples,
+           "path": "atkdsp_gpu_osx_process_n: fused transform + 64 channel folds/inverses/rolls per block, "
+                   "resampler, state carry"}
+    if cpu:
+        from oracle import oracle as O
+        ref = O.reference()
+        if ref is not None:
+            r = ref.Osx(OSX_FS, OSX_NFFT)
+            for c in chans:
+                r.add(*c)
+            xs = xh[: 1 << 20]
+            r.process(xs)
+            t0 = time.perf_counter()
+            r.process(xs)
+            tc = time.perf_counter() - t0
+            res["cpu_baseline"] = {"value": round(xs.size / tc / 1e6, 2), "unit": "MSamples/s", "cores": 1,
+                                   "kind": "reference", "sample": "2^20 samples of the same stream "
+                                   "(atkdsp_osx_process_n is single-threaded)"}
+    return res
+
+
 def _served_arm(torch, device, duration_s):
     """Serving: 4096 live streams at {2.4, 10, 40} MS/s delivering 1.6 ms ci16
     blocks with Poisson arrivals, nchan {256, 1024}, 16 taps, 2x, churn 20/s,
@@ -613,6 +720,8 @@ def run_ours(args, rep):
         for name, fn in (("single_stream", lambda: _c1_arm(torch)),
                          ("front_end", lambda: _c2_arm(torch, device, 1)),
                          ("coherent_array", lambda: _c3_arm(torch, device, args.steps)),
+                         ("extractor", lambda: _osx_arm(torch, device, args.steps,
+                                                        "cpu" in arms and not args.no_cpu)),
                          ("served", lambda: _served_arm(torch, device, 3.0))):
             if name in arms:
                 try:
@@ -680,7 +789,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--arms", default="batched,plain,e2e,dropin,cpu,single_stream,front_end,coherent_array,served",
+    ap.add_argument("--arms", default="batched,plain,e2e,dropin,cpu,single_stream,front_end,coherent_array,"
+                    "extractor,served",
                     help="comma list of arms to run (the batched arm always runs)")
     ap.add_argument("--streams", type=int, default=256)
     ap.add_argument("--min-log2", type=float, default=14.0)

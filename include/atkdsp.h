@@ -4,7 +4,8 @@
  * This header declares exactly the entry points of the reference's ABI
  * (include/atkdsp.h of atkdsp 0.25.1, ABI 26) that the polyphase-filterbank
  * path uses: identity, threads, the unpack front end, the atkdsp_pfb_* handle
- * API and the W1/W2 accumulators. Names, types, argument meaning, return
+ * API and the W1/W2 accumulators, and the channelizer's other tool, the
+ * overlap-save extractor (atkdsp_osx_*). Names, types, argument meaning, return
  * codes and the channel-major output layout are the reference's, so a caller
  * of the reference (its ctypes binding, a C program, the in-library survey)
  * links against this library unchanged for this path. Each declaration cites
@@ -116,6 +117,36 @@ ATKDSP_API void        atkdsp_pfb_cov_reset(atkdsp_cf32 *R, uint32_t *counts, un
 ATKDSP_API void        atkdsp_pfb_channel_power(const atkdsp_cf32 *out, unsigned nel,
                                                 unsigned nchan, size_t m,
                                                 float *pwr, float *mean_pwr);
+
+/* ---- overlap-save extractor: reference include/atkdsp.h:3252-3289 --------
+ * One forward FFT of nfft points per block of hop = nfft/2 new samples; each
+ * channel folds it to M = nfft/decim bins, inverts them (the integer
+ * decimation), rolls to absolute time and is landed on its out_rate by the
+ * arbitrary resampler. Limits of this build: nfft <= 2^24 (create returns
+ * NULL beyond), and for nfft > 4096 a channel's M must be <= 4096
+ * (atkdsp_osx_add returns ATKDSP_E_ARG beyond). Capacity and missing output
+ * buffers are checked before any state changes (the reference finds them
+ * part-way through a call). */
+typedef struct atkdsp_osx atkdsp_osx;
+ATKDSP_API atkdsp_osx *atkdsp_osx_create(double fs, size_t nfft, double atten_db,
+                                         unsigned max_nel);                               /* :3257 */
+ATKDSP_API void        atkdsp_osx_destroy(atkdsp_osx *x);                                 /* :3259 */
+ATKDSP_API void        atkdsp_osx_reset(atkdsp_osx *x);                                   /* :3260 */
+ATKDSP_API int         atkdsp_osx_add(atkdsp_osx *x, double offset_hz, double bw_hz,
+                                      double out_rate);                                   /* :3264 */
+ATKDSP_API int         atkdsp_osx_retune(atkdsp_osx *x, int ch, double offset_hz);        /* :3265 */
+ATKDSP_API int         atkdsp_osx_remove(atkdsp_osx *x, int ch);                          /* :3266 */
+ATKDSP_API int         atkdsp_osx_channels(const atkdsp_osx *x);                          /* :3267 */
+ATKDSP_API double      atkdsp_osx_chan_rate(const atkdsp_osx *x, int ch);                 /* :3268 */
+ATKDSP_API size_t      atkdsp_osx_out_max(const atkdsp_osx *x, int ch, size_t n);         /* :3271 */
+ATKDSP_API ptrdiff_t   atkdsp_osx_process(atkdsp_osx *x, const atkdsp_cf32 *in, size_t n,
+                                          atkdsp_cf32 *const *outs, size_t *out_counts,
+                                          size_t cap_each);                               /* :3280 */
+ATKDSP_API ptrdiff_t   atkdsp_osx_process_n(atkdsp_osx *x, const atkdsp_cf32 *const *ins,
+                                            unsigned nel, size_t n,
+                                            atkdsp_cf32 *const *outs, size_t *out_counts,
+                                            size_t cap_each);                             /* :3285 */
+ATKDSP_API int         atkdsp_osx_describe(const atkdsp_osx *x, char *buf, size_t cap);  /* :3289 */
 
 #ifdef __cplusplus
 }

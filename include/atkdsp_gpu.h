@@ -155,6 +155,21 @@ ATKDSP_API void       *atkdsp_gpu_batch_stream(atkdsp_gpu_batch *b);
  * are shared by all calls on the batch, so read it before the next call. */
 ATKDSP_API float       atkdsp_gpu_batch_kernel_ms(atkdsp_gpu_batch *b);
 
+/* ---- the overlap-save extractor on device buffers ----------------------- */
+/* atkdsp_osx_process_n (reference include/atkdsp.h:3285) with device buffers:
+ * d_ins[el] are nel device pointers of n samples, d_outs[el*nslots + ch]
+ * device pointers of cap_each samples (NULL for free slots); both arrays are
+ * host memory. The work is enqueued on the handle's stream and the call
+ * returns without waiting; out_counts (known on the host before the work
+ * runs) are set on return. Returns the slot count, or ATKDSP_E_ARG /
+ * ATKDSP_E_CAP (state untouched) / ATKDSP_E_FFT. */
+ATKDSP_API ptrdiff_t   atkdsp_gpu_osx_process_n(atkdsp_osx *x, const atkdsp_cf32 *const *d_ins,
+                                                unsigned nel, size_t n, atkdsp_cf32 *const *d_outs,
+                                                size_t *out_counts, size_t cap_each);
+/* The handle's CUDA stream, and a wait for it (ATKDSP_E_FFT if a kernel failed). */
+ATKDSP_API void       *atkdsp_gpu_osx_stream(atkdsp_osx *x);
+ATKDSP_API int         atkdsp_gpu_osx_sync(atkdsp_osx *x);
+
 #ifdef __cplusplus
 }
 #endif

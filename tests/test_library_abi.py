@@ -43,7 +43,10 @@ def test_headers_declare_the_reference_surface():
                  "atkdsp_pfb_out_hops", "atkdsp_pfb_process", "atkdsp_pfb_process_n",
                  "atkdsp_pfb_block_origin", "atkdsp_pfb_group_delay", "atkdsp_pfb_set_cal",
                  "atkdsp_pfb_describe", "atkdsp_pfb_cov_accumulate", "atkdsp_pfb_cov_reset",
-                 "atkdsp_pfb_channel_power"):
+                 "atkdsp_pfb_channel_power", "atkdsp_osx_create", "atkdsp_osx_destroy",
+                 "atkdsp_osx_reset", "atkdsp_osx_add", "atkdsp_osx_retune", "atkdsp_osx_remove",
+                 "atkdsp_osx_channels", "atkdsp_osx_chan_rate", "atkdsp_osx_out_max",
+                 "atkdsp_osx_process", "atkdsp_osx_process_n", "atkdsp_osx_describe"):
         assert name in d, name
 
 
@@ -75,6 +78,15 @@ def test_create_rejects_bad_arguments_before_touching_a_device():
     for args in ((0.0, 64, 2, 12, 80.0, 1), (1e6, 1, 1, 12, 80.0, 1), (1e6, 64, 3, 12, 80.0, 1),
                  (1e6, 64, 2, 1, 80.0, 1), (1e6, 64, 2, 12, 80.0, 0), (1e6, 8192, 2, 12, 80.0, 1)):
         assert not lib.atkdsp_pfb_create(*args), args
+    for args in ((0.0, 4096, 80.0, 1), (1e6, 32, 80.0, 1), (1e6, 100, 80.0, 1), (1e6, 4096, 80.0, 0),
+                 (1e6, 1 << 25, 80.0, 1)):
+        assert not lib.atkdsp_osx_create(*args), args
+    # void / query calls ignore a NULL handle like the reference's
+    lib.atkdsp_osx_destroy(None)
+    lib.atkdsp_osx_reset(None)
+    assert lib.atkdsp_osx_channels(None) == 0 and lib.atkdsp_osx_chan_rate(None, 0) == 0.0
+    assert lib.atkdsp_osx_out_max(None, 0, 100) == 0
+    assert lib.atkdsp_osx_add(None, 0.0, 1.0, 1.0) == -1 and lib.atkdsp_osx_remove(None, 0) == -1
 
 
 def test_no_cpu_fallback_without_a_gpu():
@@ -85,3 +97,5 @@ def test_no_cpu_fallback_without_a_gpu():
         ak.Pfb(2.4e6, 64, 2, 12)
     with pytest.raises(ak.AtkDspError):
         ak.unpack(b"\x00\x01\x02\x03", "ci16")
+    with pytest.raises(ak.AtkDspError):
+        ak.Osx(2.4e6, 4096)
