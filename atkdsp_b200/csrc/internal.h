@@ -196,6 +196,10 @@ typedef struct {
                                    * M <= ATKB_OSX_SMALL_M, then nmid with
                                    * M <= 4096, then those with M > 4096       */
     const atkb_osx_chan *h_chans; /* the same table in host memory (launcher)   */
+    const int *packs;             /* device, npacks + 1: the small channels in
+                                   * packs [packs[p], packs[p+1]) of equal M, one
+                                   * warp each                                 */
+    int npacks;
     double fs;
     long long hop_base;           /* blocks of this call before this run          */
     int par;                      /* which half of the channels' staging          */
@@ -203,8 +207,11 @@ typedef struct {
     void *X;                      /* device cf32 [nel][m][nfft]: nfft > fused max */
     void *T, *Y;                  /* device double2 scratch, same shape           */
 } atkb_osx_run;
-/* channels of at most this many bins run one warp each */
+/* channels of at most this many bins run one warp each; those with
+ * OSX_G * M <= ATKB_OSX_PACK_LANES share a warp with others of their M */
 #define ATKB_OSX_SMALL_M 64
+#define ATKB_OSX_PACK_LANES 32
+#define ATKB_OSX_G 4                  /* blocks per CTA of the fused kernel */
 /* dynamic shared memory of the fused kernel for one nfft */
 size_t atkb_osx_group_smem(int nfft);
 

@@ -26,11 +26,15 @@
 
 #define OSX_NT 512
 #define OSX_WARPS (OSX_NT / 32)
-#define OSX_G 4                              /* blocks per CTA */
+#define OSX_G ATKB_OSX_G                     /* blocks per CTA */
 #define OSX_WREG 256                         /* double2 per warp's region */
 #define OSX_WORK (OSX_WARPS * OSX_WREG)      /* 4096 double2: the work area */
 static_assert(OSX_G * ATKB_OSX_SMALL_M <= OSX_WREG, "a small channel's blocks fit its warp's region");
+static_assert(ATKB_OSX_PACK_LANES <= OSX_WREG && OSX_G == ATKB_OSX_G, "a pack's blocks fit its warp's region");
 static_assert(OSX_WORK >= ATKB_OSX_FUSED_MAX, "the work area holds one fused transform");
+#ifndef OSX_FOLD_UNROLL
+#define OSX_FOLD_UNROLL 8                    /* fold iterations in flight per lane */
+#endif
 #define OSX_PI2 6.283185307179586476925286766559
 
 namespace {
@@ -136,20 +140,65 @@ __device__ void fft_b(double2 *sm, int logn, int nb, const double2 *__restrict__
     }
 }
 
-/* bin k of a channel's decimating fold of one spectrum row (float, j
- * ascending, the reference's rounded expression, src/channelizer.c:707-716) */
-__device__ __forceinline__ double2 fold_bin(const float2 *X, const float2 *__restrict__ H, int k, int M, int decim,
-                                            int shift, int mask) {
-    float ar = 0.0f, ai = 0.0f;
-    int bin = k;
-#pragma unroll 4
-    for (int j = 0; j < decim; ++j, bin += M) {
-        const float2 xv = X[(bin + shift) & mask];
-        const float2 hv = __ldg(H + bin);
+/* bin k of a channel's decimating fold of one spectrum (float, j ascending,
+ * the reference's rounded expression, src/channelizer.c:707-716). The bins
+ * k + j*M + shift run up to nfft and then wrap once: two runs, each a
+ * fixed stride (M is a template parameter, so the unrolled loads carry it
+ * as an immediate offset). SM: the spectrum is the fused kernel's shared
+ * one, bin b of this block at shared address xs + b * 8 * OSX_G; else
+ * global, bin b at X[b]. */
+/* one run of the fold: n terms from bin address xa / x and filter h, stride
+ * M bins (M = 1 << LOGM, or the runtime m when LOGM < 0) */
+template <int LOGM, bool SM>
+__device__ __forceinline__ void fold_run(float &ar, float &ai, unsigned xa, const float2 *x, const float2 *h, int n,
+                                         int m) {
+    constexpr int kUnroll = OSX_FOLD_UNROLL;
+    constexpr int XB = SM ? 8 * OSX_G : 8;      /* bytes per bin */
+    const int M = LOGM >= 0 ? (1 << (LOGM < 0 ? 0 : LOGM)) : m;
+#pragma unroll kUnroll
+    for (int j = 0; j < n; ++j) {
+        float2 xv;
+        if (SM) asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(xv.x), "=f"(xv.y) : "r"(xa + j * M * XB));
+        else xv = __ldg(x + j * M);
+        const float2 hv = __ldg(h + j * M);
         ar = __fadd_rn(ar, __fsub_rn(__fmul_rn(xv.x, hv.x), __fmul_rn(xv.y, hv.y)));
         ai = __fadd_rn(ai, __fadd_rn(__fmul_rn(xv.x, hv.y), __fmul_rn(xv.y, hv.x)));
     }
+}
+
+/* bin k of a channel's decimating fold of one spectrum (float, j ascending,
+ * the reference's rounded expression, src/channelizer.c:707-716). The bins
+ * k + j*M + shift run up to nfft and then wrap once: two runs of a fixed
+ * stride (M a template parameter for M <= 4096, so the unrolled loads carry
+ * it in their immediate offsets). SM: the spectrum is the fused kernel's
+ * shared one, bin b of this block at shared address xs + b * 8 * OSX_G;
+ * else global, bin b at X[b]. */
+template <int LOGM, bool SM>
+__device__ __forceinline__ double2 fold_bin(const float2 *X, unsigned xs, const float2 *__restrict__ H, int k,
+                                            int m, int decim, int shift, int nfft) {
+    constexpr int XB = SM ? 8 * OSX_G : 8;
+    const int M = LOGM >= 0 ? (1 << (LOGM < 0 ? 0 : LOGM)) : m;
+    float ar = 0.0f, ai = 0.0f;
+    int start = k + shift;
+    if (start >= nfft) start -= nfft;
+    const int jw = min(decim, (nfft - start + M - 1) / M);        /* start + j*M < nfft */
+    fold_run<LOGM, SM>(ar, ai, xs + start * XB, X + start, H + k, jw, m);
+    const int s2 = start + jw * M - nfft;
+    fold_run<LOGM, SM>(ar, ai, xs + s2 * XB, X + s2, H + k + jw * M, decim - jw, m);
     return make_double2((double)ar, (double)ai);
+}
+
+template <bool SM>
+__device__ __forceinline__ double2 fold_any(int logm, const float2 *X, unsigned xs, const float2 *H, int k, int decim,
+                                            int shift, int nfft) {
+    switch (logm) {
+#define OSX_FOLD_CASE(L) case L: return fold_bin<L, SM>(X, xs, H, k, 1 << L, decim, shift, nfft);
+        OSX_FOLD_CASE(1) OSX_FOLD_CASE(2) OSX_FOLD_CASE(3) OSX_FOLD_CASE(4) OSX_FOLD_CASE(5)
+        OSX_FOLD_CASE(6) OSX_FOLD_CASE(7) OSX_FOLD_CASE(8) OSX_FOLD_CASE(9) OSX_FOLD_CASE(10)
+        OSX_FOLD_CASE(11) OSX_FOLD_CASE(12)
+#undef OSX_FOLD_CASE
+    default: return fold_bin<-1, SM>(X, xs, H, k, 1 << logm, decim, shift, nfft);   /* M > 4096 */
+    }
 }
 
 /* output k of block bi from the channel's unscaled inverse y (the float
@@ -179,46 +228,65 @@ __device__ __forceinline__ float2 *osx_dst(const atkb_osx_chan &C, const atkb_os
     return (float2 *)C.stage + R.par * C.par_stride + e * C.stage_stride + C.lead;
 }
 
-/* One channel over nb consecutive blocks (spectrum rows X + g*xs, blocks
- * i0 + g) by NTH threads in `buf` (nb*M <= 8*NTH double2): folds, batched
- * inverse, rolled outputs. Ends with a barrier of the NTH threads. */
-template <int NTH>
-__device__ void osx_channel(const float2 *X, int xs, int nb, const atkb_osx_chan &C, double2 *buf,
-                            const atkb_osx_run &R, int e, int i0, int tid) {
-    const float2 *H = (const float2 *)C.H;
-    const int logm = C.logm, M = C.M, mask = R.nfft - 1;
-    for (int it = tid; it < (nb << logm); it += NTH)
-        buf[it] = fold_bin(X + (it >> logm) * xs, H, it & (M - 1), M, C.decim, C.shift, mask);
+/* S channels of equal M (table entries c0 .. c0+S-1) over nb consecutive
+ * blocks (block i0 + g's spectrum bin b at X[b*XCOL + g*xrow]) by NTH
+ * threads in `buf` (S*nb*M <= 8*NTH double2): folds, one batched inverse,
+ * rolled outputs. Items run block-fastest within a channel, so the lanes
+ * of a warp share each filter value and, with interleaved spectra (xrow 1),
+ * read neighbouring words. Ends with a barrier of the NTH threads. */
+template <int NTH, int XCOL>
+__device__ void osx_channel(const float2 *X, int xrow, int nb, int c0, int S, double2 *buf, const atkb_osx_run &R,
+                            int e, int i0, int tid) {
+    const int logm = R.chans[c0].logm;
+    const int per = nb << logm;                /* items per channel */
+    for (int it = tid; it < S * per; it += NTH) {
+        const int sub = it / per, r = it - sub * per;
+        const int g = r % nb, k = r / nb;
+        const atkb_osx_chan &C = R.chans[c0 + sub];
+        buf[((sub * nb + g) << logm) + k] =
+            XCOL == OSX_G
+                ? fold_any<true>(logm, nullptr, (unsigned)__cvta_generic_to_shared(X) + g * 8, (const float2 *)C.H, k,
+                                 C.decim, C.shift, R.nfft)
+                : fold_any<false>(logm, X + g * xrow, 0u, (const float2 *)C.H, k, C.decim, C.shift, R.nfft);
+    }
     osx_sync<NTH>();
-    fft_b<NTH>(buf, logm, nb, (const double2 *)R.tw, R.lognfft, true, tid);
-    float2 *dst = osx_dst(C, R, e);
+    fft_b<NTH>(buf, logm, S * nb, (const double2 *)R.tw, R.lognfft, true, tid);
     const int lv = logm - 1;                   /* nvalid = M / 2 */
-    for (int it = tid; it < (nb << lv); it += NTH) {
-        const int g = it >> lv, k = it & ((1 << lv) - 1);
+    const int pero = nb << lv;
+    for (int it = tid; it < S * pero; it += NTH) {
+        const int sub = it / pero, r = it - sub * pero;
+        const int g = r >> lv, k = r & ((1 << lv) - 1);
         const int i = i0 + g;
-        dst[(long long)i * C.nvalid + k] =
-            roll_out(buf[(g << logm) + C.ovd + k], C, R.blk0 + i, k, R.hop, R.ov, R.nfft, R.fs);
+        const atkb_osx_chan C = R.chans[c0 + sub];
+        osx_dst(C, R, e)[(long long)i * C.nvalid + k] =
+            roll_out(buf[((sub * nb + g) << logm) + C.ovd + k], C, R.blk0 + i, k, R.hop, R.ov, R.nfft, R.fs);
     }
     osx_sync<NTH>();
 }
 
-/* the channels of nb blocks whose float spectra are rows X + g*xs: the
- * small ones (M * OSX_G <= OSX_WREG) one warp each in its own region of
- * `work`, then the others by the whole CTA in batches of blocks */
-__device__ void osx_channels(const float2 *X, int xs, int nb, double2 *work, const atkb_osx_run &R, int e,
-                             int i0) {
+/* the channels of nb blocks (spectra as for osx_channel): the packs of
+ * small ones (equal M, at most 32 lanes of items together; the host puts
+ * the costliest first) one warp each in its own region of `work`, taken
+ * from a shared counter; then the others by the whole CTA in batches of
+ * blocks */
+template <int XCOL>
+__device__ void osx_channels(const float2 *X, int xrow, int nb, double2 *work, const atkb_osx_run &R, int e,
+                             int i0, int *next) {
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
-    for (int c = w; c < R.nsmall; c += OSX_WARPS) {
-        const atkb_osx_chan C = R.chans[c];
-        osx_channel<32>(X, xs, nb, C, work + w * OSX_WREG, R, e, i0, lane);
+    for (;;) {
+        int p = 0;
+        if (lane == 0) p = atomicAdd(next, 1);
+        p = __shfl_sync(0xffffffffu, p, 0);
+        if (p >= R.npacks) break;
+        const int c0 = R.packs[p], c1 = R.packs[p + 1];
+        osx_channel<32, XCOL>(X, xrow, nb, c0, c1 - c0, work + w * OSX_WREG, R, e, i0, lane);
     }
     __syncthreads();
     for (int c = R.nsmall; c < R.nsmall + R.nmid; ++c) {
-        const atkb_osx_chan C = R.chans[c];
-        const int per = ATKB_OSX_FUSED_MAX >> C.logm;     /* blocks per batch */
+        const int per = ATKB_OSX_FUSED_MAX >> R.chans[c].logm;     /* blocks per batch */
         for (int g0 = 0; g0 < nb; g0 += per) {
             const int cnt = min(per, nb - g0);
-            osx_channel<OSX_NT>(X + g0 * xs, xs, cnt, C, work, R, e, i0 + g0, tid);
+            osx_channel<OSX_NT, XCOL>(X + g0 * xrow, xrow, cnt, c, 1, work, R, e, i0 + g0, tid);
         }
     }
 }
@@ -235,13 +303,15 @@ __device__ __forceinline__ const float2 *osx_in(const atkb_osx_run &R, int e) {
 
 /* nfft <= ATKB_OSX_FUSED_MAX: grid (ceil(m / OSX_G), nel). Shared memory:
  * the work area (OSX_WORK double2: each forward transform, then the
- * channels' folds and inverses) and OSX_G float spectrum rows of nfft + 1
- * (the pad staggers the rows across banks). */
+ * channels' folds and inverses) and the OSX_G blocks' float spectra,
+ * interleaved: bin b of block g at X[b * OSX_G + g]. */
 __global__ void __launch_bounds__(OSX_NT, 1) osx_group_kernel(const atkb_osx_run R, int m) {
     extern __shared__ double2 smem[];
+    __shared__ int s_next;
     double2 *work = smem;
-    const int nfft = R.nfft, xs = nfft + 1;
+    const int nfft = R.nfft;
     float2 *X = (float2 *)(smem + OSX_WORK);
+    if (threadIdx.x == 0) s_next = 0;
     const int i0 = blockIdx.x * OSX_G, e = blockIdx.y, nb = min(OSX_G, m - i0);
     const float2 *in = osx_in(R, e);
     const double2 *tw = (const double2 *)R.tw;
@@ -254,18 +324,21 @@ __global__ void __launch_bounds__(OSX_NT, 1) osx_group_kernel(const atkb_osx_run
         __syncthreads();
         fft_b<OSX_NT>(work, R.lognfft, 1, tw, R.lognfft, false, threadIdx.x);
         for (int p = threadIdx.x; p < nfft; p += OSX_NT)
-            X[g * xs + p] = make_float2(__double2float_rn(work[p].x), __double2float_rn(work[p].y));
+            X[p * OSX_G + g] = make_float2(__double2float_rn(work[p].x), __double2float_rn(work[p].y));
         __syncthreads();
     }
-    osx_channels(X, xs, nb, work, R, e, i0);
+    osx_channels<OSX_G>(X, 1, nb, work, R, e, i0, &s_next);
 }
 
 /* nfft > ATKB_OSX_FUSED_MAX: the channels read the spectra from HBM */
 __global__ void __launch_bounds__(OSX_NT, 1) osx_group_chan_kernel(const atkb_osx_run R, int m) {
     extern __shared__ double2 smem[];
+    __shared__ int s_next;
     const int i0 = blockIdx.x * OSX_G, e = blockIdx.y, nb = min(OSX_G, m - i0);
     const float2 *X = (const float2 *)R.X + ((long long)e * m + i0) * R.nfft;
-    osx_channels(X, R.nfft, nb, smem, R, e, i0);
+    if (threadIdx.x == 0) s_next = 0;
+    __syncthreads();
+    osx_channels<1>(X, R.nfft, nb, smem, R, e, i0, &s_next);
 }
 
 /* Transforms longer than 4096 points: n = n1 * n2 in the four-step form,
@@ -328,8 +401,8 @@ __global__ void osx_fold_big(const atkb_osx_run R, int c, double2 *__restrict__ 
     const int k = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y, e = blockIdx.z;
     if (k >= C.M) return;
     const long long item = (long long)e * m + i;
-    Y[(item << C.logm) + k] = fold_bin((const float2 *)R.X + item * R.nfft, (const float2 *)C.H, k, C.M,
-                                       C.decim, C.shift, R.nfft - 1);
+    Y[(item << C.logm) + k] = fold_any<false>(C.logm, (const float2 *)R.X + item * R.nfft, 0u, (const float2 *)C.H,
+                                              k, C.decim, C.shift, R.nfft);
 }
 
 /* ... and its rolled outputs from the inverse in Y, grid (ceil(nvalid / 256), m, nel) */
@@ -394,7 +467,7 @@ int set_smem(const void *fn, int bytes) {
 }  // namespace
 
 extern "C" size_t atkb_osx_group_smem(int nfft) {
-    return (size_t)OSX_WORK * 16 + (size_t)OSX_G * (nfft + 1) * 8;
+    return (size_t)OSX_WORK * 16 + (size_t)OSX_G * nfft * 8;
 }
 
 extern "C" int atkb_osx_launch(const atkb_osx_run *run, int m, int nel, void *stream) {

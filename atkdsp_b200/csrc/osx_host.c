@@ -26,6 +26,7 @@
  */
 #define _POSIX_C_SOURCE 200809L
 #include <math.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -78,6 +79,7 @@ struct atkdsp_osx {
     void *d_tbl, *h_tbl;          /* atkb_osx_chan[cap_slots] | ins[max_nel]     */
     size_t tbl_bytes;
     int nsmall, nmid, nbig;       /* the current call's table: channels by class */
+    int npacks;                   /* ... and the small ones' packs               */
     int par;                      /* which half of the channels' staging is current */
     osx_chan *ch;
     size_t *wpos;                 /* cap_slots: a call's samples per slot so far */
@@ -197,16 +199,20 @@ static int ilog2(size_t v) {
 }
 
 /* the per-call table: channel entries for `slots`, then max_nel input
- * pointers, then per entry max_nel output pointers (device-pointer calls) */
+ * pointers, then per entry max_nel output pointers (device-pointer calls),
+ * then slots + 1 pack boundaries */
 static size_t tbl_ins_off(const atkdsp_osx *x) { return atkb_align16((size_t)x->tbl_slots * sizeof(atkb_osx_chan)); }
 static size_t tbl_outs_off(const atkdsp_osx *x) { return tbl_ins_off(x) + (size_t)x->max_nel * sizeof(void *); }
+static size_t tbl_packs_off(const atkdsp_osx *x) {
+    return tbl_outs_off(x) + (size_t)x->tbl_slots * x->max_nel * sizeof(void *);
+}
 
 static int osx_table_reserve(atkdsp_osx *x, int slots) {
     if (slots <= x->tbl_slots && x->d_tbl) return ATKB_OK;
     int want = x->tbl_slots ? x->tbl_slots : 8;
     while (want < slots) want *= 2;
     const size_t bytes = atkb_align16((size_t)want * sizeof(atkb_osx_chan)) +
-                         (size_t)x->max_nel * sizeof(void *) * (1 + (size_t)want);
+                         (size_t)x->max_nel * sizeof(void *) * (1 + (size_t)want) + (size_t)(want + 1) * sizeof(int);
     void *d = NULL, *h = NULL;
     int rc = atkb_malloc(&d, bytes);
     if (rc == ATKB_OK) rc = atkb_host_alloc(&h, bytes);
@@ -510,6 +516,7 @@ static int osx_chunk(atkdsp_osx *x, const osx_io *io, size_t off, size_t sub, si
     R.fs = x->fs; R.hop_base = (long long)hop_base; R.par = x->par;
     R.nfft = (int)x->nfft; R.lognfft = x->lognfft; R.hop = (int)x->hop; R.ov = (int)x->ov;
     R.nchans = x->nsmall + x->nmid + x->nbig; R.nsmall = x->nsmall; R.nmid = x->nmid;
+    R.packs = (const int *)((char *)x->d_tbl + tbl_packs_off(x)); R.npacks = x->npacks;
     R.X = x->d_X; R.T = x->d_T; R.Y = x->d_Y;
     if (R.nchans > 0) rc = atkb_osx_launch(&R, (int)h, (int)nel, x->stream);   /* no channel: nothing to compute */
     if (rc != ATKB_OK) return rc;
@@ -569,6 +576,14 @@ static int osx_chunk(atkdsp_osx *x, const osx_io *io, size_t off, size_t sub, si
     return ATKB_OK;
 }
 
+/* the order of the small channels: costliest first (a fold of decim terms
+ * per lane, ceil(4M / 32) rounds of lanes), equal M together */
+static int small_before(const atkb_osx_chan *a, const atkb_osx_chan *b) {
+    const long ca = (long)a->decim * (long)((ATKB_OSX_G * a->M + 31) / 32);
+    const long cb = (long)b->decim * (long)((ATKB_OSX_G * b->M + 31) / 32);
+    return ca > cb || (ca == cb && a->M < b->M);
+}
+
 static ptrdiff_t osx_process(atkdsp_osx *x, const osx_io *io0, size_t n, size_t *out_counts, size_t cap_each) {
     osx_io io = *io0;
     const unsigned nel = io.nel;
@@ -616,6 +631,7 @@ static ptrdiff_t osx_process(atkdsp_osx *x, const osx_io *io0, size_t n, size_t 
     int j = 0, cls;
     x->nsmall = x->nmid = x->nbig = 0;
     for (cls = 0; cls < 3; ++cls) {
+        const int first = j;
         for (ci = 0; ci < ns; ++ci) {
             osx_chan *c = &x->ch[ci];
             if (!c->active) continue;
@@ -624,7 +640,6 @@ static ptrdiff_t osx_process(atkdsp_osx *x, const osx_io *io0, size_t n, size_t 
             atkb_osx_chan t;
             memset(&t, 0, sizeof t);
             t.H = c->d_H;
-            t.dsts = (io.dev_out && !c->rs) ? d_outs + (size_t)j * x->max_nel : NULL;
             t.stage = c->d_v;
             t.stage_stride = (long long)c->vstride;
             t.par_stride = (long long)x->max_nel * (long long)c->vstride;
@@ -632,18 +647,46 @@ static ptrdiff_t osx_process(atkdsp_osx *x, const osx_io *io0, size_t n, size_t 
             t.delta = c->delta;
             t.M = (int)c->M; t.logm = ilog2(c->M); t.ovd = (int)c->ovd; t.nvalid = (int)c->nvalid;
             t.decim = (int)c->decim; t.shift = (int)c->shift;
-            c->tix = j;
-            if (io.dev_out)
-                for (e = 0; e < nel; ++e) pout[(size_t)j * x->max_nel + e] = io.outs[(size_t)e * ns + ci];
-            tc[j++] = t;
+            t.dsts = (void *const *)(intptr_t)ci;       /* the slot, until the order is final */
+            /* small channels, one warp each, costliest first: a fold of decim
+             * terms per lane, ceil(4M / 32) rounds of lanes */
+            int at = j;
+            if (cls == 0) {
+                while (at > first && small_before(&t, &tc[at - 1])) {
+                    tc[at] = tc[at - 1];
+                    --at;
+                }
+            }
+            tc[at] = t;
+            ++j;
             x->nsmall += kind == 0;
             x->nmid += kind == 1;
             x->nbig += kind == 2;
         }
     }
+    /* packs: runs of small channels of one M, as many as fill the lanes */
+    int *pk = (int *)((char *)x->h_tbl + tbl_packs_off(x));
+    int np = 0, t0 = 0;
+    while (t0 < x->nsmall) {
+        const int lim = tc[t0].M * ATKB_OSX_G >= ATKB_OSX_PACK_LANES ? 1 : ATKB_OSX_PACK_LANES / (tc[t0].M * ATKB_OSX_G);
+        int t1 = t0 + 1;
+        while (t1 < x->nsmall && t1 - t0 < lim && tc[t1].M == tc[t0].M) ++t1;
+        pk[np++] = t0;
+        t0 = t1;
+    }
+    pk[np] = x->nsmall;
+    x->npacks = np;
+    for (int t = 0; t < j; ++t) {                         /* slots -> table entries */
+        osx_chan *c = &x->ch[(intptr_t)tc[t].dsts];
+        c->tix = t;
+        tc[t].dsts = (io.dev_out && !c->rs) ? d_outs + (size_t)t * x->max_nel : NULL;
+        if (io.dev_out)
+            for (e = 0; e < nel; ++e)
+                pout[(size_t)t * x->max_nel + e] = io.outs[(size_t)e * ns + (int)(c - x->ch)];
+    }
     for (e = 0; e < nel; ++e)
         pin[e] = io.dev_in ? (void *)io.ins[e] : (void *)((atkdsp_cf32 *)x->d_in + (size_t)e * x->chunk_in);
-    rc = atkb_h2d(x->d_tbl, x->h_tbl, io.dev_out ? x->tbl_bytes : tbl_outs_off(x), x->stream);
+    rc = atkb_h2d(x->d_tbl, x->h_tbl, x->tbl_bytes, x->stream);
     if (rc != ATKB_OK) return atkb_map_rc(rc);
     size_t *wp = x->wpos;        /* NULL only while no slot exists (ns == 0) */
     for (ci = 0; ci < ns; ++ci) wp[ci] = 0;

@@ -154,3 +154,19 @@ def ci16_block(n: int, seed: int, block: int) -> np.ndarray:
     x = tones_noise(n, 2, 15.0, rng, noise_power=2.0 * 600.0 ** 2, t0=block * n)
     iq = np.stack([np.rint(x.real), np.rint(x.imag)], axis=1)
     return np.clip(iq, -32768, 32767).astype("<i2")
+
+
+# ---- the overlap-save extractor ---------------------------------------------
+EXTRACTOR_FS = 61.44e6
+EXTRACTOR_NFFT = 4096
+
+
+def extractor_channels(nch: int = 64, fs: float = EXTRACTOR_FS, seed: int = 9) -> list:
+    """A many-channel extractor plan: nch channels at seeded offsets across
+    +-0.45 fs, bandwidths cycling 12.5 / 25 / 50 / 200 kHz; odd channels land
+    at 1.25 x bw (their decimated rate: no resampling), even ones at 1.0 x bw
+    (through the arbitrary resampler). Returns (offset_hz, bw_hz, out_rate)."""
+    rng = np.random.default_rng(seed)
+    bws = (12.5e3, 25e3, 50e3, 200e3)
+    return [(float(rng.uniform(-0.45, 0.45) * fs), bws[i % 4], bws[i % 4] * (1.25 if i % 2 else 1.0))
+            for i in range(nch)]

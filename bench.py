@@ -508,32 +508,21 @@ def _c3_arm(torch, device, steps):
             "unit": "MSamples/s (aggregate over elements)", "path": "process_n (device) + one-pass W1/W2"}
 
 
-OSX_FS = 61.44e6
-OSX_NFFT = 4096
 OSX_N = 1 << 24
-
-
-def osx_channels(nch: int = 64, seed: int = 9):
-    """The extractor workload's channel plan: nch channels at seeded offsets
-    across +-0.45 fs, bandwidths cycling 12.5 / 25 / 50 / 200 kHz, half landed
-    at 1.25 x bw (their decimated rate: no resampling), half at 1.0 x bw
-    (resampled)."""
-    rng = np.random.default_rng(seed)
-    bws = (12.5e3, 25e3, 50e3, 200e3)
-    return [(float(rng.uniform(-0.45, 0.45) * OSX_FS), bws[i % 4], bws[i % 4] * (1.25 if i % 2 else 1.0))
-            for i in range(nch)]
 
 
 def _osx_arm(torch, device, steps, cpu: bool):
     """The overlap-save extractor: one 61.44 MS/s cf32 stream (noise + tones),
-    nfft 4096, 64 channels (osx_channels). value: atkdsp_gpu_osx_process_n on
+    nfft 4096, 64 channels (workloads.extractor_channels). value: atkdsp_gpu_osx_process_n on
     2^24 samples resident in HBM per step (CUDA events on the handle's stream,
     every kernel of the call inside); e2e: atkdsp_osx_process with host
     buffers; cpu: the reference library on 2^20 samples of the same stream."""
     import ctypes as C
     import atkdsp_b200 as ak
+    from atkdsp_b200 import workloads as W
+    OSX_FS, OSX_NFFT = W.EXTRACTOR_FS, W.EXTRACTOR_NFFT
     lib = ak.load()
-    chans = osx_channels()
+    chans = W.extractor_channels()
     g = torch.Generator(device=device)
     g.manual_seed(9)
     x = torch.randn(OSX_N, dtype=torch.complex64, device=device, generator=g) * 0.5
