@@ -122,11 +122,9 @@ ATKDSP_API void        atkdsp_pfb_channel_power(const atkdsp_cf32 *out, unsigned
  * One forward FFT of nfft points per block of hop = nfft/2 new samples; each
  * channel folds it to M = nfft/decim bins, inverts them (the integer
  * decimation), rolls to absolute time and is landed on its out_rate by the
- * arbitrary resampler. Limits of this build: nfft <= 2^24 (create returns
- * NULL beyond), and for nfft > 4096 a channel's M must be <= 4096
- * (atkdsp_osx_add returns ATKDSP_E_ARG beyond). Capacity and missing output
- * buffers are checked before any state changes (the reference finds them
- * part-way through a call). */
+ * arbitrary resampler. nfft <= 2^24 in this build (create returns NULL
+ * beyond). Capacity and missing output buffers are checked before any state
+ * changes (the reference finds them part-way through a call). */
 typedef struct atkdsp_osx atkdsp_osx;
 ATKDSP_API atkdsp_osx *atkdsp_osx_create(double fs, size_t nfft, double atten_db,
                                          unsigned max_nel);                               /* :3257 */
