@@ -170,3 +170,15 @@ def extractor_channels(nch: int = 64, fs: float = EXTRACTOR_FS, seed: int = 9) -
     bws = (12.5e3, 25e3, 50e3, 200e3)
     return [(float(rng.uniform(-0.45, 0.45) * fs), bws[i % 4], bws[i % 4] * (1.25 if i % 2 else 1.0))
             for i in range(nch)]
+
+
+# ---- Undertow's per-scale filterbank bank -----------------------------------
+def scale_bank(nscales: int = 6, nchan0: int = 8, taps: int = 12) -> list:
+    """The dyadic bank Undertow runs on every input chunk (reference
+    src/undertow.c:87-95, :112-143): scale s has nchan0 << s channels, 2x
+    oversampled, taps per branch as configured (12 by default), 80 dB.
+    Returns (nchan, oversample, taps) per scale."""
+    return [(nchan0 << s, 2, taps) for s in range(nscales)]
+
+
+SCALE_BANK_BLOCK = 65536      # Undertow's max_block: samples per chunk (src/undertow.c:95)

@@ -25,7 +25,8 @@ Arms printed in ONE JSON line (rank 0):
   configs     the other configurations, each with its own rate: single
               stream (C ABI, uneven blocks), the unpack front end, the
               coherent array, the overlap-save extractor (64 channels from
-              one 61.44 MS/s stream), the serving loop
+              one 61.44 MS/s stream), Undertow's six-scale filterbank bank
+              (one launch per chunk), the serving loop
 
 --impl reference runs only the reference's CPU channelizer (all host threads)
 on the same workload and prints its line.
@@ -600,6 +601,70 @@ def _osx_arm(torch, device, steps, cpu: bool):
     return res
 
 
+def _bank_arm(torch, device, steps, cpu: bool):
+    """Undertow's per-scale bank (workloads.scale_bank: 8 .. 256 channels, 2x,
+    12 taps) on one stream of 65536-sample chunks: every chunk goes through
+    all six scales. value: one batch launch per chunk (CUDA graph replay),
+    64 chunks per step; plain: one device call per scale per chunk; cpu: the
+    reference library's six atkdsp_pfb_process calls per chunk (all host
+    threads, the survey's own loop)."""
+    import atkdsp_b200 as ak
+    from atkdsp_b200 import gpu
+    from atkdsp_b200 import workloads as W
+    from atkdsp_b200.gpu import Batch
+    bank = W.scale_bank(6)
+    blk, nchunk = W.SCALE_BANK_BLOCK, 64
+    g = torch.Generator(device=device)
+    g.manual_seed(11)
+    x = torch.randn(blk * nchunk, dtype=torch.complex64, device=device, generator=g)
+    chunks = [x[i * blk:(i + 1) * blk] for i in range(nchunk)]
+    hs = [ak.Pfb(FS, M, os_, K) for M, os_, K in bank]
+    batch = Batch(hs)
+    outs = [torch.empty(M * (blk // (M // 2) + 2), dtype=torch.complex64, device=device) for M, _, _ in bank]
+    st = torch.cuda.ExternalStream(batch.stream_ptr, device=device)
+
+    def step_batched():
+        for c in chunks:
+            batch.process([c] * len(bank), outs)
+
+    ps = [ak.Pfb(FS, M, os_, K) for M, os_, K in bank]
+
+    def step_plain():
+        for c in chunks:
+            for p, o in zip(ps, outs):
+                gpu.process_n(p, [c], 1, out=o, stream=st)
+
+    res = {"workload": "scale_bank_6_scales_8-256ch_os2_k12_chunks_65536", "unit": "MSamples/s",
+           "path": "atkdsp_gpu_batch_process: one launch per chunk over all six scales"}
+    for name, fn in (("value", step_batched), ("plain", step_plain)):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(max(steps, 1)):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        res[name] = round(blk * nchunk * max(steps, 1) / (e0.elapsed_time(e1) / 1e3) / 1e6, 2)
+    if cpu:
+        from oracle import oracle as O
+        ref = O.reference()
+        if ref is not None:
+            nth = os.cpu_count() or 1
+            ref.lib.atkdsp_set_threads(nth)
+            rp = [ref.Pfb(FS, M, os_, K) for M, os_, K in bank]
+            xh = x[: blk * 8].cpu().numpy()
+            t0 = time.perf_counter()
+            for i in range(8):
+                for p in rp:
+                    p.process(xh[i * blk:(i + 1) * blk])
+            res["cpu_baseline"] = {"value": round(8 * blk / (time.perf_counter() - t0) / 1e6, 2),
+                                   "unit": "MSamples/s", "cores": nth, "kind": "reference",
+                                   "sample": "8 chunks through the six scales"}
+    return res
+
+
 def _served_arm(torch, device, duration_s):
     """Serving: 4096 live streams at {2.4, 10, 40} MS/s delivering 1.6 ms ci16
     blocks with Poisson arrivals, nchan {256, 1024}, 16 taps, 2x, churn 20/s,
@@ -711,6 +776,8 @@ def run_ours(args, rep):
                          ("coherent_array", lambda: _c3_arm(torch, device, args.steps)),
                          ("extractor", lambda: _osx_arm(torch, device, args.steps,
                                                         "cpu" in arms and not args.no_cpu)),
+                         ("scale_bank", lambda: _bank_arm(torch, device, args.steps,
+                                                          "cpu" in arms and not args.no_cpu)),
                          ("served", lambda: _served_arm(torch, device, 3.0))):
             if name in arms:
                 try:
@@ -779,7 +846,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--arms", default="batched,plain,e2e,dropin,cpu,single_stream,front_end,coherent_array,"
-                    "extractor,served",
+                    "extractor,scale_bank,served",
                     help="comma list of arms to run (the batched arm always runs)")
     ap.add_argument("--streams", type=int, default=256)
     ap.add_argument("--min-log2", type=float, default=14.0)
