@@ -110,6 +110,24 @@ class CpuLib:
         f("osx_describe").argtypes = [vp, C.c_char_p, sz]
         f("osx_describe").restype = C.c_int
         if self.prefix == "orc_":
+            self.lib.orc_window.argtypes = [C.c_int, sz, _P(C.c_float)]
+            self.lib.orc_window.restype = C.c_int
+            self.lib.orc_spectrum_reduce.argtypes = [sz, _pcf, sz, sz, _P(C.c_float), C.c_int, _P(C.c_float)]
+            self.lib.orc_spectrum_reduce.restype = C.c_longlong
+            self.lib.orc_spectrum_stats.argtypes = [sz, _pcf, sz, sz, _P(C.c_float)] + [_P(C.c_float)] * 4
+            self.lib.orc_spectrum_stats.restype = C.c_longlong
+        else:
+            self.lib.atkdsp_window.argtypes = [C.c_int, sz, _P(C.c_float)]
+            self.lib.atkdsp_window.restype = C.c_int
+            self.lib.atkdsp_fft_create.argtypes = [sz]
+            self.lib.atkdsp_fft_create.restype = vp
+            self.lib.atkdsp_fft_destroy.argtypes = [vp]
+            self.lib.atkdsp_fft_destroy.restype = None
+            self.lib.atkdsp_spectrum_reduce.argtypes = [vp, _pcf, sz, sz, _P(C.c_float), C.c_int, _P(C.c_float)]
+            self.lib.atkdsp_spectrum_reduce.restype = C.c_ssize_t
+            self.lib.atkdsp_spectrum_stats.argtypes = [vp, _pcf, sz, sz, _P(C.c_float)] + [_P(C.c_float)] * 4
+            self.lib.atkdsp_spectrum_stats.restype = C.c_ssize_t
+        if self.prefix == "orc_":
             self.lib.orc_pfb_prototype.argtypes = [u, u, d, _P(C.c_double)]
             self.lib.orc_pfb_prototype.restype = None
         else:
@@ -126,6 +144,43 @@ class CpuLib:
         self.lib.orc_pfb_prototype(int(nchan), int(taps_per_poly), float(atten_db),
                                    h.ctypes.data_as(_P(C.c_double)))
         return h
+
+    # -- the spectrum reduction (python/atkdsp/__init__.py:566-600) -------------
+    def window(self, kind, n):
+        kinds = {"rect": 0, "hann": 1, "hamming": 2, "blackmanharris": 3}
+        out = np.empty(int(n), np.float32)
+        f = self.lib.orc_window if self.prefix == "orc_" else self.lib.atkdsp_window
+        if f(kinds[kind] if isinstance(kind, str) else int(kind), int(n), out.ctypes.data_as(_P(C.c_float))):
+            raise RuntimeError("window")
+        return out
+
+    def _spec(self, name, n, x, hop, win, *rest):
+        x = np.ascontiguousarray(x, np.complex64)
+        wp = None if win is None else np.ascontiguousarray(win, np.float32).ctypes.data_as(_P(C.c_float))
+        if self.prefix == "orc_":
+            return getattr(self.lib, "orc_" + name)(int(n), _cfp(x), x.size, int(hop or n), wp, *rest)
+        h = self.lib.atkdsp_fft_create(int(n))
+        try:
+            return getattr(self.lib, "atkdsp_" + name)(h, _cfp(x), x.size, int(hop or n), wp, *rest)
+        finally:
+            self.lib.atkdsp_fft_destroy(h)
+
+    def spectrum_reduce(self, x, n, hop=None, win=None, detector="max"):
+        det = {"max": 0, "min": 1, "avg": 2}[detector] if isinstance(detector, str) else int(detector)
+        out = np.empty(int(n), np.float32)
+        fr = self._spec("spectrum_reduce", n, x, hop, win, det, out.ctypes.data_as(_P(C.c_float)))
+        if fr < 0:
+            raise RuntimeError(f"spectrum_reduce: {fr}")
+        return out, int(fr)
+
+    def spectrum_stats(self, x, n, hop=None, win=None):
+        outs = {k: np.empty(int(n), np.float32) for k in ("max", "avg", "min", "sk")}
+        fr = self._spec("spectrum_stats", n, x, hop, win,
+                        *[outs[k].ctypes.data_as(_P(C.c_float)) for k in ("max", "avg", "min", "sk")])
+        if fr < 0:
+            raise RuntimeError(f"spectrum_stats: {fr}")
+        outs["frames"] = int(fr)
+        return outs
 
     # -- the overlap-save extractor ----------------------------------------------
     def Osx(self, fs, nfft=4096, atten_db=80.0, max_nel=1):

@@ -75,3 +75,12 @@ def golden_proto():
 @pytest.fixture(scope="session")
 def golden_osx():
     return load_golden("osx.npz")
+
+
+@pytest.fixture(scope="session")
+def golden_spectrum():
+    return load_golden("spectrum.npz")
+
+
+def spectrum_case_names(data: dict) -> list:
+    return sorted({k.split("/")[0] for k in data if k.endswith("/line")})

@@ -22,6 +22,9 @@ Fixture files (tests/golden/*.npz):
                     and hashes of the C restatement's for long prototypes
   osx.npz           overlap-save extractor outputs per channel slot for the
                     cases of tests/osx_cases.py (reference C library)
+  spectrum.npz      spectrum reduction lines (max / min / avg detector) and
+                    per-bin stats (max, avg, min dB, spectral kurtosis) from
+                    the reference C library run with one thread
 """
 
 from __future__ import annotations
@@ -191,6 +194,40 @@ def make_osx(ref):
     return out
 
 
+# (name, n, hop, window kind or None, detector, samples, seed)
+SPECTRUM_CASES = [
+    ("n64_rect_avg", 64, 0, None, "avg", 5000, 61),
+    ("n1024_hann_max_hop512", 1024, 512, "hann", "max", 40000, 62),
+    ("n4096_bh_min_hop1000", 4096, 1000, "blackmanharris", "min", 70000, 63),
+    ("n256_hamming_avg_hop100", 256, 100, "hamming", "avg", 30000, 64),
+    ("n16_rect_max_hop3", 16, 3, None, "max", 100, 65),
+    ("n2048_hann_avg_one_frame", 2048, 2048, "hann", "avg", 3000, 66),
+]
+
+
+def make_spectrum(ref):
+    ref.lib.atkdsp_set_threads(1)      # frames in order: the sums have one rounding sequence
+    out = {}
+    kinds = {"rect": 0, "hann": 1, "hamming": 2, "blackmanharris": 3}
+    for name, n, hop, win, det, N, seed in SPECTRUM_CASES:
+        rng = np.random.default_rng(seed)
+        k = np.arange(N)
+        x = ((rng.standard_normal(N) + 1j * rng.standard_normal(N)) * 0.3
+             + np.exp(2j * np.pi * rng.uniform(-0.5, 0.5) * k)).astype(np.complex64)
+        w = None if win is None else ref.window(win, n)
+        line, frames = ref.spectrum_reduce(x, n, hop, w, det)
+        st = ref.spectrum_stats(x, n, hop, w)
+        out[f"{name}/in"] = x
+        out[f"{name}/params"] = np.array([n, hop, -1 if win is None else kinds[win],
+                                          {"max": 0, "min": 1, "avg": 2}[det], frames], np.int64)
+        out[f"{name}/line"] = line
+        for q in ("max", "avg", "min", "sk"):
+            out[f"{name}/{q}"] = st[q]
+        print(f"{name}: {frames} frames")
+    ref.lib.atkdsp_set_threads(0)
+    return out
+
+
 def main():
     ref = O.reference()
     if ref is None:
@@ -208,6 +245,8 @@ def main():
         np.savez_compressed(HERE / "proto.npz", **make_proto())
     if want("osx"):
         np.savez_compressed(HERE / "osx.npz", **make_osx(ref))
+    if want("spectrum"):
+        np.savez_compressed(HERE / "spectrum.npz", **make_spectrum(ref))
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

@@ -181,3 +181,20 @@ def test_osx_oracle_bookkeeping_matches_reference_semantics():
     with pytest.raises(RuntimeError):
         o.retune(5, 0.0)
     assert "2 channel(s)" in o.describe()
+
+
+# ---- the spectrum reduction (oracle/spectrum_oracle.c) -------------------------
+def test_spectrum_oracle_matches_reference_golden(golden_spectrum):
+    from conftest import spectrum_case_names
+    orc = _orc()
+    kinds = {-1: None, 0: "rect", 1: "hann", 2: "hamming", 3: "blackmanharris"}
+    for name in spectrum_case_names(golden_spectrum):
+        n, hop, kind, det, frames = (int(v) for v in golden_spectrum[f"{name}/params"])
+        x = golden_spectrum[f"{name}/in"]
+        w = None if kinds[kind] is None else orc.window(kinds[kind], n)
+        line, fr = orc.spectrum_reduce(x, n, hop, w, det)
+        assert fr == frames
+        assert np.array_equal(line, golden_spectrum[f"{name}/line"]), name
+        st = orc.spectrum_stats(x, n, hop, w)
+        for q in ("max", "avg", "min", "sk"):
+            assert np.array_equal(st[q], golden_spectrum[f"{name}/{q}"]), (name, q)
