@@ -120,6 +120,10 @@ def _bind(lib) -> None:
         "atkdsp_gpu_osx_process_n": ([vp, P(vp), u, sz, P(vp), P(sz), sz], ssz),
         "atkdsp_gpu_osx_stream": ([vp], vp),
         "atkdsp_gpu_osx_sync": ([vp], C.c_int),
+        "atkdsp_gpu_spectrum_create": ([sz], vp),
+        "atkdsp_gpu_spectrum_destroy": ([vp], None),
+        "atkdsp_gpu_spectrum_reduce": ([vp, vp, sz, sz, vp, C.c_int, vp, vp], ssz),
+        "atkdsp_gpu_spectrum_stats": ([vp, vp, sz, sz, vp, vp, vp, vp, vp, vp], ssz),
         "atkdsp_gpu_tune_set": ([u, u, u, C.c_int], C.c_int),
         "atkdsp_gpu_tune_get": ([u, u, u], C.c_int),
     }

@@ -237,6 +237,18 @@ int  atkb_osx_carry(const void *state, long long state_stride, const void *const
                     long long head, long long from, long long len, void *dst, long long dst_stride,
                     int nel, void *stream);
 
+/* spectrum reduction --------------------------------------------------------
+ * frames f < `frames` of n = 2^logn samples at in + f*hop (device cf32),
+ * windowed by win (device, n floats, or NULL), transformed with the n-point
+ * table tw; nblk CTAs take `per` consecutive frames each into `part`
+ * (nblk lines: float for modes 0/1/2, 4 double planes for mode 3), then the
+ * merged line goes to o0 (modes 0/1/2: max / min / average detector, dB) or
+ * o0..o3 (mode 3: max / avg / min dB and kurtosis; NULL skips one). */
+#define ATKB_SPEC_NMAX 4096
+int  atkb_spec_launch(int mode, const void *in, long long frames, long long hop, int logn, const float *win,
+                      const void *tw, int nblk, int per, void *part, float *o0, float *o1, float *o2,
+                      float *o3, void *stream);
+
 /* unpack ------------------------------------------------------------------- */
 /* device raw -> device cf32 (out may be NULL: mean only), (x - c) * k per component; the means (double,
  * BEFORE subtraction of the offset, i.e. sum(out)/n + off) go to d_mean[0..1]

@@ -15,7 +15,7 @@ import torch
 
 from . import AtkDspError, Pfb, _check, _fmt, bytes_per_sample, load
 
-__all__ = ["process_n", "process_n_raw", "unpack_dc", "unpack", "block_mean", "accumulate",
+__all__ = ["Spectrum", "process_n", "process_n_raw", "unpack_dc", "unpack", "block_mean", "accumulate",
            "cov_accumulate", "channel_power", "Batch", "sync"]
 
 
@@ -209,3 +209,50 @@ class Batch:
                                                      self._outs, self._ms, _stream(stream))
         _check(int(got), "gpu_batch_process_raw")
         return [int(self._ms[i]) for i in range(n)]
+
+
+DET = {"max": 0, "min": 1, "avg": 2}
+
+
+class Spectrum:
+    """atkdsp_gpu_spectrum: the display reduction of the binding's
+    ``Fft.spectrum_reduce`` / ``Fft.spectrum_stats`` (python/atkdsp/__init__.py:
+    566-600) on device tensors, for power-of-two n from 16 to 4096."""
+
+    def __init__(self, n: int):
+        self._lib = load()
+        self.n = int(n)
+        self._p = self._lib.atkdsp_gpu_spectrum_create(self.n)
+        if not self._p:
+            raise AtkDspError(f"gpu_spectrum_create({n}): n must be a power of two in 16..4096")
+
+    def __del__(self):
+        p = getattr(self, "_p", None)
+        if p:
+            self._lib.atkdsp_gpu_spectrum_destroy(p)
+            self._p = None
+
+    def reduce(self, x: torch.Tensor, hop: int | None = None, win: torch.Tensor | None = None,
+               detector="max", out: torch.Tensor | None = None, stream=None):
+        """Every frame of x reduced to one fftshifted dB line: (line, frames)."""
+        if out is None:
+            out = torch.empty(self.n, dtype=torch.float32, device=x.device)
+        det = DET[detector] if isinstance(detector, str) else int(detector)
+        fr = self._lib.atkdsp_gpu_spectrum_reduce(self._p, _ptr(x), x.numel(), int(hop or self.n), _ptr(win),
+                                                  det, _ptr(out), _stream(stream))
+        _check(int(fr), "gpu_spectrum_reduce")
+        return out, int(fr)
+
+    def stats(self, x: torch.Tensor, hop: int | None = None, win: torch.Tensor | None = None,
+              want=("max", "avg", "min", "sk"), stream=None) -> dict:
+        """Per-bin peak / mean / floor (dB) and spectral kurtosis in one pass."""
+        want = set(want)
+        outs = {k: (torch.empty(self.n, dtype=torch.float32, device=x.device) if k in want else None)
+                for k in ("max", "avg", "min", "sk")}
+        fr = self._lib.atkdsp_gpu_spectrum_stats(self._p, _ptr(x), x.numel(), int(hop or self.n), _ptr(win),
+                                                 *[_ptr(outs[k]) for k in ("max", "avg", "min", "sk")],
+                                                 _stream(stream))
+        _check(int(fr), "gpu_spectrum_stats")
+        res = {k: v for k, v in outs.items() if v is not None}
+        res["frames"] = int(fr)
+        return res

@@ -26,7 +26,8 @@ Arms printed in ONE JSON line (rank 0):
               stream (C ABI, uneven blocks), the unpack front end, the
               coherent array, the overlap-save extractor (64 channels from
               one 61.44 MS/s stream), Undertow's six-scale filterbank bank
-              (one launch per chunk), the serving loop
+              (one launch per chunk), the spectrum reduction, the serving
+              loop
 
 --impl reference runs only the reference's CPU channelizer (all host threads)
 on the same workload and prints its line.
@@ -665,6 +666,50 @@ def _bank_arm(torch, device, steps, cpu: bool):
     return res
 
 
+def _spectrum_arm(torch, device, steps, cpu: bool):
+    """The display reduction on the same kind of device block: 2^24 cf32
+    samples, n 4096, hop 2048 (50 % overlap), Hann window; value: the
+    average-detector line (atkdsp_gpu_spectrum_reduce); stats: the four
+    stats lines in one pass; cpu: the reference's atkdsp_spectrum_reduce on
+    2^22 samples with every host thread."""
+    from atkdsp_b200.gpu import Spectrum
+    from oracle import oracle as O
+    n, hop, N = 4096, 2048, 1 << 24
+    g = torch.Generator(device=device)
+    g.manual_seed(13)
+    x = torch.randn(N, dtype=torch.complex64, device=device, generator=g)
+    w = torch.from_numpy(O.oracle().window("hann", n)).to(device)
+    sp = Spectrum(n)
+    res = {"workload": "spectrum_n4096_hop2048_hann_2^24", "unit": "MSamples/s",
+           "path": "atkdsp_gpu_spectrum_reduce (average detector) / atkdsp_gpu_spectrum_stats"}
+    for name, fn in (("value", lambda: sp.reduce(x, hop, w, "avg")), ("stats", lambda: sp.stats(x, hop, w))):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(max(steps, 1)):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        res[name] = round(N * max(steps, 1) / (e0.elapsed_time(e1) / 1e3) / 1e6, 2)
+    res["frames_per_call"] = (N - n) // hop + 1
+    if cpu:
+        ref = O.reference()
+        if ref is not None:
+            nth = os.cpu_count() or 1
+            ref.lib.atkdsp_set_threads(nth)
+            xs = x[: 1 << 22].cpu().numpy()
+            wh = w.cpu().numpy()
+            ref.spectrum_reduce(xs, n, hop, wh, "avg")
+            t0 = time.perf_counter()
+            ref.spectrum_reduce(xs, n, hop, wh, "avg")
+            res["cpu_baseline"] = {"value": round(xs.size / (time.perf_counter() - t0) / 1e6, 2),
+                                   "unit": "MSamples/s", "cores": nth, "kind": "reference",
+                                   "sample": "2^22 samples, same n / hop / window"}
+    return res
+
+
 def _served_arm(torch, device, duration_s):
     """Serving: 4096 live streams at {2.4, 10, 40} MS/s delivering 1.6 ms ci16
     blocks with Poisson arrivals, nchan {256, 1024}, 16 taps, 2x, churn 20/s,
@@ -778,6 +823,8 @@ def run_ours(args, rep):
                                                         "cpu" in arms and not args.no_cpu)),
                          ("scale_bank", lambda: _bank_arm(torch, device, args.steps,
                                                           "cpu" in arms and not args.no_cpu)),
+                         ("spectrum", lambda: _spectrum_arm(torch, device, args.steps,
+                                                            "cpu" in arms and not args.no_cpu)),
                          ("served", lambda: _served_arm(torch, device, 3.0))):
             if name in arms:
                 try:
@@ -846,7 +893,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--arms", default="batched,plain,e2e,dropin,cpu,single_stream,front_end,coherent_array,"
-                    "extractor,scale_bank,served",
+                    "extractor,scale_bank,spectrum,served",
                     help="comma list of arms to run (the batched arm always runs)")
     ap.add_argument("--streams", type=int, default=256)
     ap.add_argument("--min-log2", type=float, default=14.0)

@@ -170,6 +170,29 @@ ATKDSP_API ptrdiff_t   atkdsp_gpu_osx_process_n(atkdsp_osx *x, const atkdsp_cf32
 ATKDSP_API void       *atkdsp_gpu_osx_stream(atkdsp_osx *x);
 ATKDSP_API int         atkdsp_gpu_osx_sync(atkdsp_osx *x);
 
+/* ---- spectrum reduction on device buffers ------------------------------- */
+/* atkdsp_spectrum_reduce / atkdsp_spectrum_stats (reference
+ * include/atkdsp.h:400-433, src/fft.c:176-430) on a device block, for the
+ * power-of-two lengths 16 <= n <= 4096: every frame of n samples at stride
+ * hop (0 or > n means n) of d_in[0, n_samples) windowed by d_window (n device
+ * floats, or NULL for rectangular), transformed, and reduced per bin into
+ * one fftshifted line of n device floats in dB (detector ATKDSP_DET_MAX 0,
+ * MIN 1, AVG 2), or into the four stats lines (peak, mean, floor dB, spectral
+ * kurtosis; any may be NULL, not all). Enqueued on `stream` (NULL: the
+ * legacy default stream); returns the frame count (0 when n_samples < n) or
+ * ATKDSP_E_ARG / ATKDSP_E_FFT. One call at a time per plan: its partial
+ * lines live in the plan. */
+typedef struct atkdsp_gpu_spectrum atkdsp_gpu_spectrum;
+ATKDSP_API atkdsp_gpu_spectrum *atkdsp_gpu_spectrum_create(size_t n);
+ATKDSP_API void        atkdsp_gpu_spectrum_destroy(atkdsp_gpu_spectrum *p);
+ATKDSP_API ptrdiff_t   atkdsp_gpu_spectrum_reduce(atkdsp_gpu_spectrum *p, const atkdsp_cf32 *d_in,
+                                                  size_t n_samples, size_t hop, const float *d_window,
+                                                  int detector, float *d_out_line, void *stream);
+ATKDSP_API ptrdiff_t   atkdsp_gpu_spectrum_stats(atkdsp_gpu_spectrum *p, const atkdsp_cf32 *d_in,
+                                                 size_t n_samples, size_t hop, const float *d_window,
+                                                 float *d_max_db, float *d_avg_db, float *d_min_db,
+                                                 float *d_sk, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
