@@ -156,3 +156,40 @@ def test_w12_many_elements_and_empty_block():
     assert np.array_equal(_bits(R), _bits(R0))
     p0, m0 = ak.pfb_channel_power(empty, nel, M)
     assert not p0.any() and not m0.any()
+
+
+def test_w2_powers_gate_w1_on_the_device():
+    """W3's data flow without a host round trip: a block's W2 channel powers,
+    a per-channel gate made from them on the device (here a level test
+    against the median channel; the reference's CFAR would supply it), and
+    W1 accumulated only where the gate is set: the oracle's gated W1 with the
+    same gate to W1's bar (1e-5 of the largest entry; the device sums in
+    another order), counts exact, ungated channels untouched."""
+    torch = pytest.importorskip("torch")
+    from atkdsp_b200 import gpu
+    from oracle import oracle as O
+    M, nel, n = 192, 4, 192 * 40
+    rng = np.random.default_rng(91)
+    k = np.arange(n)
+    base = np.exp(2j * np.pi * (40 * 2.4e6 / M) / 2.4e6 * k)
+    xs = [(3.0 * base * np.exp(1j * 0.7 * e) + 0.3 * (rng.standard_normal(n) + 1j * rng.standard_normal(n)))
+          .astype(np.complex64) for e in range(nel)]
+    p = ak.Pfb(2.4e6, M, 2, 12, 80.0, nel)
+    y = gpu.process_n(p, [torch.from_numpy(x).cuda() for x in xs], nel)
+    gpu.sync(p)                       # the handle's stream is not the default one
+    pwr, meanp = gpu.channel_power(y, nel, M)
+    gate = (meanp > 4.0 * torch.median(meanp)).to(torch.uint8)
+    assert 0 < int(gate.sum()) < M
+    R = torch.zeros((M, nel, nel), dtype=torch.complex64, device="cuda")
+    cnt = torch.zeros(M, dtype=torch.int32, device="cuda")
+    gpu.cov_accumulate(y, nel, M, gate, R, cnt)
+    torch.cuda.synchronize()
+    yh, gh = y.cpu().numpy(), gate.cpu().numpy()
+    Ro = np.zeros((M, nel, nel), np.complex64)
+    co = np.zeros(M, np.uint32)
+    O.oracle().pfb_cov_accumulate(yh, nel, M, gh, Ro, co)
+    Rd = R.cpu().numpy()
+    assert np.max(np.abs(Rd - Ro)) / np.max(np.abs(Ro)) < 1e-5
+    assert np.all(Rd[gh == 0] == 0)
+    assert np.array_equal(cnt.cpu().numpy().astype(np.uint32), co)
+    assert np.all(co[gh == 0] == 0) and np.all(co[gh == 1] == y.shape[-1])
