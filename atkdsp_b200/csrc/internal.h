@@ -226,11 +226,26 @@ int  atkb_osx_launch(const atkb_osx_run *run, int m, int nel, void *stream);
  * formula) go to outs[e] + out_off (outs: a device array of nel device
  * pointers) or, when outs is NULL, to stage + e*stage_stride + k. The new
  * history, the last Q of hist ++ new, goes to v_next + e*v_stride. pd = P*Q
- * prototype taps then P*Q forward differences. */
-int  atkb_osx_resample(const void *v, void *v_next, long long v_stride, long long nv, int Q, int P,
-                       const float *pd, double base, double step, double inoff, unsigned long long K0,
-                       long long count, void *const *outs, long long out_off, void *stage,
-                       long long stage_stride, int nel, void *stream);
+ * prototype taps then P*Q forward differences. blocks: the launcher's
+ * 128-thread blocks per element (set by atkb_osx_resample_batch). */
+typedef struct {
+    const void *v;
+    void *v_next;
+    long long v_stride, nv;
+    const float *pd;
+    double base, step, inoff;
+    unsigned long long K0;
+    long long count;
+    void *const *outs;
+    long long out_off;
+    void *stage;
+    long long stage_stride;
+    int Q, P, nel, blocks;
+} atkb_osx_rs;
+#define ATKB_OSX_RS_MAX 128
+/* n <= ATKB_OSX_RS_MAX resampler runs in one launch (their descriptors
+ * travel as the kernel's parameters) */
+int  atkb_osx_resample_batch(const atkb_osx_rs *runs, int n, void *stream);
 /* dst[e][0, len) = s[from, from + len) of s = state[e][0, head) ++
  * ins[e][in_off, ...), ins a device array of nel device pointers */
 int  atkb_osx_carry(const void *state, long long state_stride, const void *const *ins, long long in_off,

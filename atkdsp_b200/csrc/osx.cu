@@ -311,23 +311,39 @@ __global__ void osx_roll_big(const atkb_osx_run R, int c, const double2 *__restr
                                                 R.nfft, R.fs);
 }
 
-__global__ void osx_resample_kernel(const float2 *__restrict__ v, float2 *__restrict__ v_next, long long v_stride,
-                                    long long nv, int Q, int P, const float *__restrict__ pp,
-                                    const float *__restrict__ dd, double base, double step, double inoff,
-                                    unsigned long long K0, long long count, void *const *__restrict__ outs,
-                                    long long out_off, float2 *__restrict__ stage, long long stage_stride) {
-    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int e = blockIdx.y;
-    const float2 *x = v + (long long)e * v_stride + Q;       /* x[m], m >= -Q */
-    if (k < Q) v_next[(long long)e * v_stride + k] = x[nv - Q + k];
-    if (k >= count) return;
-    const double local = __dsub_rn(__dadd_rn(base, __dmul_rn((double)(K0 + (unsigned long long)k), step)), inoff);
-    const long long i = (long long)floor(local);
-    const double frac = __dsub_rn(local, (double)i);
+/* every resampler run of a chunk: run r owns blocks [first[r], first[r+1]),
+ * blocks_r per element, one thread per output (and per history sample) */
+struct RsBatch {
+    int n;
+    int first[ATKB_OSX_RS_MAX + 1];
+    atkb_osx_rs r[ATKB_OSX_RS_MAX];
+};
+
+__global__ void __launch_bounds__(128) osx_resample_batch_kernel(const __grid_constant__ RsBatch B) {
+    const int bid = blockIdx.x;
+    int lo = 0, hi = B.n - 1;                       /* the run whose blocks hold bid */
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (B.first[mid] <= bid) lo = mid;
+        else hi = mid - 1;
+    }
+    const atkb_osx_rs &D = B.r[lo];
+    const int local = bid - B.first[lo];
+    const int e = local / D.blocks;
+    const long long k = (long long)(local - e * D.blocks) * blockDim.x + threadIdx.x;
+    const int Q = D.Q, P = D.P;
+    const float2 *x = (const float2 *)D.v + (long long)e * D.v_stride + Q;   /* x[m], m >= -Q */
+    if (k < Q) ((float2 *)D.v_next)[(long long)e * D.v_stride + k] = x[D.nv - Q + k];
+    if (k >= D.count) return;
+    const double local_pos =
+        __dsub_rn(__dadd_rn(D.base, __dmul_rn((double)(D.K0 + (unsigned long long)k), D.step)), D.inoff);
+    const long long i = (long long)floor(local_pos);
+    const double frac = __dsub_rn(local_pos, (double)i);
     const double ph = __dmul_rn(frac, (double)P);
     int b = (int)ph;
     if (b >= P) b = P - 1;
     const float mu = __double2float_rn(__dsub_rn(ph, (double)b));
+    const float *pp = D.pd, *dd = D.pd + (size_t)P * Q;
     float ar = 0.0f, ai = 0.0f;
     for (int q = 0; q < Q; ++q) {
         const long long mm = i - q;
@@ -337,7 +353,7 @@ __global__ void osx_resample_kernel(const float2 *__restrict__ v, float2 *__rest
         ar = __fadd_rn(ar, __fmul_rn(c, xv.x));
         ai = __fadd_rn(ai, __fmul_rn(c, xv.y));
     }
-    float2 *o = outs ? (float2 *)outs[e] + out_off : stage + (long long)e * stage_stride;
+    float2 *o = D.outs ? (float2 *)D.outs[e] + D.out_off : (float2 *)D.stage + (long long)e * D.stage_stride;
     o[k] = make_float2(ar, ai);
 }
 
@@ -406,18 +422,23 @@ extern "C" int atkb_osx_launch(const atkb_osx_run *run, int m, int nel, void *st
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }
 
-extern "C" int atkb_osx_resample(const void *v, void *v_next, long long v_stride, long long nv, int Q, int P,
-                                 const float *pd, double base, double step, double inoff, unsigned long long K0,
-                                 long long count, void *const *outs, long long out_off, void *stage,
-                                 long long stage_stride, int nel, void *stream) {
-    if (nel <= 0) return ATKB_OK;
-    const int nt = 128;
-    const long long work = count > Q ? count : Q;
-    if (work <= 0) return ATKB_OK;
-    const long long blocks = (work + nt - 1) / nt;
-    osx_resample_kernel<<<dim3((unsigned)blocks, nel), nt, 0, (cudaStream_t)stream>>>(
-        (const float2 *)v, (float2 *)v_next, v_stride, nv, Q, P, pd, pd + (size_t)P * Q, base, step, inoff, K0,
-        count, outs, out_off, (float2 *)stage, stage_stride);
+extern "C" int atkb_osx_resample_batch(const atkb_osx_rs *runs, int n, void *stream) {
+    if (n <= 0) return ATKB_OK;
+    if (n > ATKB_OSX_RS_MAX) return ATKB_E_ARG;
+    RsBatch B;
+    B.n = n;
+    long long total = 0;
+    for (int r = 0; r < n; ++r) {
+        B.r[r] = runs[r];
+        const long long work = runs[r].count > runs[r].Q ? runs[r].count : runs[r].Q;
+        B.r[r].blocks = (int)((work + 127) / 128);
+        B.first[r] = (int)total;
+        total += (long long)B.r[r].blocks * runs[r].nel;
+    }
+    B.first[n] = (int)total;
+    if (total <= 0) return ATKB_OK;
+    if (total > 0x7fffffffLL) return ATKB_E_ARG;
+    osx_resample_batch_kernel<<<(unsigned)total, 128, 0, (cudaStream_t)stream>>>(B);
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }
 

@@ -58,6 +58,7 @@ typedef struct {
     double *base;                 /* per element: the anchor, outputs and inputs */
     uint64_t *K, *in_off;         /* since it (src/resample.c:110-128)           */
     void *d_out;                  /* [max_nel][ostride] resampled output staging */
+    uint64_t last_got;            /* outputs of the current chunk (per element) */
     size_t ostride;
 } osx_chan;
 
@@ -520,44 +521,59 @@ static int osx_chunk(atkdsp_osx *x, const osx_io *io, size_t off, size_t sub, si
     R.X = x->d_X; R.T = x->d_T; R.Y = x->d_Y;
     if (R.nchans > 0) rc = atkb_osx_launch(&R, (int)h, (int)nel, x->stream);   /* no channel: nothing to compute */
     if (rc != ATKB_OK) return rc;
-    /* each channel's samples of this chunk: resampled, and out to the host */
+    /* the resampled channels: one launch for every run of the chunk (a run
+     * is a channel and a group of elements whose resamplers stand at the
+     * same place), then every channel's samples out to the host */
+    atkb_osx_rs runs[ATKB_OSX_RS_MAX];
+    int nruns = 0;
     for (ci = 0; ci < x->nslots && rc == ATKB_OK; ++ci) {
         osx_chan *c = &x->ch[ci];
-        if (!c->active) continue;
+        if (!c->active || !c->rs) continue;
         const size_t nv = h * c->nvalid;
         const size_t half = (size_t)x->max_nel * c->vstride;
         atkdsp_cf32 *v = (atkdsp_cf32 *)c->d_v + (size_t)x->par * half;
-        if (!c->rs) {
-            if (!io->dev_out)
-                for (e = 0; e < nel && rc == ATKB_OK; ++e)
-                    rc = atkb_d2h(io->outs[(size_t)e * x->nslots + ci] + io->wpos[ci], v + (size_t)e * c->vstride,
-                                  nv * sizeof(atkdsp_cf32), x->stream);
-            io->wpos[ci] += nv;
-            continue;
-        }
-        /* resample, grouping elements whose resamplers stand at the same place */
         atkdsp_cf32 *vn = (atkdsp_cf32 *)c->d_v + (size_t)(x->par ^ 1) * half;
-        uint64_t got = 0;
         for (e = 0; e < nel && rc == ATKB_OK;) {
             unsigned e1 = e + 1, u;
             while (e1 < nel && same_rs_state(c, e, e1)) ++e1;
-            got = rs_count(c, e, nv);
-            rc = atkb_osx_resample(v + (size_t)e * c->vstride, vn + (size_t)e * c->vstride, (long long)c->vstride,
-                                   (long long)nv, (int)c->Q, (int)c->P, (const float *)c->d_pd, c->base[e], c->step,
-                                   (double)c->in_off[e], (unsigned long long)c->K[e], (long long)got,
-                                   io->dev_out ? d_outs + (size_t)c->tix * x->max_nel + e : NULL,
-                                   (long long)io->wpos[ci], (atkdsp_cf32 *)c->d_out + (size_t)e * c->ostride,
-                                   (long long)c->ostride, (int)(e1 - e), x->stream);
+            const uint64_t got = rs_count(c, e, nv);
+            atkb_osx_rs *r = &runs[nruns++];
+            memset(r, 0, sizeof *r);
+            r->v = v + (size_t)e * c->vstride;
+            r->v_next = vn + (size_t)e * c->vstride;
+            r->v_stride = (long long)c->vstride;
+            r->nv = (long long)nv;
+            r->pd = (const float *)c->d_pd;
+            r->base = c->base[e]; r->step = c->step; r->inoff = (double)c->in_off[e];
+            r->K0 = (unsigned long long)c->K[e];
+            r->count = (long long)got;
+            r->outs = io->dev_out ? d_outs + (size_t)c->tix * x->max_nel + e : NULL;
+            r->out_off = (long long)io->wpos[ci];
+            r->stage = (atkdsp_cf32 *)c->d_out + (size_t)e * c->ostride;
+            r->stage_stride = (long long)c->ostride;
+            r->Q = (int)c->Q; r->P = (int)c->P; r->nel = (int)(e1 - e);
             for (u = e; u < e1; ++u) { c->K[u] += got; c->in_off[u] += nv; }
-            if (!io->dev_out)
-                for (u = e; u < e1 && rc == ATKB_OK; ++u)
-                    if (got)
-                        rc = atkb_d2h(io->outs[(size_t)u * x->nslots + ci] + io->wpos[ci],
-                                      (const atkdsp_cf32 *)c->d_out + (size_t)u * c->ostride,
-                                      got * sizeof(atkdsp_cf32), x->stream);
+            c->last_got = got;
+            if (nruns == ATKB_OSX_RS_MAX) {
+                rc = atkb_osx_resample_batch(runs, nruns, x->stream);
+                nruns = 0;
+            }
             e = e1;
         }
-        io->wpos[ci] += (size_t)got;
+    }
+    if (rc == ATKB_OK) rc = atkb_osx_resample_batch(runs, nruns, x->stream);
+    for (ci = 0; ci < x->nslots && rc == ATKB_OK; ++ci) {
+        osx_chan *c = &x->ch[ci];
+        if (!c->active) continue;
+        const size_t got = c->rs ? (size_t)c->last_got : h * c->nvalid;
+        const atkdsp_cf32 *src = c->rs ? (const atkdsp_cf32 *)c->d_out
+                                       : (const atkdsp_cf32 *)c->d_v + (size_t)x->par * x->max_nel * c->vstride;
+        const size_t sstride = c->rs ? c->ostride : c->vstride;
+        if (!io->dev_out && got)
+            for (e = 0; e < nel && rc == ATKB_OK; ++e)
+                rc = atkb_d2h(io->outs[(size_t)e * x->nslots + ci] + io->wpos[ci], src + (size_t)e * sstride,
+                              got * sizeof(atkdsp_cf32), x->stream);
+        io->wpos[ci] += got;
     }
     if (rc != ATKB_OK) return rc;
     /* the new state: s[h*hop, avail + ov) per element; untouched elements keep theirs */
