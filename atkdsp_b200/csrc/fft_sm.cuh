@@ -117,6 +117,134 @@ __device__ void fft_b(double2 *sm, int logn, int nb, const double2 *__restrict__
  * as an immediate offset). SM: the spectrum is the fused kernel's shared
  * one, bin b of this block at shared address xs + b * 8 * OSX_G; else
  * global, bin b at X[b]. */
+
+/* ---- radix-8 transforms in a swizzled layout --------------------------------
+ * Element p of a transform lives at sm[swz(p)]: the low 3 index bits XORed
+ * with the next 3, so the stride-8 stores of a radix-8 pass and the
+ * unit-stride loads both spread over distinct 16-byte slots of a wavefront. */
+__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 3) & 7); }
+
+__device__ __forceinline__ double2 d2sq(double2 a) { return make_double2(a.x * a.x - a.y * a.y, 2.0 * a.x * a.y); }
+
+/* 8-point DFT in place (two 4-point DFTs and the W8 twiddles); the inverse
+ * conjugates every root */
+__device__ __forceinline__ void dft8(double2 *v, bool inv) {
+    const double h = 0.70710678118654752440;   /* sqrt(1/2) */
+    double2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+    dft4(e, inv);
+    dft4(o, inv);
+    /* W8^1 = (1 -+ i) h, W8^2 = -+ i, W8^3 = (-1 -+ i) h */
+    const double s = inv ? 1.0 : -1.0;
+    const double2 t1 = make_double2((o[1].x - s * o[1].y) * h, (o[1].y + s * o[1].x) * h);
+    const double2 t2 = make_double2(-s * o[2].y, s * o[2].x);
+    const double2 t3 = make_double2((-o[3].x - s * o[3].y) * h, (-o[3].y + s * o[3].x) * h);
+    v[0] = d2add(e[0], o[0]);
+    v[4] = d2sub(e[0], o[0]);
+    v[1] = d2add(e[1], t1);
+    v[5] = d2sub(e[1], t1);
+    v[2] = d2add(e[2], t2);
+    v[6] = d2sub(e[2], t2);
+    v[3] = d2add(e[3], t3);
+    v[7] = d2sub(e[3], t3);
+}
+
+/* One transform of n = 2^logn points (8 <= n <= 8*NTH) in the swizzled
+ * layout by NTH threads, natural order in and out: radix-8 Stockham passes,
+ * then one radix-4 or radix-2 pass for the bits left. A butterfly's
+ * twiddles W^(r k), r = 1..7, come from one table entry W^k (the nfft-point
+ * table at the stride of this pass) and its powers by multiplication, each
+ * at most three roundings from the exact root. Ends with a barrier. */
+template <int NTH>
+__device__ void fft_r8(double2 *sm, int logn, const double2 *__restrict__ tw, int lognfft, bool inv, int tid) {
+    const int n = 1 << logn;
+    int lg = 0;
+    for (; logn - lg >= 3; lg += 3) {
+        const int Ns = 1 << lg, q = n >> 3, sh = lognfft - lg - 3;
+        double2 v[8];
+        const int t = tid;
+        const bool on = t < q;                 /* n <= 8*NTH: one butterfly per thread */
+        int k = 0;
+        if (on) {
+            k = t & (Ns - 1);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[r] = sm[swz(t + r * q)];
+            if (lg) {
+                double2 w[8];
+                w[1] = tw_at(tw, k, sh, inv);
+                w[2] = d2sq(w[1]);
+                w[3] = d2mul(w[2], w[1]);
+                w[4] = d2sq(w[2]);
+                w[5] = d2mul(w[4], w[1]);
+                w[6] = d2sq(w[3]);
+                w[7] = d2mul(w[4], w[3]);
+#pragma unroll
+                for (int r = 1; r < 8; ++r) v[r] = d2mul(v[r], w[r]);
+            }
+            dft8(v, inv);
+        }
+        __syncthreads();
+        if (on) {
+            const int o = ((t >> lg) << (lg + 3)) + k;
+#pragma unroll
+            for (int r = 0; r < 8; ++r) sm[swz(o + r * Ns)] = v[r];
+        }
+        __syncthreads();
+    }
+    if (logn - lg == 2) {                      /* a radix-4 pass for the last two bits */
+        const int Ns = 1 << lg, q = n >> 2, sh = lognfft - lg - 2;
+        double2 v[2][4];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int t = tid + u * NTH;
+            if (t < q) {
+                const int k = t & (Ns - 1);
+#pragma unroll
+                for (int r = 0; r < 4; ++r) v[u][r] = sm[swz(t + r * q)];
+                if (lg) {
+#pragma unroll
+                    for (int r = 1; r < 4; ++r) v[u][r] = d2mul(v[u][r], tw_at(tw, r * k, sh, inv));
+                }
+                dft4(v[u], inv);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int t = tid + u * NTH;
+            if (t < q) {
+                const int k = t & (Ns - 1), o = ((t >> lg) << (lg + 2)) + k;
+#pragma unroll
+                for (int r = 0; r < 4; ++r) sm[swz(o + r * Ns)] = v[u][r];
+            }
+        }
+        __syncthreads();
+    } else if (logn - lg == 1) {               /* ... or a radix-2 pass for the last bit */
+        const int Ns = 1 << lg, q = n >> 1, sh = lognfft - lg - 1;
+        double2 a[4], c[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int t = tid + u * NTH;
+            if (t < q) {
+                const int k = t & (Ns - 1);
+                a[u] = sm[swz(t)];
+                c[u] = sm[swz(t + q)];
+                if (lg) c[u] = d2mul(c[u], tw_at(tw, k, sh, inv));
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int t = tid + u * NTH;
+            if (t < q) {
+                const int k = t & (Ns - 1), o = ((t >> lg) << (lg + 1)) + k;
+                sm[swz(o)] = d2add(a[u], c[u]);
+                sm[swz(o + Ns)] = d2sub(a[u], c[u]);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace atkb_fft
 
 #endif

@@ -2,8 +2,8 @@
  *
  * One CTA per (block, element). For nfft <= ATKB_OSX_FUSED_MAX the whole chain
  * stays in shared memory: the block's nfft samples are gathered from the
- * element's state and input, transformed in double (Stockham, radix 4 with
- * one radix-2 pass when log2 nfft is odd), and rounded to a float spectrum X
+ * element's state and input, transformed in double (Stockham, radix 8 with
+ * a radix-4 or radix-2 pass for the bits left), and rounded to a float spectrum X
  * as the reference stores it. Then, per channel: the decimating fold of X
  * against the channel filter's spectrum into M bins (float, the reference's
  * expression order with rounded operations: src/channelizer.c:707-716), the
@@ -214,12 +214,14 @@ __global__ void __launch_bounds__(OSX_NT, 1) osx_group_kernel(const atkb_osx_run
         const long long g0 = (long long)(i0 + g) * R.hop;
         for (int p = threadIdx.x; p < nfft; p += OSX_NT) {
             const float2 v = osx_sample(R, in, e, g0 + p);
-            work[p] = make_double2((double)v.x, (double)v.y);
+            work[swz(p)] = make_double2((double)v.x, (double)v.y);
         }
         __syncthreads();
-        fft_b<OSX_NT>(work, R.lognfft, 1, tw, R.lognfft, false, threadIdx.x);
-        for (int p = threadIdx.x; p < nfft; p += OSX_NT)
-            X[p * OSX_G + g] = make_float2(__double2float_rn(work[p].x), __double2float_rn(work[p].y));
+        fft_r8<OSX_NT>(work, R.lognfft, tw, R.lognfft, false, threadIdx.x);
+        for (int p = threadIdx.x; p < nfft; p += OSX_NT) {
+            const double2 y = work[swz(p)];
+            X[p * OSX_G + g] = make_float2(__double2float_rn(y.x), __double2float_rn(y.y));
+        }
         __syncthreads();
     }
     osx_channels<OSX_G>(X, 1, nb, work, R, e, i0, &s_next);

@@ -2,8 +2,8 @@
  * :176-295 atkdsp_spectrum_reduce, :315-430 atkdsp_spectrum_stats).
  *
  * Every frame of n samples (stride hop) of a device cf32 block is windowed
- * and transformed in double in shared memory (the Stockham transform of
- * fft_sm.cuh), and its per-bin power folded into per-CTA accumulators held
+ * and transformed in double in shared memory (the radix-8 Stockham transform
+ * of fft_sm.cuh), and its per-bin power folded into per-CTA accumulators held
  * in registers: each CTA takes a contiguous run of frames, as the
  * reference's OpenMP threads do, and writes one partial line (reduce: float
  * max / min / sum of |X|^2/n^2 from the float-rounded bin; stats: double
@@ -46,18 +46,18 @@ __global__ void __launch_bounds__(SP_NT) spec_frames_kernel(const float2 *__rest
             const float2 v = __ldg(x + p);
             if (win) {
                 const double g = (double)__ldg(win + p);
-                sm[p] = make_double2(__dmul_rn((double)v.x, g), __dmul_rn((double)v.y, g));
+                sm[swz(p)] = make_double2(__dmul_rn((double)v.x, g), __dmul_rn((double)v.y, g));
             } else {
-                sm[p] = make_double2((double)v.x, (double)v.y);
+                sm[swz(p)] = make_double2((double)v.x, (double)v.y);
             }
         }
         __syncthreads();
-        fft_b<SP_NT>(sm, logn, 1, tw, logn, false, tid);
+        fft_r8<SP_NT>(sm, logn, tw, logn, false, tid);
 #pragma unroll
         for (int u = 0; u < SP_BINS; ++u) {
             const int i = tid + u * SP_NT;
             if (i >= n) break;
-            const double2 X = sm[(i + half) & (n - 1)];
+            const double2 X = sm[swz((i + half) & (n - 1))];
             if (MODE < 3) {
                 const float re = __double2float_rn(X.x), im = __double2float_rn(X.y);
                 const float pw = __fmul_rn(__fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im)), inv2f);
