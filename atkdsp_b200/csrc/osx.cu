@@ -166,18 +166,18 @@ __device__ void osx_channel(const float2 *X, int xrow, int nb, int c0, int S, do
  * blocks */
 template <int XCOL>
 __device__ void osx_channels(const float2 *X, int xrow, int nb, double2 *work, const atkb_osx_run &R, int e,
-                             int i0, int *next) {
+                             int i0, int *next, int slice = 0, int nslices = 1) {
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     for (;;) {
         int p = 0;
-        if (lane == 0) p = atomicAdd(next, 1);
+        if (lane == 0) p = slice + nslices * atomicAdd(next, 1);
         p = __shfl_sync(0xffffffffu, p, 0);
         if (p >= R.npacks) break;
         const int c0 = R.packs[p], c1 = R.packs[p + 1];
         osx_channel<32, XCOL>(X, xrow, nb, c0, c1 - c0, work + w * OSX_WREG, R, e, i0, lane);
     }
     __syncthreads();
-    for (int c = R.nsmall; c < R.nsmall + R.nmid; ++c) {
+    for (int c = R.nsmall + slice; c < R.nsmall + R.nmid; c += nslices) {
         const int per = ATKB_OSX_FUSED_MAX >> R.chans[c].logm;     /* blocks per batch */
         for (int g0 = 0; g0 < nb; g0 += per) {
             const int cnt = min(per, nb - g0);
@@ -227,7 +227,9 @@ __global__ void __launch_bounds__(OSX_NT, 1) osx_group_kernel(const atkb_osx_run
     osx_channels<OSX_G>(X, 1, nb, work, R, e, i0, &s_next);
 }
 
-/* nfft > ATKB_OSX_FUSED_MAX: the channels read the spectra from HBM */
+/* nfft > ATKB_OSX_FUSED_MAX: the channels read the spectra from HBM, so the
+ * channels split over gridDim.z slices (packs and CTA-wide channels dealt
+ * round-robin) as well as over blocks */
 __global__ void __launch_bounds__(OSX_NT, 1) osx_group_chan_kernel(const atkb_osx_run R, int m) {
     extern __shared__ double2 smem[];
     __shared__ int s_next;
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(OSX_NT, 1) osx_group_chan_kernel(const atkb_os
     const float2 *X = (const float2 *)R.X + ((long long)e * m + i0) * R.nfft;
     if (threadIdx.x == 0) s_next = 0;
     __syncthreads();
-    osx_channels<1>(X, R.nfft, nb, smem, R, e, i0, &s_next);
+    osx_channels<1>(X, R.nfft, nb, smem, R, e, i0, &s_next, blockIdx.z, gridDim.z);
 }
 
 /* Transforms longer than 4096 points: n = n1 * n2 in the four-step form,
@@ -257,18 +259,20 @@ __global__ void __launch_bounds__(OSX_NT) osx_four_a(const atkb_osx_run R, const
         const long long g0 = (long long)i * R.hop + q;
         for (int r = threadIdx.x; r < n1; r += OSX_NT) {
             const float2 v = osx_sample(R, in, e, g0 + ((long long)r << logn2));
-            sm[r] = make_double2((double)v.x, (double)v.y);
+            sm[swz(r)] = make_double2((double)v.x, (double)v.y);
         }
     } else {
         const double2 *s = src + (item << logn) + q;
-        for (int r = threadIdx.x; r < n1; r += OSX_NT) sm[r] = s[(long long)r << logn2];
+        for (int r = threadIdx.x; r < n1; r += OSX_NT) sm[swz(r)] = s[(long long)r << logn2];
     }
     __syncthreads();
-    fft_b<OSX_NT>(sm, logn1, 1, tw, R.lognfft, inv, threadIdx.x);
+    fft_r8<OSX_NT>(sm, logn1, tw, R.lognfft, inv, threadIdx.x);
     double2 *t = T + (item << logn);
     const int sh = R.lognfft - logn, mask = (1 << logn) - 1;
-    for (int k1 = threadIdx.x; k1 < n1; k1 += OSX_NT)
-        t[((long long)k1 << logn2) + q] = q ? d2mul(sm[k1], tw_at(tw, (q * k1) & mask, sh, inv)) : sm[k1];
+    for (int k1 = threadIdx.x; k1 < n1; k1 += OSX_NT) {
+        const double2 y = sm[swz(k1)];
+        t[((long long)k1 << logn2) + q] = q ? d2mul(y, tw_at(tw, (q * k1) & mask, sh, inv)) : y;
+    }
 }
 
 /* Pass B, grid (n1, m, nel): row k1's n2-point transform, to a float
@@ -281,13 +285,14 @@ __global__ void __launch_bounds__(OSX_NT) osx_four_b(const atkb_osx_run R, const
     const int n2 = 1 << logn2, logn = logn1 + logn2;
     const long long item = (long long)e * m + i;
     const double2 *t = T + (item << logn) + ((long long)k1 << logn2);
-    for (int q = threadIdx.x; q < n2; q += OSX_NT) sm[q] = t[q];
+    for (int q = threadIdx.x; q < n2; q += OSX_NT) sm[swz(q)] = t[q];
     __syncthreads();
-    fft_b<OSX_NT>(sm, logn2, 1, (const double2 *)R.tw, R.lognfft, inv, threadIdx.x);
+    fft_r8<OSX_NT>(sm, logn2, (const double2 *)R.tw, R.lognfft, inv, threadIdx.x);
     for (int k2 = threadIdx.x; k2 < n2; k2 += OSX_NT) {
         const long long o = (item << logn) + k1 + ((long long)k2 << logn1);
-        if (DST == 0) ((float2 *)out)[o] = make_float2(__double2float_rn(sm[k2].x), __double2float_rn(sm[k2].y));
-        else ((double2 *)out)[o] = sm[k2];
+        const double2 y = sm[swz(k2)];
+        if (DST == 0) ((float2 *)out)[o] = make_float2(__double2float_rn(y.x), __double2float_rn(y.y));
+        else ((double2 *)out)[o] = y;
     }
 }
 
@@ -408,7 +413,18 @@ extern "C" int atkb_osx_launch(const atkb_osx_run *run, int m, int nel, void *st
                                                                                 (double2 *)R.T, m);
     osx_four_b<0><<<dim3(1 << logn1, m, nel), OSX_NT, (size_t)16 << logn2, s>>>(R, (const double2 *)R.T, logn1,
                                                                                 logn2, false, R.X, m);
-    if (R.nsmall + R.nmid > 0) osx_group_chan_kernel<<<groups, OSX_NT, OSX_WORK * 16, s>>>(R, m);
+    if (R.nsmall + R.nmid > 0) {
+        /* enough channel slices to give every SM two CTAs, no more than
+         * there are packs or CTA-wide channels to deal */
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const long long ctas = (long long)groups.x * groups.y;
+        int slices = (int)((2LL * sms + ctas - 1) / ctas);
+        const int units = R.npacks > R.nmid ? R.npacks : R.nmid;
+        if (slices > units) slices = units;
+        if (slices < 1) slices = 1;
+        osx_group_chan_kernel<<<dim3(groups.x, groups.y, slices), OSX_NT, OSX_WORK * 16, s>>>(R, m);
+    }
     for (int c = R.nsmall + R.nmid; c < R.nchans; ++c) {
         /* M > 4096: fold to Y, four-step inverse through T back into Y, roll */
         const int logm = R.h_chans[c].logm;

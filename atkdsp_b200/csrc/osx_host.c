@@ -36,7 +36,7 @@
 #define OSX_PI 3.14159265358979323846
 /* input samples per element per chunk: enough blocks to fill the GPU */
 #define OSX_CHUNK_SAMPLES ((size_t)1 << 22)
-#define OSX_CHUNK_SAMPLES_BIG ((size_t)1 << 20)  /* nfft > 4096: the spectra go through HBM */
+#define OSX_CHUNK_SAMPLES_BIG ((size_t)1 << 21)  /* nfft > 4096: the spectra go through HBM */
 #define OSX_RS_PHASES 64                       /* resampler phases (:635) */
 
 typedef struct {

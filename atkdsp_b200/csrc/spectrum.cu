@@ -4,7 +4,8 @@
  * Every frame of n samples (stride hop) of a device cf32 block is windowed
  * and transformed in double in shared memory (the radix-8 Stockham transform
  * of fft_sm.cuh), and its per-bin power folded into per-CTA accumulators held
- * in registers: each CTA takes a contiguous run of frames, as the
+ * in registers (stats: in shared memory beside the transform): each CTA
+ * takes a contiguous run of frames, as the
  * reference's OpenMP threads do, and writes one partial line (reduce: float
  * max / min / sum of |X|^2/n^2 from the float-rounded bin; stats: double
  * max, min, sum P, sum P^2). A second kernel merges the partials in CTA
@@ -38,8 +39,8 @@ __global__ void __launch_bounds__(SP_NT) spec_frames_kernel(const float2 *__rest
     const float inv2f = __fdiv_rn(1.0f, __fmul_rn((float)n, (float)n));
     const double inv2d = 1.0 / ((double)n * (double)n);
     float acc[SP_BINS];
-    double mx[MODE == 3 ? SP_BINS : 1], mn[MODE == 3 ? SP_BINS : 1], su[MODE == 3 ? SP_BINS : 1],
-        s2[MODE == 3 ? SP_BINS : 1];
+    /* stats: the four accumulator planes in shared memory after the transform */
+    double *mx = (double *)(sm + n), *mn = mx + n, *su = mn + n, *s2 = su + n;
     for (long long f = f0; f < f1; ++f) {
         const float2 *x = in + f * hop;
         for (int p = tid; p < n; p += SP_NT) {
@@ -68,13 +69,13 @@ __global__ void __launch_bounds__(SP_NT) spec_frames_kernel(const float2 *__rest
             } else {
                 const double pw = __dmul_rn(__dadd_rn(__dmul_rn(X.x, X.x), __dmul_rn(X.y, X.y)), inv2d);
                 if (f == f0) {
-                    mx[u] = mn[u] = su[u] = pw;
-                    s2[u] = __dmul_rn(pw, pw);
+                    mx[i] = mn[i] = su[i] = pw;
+                    s2[i] = __dmul_rn(pw, pw);
                 } else {
-                    if (pw > mx[u]) mx[u] = pw;
-                    if (pw < mn[u]) mn[u] = pw;
-                    su[u] = __dadd_rn(su[u], pw);
-                    s2[u] = __dadd_rn(s2[u], __dmul_rn(pw, pw));
+                    if (pw > mx[i]) mx[i] = pw;
+                    if (pw < mn[i]) mn[i] = pw;
+                    su[i] = __dadd_rn(su[i], pw);
+                    s2[i] = __dadd_rn(s2[i], __dmul_rn(pw, pw));
                 }
             }
         }
@@ -88,10 +89,10 @@ __global__ void __launch_bounds__(SP_NT) spec_frames_kernel(const float2 *__rest
             ((float *)part)[(long long)blockIdx.x * n + i] = acc[u];
         } else {
             double *d = (double *)part + (long long)blockIdx.x * 4 * n;
-            d[i] = mx[u];
-            d[n + i] = mn[u];
-            d[2 * n + i] = su[u];
-            d[3 * n + i] = s2[u];
+            d[i] = mx[i];
+            d[n + i] = mn[i];
+            d[2 * n + i] = su[i];
+            d[3 * n + i] = s2[i];
         }
     }
 }
@@ -141,7 +142,7 @@ template <int MODE>
 int spec_launch(const void *in, long long frames, long long hop, int logn, const float *win, const void *tw,
                 int nblk, int per, void *part, float *o0, float *o1, float *o2, float *o3, cudaStream_t s) {
     const int n = 1 << logn;
-    spec_frames_kernel<MODE><<<nblk, SP_NT, (size_t)n * 16, s>>>((const float2 *)in, frames, hop, logn, win,
+    spec_frames_kernel<MODE><<<nblk, SP_NT, (size_t)n * (MODE == 3 ? 48 : 16), s>>>((const float2 *)in, frames, hop, logn, win,
                                                                 (const double2 *)tw, per, part);
     spec_final_kernel<MODE><<<(n + 255) / 256, 256, 0, s>>>(part, nblk, n, frames, o0, o1, o2, o3);
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
@@ -161,7 +162,7 @@ extern "C" int atkb_spec_launch(int mode, const void *in, long long frames, long
         if (cudaFuncSetAttribute(spec_frames_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess ||
             cudaFuncSetAttribute(spec_frames_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess ||
             cudaFuncSetAttribute(spec_frames_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess ||
-            cudaFuncSetAttribute(spec_frames_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess)
+            cudaFuncSetAttribute(spec_frames_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * b) != cudaSuccess)
             return ATKB_E_KERNEL;
         g_configured[dev] = true;
     }
