@@ -273,3 +273,33 @@ def test_device_pointer_entry_point_matches_the_host_call():
         for ci in range(2):
             v = dy[e][ci].cpu().numpy().view(np.complex64)[: counts[ci]]
             assert np.array_equal(v, yh[ci][e])
+
+
+def test_multi_element_long_call_through_host_buffers():
+    """Two elements, a call longer than one internal chunk (host staging
+    reused chunk after chunk), equal bit for bit to the same samples fed in
+    uneven pieces, and each element equal to its single-element run."""
+    rng = np.random.default_rng(17)
+    n = (1 << 22) + 4097
+    xs = [((rng.standard_normal(n) + 1j * rng.standard_normal(n)) * 0.5).astype(np.complex64) for _ in range(2)]
+    plan = [(300e3, 50e3, 50e3), (-700e3, 200e3, 300e3), (41e3, 12.5e3, 15.625e3)]
+
+    def make(nel):
+        o = ak.Osx(FS, 4096, 80.0, nel)
+        for c in plan:
+            o.add(*c)
+        return o
+
+    whole, cw = make(2).process_n(xs, 2, cap=n)
+    p = make(2)
+    parts = {ci: [] for ci in range(len(plan))}
+    for a, b in ((0, 1), (1, 2_000_000), (2_000_000, 2_000_007), (2_000_007, n)):
+        y, _ = p.process_n([x[a:b] for x in xs], 2, cap=n)
+        for ci in parts:
+            parts[ci].append(y[ci])
+    for ci in parts:
+        assert np.array_equal(whole[ci], np.concatenate(parts[ci], axis=1))
+    for e in range(2):
+        ye, _ = make(1).process(xs[e], cap=n)
+        for ci in parts:
+            assert np.array_equal(ye[ci], whole[ci][e])
