@@ -11,7 +11,9 @@
  *   state     two buffers (ping-pong) of max_nel x nfft samples: each
  *             element's hist (ov) ++ leftover (lc), the reference's
  *             x->hist ++ x->leftover
- *   in        max_nel x chunk_in samples of input staging (host calls)
+ *   in        2 x max_nel x chunk_in samples of input staging (host calls),
+ *             alternating chunk by chunk: a chunk's upload runs on a copy stream
+ *             while the previous chunk's kernels run
  *   tw        nfft double2 (cos, -sin)(2 pi j / nfft), every transform's roots
  *   X, T, Y   a chunk's spectra and the four-step scratch (nfft > 4096 only)
  *   table     the per-call channel table and input pointer array (+ a
@@ -73,7 +75,12 @@ struct atkdsp_osx {
     void *stream;
     void *d_state;                /* 2 * max_nel * nfft cf32                     */
     int cur;
-    void *d_in;                   /* max_nel * chunk_in cf32                     */
+    void *d_in;                   /* 2 * max_nel * chunk_in cf32: two input stagings
+                                   * that alternate chunk by chunk (host calls) */
+    int inb;                      /* the staging the next chunk fills            */
+    void *cstream;                /* the copy stream: a chunk's upload overlaps the
+                                   * previous chunk's kernels                    */
+    void *ev_up[2], *ev_done[2];  /* staging b uploaded / read by its kernels     */
     size_t chunk_hops, chunk_in;
     void *d_tw;
     void *d_X, *d_T, *d_Y;
@@ -187,6 +194,9 @@ ATKDSP_API void atkdsp_osx_destroy(atkdsp_osx *x) {
     if (x->stream) atkb_stream_sync(x->stream);
     for (i = 0; i < x->nslots; ++i) osx_chan_free(&x->ch[i]);
     free(x->ch); free(x->wpos);
+    if (x->cstream) atkb_stream_sync(x->cstream);
+    for (i = 0; i < 2; ++i) { atkb_event_destroy(x->ev_up[i]); atkb_event_destroy(x->ev_done[i]); }
+    atkb_stream_destroy(x->cstream);
     atkb_free(x->d_state); atkb_free(x->d_in); atkb_free(x->d_tw); atkb_free(x->d_X); atkb_free(x->d_T); atkb_free(x->d_Y);
     atkb_free(x->d_tbl); atkb_host_free(x->h_tbl);
     atkb_stream_destroy(x->stream);
@@ -199,11 +209,12 @@ static int ilog2(size_t v) {
     return l;
 }
 
-/* the per-call table: channel entries for `slots`, then max_nel input
- * pointers, then per entry max_nel output pointers (device-pointer calls),
+/* the per-call table: channel entries for `slots`, then two sets of max_nel
+ * input pointers (one per input staging; device-pointer calls use the
+ * first), then per entry max_nel output pointers (device-pointer calls),
  * then slots + 1 pack boundaries */
 static size_t tbl_ins_off(const atkdsp_osx *x) { return atkb_align16((size_t)x->tbl_slots * sizeof(atkb_osx_chan)); }
-static size_t tbl_outs_off(const atkdsp_osx *x) { return tbl_ins_off(x) + (size_t)x->max_nel * sizeof(void *); }
+static size_t tbl_outs_off(const atkdsp_osx *x) { return tbl_ins_off(x) + 2 * (size_t)x->max_nel * sizeof(void *); }
 static size_t tbl_packs_off(const atkdsp_osx *x) {
     return tbl_outs_off(x) + (size_t)x->tbl_slots * x->max_nel * sizeof(void *);
 }
@@ -213,7 +224,7 @@ static int osx_table_reserve(atkdsp_osx *x, int slots) {
     int want = x->tbl_slots ? x->tbl_slots : 8;
     while (want < slots) want *= 2;
     const size_t bytes = atkb_align16((size_t)want * sizeof(atkb_osx_chan)) +
-                         (size_t)x->max_nel * sizeof(void *) * (1 + (size_t)want) + (size_t)(want + 1) * sizeof(int);
+                         (size_t)x->max_nel * sizeof(void *) * (2 + (size_t)want) + (size_t)(want + 1) * sizeof(int);
     void *d = NULL, *h = NULL;
     int rc = atkb_malloc(&d, bytes);
     if (rc == ATKB_OK) rc = atkb_host_alloc(&h, bytes);
@@ -239,7 +250,14 @@ ATKDSP_API atkdsp_osx *atkdsp_osx_create(double fs, size_t nfft, double atten_db
     int rc = atkb_get_device(&x->dev);
     if (rc == ATKB_OK) rc = atkb_stream_create(&x->stream);
     if (rc == ATKB_OK) rc = atkb_malloc(&x->d_state, 2 * (size_t)max_nel * nfft * sizeof(atkdsp_cf32));
-    if (rc == ATKB_OK) rc = atkb_malloc(&x->d_in, (size_t)max_nel * x->chunk_in * sizeof(atkdsp_cf32));
+    if (rc == ATKB_OK) rc = atkb_malloc(&x->d_in, 2 * (size_t)max_nel * x->chunk_in * sizeof(atkdsp_cf32));
+    if (rc == ATKB_OK) rc = atkb_stream_create(&x->cstream);
+    for (int b = 0; b < 2 && rc == ATKB_OK; ++b) {
+        rc = atkb_event_create(&x->ev_up[b]);
+        if (rc == ATKB_OK) rc = atkb_event_create(&x->ev_done[b]);
+        /* both stagings start free */
+        if (rc == ATKB_OK) rc = atkb_event_record(x->ev_done[b], x->stream);
+    }
     if (rc == ATKB_OK) rc = atkb_malloc(&x->d_tw, nfft * 2 * sizeof(double));
     if (rc == ATKB_OK && nfft > ATKB_OSX_FUSED_MAX) {
         const size_t pts = (size_t)max_nel * x->chunk_hops * nfft;
@@ -496,15 +514,23 @@ typedef struct {
 static int osx_chunk(atkdsp_osx *x, const osx_io *io, size_t off, size_t sub, size_t hop_base) {
     const unsigned nel = io->nel;
     const size_t avail = x->lc + sub, h = avail / x->hop;
-    const void *const *d_ins = (const void *const *)((char *)x->d_tbl + tbl_ins_off(x));
+    const int b = io->dev_in ? 0 : x->inb;
+    const void *const *d_ins = (const void *const *)((char *)x->d_tbl + tbl_ins_off(x)) + (size_t)b * x->max_nel;
     void *const *d_outs = (void *const *)((char *)x->d_tbl + tbl_outs_off(x));
     unsigned e;
     int rc = ATKB_OK, ci;
-    if (!io->dev_in)
+    if (!io->dev_in) {
+        /* the upload on the copy stream, once the chunk that last read this
+         * staging is done; this chunk's kernels wait for the upload */
+        atkdsp_cf32 *stage = (atkdsp_cf32 *)x->d_in + (size_t)b * x->max_nel * x->chunk_in;
+        rc = atkb_stream_wait(x->cstream, x->ev_done[b]);
         for (e = 0; e < nel && rc == ATKB_OK; ++e)
             if (sub)
-                rc = atkb_h2d((atkdsp_cf32 *)x->d_in + (size_t)e * x->chunk_in, io->ins[e] + off,
-                              sub * sizeof(atkdsp_cf32), x->stream);
+                rc = atkb_h2d(stage + (size_t)e * x->chunk_in, io->ins[e] + off, sub * sizeof(atkdsp_cf32),
+                              x->cstream);
+        if (rc == ATKB_OK) rc = atkb_event_record(x->ev_up[b], x->cstream);
+        if (rc == ATKB_OK) rc = atkb_stream_wait(x->stream, x->ev_up[b]);
+    }
     if (rc != ATKB_OK) return rc;
     atkdsp_cf32 *st = (atkdsp_cf32 *)x->d_state + (size_t)x->cur * x->max_nel * x->nfft;
     atkdsp_cf32 *st2 = (atkdsp_cf32 *)x->d_state + (size_t)(x->cur ^ 1) * x->max_nel * x->nfft;
@@ -584,6 +610,10 @@ static int osx_chunk(atkdsp_osx *x, const osx_io *io, size_t off, size_t sub, si
     if (rc == ATKB_OK && nel < x->max_nel)
         rc = atkb_d2d(st2 + (size_t)nel * x->nfft, st + (size_t)nel * x->nfft,
                       (size_t)(x->max_nel - nel) * x->nfft * sizeof(atkdsp_cf32), x->stream);
+    if (rc == ATKB_OK && !io->dev_in) {
+        rc = atkb_event_record(x->ev_done[b], x->stream);   /* the staging's last reader */
+        x->inb ^= 1;
+    }
     if (rc != ATKB_OK) return rc;
     x->cur ^= 1;
     x->par ^= 1;
@@ -700,8 +730,10 @@ static ptrdiff_t osx_process(atkdsp_osx *x, const osx_io *io0, size_t n, size_t 
             for (e = 0; e < nel; ++e)
                 pout[(size_t)t * x->max_nel + e] = io.outs[(size_t)e * ns + (int)(c - x->ch)];
     }
-    for (e = 0; e < nel; ++e)
+    for (e = 0; e < nel; ++e) {
         pin[e] = io.dev_in ? (void *)io.ins[e] : (void *)((atkdsp_cf32 *)x->d_in + (size_t)e * x->chunk_in);
+        pin[x->max_nel + e] = (void *)((atkdsp_cf32 *)x->d_in + ((size_t)x->max_nel + e) * x->chunk_in);
+    }
     rc = atkb_h2d(x->d_tbl, x->h_tbl, x->tbl_bytes, x->stream);
     if (rc != ATKB_OK) return atkb_map_rc(rc);
     size_t *wp = x->wpos;        /* NULL only while no slot exists (ns == 0) */
