@@ -12,9 +12,14 @@
  * here every sum is double, reduced in a fixed order, so the results are
  * deterministic and at least as accurate.
  *
- * Work split inside a CTA: P = nel(nel+1)/2 pairs; threads are (pair, lane
- * group) so that small arrays still use every thread; the block of hops is
- * staged through shared memory in chunks of CHUNK hops.
+ * Work split inside a CTA: the upper triangle of the nel x nel matrix is cut
+ * into TB x TB tiles (TB = 1, 2 or 4 by nel), and the threads into (tile, hop
+ * group) pairs: each thread keeps a tile's TB*TB sums in registers over its
+ * share of the hops, so one hop's 2*TB loads feed TB*TB products (the old
+ * one-pair-per-thread split loaded both operands for every product). The
+ * block of hops is staged through shared memory in chunks of CHUNK hops; the
+ * hop groups' partial sums are then added in group order, so the results
+ * are deterministic.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -26,78 +31,96 @@
 
 namespace {
 
+template <int TB>
 __global__ void __launch_bounds__(W_NT)
 w12_kernel(const float2 *__restrict__ out, int nel, int nchan, long long m,
            const uint8_t *__restrict__ gate, float2 *__restrict__ R, uint32_t *__restrict__ counts,
            float *__restrict__ pwr, float *__restrict__ mean_pwr) {
     __shared__ float2 ys[MAX_NEL][CHUNK];
-    __shared__ double red[W_NT][2];
     __shared__ double diag[MAX_NEL];
-    const int P = nel * (nel + 1) / 2;
+    extern __shared__ double red[];            /* [W_NT][TB*TB][2]: the groups' partial sums */
+    const int nb = (nel + TB - 1) / TB;
+    const int T = nb * (nb + 1) / 2;           /* tiles of the upper triangle */
+    const int groups = T >= W_NT ? 1 : W_NT / T;
+    const int tid = threadIdx.x;
+    const int tile = tid % T, g = tid / T;
+    const bool active = g < groups;
+    /* tile -> (A, B), A <= B, row-major over the upper triangle of tiles */
+    int A = 0, rem = tile;
+    while (rem >= nb - A) { rem -= nb - A; ++A; }
+    const int B = A + rem;
     for (int k = blockIdx.x; k < nchan; k += gridDim.x) {
         const bool w1 = R && counts && (!gate || gate[k]);
         const bool w2 = pwr || mean_pwr;
         if (!w1 && !w2) continue;
-        /* pairs this thread owns: p = tid % P_eff + j * W_NT ...; lane group g */
-        const int groups = P >= W_NT ? 1 : W_NT / P;
-        const int tpair = threadIdx.x % (P >= W_NT ? W_NT : P);
-        const int g = P >= W_NT ? 0 : threadIdx.x / P;
-        const bool active = g < groups && (P >= W_NT || threadIdx.x < groups * P);
-        double sr[4] = {0, 0, 0, 0}, si[4] = {0, 0, 0, 0};
-        int pa[4], pb[4], np = 0;
-        for (int p = tpair; p < P && np < 4; p += (P >= W_NT ? W_NT : P), ++np) {
-            /* p -> (a, b), a <= b, row-major over the upper triangle */
-            int a = 0, rem = p;
-            while (rem >= nel - a) { rem -= nel - a; ++a; }
-            pa[np] = a; pb[np] = a + rem;
-        }
+        double sr[TB][TB], si[TB][TB];
+#pragma unroll
+        for (int r = 0; r < TB; ++r)
+#pragma unroll
+            for (int c = 0; c < TB; ++c) sr[r][c] = si[r][c] = 0.0;
         for (long long i0 = 0; i0 < m; i0 += CHUNK) {
             const int cnt = (int)((m - i0) < CHUNK ? (m - i0) : CHUNK);
-            for (int e = threadIdx.x; e < nel * CHUNK; e += W_NT) {
+            for (int e = tid; e < nb * TB * CHUNK; e += W_NT) {
                 const int a = e / CHUNK, i = e - a * CHUNK;
-                ys[a][i] = i < cnt ? out[((long long)a * nchan + k) * m + i0 + i] : make_float2(0.f, 0.f);
+                ys[a][i] = (a < nel && i < cnt) ? out[((long long)a * nchan + k) * m + i0 + i]
+                                                : make_float2(0.f, 0.f);
             }
             __syncthreads();
-            if (active) {
-                for (int q = 0; q < np; ++q) {
-                    const bool need = w1 || pa[q] == pb[q];
-                    if (!need) continue;
-                    const int a = pa[q], b = pb[q];
-                    for (int i = g; i < cnt; i += groups) {
-                        const float2 ya = ys[a][i], yb = ys[b][i];
-                        sr[q] += (double)ya.x * yb.x + (double)ya.y * yb.y;
-                        si[q] += (double)ya.y * yb.x - (double)ya.x * yb.y;
+            if (active && (w1 || A == B)) {
+                for (int i = g; i < cnt; i += groups) {
+                    float2 ya[TB], yb[TB];
+#pragma unroll
+                    for (int r = 0; r < TB; ++r) {
+                        ya[r] = ys[A * TB + r][i];
+                        yb[r] = ys[B * TB + r][i];
                     }
+#pragma unroll
+                    for (int r = 0; r < TB; ++r)
+#pragma unroll
+                        for (int c = 0; c < TB; ++c) {
+                            sr[r][c] += (double)ya[r].x * yb[c].x + (double)ya[r].y * yb[c].y;
+                            si[r][c] += (double)ya[r].y * yb[c].x - (double)ya[r].x * yb[c].y;
+                        }
                 }
             }
             __syncthreads();
         }
-        /* reduce over lane groups (fixed order), pair by pair */
-        for (int q = 0; q < 4; ++q) {
-            red[threadIdx.x][0] = (active && q < np) ? sr[q] : 0.0;
-            red[threadIdx.x][1] = (active && q < np) ? si[q] : 0.0;
-            __syncthreads();
-            if (active && q < np && g == 0) {
-                double tr = 0.0, ti = 0.0;
-                for (int gg = 0; gg < groups; ++gg) {
-                    tr += red[gg * (P >= W_NT ? W_NT : P) + tpair][0];
-                    ti += red[gg * (P >= W_NT ? W_NT : P) + tpair][1];
-                }
-                const int a = pa[q], b = pb[q];
-                if (a == b) diag[a] = tr;
-                if (w1 && m > 0) {
-                    float2 *Rk = R + (long long)k * nel * nel;
-                    float2 r = Rk[a * nel + b];
-                    Rk[a * nel + b] = make_float2((float)((double)r.x + tr), (float)((double)r.y + ti));
-                    if (a != b) {
-                        r = Rk[b * nel + a];
-                        Rk[b * nel + a] = make_float2((float)((double)r.x + tr), (float)((double)r.y - ti));
-                    }
+        /* the groups' partials, then each tile entry summed over groups in order */
+        double *mine = red + (size_t)tid * TB * TB * 2;
+#pragma unroll
+        for (int r = 0; r < TB; ++r)
+#pragma unroll
+            for (int c = 0; c < TB; ++c) {
+                mine[2 * (r * TB + c)] = active ? sr[r][c] : 0.0;
+                mine[2 * (r * TB + c) + 1] = active ? si[r][c] : 0.0;
+            }
+        __syncthreads();
+        for (int idx = tid; idx < T * TB * TB; idx += W_NT) {
+            const int t = idx / (TB * TB), e = idx - t * TB * TB;
+            const int r = e / TB, c = e - r * TB;
+            int tA = 0, trem = t;
+            while (trem >= nb - tA) { trem -= nb - tA; ++tA; }
+            const int a = tA * TB + r, b = (tA + trem) * TB + c;
+            if (a >= nel || b >= nel || a > b) continue;
+            double tr = 0.0, ti = 0.0;
+            for (int gg = 0; gg < groups; ++gg) {
+                const double *p = red + (size_t)(gg * T + t) * TB * TB * 2;
+                tr += p[2 * e];
+                ti += p[2 * e + 1];
+            }
+            if (a == b) diag[a] = tr;
+            if (w1 && m > 0) {
+                float2 *Rk = R + (long long)k * nel * nel;
+                float2 v = Rk[a * nel + b];
+                Rk[a * nel + b] = make_float2((float)((double)v.x + tr), (float)((double)v.y + ti));
+                if (a != b) {
+                    v = Rk[b * nel + a];
+                    Rk[b * nel + a] = make_float2((float)((double)v.x + tr), (float)((double)v.y - ti));
                 }
             }
-            __syncthreads();
         }
-        if (threadIdx.x == 0) {
+        __syncthreads();
+        if (tid == 0) {
             if (w1) counts[k] += (uint32_t)m;
             if (w2) {
                 const double inv = m ? 1.0 / (double)m : 0.0;
@@ -125,16 +148,35 @@ __global__ void cov_reset_kernel(float2 *R, uint32_t *counts, int nel, int nchan
     }
 }
 
+
+template <int TB>
+int w12_launch(const void *out, unsigned nel, unsigned nchan, size_t m, const uint8_t *gate, void *R,
+               uint32_t *counts, float *pwr, float *mean_pwr, cudaStream_t s) {
+    static bool configured[64];
+    const size_t smem = (size_t)W_NT * TB * TB * 2 * sizeof(double);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        if (cudaFuncSetAttribute(w12_kernel<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return ATKB_E_KERNEL;
+        configured[dev] = true;
+    }
+    const int grid = (int)(nchan < 4096 ? nchan : 4096);
+    w12_kernel<TB><<<grid, W_NT, smem, s>>>((const float2 *)out, (int)nel, (int)nchan, (long long)m, gate,
+                                            (float2 *)R, counts, pwr, mean_pwr);
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
 }  // namespace
 
 extern "C" int atkb_w12(const void *out, unsigned nel, unsigned nchan, size_t m, const uint8_t *gate,
                         void *R, uint32_t *counts, float *pwr, float *mean_pwr, void *stream) {
     if (nel < 1 || nel > MAX_NEL || nchan < 1) return ATKB_E_ARG;
-    int grid = (int)(nchan < 4096 ? nchan : 4096);
-    w12_kernel<<<grid, W_NT, 0, (cudaStream_t)stream>>>((const float2 *)out, (int)nel, (int)nchan,
-                                                        (long long)m, gate, (float2 *)R, counts, pwr,
-                                                        mean_pwr);
-    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (nel == 1) return w12_launch<1>(out, nel, nchan, m, gate, R, counts, pwr, mean_pwr, s);
+    if (nel == 2) return w12_launch<2>(out, nel, nchan, m, gate, R, counts, pwr, mean_pwr, s);
+    return w12_launch<4>(out, nel, nchan, m, gate, R, counts, pwr, mean_pwr, s);
 }
 
 extern "C" int atkb_cov_reset(void *R, uint32_t *counts, unsigned nel, unsigned nchan,

@@ -3,6 +3,7 @@
     python -m atkdsp_b200.microbench --nchan 4096 --taps 16 --oversample 2
     python -m atkdsp_b200.microbench --sweep
     python -m atkdsp_b200.microbench --osx --nfft 4096 --channels 64
+    python -m atkdsp_b200.microbench --kernels
 
 Each configuration channelizes one device-resident block of 2^log2n cf32
 samples (seeded noise, larger than L2 at the default 2^24) through a
@@ -12,6 +13,13 @@ event pair, the median of the timed repetitions after two warm-ups. One JSON
 line per configuration: {"nchan", "taps", "oversample", "samples",
 "kernel_ms", "gsps", "hbm_gbs"} where hbm_gbs counts the algorithmic bytes
 (8 B in + 8*oversample B out per input sample).
+
+--kernels times the other device building blocks once each, on blocks
+larger than L2: unpack_dc of 2^25 ci16 samples (conversion + mean),
+block_mean alone, the one-pass W1/W2 over an 8-element 2048-channel output
+of 2048 hops, and the spectrum reduction / stats of 2^24 samples (n 4096,
+hop 2048, Hann). One JSON line per kernel: {"op", "ms", "gbs"} with gbs the
+algorithmic bytes (read + written once) per second.
 
 --osx times the overlap-save extractor instead: one device-resident cf32
 stream through atkdsp_gpu_osx_process_n with the extractor_channels plan of
@@ -87,6 +95,59 @@ def run_osx(nfft: int = 4096, channels: int = 64, log2n: int = 24, reps: int = 5
             "msps": round(nel * n / t / 1e3, 1), "out_samples": int(sum(counts)) * nel}
 
 
+def run_kernels(reps: int = 5) -> list:
+    import torch
+
+    from . import gpu
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    g = torch.Generator(device="cuda").manual_seed(5)
+    res = []
+    n = 1 << 25
+    raw = torch.randint(-2048, 2048, (2 * n,), dtype=torch.int16, device="cuda", generator=g)
+    out = torch.empty(n, dtype=torch.complex64, device="cuda")
+    mean = torch.empty(2, dtype=torch.float64, device="cuda")
+    t = timed(lambda: gpu.unpack_dc(raw, "ci16q11", 0.01 - 0.02j, out=out))
+    res.append({"op": "unpack_dc ci16q11 2^25", "ms": round(t, 4), "gbs": round(12 * n / t / 1e6, 1)})
+    t = timed(lambda: gpu.block_mean(raw, "ci16q11", 0.01 - 0.02j, mean))
+    res.append({"op": "block_mean ci16q11 2^25", "ms": round(t, 4), "gbs": round(4 * n / t / 1e6, 1)})
+    del raw, out
+    nel, M, m = 8, 2048, 2048
+    y = torch.randn(nel * M * m, dtype=torch.complex64, device="cuda", generator=g).view(nel, M, m)
+    R = torch.zeros((M, nel, nel), dtype=torch.complex64, device="cuda")
+    cnt = torch.zeros(M, dtype=torch.int32, device="cuda")
+    pwr = torch.zeros((nel, M), dtype=torch.float32, device="cuda")
+    mp = torch.zeros(M, dtype=torch.float32, device="cuda")
+    t = timed(lambda: gpu.accumulate(y, nel, M, R, cnt, pwr, mp))
+    res.append({"op": "W1+W2 one pass, 8 elements x 2048 channels x 2048 hops", "ms": round(t, 4),
+                "gbs": round(8 * nel * M * m / t / 1e6, 1)})
+    del y
+    xs = torch.randn(1 << 24, dtype=torch.complex64, device="cuda", generator=g)
+    k = np.arange(4096)
+    w = torch.from_numpy((0.5 - 0.5 * np.cos(2 * np.pi * k / 4095)).astype(np.float32)).cuda()
+    sp = gpu.Spectrum(4096)
+    t = timed(lambda: sp.reduce(xs, 2048, w, "avg"))
+    res.append({"op": "spectrum_reduce avg n4096 hop2048 2^24", "ms": round(t, 4),
+                "gbs": round(8 * (1 << 24) / t / 1e6, 1)})
+    t = timed(lambda: sp.stats(xs, 2048, w))
+    res.append({"op": "spectrum_stats n4096 hop2048 2^24", "ms": round(t, 4),
+                "gbs": round(8 * (1 << 24) / t / 1e6, 1)})
+    return res
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--nchan", type=int, default=1024)
@@ -97,11 +158,15 @@ def main(argv=None):
     ap.add_argument("--sweep", action="store_true",
                     help="nchan 64/256/1024/4096 x taps 8/12/16 x oversample 1/2")
     ap.add_argument("--osx", action="store_true", help="the overlap-save extractor instead")
+    ap.add_argument("--kernels", action="store_true", help="unpack, W1/W2 and spectrum kernels")
     ap.add_argument("--nfft", type=int, default=4096)
     ap.add_argument("--channels", type=int, default=64)
     ap.add_argument("--elements", type=int, default=1)
     a = ap.parse_args(argv)
-    if a.osx:
+    if a.kernels:
+        for r in run_kernels(a.reps):
+            print(json.dumps(r), flush=True)
+    elif a.osx:
         print(json.dumps(run_osx(a.nfft, a.channels, a.log2n, a.reps, a.elements)), flush=True)
     elif a.sweep:
         for M in (64, 256, 1024, 4096):
