@@ -6,7 +6,8 @@ atkdsp_b200``), a C-ABI library that exports the reference's
 The Python names, arguments, return shapes and errors below mirror the
 reference binding's (python/atkdsp/__init__.py: ``Pfb`` at :4159-4219,
 ``unpack`` / ``unpack_dc`` at :337-385, W1/W2 at :4222-4266, ``Osx`` at
-:4269-4342, identity at :285-313), so code and tests written against ``atkdsp`` read the same here.
+:4269-4342, ``Cfar`` / ``cfar_alpha`` / ``cfar_n_eff`` / ``cfar_window_rho2``
+at :2315-2541, identity at :285-313), so code and tests written against ``atkdsp`` read the same here.
 
 There is no CPU fallback: if the library is missing or no GPU is usable,
 ``load()`` / ``Pfb(...)`` raise ``AtkDspError``.
@@ -26,7 +27,10 @@ import numpy as np
 __all__ = ["ABI_VERSION", "AtkDspError", "load", "available", "lib_path", "version",
            "build_info", "set_threads", "get_threads", "FMT", "bytes_per_sample",
            "unpack", "unpack_dc", "Pfb", "pfb_cov_accumulate", "pfb_cov_reset",
-           "pfb_channel_power", "Osx"]
+           "pfb_channel_power", "Osx", "Cfar", "cfar_defaults", "cfar_alpha", "cfar_n_eff",
+           "cfar_window_rho2", "CFAR_MODES", "CFAR_OPEN", "CFAR_UPDATE", "CFAR_CLOSE",
+           "CFAR_T0_COARSE", "CFAR_T1_COARSE", "CFAR_EDGE", "CFAR_MASK_ADJ", "CFAR_FLUSHED",
+           "E_EMPTY"]
 
 #: the ABI the library reports (the reference's, include/atkdsp.h:63)
 ABI_VERSION = 26
@@ -35,7 +39,8 @@ FMT = {"cu8": 0, "ci8": 1, "ci16": 2, "ci16_le": 2, "cs16": 2,
        "ci16q11": 3, "cf32": 4, "cf32_le": 4}
 
 _ERRORS = {-1: "bad argument", -2: "out of memory", -3: "output buffer too small",
-           -4: "FFT backend failure"}
+           -4: "FFT backend failure", -7: "nothing to return"}
+E_EMPTY = -7
 
 HERE = Path(__file__).resolve().parent
 LIB_FILE = HERE / "lib" / "libatkdsp_b200.so"
@@ -50,6 +55,31 @@ class AtkDspError(RuntimeError):
 
 class _Cf32(C.Structure):
     _fields_ = [("re", C.c_float), ("im", C.c_float)]
+
+
+class _CfarConfig(C.Structure):
+    """atkdsp_cfar_config (96 bytes)"""
+    _fields_ = [("mode", C.c_int32), ("n_ref", C.c_int32), ("n_guard", C.c_int32),
+                ("k_frames", C.c_int32), ("pfa", C.c_double), ("looks", C.c_double),
+                ("os_k", C.c_int32), ("open_m", C.c_int32), ("open_n", C.c_int32),
+                ("close_k", C.c_int32), ("merge_gap", C.c_int32), ("min_bins", C.c_int32),
+                ("max_tracks", C.c_int32), ("reserved", C.c_int32), ("rho2", C.c_double * 4)]
+
+
+class _CfarEvent(C.Structure):
+    """atkdsp_cfar_event (64 bytes)"""
+    _fields_ = [("t0", C.c_double), ("t1", C.c_double), ("fc_bin", C.c_double),
+                ("type", C.c_int32), ("id", C.c_uint32), ("flags", C.c_uint32),
+                ("lo_bin", C.c_int32), ("hi_bin", C.c_int32), ("n_hits", C.c_int32),
+                ("level_db", C.c_float), ("noise_db", C.c_float), ("snr_db", C.c_float),
+                ("band_snr_db", C.c_float)]
+
+
+class _CfarCounters(C.Structure):
+    """atkdsp_cfar_counters (88 bytes)"""
+    _fields_ = [(n, C.c_uint64) for n in
+                ("frames", "warmup", "cells_tested", "cell_hits", "untestable",
+                 "opened", "closed", "updates", "dropped", "resets", "tracks")]
 
 
 def _check(rc: int, what: str) -> int:
@@ -124,6 +154,22 @@ def _bind(lib) -> None:
         "atkdsp_gpu_spectrum_destroy": ([vp], None),
         "atkdsp_gpu_spectrum_reduce": ([vp, vp, sz, sz, vp, C.c_int, vp, vp], ssz),
         "atkdsp_gpu_spectrum_stats": ([vp, vp, sz, sz, vp, vp, vp, vp, vp, vp], ssz),
+        "atkdsp_cfar_defaults": ([P(_CfarConfig)], None),
+        "atkdsp_cfar_alpha": ([C.c_int, C.c_int, d, d, C.c_int, P(d), P(d), P(d)], C.c_int),
+        "atkdsp_cfar_n_eff": ([C.c_int, P(d)], d),
+        "atkdsp_cfar_window_rho2": ([P(C.c_float), sz, P(d)], C.c_int),
+        "atkdsp_cfar_create": ([sz, P(_CfarConfig)], vp),
+        "atkdsp_cfar_destroy": ([vp], None),
+        "atkdsp_cfar_reset": ([vp], None),
+        "atkdsp_cfar_set_mask": ([vp, P(C.c_uint8)], C.c_int),
+        "atkdsp_cfar_events_max": ([vp, sz], sz),
+        "atkdsp_cfar_process": ([vp, P(C.c_float), sz, d, d, P(_CfarEvent), sz], ssz),
+        "atkdsp_cfar_flush": ([vp, P(_CfarEvent), sz], ssz),
+        "atkdsp_cfar_last": ([vp, P(C.c_float), P(C.c_float), P(C.c_uint8)], C.c_int),
+        "atkdsp_cfar_info": ([vp, P(d), P(d), P(d), P(_CfarConfig)], C.c_int),
+        "atkdsp_cfar_describe": ([vp, C.c_char_p, sz], C.c_int),
+        "atkdsp_cfar_stats": ([vp, P(_CfarCounters)], C.c_int),
+        "atkdsp_gpu_cfar_process": ([vp, vp, C.c_int, sz, d, d, P(_CfarEvent), sz, vp, vp], ssz),
         "atkdsp_gpu_tune_set": ([u, u, u, C.c_int], C.c_int),
         "atkdsp_gpu_tune_get": ([u, u, u], C.c_int),
     }
@@ -446,3 +492,166 @@ def pfb_channel_power(out, nel, nchan):
                                  pwr.ctypes.data_as(C.POINTER(C.c_float)),
                                  meanp.ctypes.data_as(C.POINTER(C.c_float)))
     return pwr.reshape(nel, nchan), meanp
+
+
+# ---- CFAR across frequency and the burst tracker ---------------------------
+
+CFAR_MODES = {"ca": 0, "os": 1, "go": 2, "so": 3}
+CFAR_OPEN, CFAR_UPDATE, CFAR_CLOSE = 1, 2, 3
+CFAR_T0_COARSE, CFAR_T1_COARSE, CFAR_EDGE, CFAR_MASK_ADJ, CFAR_FLUSHED = 1, 2, 4, 8, 16
+
+
+def cfar_defaults() -> dict:
+    """The default atkdsp_cfar_config as a dict (rho2 a 4-tuple)."""
+    k = _CfarConfig()
+    load().atkdsp_cfar_defaults(C.byref(k))
+    d = {n: getattr(k, n) for n, _t in _CfarConfig._fields_ if n != "reserved"}
+    d["rho2"] = tuple(float(v) for v in k.rho2)
+    return d
+
+
+def _rho2_arg(rho2):
+    if rho2 is None:
+        return None
+    v = [float(x) for x in rho2]
+    if len(v) != 4:
+        raise AtkDspError(f"rho2 needs 4 values, got {len(v)}")
+    return (C.c_double * 4)(*v)
+
+
+def cfar_alpha(mode, n_ref: int, pfa: float, looks: float = 1.0, os_k: int = 0, rho2=None) -> tuple:
+    """(alpha, E[T]): the CFAR threshold multiplier solved for `pfa` per cell."""
+    m = CFAR_MODES.get(mode, mode) if isinstance(mode, str) else int(mode)
+    a, et = C.c_double(), C.c_double()
+    _check(load().atkdsp_cfar_alpha(int(m), int(n_ref), float(pfa), float(looks), int(os_k),
+                                    _rho2_arg(rho2), C.byref(a), C.byref(et)), "cfar_alpha")
+    return a.value, et.value
+
+
+def cfar_n_eff(n_ref: int, rho2=None) -> float:
+    """Equivalent independent cells among 2 n_ref correlated ones."""
+    return float(load().atkdsp_cfar_n_eff(int(n_ref), _rho2_arg(rho2)))
+
+
+def cfar_window_rho2(window) -> tuple:
+    """The power correlation of bins 1..4 apart through `window`."""
+    w = np.ascontiguousarray(window, np.float32)
+    out = (C.c_double * 4)()
+    _check(load().atkdsp_cfar_window_rho2(w.ctypes.data_as(C.POINTER(C.c_float)), w.size, out),
+           "cfar_window_rho2")
+    return tuple(float(v) for v in out)
+
+
+def _cfar_event_dict(e) -> dict:
+    return {"type": int(e.type), "id": int(e.id), "flags": int(e.flags), "lo": int(e.lo_bin),
+            "hi": int(e.hi_bin), "n_hits": int(e.n_hits), "t0": float(e.t0),
+            "t1": float(e.t1), "fc_bin": float(e.fc_bin), "level_db": float(e.level_db),
+            "noise_db": float(e.noise_db), "snr_db": float(e.snr_db),
+            "band_snr_db": float(e.band_snr_db)}
+
+
+class Cfar:
+    """CFAR across frequency and the burst tracker. Options are the
+    atkdsp_cfar_config fields as keywords (mode may be 'ca' / 'os' / 'go' /
+    'so'). process() returns the OPEN / UPDATE / CLOSE events as dicts. The
+    per-cell work of each call runs on the GPU; the tracker on the host."""
+
+    def __init__(self, nbins: int, **cfg):
+        self._lib = load()
+        c = cfar_defaults()
+        for key, v in cfg.items():
+            if key not in c:
+                raise AtkDspError(f"unknown CFAR option {key!r}; known: {sorted(c)}")
+            c[key] = CFAR_MODES.get(v, v) if key == "mode" and isinstance(v, str) else v
+        k = _CfarConfig()
+        for key, v in c.items():
+            if key == "rho2":
+                k.rho2 = (C.c_double * 4)(*[float(x) for x in v])
+            else:
+                setattr(k, key, float(v) if key in ("pfa", "looks") else int(v))
+        self.nbins = int(nbins)
+        self._h = self._lib.atkdsp_cfar_create(self.nbins, C.byref(k))
+        if not self._h:
+            raise AtkDspError(f"cfar_create({nbins} bins, {c}) refused: a configuration outside the "
+                              "ranges, a threshold that could not be solved, or no GPU memory")
+        self._buf = None
+        a, ac, et, rc = C.c_double(), C.c_double(), C.c_double(), _CfarConfig()
+        self._lib.atkdsp_cfar_info(self._h, C.byref(a), C.byref(ac), C.byref(et), C.byref(rc))
+        self.alpha, self.alpha_ca, self.et = a.value, ac.value, et.value
+        self.cfg = {n: getattr(rc, n) for n, _t in _CfarConfig._fields_ if n != "reserved"}
+        self.cfg["rho2"] = tuple(float(v) for v in rc.rho2)
+        self.n_eff = cfar_n_eff(self.cfg["n_ref"], self.cfg["rho2"])
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            self._lib.atkdsp_cfar_destroy(h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def describe(self) -> str:
+        buf = C.create_string_buffer(1024)
+        self._lib.atkdsp_cfar_describe(self._h, buf, 1024)
+        return buf.value.decode()
+
+    def stats(self) -> dict:
+        s = _CfarCounters()
+        self._lib.atkdsp_cfar_stats(self._h, C.byref(s))
+        return {n: int(getattr(s, n)) for n, _t in s._fields_}
+
+    def reset(self) -> None:
+        self._lib.atkdsp_cfar_reset(self._h)
+
+    def set_mask(self, mask) -> None:
+        if mask is None:
+            self._lib.atkdsp_cfar_set_mask(self._h, None)
+            return
+        m = np.ascontiguousarray(np.asarray(mask).ravel() != 0, dtype=np.uint8)
+        if m.size != self.nbins:
+            raise AtkDspError(f"mask has {m.size} entries; the CFAR has {self.nbins} bins")
+        _check(self._lib.atkdsp_cfar_set_mask(self._h, m.ctypes.data_as(C.POINTER(C.c_uint8))),
+               "cfar_set_mask")
+
+    def events_max(self, nframes: int) -> int:
+        return int(self._lib.atkdsp_cfar_events_max(self._h, int(nframes)))
+
+    def _events(self, nf):
+        cap = self.events_max(nf)
+        if self._buf is None or len(self._buf) < cap:
+            self._buf = (_CfarEvent * max(cap, 1))()
+        return cap
+
+    def process(self, frames_db, frame_t0: float, frame_dt: float) -> list:
+        f = np.ascontiguousarray(frames_db, dtype=np.float32)
+        if f.ndim == 1:
+            f = f.reshape(1, -1)
+        if f.ndim != 2 or f.shape[1] != self.nbins:
+            raise AtkDspError(f"frames must be (nframes, {self.nbins}); got {f.shape}")
+        nf = f.shape[0]
+        cap = self._events(nf)
+        n = _check(self._lib.atkdsp_cfar_process(self._h, f.ctypes.data_as(C.POINTER(C.c_float)), nf,
+                                                 float(frame_t0), float(frame_dt), self._buf, cap),
+                   "cfar_process")
+        return [_cfar_event_dict(self._buf[j]) for j in range(n)]
+
+    def flush(self) -> list:
+        cap = int(self.cfg["max_tracks"])
+        buf = (_CfarEvent * cap)()
+        n = _check(self._lib.atkdsp_cfar_flush(self._h, buf, cap), "cfar_flush")
+        return [_cfar_event_dict(buf[j]) for j in range(n)]
+
+    def last(self):
+        """(averaged power dB, threshold dB (NaN untested), hits) of the last
+        tested frame, or None before one."""
+        a = np.empty(self.nbins, np.float32)
+        t = np.empty(self.nbins, np.float32)
+        h = np.empty(self.nbins, np.uint8)
+        P = C.POINTER
+        rc = self._lib.atkdsp_cfar_last(self._h, a.ctypes.data_as(P(C.c_float)),
+                                        t.ctypes.data_as(P(C.c_float)), h.ctypes.data_as(P(C.c_uint8)))
+        if rc == E_EMPTY:
+            return None
+        _check(rc, "cfar_last")
+        return a, t, h

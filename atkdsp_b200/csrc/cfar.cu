@@ -1,0 +1,151 @@
+/* The CFAR detector's per-cell work on sm_100a (reference src/cfar.c:524-592,
+ * the first half of one_frame): the conversion of each frame to linear power,
+ * the average over k_frames frames, and each bin's test against alpha x T.
+ *
+ * One call covers every frame a process call brings, as a grid of (bins x
+ * frames): the per-cell work of different frames is independent once the raw
+ * ring holds the k - 1 frames before them. Every sum runs in the reference's
+ * order (the k frames oldest first; the reference cells in table order), so
+ * X, T and the threshold differ from the reference's only where the device
+ * exp rounds the dB conversion differently in the last bit.
+ *
+ * The reference-cell table is cell-major (idx[q * nbins + i]), so the threads
+ * of a warp, one bin each, read one table row with coalesced loads; the
+ * frame's X row they index stays in L1 / L2.
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "internal.h"
+
+namespace {
+
+constexpr double kLn10Over10 = 0.23025850929940458;   /* ln(10) / 10 */
+constexpr int kThreads = 256;
+
+__global__ void __launch_bounds__(kThreads) cfar_raw_kernel(const float *__restrict__ frames, int units,
+                                                            long long f0, int nf, long long nbins,
+                                                            double *__restrict__ raw, int ring) {
+    const long long total = (long long)nf * nbins;
+    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < total;
+         e += (long long)gridDim.x * kThreads) {
+        const long long j = e / nbins, i = e - j * nbins;
+        double v = (double)frames[e];
+        if (units == 0) {
+            if (v < -300.0) v = -300.0;
+            v = exp(v * kLn10Over10);
+        } else if (v < 1e-30) {
+            v = 1e-30;
+        }
+        raw[((f0 + j) % ring) * nbins + i] = v;
+    }
+}
+
+/* X row of frame f: the mean of raw rows f-k+1 .. f, oldest first */
+__global__ void __launch_bounds__(kThreads) cfar_mean_kernel(const double *__restrict__ raw, int ring, long long f0,
+                                                             long long t0, long long nbins, int k,
+                                                             double *__restrict__ X) {
+    const long long i = (long long)blockIdx.x * kThreads + threadIdx.x;
+    const long long f = t0 + blockIdx.y;
+    if (i >= nbins) return;
+    double s = 0.0;
+    for (int r = 0; r < k; ++r) s = __dadd_rn(s, raw[((f - k + 1 + r) % ring) * nbins + i]);
+    X[(f - f0) * nbins + i] = __ddiv_rn(s, (double)k);
+}
+
+__global__ void __launch_bounds__(kThreads) cfar_cell_kernel(long long f0, long long t0, long long nbins, int mode,
+                                                             int n_ref, int N, int os_k, double alpha,
+                                                             double alpha_ca, double et,
+                                                             const uint8_t *__restrict__ ok,
+                                                             const uint8_t *__restrict__ sided,
+                                                             const int32_t *__restrict__ idx,
+                                                             const double *__restrict__ X,
+                                                             double *__restrict__ noise, double *__restrict__ thr,
+                                                             uint8_t *__restrict__ hits) {
+    const long long i = (long long)blockIdx.x * kThreads + threadIdx.x;
+    const long long row = (t0 - f0 + blockIdx.y) * nbins;
+    if (i >= nbins) return;
+    if (!ok[i]) {
+        noise[row + i] = CUDART_NAN;
+        thr[row + i] = CUDART_NAN;
+        hits[row + i] = 0;
+        return;
+    }
+    const double *Xr = X + row;
+    double Z, a = alpha, scale = et;
+    if (mode == 1) {
+        /* the os_k-th smallest: the value v with #(< v) <= os_k - 1 < #(<= v);
+         * a NaN among the cells makes T NaN */
+        bool has_nan = false;
+        for (int q = 0; q < N; ++q) has_nan |= isnan(Xr[idx[(long long)q * nbins + i]]);
+        Z = CUDART_NAN;
+        if (!has_nan) {
+            const int want = os_k - 1;
+            for (int q = 0; q < N; ++q) {
+                const double v = Xr[idx[(long long)q * nbins + i]];
+                int lt = 0, le = 0;
+                for (int p = 0; p < N; ++p) {
+                    const double w = Xr[idx[(long long)p * nbins + i]];
+                    lt += w < v;
+                    le += w <= v;
+                }
+                if (lt <= want && want < le) {
+                    Z = v;
+                    break;
+                }
+            }
+        }
+    } else if ((mode == 2 || mode == 3) && sided[i]) {
+        double L = 0.0, R = 0.0;
+        for (int q = 0; q < n_ref; ++q) L = __dadd_rn(L, Xr[idx[(long long)q * nbins + i]]);
+        for (int q = n_ref; q < N; ++q) R = __dadd_rn(R, Xr[idx[(long long)q * nbins + i]]);
+        L = __ddiv_rn(L, (double)n_ref);
+        R = __ddiv_rn(R, (double)n_ref);
+        if (isnan(L) || isnan(R)) Z = CUDART_NAN;
+        else Z = mode == 2 ? (L > R ? L : R) : (L < R ? L : R);
+    } else {
+        double s = 0.0;
+        for (int q = 0; q < N; ++q) s = __dadd_rn(s, Xr[idx[(long long)q * nbins + i]]);
+        Z = __ddiv_rn(s, (double)N);
+        if (mode == 2 || mode == 3) {
+            a = alpha_ca;
+            scale = 1.0;
+        }
+    }
+    const double t = __dmul_rn(a, Z);
+    thr[row + i] = t;
+    noise[row + i] = __ddiv_rn(Z, scale);
+    hits[row + i] = Xr[i] > t;
+}
+
+int grid_for(long long work) {
+    long long g = (work + kThreads - 1) / kThreads;
+    return (int)(g < 148LL * 16 ? (g < 1 ? 1 : g) : 148LL * 16);
+}
+
+}  // namespace
+
+extern "C" int atkb_cfar_raw(const float *frames, int units, long long f0, int nf, long long nbins, double *raw,
+                             int ring, void *stream) {
+    if (nf <= 0) return ATKB_OK;
+    cfar_raw_kernel<<<grid_for((long long)nf * nbins), kThreads, 0, (cudaStream_t)stream>>>(frames, units, f0, nf,
+                                                                                             nbins, raw, ring);
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
+extern "C" int atkb_cfar_test(const double *raw, int ring, long long f0, long long t0, int nf, long long nbins,
+                              int k, int mode, int n_ref, int n_cells, int os_k, double alpha, double alpha_ca,
+                              double et, const uint8_t *ok, const uint8_t *sided, const int32_t *idx, double *X,
+                              double *noise, double *thr, uint8_t *hits, void *stream) {
+    const long long ntest = f0 + nf - t0;
+    if (ntest <= 0) return ATKB_OK;
+    if (ntest > 65535 || nbins <= 0) return ATKB_E_ARG;
+    const dim3 grid((unsigned)((nbins + kThreads - 1) / kThreads), (unsigned)ntest);
+    cudaStream_t s = (cudaStream_t)stream;
+    cfar_mean_kernel<<<grid, kThreads, 0, s>>>(raw, ring, f0, t0, nbins, k, X);
+    cfar_cell_kernel<<<grid, kThreads, 0, s>>>(f0, t0, nbins, mode, n_ref, n_cells, os_k, alpha, alpha_ca, et, ok,
+                                               sided, idx, X, noise, thr, hits);
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}

@@ -264,6 +264,23 @@ int  atkb_spec_launch(int mode, const void *in, long long frames, long long hop,
                       const void *tw, int nblk, int per, void *part, float *o0, float *o1, float *o2,
                       float *o3, void *stream);
 
+/* CFAR cell test ------------------------------------------------------------
+ * Frames f0 .. f0+nf-1 (absolute frame numbers since reset) of nbins powers
+ * each; raw is a ring of `ring` rows (frame F in row F % ring).
+ * atkb_cfar_raw: raw[F] = linear power of frames[f - f0] (units 0: dB, read
+ * as exp(v ln10/10) with v clamped at -300; 1: linear, clamped at 1e-30).
+ * atkb_cfar_test: for the frames f >= t0 (t0 >= f0 + k - 1), X = the mean of
+ * raw rows f-k+1 .. f (oldest first), then each testable bin's statistic over
+ * its n_cells reference cells (idx: n_cells x nbins, cell-major) and the
+ * test; X, noise, thr (double) and hits (u8) rows go to row f - f0 of the
+ * outputs (frames below t0 are left alone). */
+int  atkb_cfar_raw(const float *frames, int units, long long f0, int nf, long long nbins, double *raw, int ring,
+                   void *stream);
+int  atkb_cfar_test(const double *raw, int ring, long long f0, long long t0, int nf, long long nbins, int k,
+                    int mode, int n_ref, int n_cells, int os_k, double alpha, double alpha_ca, double et,
+                    const uint8_t *ok, const uint8_t *sided, const int32_t *idx, double *X, double *noise,
+                    double *thr, uint8_t *hits, void *stream);
+
 /* unpack ------------------------------------------------------------------- */
 /* device raw -> device cf32 (out may be NULL: mean only), (x - c) * k per component; the means (double,
  * BEFORE subtraction of the offset, i.e. sum(out)/n + off) go to d_mean[0..1]

@@ -13,9 +13,9 @@ import ctypes as C
 
 import torch
 
-from . import AtkDspError, Pfb, _check, _fmt, bytes_per_sample, load
+from . import AtkDspError, Cfar, Pfb, _cfar_event_dict, _check, _fmt, bytes_per_sample, load
 
-__all__ = ["Spectrum", "process_n", "process_n_raw", "unpack_dc", "unpack", "block_mean", "accumulate",
+__all__ = ["Spectrum", "cfar_process", "process_n", "process_n_raw", "unpack_dc", "unpack", "block_mean", "accumulate",
            "cov_accumulate", "channel_power", "Batch", "sync"]
 
 
@@ -256,3 +256,32 @@ class Spectrum:
         res = {k: v for k, v in outs.items() if v is not None}
         res["frames"] = int(fr)
         return res
+
+
+def cfar_process(c: Cfar, frames: torch.Tensor, frame_t0: float, frame_dt: float, units: str = "db",
+                 hits: bool | torch.Tensor = False, stream=None):
+    """atkdsp_gpu_cfar_process: the CFAR and tracker over device frames
+    (nframes, nbins) float32, in dB (units "db", as atkdsp_cfar_process takes
+    them) or linear power ("linear": W2's channel powers as they come).
+    Returns (events, hit masks): with hits=True (or a uint8 device tensor of
+    the frames' shape) every frame's hit mask stays on the device, ready as
+    the W1 gate of that frame; otherwise None. `stream`: the frames'
+    producer, waited for on the device (None: the legacy default stream)."""
+    f = frames if frames.dim() == 2 else frames.reshape(1, -1)
+    if f.dtype != torch.float32 or f.shape[1] != c.nbins:
+        raise AtkDspError(f"frames must be float32 (nframes, {c.nbins}); got {f.dtype} {tuple(f.shape)}")
+    if units not in ("db", "linear"):
+        raise AtkDspError(f"units must be 'db' or 'linear', not {units!r}")
+    h = None
+    if isinstance(hits, torch.Tensor):
+        h = hits
+        if h.dtype != torch.uint8 or h.shape != f.shape:
+            raise AtkDspError("hits must be a uint8 tensor of the frames' shape")
+    elif hits:
+        h = torch.empty(f.shape, dtype=torch.uint8, device=f.device)
+    nf = f.shape[0]
+    cap = c._events(nf)
+    n = _check(load().atkdsp_gpu_cfar_process(c.handle, _ptr(f), 0 if units == "db" else 1, nf,
+                                              float(frame_t0), float(frame_dt), c._buf, cap, _ptr(h),
+                                              _stream(stream)), "gpu_cfar_process")
+    return [_cfar_event_dict(c._buf[j]) for j in range(n)], h

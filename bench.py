@@ -723,6 +723,56 @@ def _spectrum_arm(torch, device, steps, cpu: bool):
     return res
 
 
+def _cfar_arm(torch, device, steps, cpu: bool):
+    """The CFAR detector and tracker over spectrum lines: 4096 bins, 1024
+    frames per call (gamma noise floor with a slope, 64 bursts), CA with 16 +
+    16 reference cells, 4 guard, k_frames 4, Pfa 1e-6. value: device frames
+    (atkdsp_gpu_cfar_process, events to the host); gate: the same with every
+    frame's hit mask kept on the device; e2e: host frames through
+    atkdsp_cfar_process; cpu: the reference's atkdsp_cfar_process (one
+    thread: it has no threading) on 128 frames."""
+    import atkdsp_b200 as ak
+    from atkdsp_b200.gpu import cfar_process
+    from oracle import oracle as O
+    nb, nf = 4096, 1024
+    rng = np.random.default_rng(21)
+    floor = rng.gamma(1.0, 1.0, size=(nf, nb)) * np.linspace(1.0, 2.0, nb)[None, :]
+    for _ in range(64):
+        lo, f0 = int(rng.integers(0, nb - 8)), int(rng.integers(0, nf - 8))
+        floor[f0:f0 + int(rng.integers(4, 200)), lo:lo + int(rng.integers(1, 8))] += 10 ** rng.uniform(1, 3)
+    xs = (10.0 * np.log10(floor)).astype(np.float32)
+    cfg = dict(k_frames=4)
+    d = torch.from_numpy(xs).to(device)
+    hits = torch.empty(d.shape, dtype=torch.uint8, device=device)
+    res = {"workload": "cfar_ca_4096bins_1024frames_k4", "unit": "Mcells/s",
+           "path": "atkdsp_gpu_cfar_process (device frames) / atkdsp_cfar_process (host frames)"}
+    for name, fn in (("value", lambda c: cfar_process(c, d, 0.0, 1e-3)),
+                     ("gate", lambda c: cfar_process(c, d, 0.0, 1e-3, hits=hits)),
+                     ("e2e", lambda c: c.process(xs, 0.0, 1e-3))):
+        c = ak.Cfar(nb, **cfg)
+        for _ in range(2):
+            fn(c)
+        n = max(steps, 1)
+        t0 = time.perf_counter()
+        for _ in range(n):
+            ev = fn(c)
+        dt = time.perf_counter() - t0
+        res[name] = round(nb * nf * n / dt / 1e6, 1)
+        res[f"{name}_events_per_call"] = len(ev[0] if isinstance(ev, tuple) else ev)
+    res["frames_per_s"] = round(res["value"] * 1e6 / nb, 0)
+    if cpu:
+        ref = O.reference()
+        if ref is not None:
+            rc = O.RefCfar(ref, nb, **cfg)
+            rc.process(xs[:16], 0.0, 1e-3)
+            t0 = time.perf_counter()
+            rc.process(xs[16:144], 0.0, 1e-3)
+            res["cpu_baseline"] = {"value": round(nb * 128 / (time.perf_counter() - t0) / 1e6, 2),
+                                   "unit": "Mcells/s", "cores": 1, "kind": "reference",
+                                   "sample": "128 frames of the same workload"}
+    return res
+
+
 def _served_arm(torch, device, duration_s):
     """Serving: 4096 live streams at {2.4, 10, 40} MS/s delivering 1.6 ms ci16
     blocks with Poisson arrivals, nchan {256, 1024}, 16 taps, 2x, churn 20/s,
@@ -838,6 +888,8 @@ def run_ours(args, rep):
                                                           "cpu" in arms and not args.no_cpu)),
                          ("spectrum", lambda: _spectrum_arm(torch, device, args.steps,
                                                             "cpu" in arms and not args.no_cpu)),
+                         ("cfar", lambda: _cfar_arm(torch, device, args.steps,
+                                                    "cpu" in arms and not args.no_cpu)),
                          ("served", lambda: _served_arm(torch, device, 3.0))):
             if name in arms:
                 try:
@@ -906,7 +958,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--arms", default="batched,plain,e2e,dropin,cpu,single_stream,front_end,coherent_array,"
-                    "extractor,scale_bank,spectrum,served",
+                    "extractor,scale_bank,spectrum,cfar,served",
                     help="comma list of arms to run (the batched arm always runs)")
     ap.add_argument("--streams", type=int, default=256)
     ap.add_argument("--min-log2", type=float, default=14.0)

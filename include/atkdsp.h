@@ -4,8 +4,9 @@
  * This header declares exactly the entry points of the reference's ABI
  * (include/atkdsp.h of atkdsp 0.25.1, ABI 26) that the polyphase-filterbank
  * path uses: identity, threads, the unpack front end, the atkdsp_pfb_* handle
- * API and the W1/W2 accumulators, and the channelizer's other tool, the
- * overlap-save extractor (atkdsp_osx_*). Names, types, argument meaning, return
+ * API and the W1/W2 accumulators, the channelizer's other tool, the
+ * overlap-save extractor (atkdsp_osx_*), and the CFAR detector and burst
+ * tracker that gates W1 on W2's powers (atkdsp_cfar_*). Names, types, argument meaning, return
  * codes and the channel-major output layout are the reference's, so a caller
  * of the reference (its ctypes binding, a C program, the in-library survey)
  * links against this library unchanged for this path. Each declaration cites
@@ -48,6 +49,8 @@ extern "C" {
 #define ATKDSP_E_NOMEM      -2   /* allocation failed (host or device)            */
 #define ATKDSP_E_CAP        -3   /* caller's output buffer too small              */
 #define ATKDSP_E_FFT        -4   /* the transform failed: a GPU launch or kernel error */
+/* reference include/atkdsp.h:210 */
+#define ATKDSP_E_EMPTY      -7   /* nothing there to return (atkdsp_cfar_last)    */
 
 /* reference include/atkdsp.h:213 -- complex float32, numpy complex64 layout */
 typedef struct { float re, im; } atkdsp_cf32;
@@ -145,6 +148,99 @@ ATKDSP_API ptrdiff_t   atkdsp_osx_process_n(atkdsp_osx *x, const atkdsp_cf32 *co
                                             atkdsp_cf32 *const *outs, size_t *out_counts,
                                             size_t cap_each);                             /* :3285 */
 ATKDSP_API int         atkdsp_osx_describe(const atkdsp_osx *x, char *buf, size_t cap);  /* :3289 */
+
+/* ---- CFAR across frequency and the burst tracker: reference
+ * include/atkdsp.h:1821-1924 ------------------------------------------------
+ * Each frame (nbins powers in dB) is converted to linear power, averaged over
+ * k_frames frames, and every unmasked bin is tested against alpha x T, T the
+ * CA / OS / GO / SO statistic of its 2 n_ref reference cells beyond n_guard
+ * guard cells (a side that runs short at an edge or a mask borrows from the
+ * other). alpha is solved for the per-cell false-alarm rate. Hit bins merge
+ * into blobs, blobs into tracks, tracks report OPEN / UPDATE / CLOSE events.
+ * Here the per-cell work of a whole call (conversion, average, statistic,
+ * test) runs on the GPU in one pass over all its frames; the tracker walks
+ * the hit rows on the host in frame order. The layouts of the three structs
+ * are the reference's (96, 64 and 88 bytes as compiled; the reference's
+ * own comment on the config says 104). */
+#define ATKDSP_CFAR_CA 0
+#define ATKDSP_CFAR_OS 1
+#define ATKDSP_CFAR_GO 2
+#define ATKDSP_CFAR_SO 3
+#define ATKDSP_CFAR_OPEN   1
+#define ATKDSP_CFAR_UPDATE 2
+#define ATKDSP_CFAR_CLOSE  3
+#define ATKDSP_CFAR_T0_COARSE 1u
+#define ATKDSP_CFAR_T1_COARSE 2u
+#define ATKDSP_CFAR_EDGE      4u
+#define ATKDSP_CFAR_MASK_ADJ  8u
+#define ATKDSP_CFAR_FLUSHED  16u
+#define ATKDSP_CFAR_EDGE_PFA 1e-3
+#define ATKDSP_CFAR_RHO_MAX  4
+
+typedef struct {                                                                          /* :1836 */
+    int32_t mode;        /* ATKDSP_CFAR_CA (default) / OS / GO / SO           */
+    int32_t n_ref;       /* reference cells each side, 1..256 (16)            */
+    int32_t n_guard;     /* guard cells each side, 0..256 (4)                 */
+    int32_t k_frames;    /* frames averaged before testing, 1..64 (1)         */
+    double  pfa;         /* per cell per frame, 1e-15..0.5 (1e-6)             */
+    double  looks;       /* periodograms averaged into one frame, 0.25..1e4 (1) */
+    int32_t os_k;        /* OS rank 1..2 n_ref; 0 = ceil(3N/4)                */
+    int32_t open_m;      /* open after open_m hit frames ... (2)              */
+    int32_t open_n;      /* ... in the last open_n, 1..64 (3)                 */
+    int32_t close_k;     /* close after close_k misses in a row, 1..1000 (3)  */
+    int32_t merge_gap;   /* non-hit bins inside one detection (1)             */
+    int32_t min_bins;    /* narrower blobs ignored (1)                        */
+    int32_t max_tracks;  /* pending + open at once, 1..65536 (256)            */
+    int32_t reserved;
+    double  rho2[4];     /* power correlation of bins 1..4 apart, [0, 1)      */
+} atkdsp_cfar_config;
+
+typedef struct {                                                                          /* :1856 */
+    double   t0, t1;     /* seconds; t1 NaN until CLOSE                       */
+    double   fc_bin;     /* excess-weighted centroid, fractional bin          */
+    int32_t  type;       /* OPEN / UPDATE / CLOSE                             */
+    uint32_t id;         /* unique per handle (from 1)                        */
+    uint32_t flags;
+    int32_t  lo_bin, hi_bin;
+    int32_t  n_hits;     /* frames with a hit                                 */
+    float    level_db, noise_db, snr_db, band_snr_db;
+} atkdsp_cfar_event;
+
+typedef struct {                                                                          /* :1867 */
+    uint64_t frames, warmup;
+    uint64_t cells_tested, cell_hits, untestable;
+    uint64_t opened, closed, updates;
+    uint64_t dropped;
+    uint64_t resets;
+    uint64_t tracks;
+} atkdsp_cfar_counters;
+
+typedef struct atkdsp_cfar atkdsp_cfar;
+ATKDSP_API void         atkdsp_cfar_defaults(atkdsp_cfar_config *cfg);                  /* :1877 */
+ATKDSP_API int          atkdsp_cfar_alpha(int mode, int n_ref, double pfa, double looks,
+                                          int os_k, const double *rho2,
+                                          double *alpha, double *et);                    /* :1882 */
+ATKDSP_API double       atkdsp_cfar_n_eff(int n_ref, const double *rho2);                /* :1888 */
+ATKDSP_API int          atkdsp_cfar_window_rho2(const float *window, size_t n,
+                                                double *rho2);                           /* :1892 */
+ATKDSP_API atkdsp_cfar *atkdsp_cfar_create(size_t nbins, const atkdsp_cfar_config *cfg); /* :1894 */
+ATKDSP_API void         atkdsp_cfar_destroy(atkdsp_cfar *c);                             /* :1895 */
+ATKDSP_API void         atkdsp_cfar_reset(atkdsp_cfar *c);                               /* :1897 */
+ATKDSP_API int          atkdsp_cfar_set_mask(atkdsp_cfar *c, const uint8_t *mask);       /* :1900 */
+ATKDSP_API size_t       atkdsp_cfar_events_max(const atkdsp_cfar *c, size_t nframes);    /* :1901 */
+ATKDSP_API ptrdiff_t    atkdsp_cfar_process(atkdsp_cfar *c, const float *frames_db,
+                                            size_t nframes, double frame_t0,
+                                            double frame_dt, atkdsp_cfar_event *ev,
+                                            size_t cap);                                 /* :1903 */
+ATKDSP_API ptrdiff_t    atkdsp_cfar_flush(atkdsp_cfar *c, atkdsp_cfar_event *ev,
+                                          size_t cap);                                   /* :1909 */
+ATKDSP_API int          atkdsp_cfar_last(const atkdsp_cfar *c, float *avg_db, float *thr_db,
+                                         uint8_t *hits);                                 /* :1913 */
+ATKDSP_API int          atkdsp_cfar_info(const atkdsp_cfar *c, double *alpha,
+                                         double *alpha_ca, double *et,
+                                         atkdsp_cfar_config *cfg);                       /* :1917 */
+ATKDSP_API int          atkdsp_cfar_describe(const atkdsp_cfar *c, char *buf, size_t cap); /* :1923 */
+ATKDSP_API int          atkdsp_cfar_stats(const atkdsp_cfar *c, atkdsp_cfar_counters *st);  /* :1924 */
 
 #ifdef __cplusplus
 }

@@ -193,6 +193,25 @@ ATKDSP_API ptrdiff_t   atkdsp_gpu_spectrum_stats(atkdsp_gpu_spectrum *p, const a
                                                  float *d_max_db, float *d_avg_db, float *d_min_db,
                                                  float *d_sk, void *stream);
 
+/* ---- CFAR on device frames ---------------------------------------------- */
+/* atkdsp_cfar_process (reference include/atkdsp.h:1903) on nframes frames of
+ * nbins floats in device memory: units 0 = dB, as the reference takes them
+ * (a spectrum line from atkdsp_gpu_spectrum_*); units 1 = linear power (W2's
+ * channel powers as they come, clamped below at 1e-30, the linear value of
+ * the reference's -300 dB floor). The handle's stream first waits for
+ * `stream`'s pending work (NULL: the legacy default stream), so the frames'
+ * producer needs no host synchronisation. The events go to the caller's host array
+ * as from atkdsp_cfar_process; when d_hits is not NULL, every frame's hit
+ * mask (nframes x nbins bytes, 1 = hit, 0 for warm-up frames) is also
+ * written there in device memory: a row is the gate W1 takes
+ * (atkdsp_gpu_pfb_cov_accumulate), with no host round trip. Synchronous on
+ * return; returns the event count or ATKDSP_E_ARG / ATKDSP_E_CAP /
+ * ATKDSP_E_FFT (a kernel failure). */
+ATKDSP_API ptrdiff_t   atkdsp_gpu_cfar_process(atkdsp_cfar *c, const float *d_frames, int units,
+                                               size_t nframes, double frame_t0, double frame_dt,
+                                               atkdsp_cfar_event *ev, size_t cap, uint8_t *d_hits,
+                                               void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -392,3 +392,121 @@ def reference() -> CpuLib | None:
     if "ref" not in _cache:
         _cache["ref"] = CpuLib(REF_SO, "atkdsp_") if REF_SO.exists() else None
     return _cache["ref"]
+
+
+# -- the reference's CFAR (its C library only: the product's is the thing tested)
+class _CfarConfig(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("n_ref", C.c_int32), ("n_guard", C.c_int32),
+                ("k_frames", C.c_int32), ("pfa", C.c_double), ("looks", C.c_double),
+                ("os_k", C.c_int32), ("open_m", C.c_int32), ("open_n", C.c_int32),
+                ("close_k", C.c_int32), ("merge_gap", C.c_int32), ("min_bins", C.c_int32),
+                ("max_tracks", C.c_int32), ("reserved", C.c_int32), ("rho2", C.c_double * 4)]
+
+
+class _CfarEvent(C.Structure):
+    _fields_ = [("t0", C.c_double), ("t1", C.c_double), ("fc_bin", C.c_double),
+                ("type", C.c_int32), ("id", C.c_uint32), ("flags", C.c_uint32),
+                ("lo_bin", C.c_int32), ("hi_bin", C.c_int32), ("n_hits", C.c_int32),
+                ("level_db", C.c_float), ("noise_db", C.c_float), ("snr_db", C.c_float),
+                ("band_snr_db", C.c_float)]
+
+
+class _CfarCounters(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in
+                ("frames", "warmup", "cells_tested", "cell_hits", "untestable",
+                 "opened", "closed", "updates", "dropped", "resets", "tracks")]
+
+
+_CFAR_MODES = {"ca": 0, "os": 1, "go": 2, "so": 3}
+
+
+def _ev_dict(e) -> dict:
+    return {"type": int(e.type), "id": int(e.id), "flags": int(e.flags), "lo": int(e.lo_bin),
+            "hi": int(e.hi_bin), "n_hits": int(e.n_hits), "t0": float(e.t0), "t1": float(e.t1),
+            "fc_bin": float(e.fc_bin), "level_db": float(e.level_db), "noise_db": float(e.noise_db),
+            "snr_db": float(e.snr_db), "band_snr_db": float(e.band_snr_db)}
+
+
+class RefCfar:
+    """atkdsp_cfar_* of the reference library, with the surface of the
+    reference binding's Cfar (python/atkdsp/__init__.py:2431-2541)."""
+
+    def __init__(self, lib: CpuLib, nbins: int, **cfg):
+        L = self._L = lib.lib
+        vp, sz, d = C.c_void_p, C.c_size_t, C.c_double
+        for name, args, res in (
+                ("atkdsp_cfar_defaults", [_P(_CfarConfig)], None),
+                ("atkdsp_cfar_create", [sz, _P(_CfarConfig)], vp),
+                ("atkdsp_cfar_destroy", [vp], None),
+                ("atkdsp_cfar_set_mask", [vp, _P(C.c_uint8)], C.c_int),
+                ("atkdsp_cfar_process", [vp, _P(C.c_float), sz, d, d, _P(_CfarEvent), sz], C.c_ssize_t),
+                ("atkdsp_cfar_flush", [vp, _P(_CfarEvent), sz], C.c_ssize_t),
+                ("atkdsp_cfar_last", [vp, _P(C.c_float), _P(C.c_float), _P(C.c_uint8)], C.c_int),
+                ("atkdsp_cfar_info", [vp, _P(d), _P(d), _P(d), _P(_CfarConfig)], C.c_int),
+                ("atkdsp_cfar_describe", [vp, C.c_char_p, sz], C.c_int),
+                ("atkdsp_cfar_stats", [vp, _P(_CfarCounters)], C.c_int),
+                ("atkdsp_cfar_reset", [vp], None)):
+            getattr(L, name).argtypes = args
+            getattr(L, name).restype = res
+        k = _CfarConfig()
+        L.atkdsp_cfar_defaults(C.byref(k))
+        for key, v in cfg.items():
+            if key == "mode" and isinstance(v, str):
+                v = _CFAR_MODES[v]
+            if key == "rho2":
+                k.rho2 = (C.c_double * 4)(*[float(x) for x in v])
+            else:
+                setattr(k, key, float(v) if key in ("pfa", "looks") else int(v))
+        self.nbins = int(nbins)
+        self.max_tracks = k.max_tracks
+        self._h = L.atkdsp_cfar_create(self.nbins, C.byref(k))
+        if not self._h:
+            raise ValueError(f"reference cfar_create refused {cfg}")
+        a, ac, et = C.c_double(), C.c_double(), C.c_double()
+        L.atkdsp_cfar_info(self._h, C.byref(a), C.byref(ac), C.byref(et), None)
+        self.alpha, self.alpha_ca, self.et = a.value, ac.value, et.value
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            self._L.atkdsp_cfar_destroy(h)
+
+    def set_mask(self, mask):
+        m = None if mask is None else np.ascontiguousarray(np.asarray(mask) != 0, np.uint8)
+        self._L.atkdsp_cfar_set_mask(self._h, None if m is None else m.ctypes.data_as(_P(C.c_uint8)))
+
+    def reset(self):
+        self._L.atkdsp_cfar_reset(self._h)
+
+    def process(self, frames_db, frame_t0, frame_dt):
+        f = np.ascontiguousarray(frames_db, np.float32).reshape(-1, self.nbins)
+        cap = max(1, f.shape[0] * self.max_tracks)
+        buf = (_CfarEvent * cap)()
+        n = self._L.atkdsp_cfar_process(self._h, f.ctypes.data_as(_P(C.c_float)), f.shape[0],
+                                        float(frame_t0), float(frame_dt), buf, cap)
+        if n < 0:
+            raise ValueError(f"reference cfar_process: {n}")
+        return [_ev_dict(buf[j]) for j in range(n)]
+
+    def flush(self):
+        buf = (_CfarEvent * self.max_tracks)()
+        n = self._L.atkdsp_cfar_flush(self._h, buf, self.max_tracks)
+        return [_ev_dict(buf[j]) for j in range(n)]
+
+    def last(self):
+        a = np.empty(self.nbins, np.float32)
+        t = np.empty(self.nbins, np.float32)
+        h = np.empty(self.nbins, np.uint8)
+        rc = self._L.atkdsp_cfar_last(self._h, a.ctypes.data_as(_P(C.c_float)),
+                                      t.ctypes.data_as(_P(C.c_float)), h.ctypes.data_as(_P(C.c_uint8)))
+        return None if rc else (a, t, h)
+
+    def stats(self):
+        s = _CfarCounters()
+        self._L.atkdsp_cfar_stats(self._h, C.byref(s))
+        return {n: int(getattr(s, n)) for n, _t in s._fields_}
+
+    def describe(self):
+        buf = C.create_string_buffer(1024)
+        self._L.atkdsp_cfar_describe(self._h, buf, 1024)
+        return buf.value.decode()

@@ -82,5 +82,10 @@ def golden_spectrum():
     return load_golden("spectrum.npz")
 
 
+@pytest.fixture(scope="session")
+def golden_cfar():
+    return load_golden("cfar.npz")
+
+
 def spectrum_case_names(data: dict) -> list:
     return sorted({k.split("/")[0] for k in data if k.endswith("/line")})

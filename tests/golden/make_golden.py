@@ -25,6 +25,10 @@ Fixture files (tests/golden/*.npz):
   spectrum.npz      spectrum reduction lines (max / min / avg detector) and
                     per-bin stats (max, avg, min dB, spectral kurtosis) from
                     the reference C library run with one thread
+  cfar.npz          the CFAR solver over a grid of (mode, n_ref, pfa, looks,
+                    os_k, rho2), n_eff and window correlations, and the
+                    detector's events, counters and last-frame lines for the
+                    cases of tests/cfar_cases.py (reference C library)
 """
 
 from __future__ import annotations
@@ -44,6 +48,7 @@ from atkdsp_b200 import workloads as W         # noqa: E402
 
 sys.path.insert(0, str(HERE.parent))
 from osx_cases import OSX_CASES, run_case      # noqa: E402
+import cfar_cases                              # noqa: E402
 
 _ARGS = [a for a in sys.argv[1:] if not a.startswith("--")]
 ONLY = sys.argv[sys.argv.index("--only") + 1:] if "--only" in sys.argv else None
@@ -228,6 +233,63 @@ def make_spectrum(ref):
     return out
 
 
+# the solver grid: (mode, n_ref, pfa, looks, os_k, rho2 or None)
+CFAR_RHO = {"none": None, "hann": (4 / 9, 1 / 36, 0.0, 0.0), "mild": (0.3, 0.05, 0.01, 0.0)}
+CFAR_ALPHA_GRID = [(mode, nref, pfa, looks, os_k, rho)
+                   for mode in range(4) for nref in (1, 3, 16, 64, 256) for pfa in (0.5, 1e-3, 1e-6, 1e-15)
+                   for looks in (0.25, 1.0, 7.5, 400.0) for os_k in (0, 1) for rho in CFAR_RHO
+                   if not (os_k and mode != 1)]
+
+
+def make_cfar(ref):
+    import ctypes as C
+    L = ref.lib
+    L.atkdsp_cfar_alpha.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.atkdsp_cfar_alpha.restype = C.c_int
+    L.atkdsp_cfar_n_eff.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    L.atkdsp_cfar_n_eff.restype = C.c_double
+    L.atkdsp_cfar_window_rho2.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.POINTER(C.c_double)]
+    L.atkdsp_cfar_window_rho2.restype = C.c_int
+    out = {}
+    grid, res = [], []
+    for mode, nref, pfa, looks, os_k, rho in CFAR_ALPHA_GRID:
+        r = None if CFAR_RHO[rho] is None else (C.c_double * 4)(*CFAR_RHO[rho])
+        a, e = C.c_double(), C.c_double()
+        rc = L.atkdsp_cfar_alpha(mode, nref, pfa, looks, os_k, r, C.byref(a), C.byref(e))
+        grid.append([mode, nref, pfa, looks, os_k, list(CFAR_RHO).index(rho)])
+        res.append([rc, a.value if rc == 0 else np.nan, e.value if rc == 0 else np.nan])
+    out["alpha/grid"] = np.array(grid, np.float64)
+    out["alpha/res"] = np.array(res, np.float64)
+    out["alpha/rho"] = np.array([v or (0.0,) * 4 for v in CFAR_RHO.values()], np.float64)
+    neff = []
+    for nref in range(0, 12):
+        for rho in CFAR_RHO.values():
+            r = None if rho is None else (C.c_double * 4)(*rho)
+            neff.append([nref, 0 if rho is None else 1 + list(CFAR_RHO.values()).index(rho) - 1,
+                         L.atkdsp_cfar_n_eff(nref, r)])
+    out["n_eff"] = np.array(neff, np.float64)
+    for kind in ("rect", "hann", "hamming", "blackmanharris"):
+        for n in (16, 1000, 4096):
+            w = ref.window(kind, n)
+            r = (C.c_double * 4)()
+            assert L.atkdsp_cfar_window_rho2(w.ctypes.data_as(C.POINTER(C.c_float)), n, r) == 0
+            out[f"rho2/{kind}/{n}"] = np.array(list(r))
+    print(f"alpha grid: {len(grid)} points, {sum(1 for v in res if v[0] == 0)} solved")
+    for name in cfar_cases.CFAR_CASES:
+        xs = cfar_cases.frames(name)
+        ev, last, st, desc, al = cfar_cases.run_case(lambda nb, **cfg: O.RefCfar(ref, nb, **cfg), name, xs)
+        out[f"{name}/in"] = xs
+        out[f"{name}/events"] = ev
+        out[f"{name}/stats"] = np.array([st[k] for k in sorted(st)], np.uint64)
+        out[f"{name}/describe"] = np.array(desc)
+        out[f"{name}/alpha"] = np.array(al)
+        if last is not None:
+            out[f"{name}/last_avg"], out[f"{name}/last_thr"], out[f"{name}/last_hits"] = last
+        print(f"{name}: {len(ev)} events, stats {st}")
+    return out
+
+
 def main():
     ref = O.reference()
     if ref is None:
@@ -247,6 +309,8 @@ def main():
         np.savez_compressed(HERE / "osx.npz", **make_osx(ref))
     if want("spectrum"):
         np.savez_compressed(HERE / "spectrum.npz", **make_spectrum(ref))
+    if want("cfar"):
+        np.savez_compressed(HERE / "cfar.npz", **make_cfar(ref))
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

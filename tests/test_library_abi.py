@@ -46,7 +46,12 @@ def test_headers_declare_the_reference_surface():
                  "atkdsp_pfb_channel_power", "atkdsp_osx_create", "atkdsp_osx_destroy",
                  "atkdsp_osx_reset", "atkdsp_osx_add", "atkdsp_osx_retune", "atkdsp_osx_remove",
                  "atkdsp_osx_channels", "atkdsp_osx_chan_rate", "atkdsp_osx_out_max",
-                 "atkdsp_osx_process", "atkdsp_osx_process_n", "atkdsp_osx_describe"):
+                 "atkdsp_osx_process", "atkdsp_osx_process_n", "atkdsp_osx_describe",
+                 "atkdsp_cfar_defaults", "atkdsp_cfar_alpha", "atkdsp_cfar_n_eff",
+                 "atkdsp_cfar_window_rho2", "atkdsp_cfar_create", "atkdsp_cfar_destroy",
+                 "atkdsp_cfar_reset", "atkdsp_cfar_set_mask", "atkdsp_cfar_events_max",
+                 "atkdsp_cfar_process", "atkdsp_cfar_flush", "atkdsp_cfar_last", "atkdsp_cfar_info",
+                 "atkdsp_cfar_describe", "atkdsp_cfar_stats"):
         assert name in d, name
 
 
@@ -89,6 +94,50 @@ def test_create_rejects_bad_arguments_before_touching_a_device():
     assert lib.atkdsp_osx_add(None, 0.0, 1.0, 1.0) == -1 and lib.atkdsp_osx_remove(None, 0) == -1
 
 
+def test_cfar_layouts_and_argument_rules_without_a_device():
+    """The three CFAR structs have the reference's compiled sizes (96, 64, 88
+    bytes: gcc on the reference header gives 96 for the config, whose comment
+    says 104); every configuration
+    outside the reference's ranges is refused before any device work; the
+    NULL-handle rules are the reference's (src/cfar.c:324-340, :745-819)."""
+    import ctypes as C
+    assert C.sizeof(ak._CfarConfig) == 96 and C.sizeof(ak._CfarEvent) == 64
+    assert C.sizeof(ak._CfarCounters) == 88
+    lib = ak.load()
+    base = ak.cfar_defaults()
+    assert base["n_ref"] == 16 and base["n_guard"] == 4 and base["pfa"] == 1e-6 and base["max_tracks"] == 256
+    bad = [dict(mode=4), dict(n_ref=0), dict(n_ref=257), dict(n_guard=-1), dict(k_frames=0), dict(k_frames=65),
+           dict(looks=0.2), dict(looks=2e4), dict(pfa=0.6), dict(pfa=1e-16), dict(mode=1, os_k=33),
+           dict(open_m=4, open_n=3), dict(open_n=65), dict(close_k=0), dict(close_k=1001), dict(merge_gap=-1),
+           dict(min_bins=0), dict(max_tracks=0), dict(max_tracks=65537), dict(rho2=(1.0, 0, 0, 0)),
+           dict(rho2=(-0.1, 0, 0, 0))]
+    for b in bad:
+        k = ak._CfarConfig()
+        lib.atkdsp_cfar_defaults(C.byref(k))
+        for key, v in b.items():
+            if key == "rho2":
+                k.rho2 = (C.c_double * 4)(*v)
+            else:
+                setattr(k, key, v)
+        assert not lib.atkdsp_cfar_create(1024, C.byref(k)), b
+    k = ak._CfarConfig()
+    lib.atkdsp_cfar_defaults(C.byref(k))
+    for nb in (0, 40, (1 << 24) + 1):
+        assert not lib.atkdsp_cfar_create(nb, C.byref(k)), nb
+    assert not lib.atkdsp_cfar_create(1024, None)
+    lib.atkdsp_cfar_destroy(None)
+    lib.atkdsp_cfar_reset(None)
+    assert lib.atkdsp_cfar_events_max(None, 10) == 0
+    assert lib.atkdsp_cfar_set_mask(None, None) == -1
+    assert lib.atkdsp_cfar_flush(None, None, 0) == -1 and lib.atkdsp_cfar_last(None, None, None, None) == -1
+    assert lib.atkdsp_cfar_stats(None, None) == -1 and lib.atkdsp_cfar_describe(None, None, 0) == -1
+    assert lib.atkdsp_cfar_process(None, None, 0, 0.0, 0.0, None, 0) == -1
+    with pytest.raises(ak.AtkDspError):
+        ak.cfar_alpha("ca", 0, 1e-6)
+    with pytest.raises(ak.AtkDspError):
+        ak.cfar_window_rho2([0.0, 0.0, 0.0])
+
+
 def test_no_cpu_fallback_without_a_gpu():
     torch = pytest.importorskip("torch")
     if torch.cuda.is_available():
@@ -99,3 +148,5 @@ def test_no_cpu_fallback_without_a_gpu():
         ak.unpack(b"\x00\x01\x02\x03", "ci16")
     with pytest.raises(ak.AtkDspError):
         ak.Osx(2.4e6, 4096)
+    with pytest.raises(ak.AtkDspError):
+        ak.Cfar(1024)

@@ -198,3 +198,61 @@ def test_spectrum_oracle_matches_reference_golden(golden_spectrum):
         st = orc.spectrum_stats(x, n, hop, w)
         for q in ("max", "avg", "min", "sk"):
             assert np.array_equal(st[q], golden_spectrum[f"{name}/{q}"]), (name, q)
+
+
+# -- CFAR ---------------------------------------------------------------------
+
+def test_cfar_solver_bit_exact_against_the_reference(golden_cfar):
+    """The threshold solver is host code of the product (no GPU needed):
+    alpha and E[T] over 1200 configurations of (mode, n_ref, pfa, looks, OS
+    rank, window correlation) come out as the reference's numbers, bit for
+    bit, and the refusals are the reference's."""
+    import atkdsp_b200 as ak
+    grid, res, rhos = golden_cfar["alpha/grid"], golden_cfar["alpha/res"], golden_cfar["alpha/rho"]
+    for (mode, nref, pfa, looks, os_k, ri), (rc, a, et) in zip(grid, res):
+        rho = None if ri == 0 else tuple(rhos[int(ri)])
+        try:
+            got = ak.cfar_alpha(int(mode), int(nref), pfa, looks, int(os_k), rho)
+        except ak.AtkDspError:
+            assert rc != 0, (mode, nref, pfa, looks, os_k, ri)
+            continue
+        assert rc == 0 and got == (a, et), (mode, nref, pfa, looks, os_k, ri, got, a, et)
+
+
+def test_cfar_n_eff_and_window_correlation_bit_exact(golden_cfar):
+    import atkdsp_b200 as ak
+    rhos = golden_cfar["alpha/rho"]
+    for nref, ri, v in golden_cfar["n_eff"]:
+        rho = None if ri == 0 else tuple(rhos[int(ri)])
+        assert ak.cfar_n_eff(int(nref), rho) == v
+    for key in golden_cfar:
+        if key.startswith("rho2/"):
+            _, kind, n = key.split("/")
+            w = O.oracle().window(kind, int(n))
+            assert ak.cfar_window_rho2(w) == tuple(golden_cfar[key]), key
+
+
+def test_cfar_cell_oracle_matches_reference_last_frames(golden_cfar):
+    """The numpy restatement of the per-cell test, pinned to the reference's
+    last tested frame of every case: averaged power and threshold in dB as
+    the reference rounds them to float, and the hit mask."""
+    import cfar_cases
+    from oracle import cfar_oracle as CO
+    for name in cfar_cases.CFAR_CASES:
+        xs = golden_cfar[f"{name}/in"]
+        a, ac, _et = golden_cfar[f"{name}/alpha"]
+        X, thr, hits = CO.cell_test(xs, cfar_cases.cfg_of(name), a, ac, cfar_cases.mask_of(name))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            avg = (10.0 * np.log10(X[-1])).astype(np.float32)
+            tdb = (10.0 * np.log10(thr[-1])).astype(np.float32)
+        ref_avg, ref_thr = golden_cfar[f"{name}/last_avg"], golden_cfar[f"{name}/last_thr"]
+        assert np.array_equal(hits[-1], golden_cfar[f"{name}/last_hits"]), name
+        fin = np.isfinite(ref_avg)
+        assert np.array_equal(np.isfinite(avg), fin), name
+        assert np.max(np.abs(avg[fin] - ref_avg[fin]), initial=0.0) <= 1e-5, name
+        fin = np.isfinite(ref_thr)
+        assert np.array_equal(np.isfinite(tdb), fin), name
+        assert np.max(np.abs(tdb[fin] - ref_thr[fin]), initial=0.0) <= 1e-5, name
+        st = dict(zip(sorted(["frames", "warmup", "cells_tested", "cell_hits", "untestable", "opened", "closed",
+                              "updates", "dropped", "resets", "tracks"]), golden_cfar[f"{name}/stats"]))
+        assert int(hits.sum()) == int(st["cell_hits"]), name
