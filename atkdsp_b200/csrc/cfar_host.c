@@ -26,7 +26,7 @@
 #define CF_PI 3.14159265358979323846
 #define CF_LN10 2.302585092994045684
 /* frames per device pass: at most this many cells, and at most 4096 frames */
-#define CF_PASS_CELLS ((size_t)1 << 22)
+#define CF_PASS_CELLS ((size_t)1 << 19)
 #define CF_PASS_FRAMES 4096
 /* host buffers up to this size are pinned */
 #define CF_PINNED_MAX ((size_t)256 << 20)
@@ -404,12 +404,12 @@ struct atkdsp_cfar {
     uint8_t *last_hits;
     /* device: tables, the raw ring (frame F in row F % ring), a pass's rows */
     int fc, ring;
-    void *stream, *ev_in;
+    void *stream, *ev_in, *ev_pass[2];
     uint8_t *d_ok, *d_sided, *d_hits;
     int32_t *d_idx;
     double *d_raw, *d_X, *d_noise, *d_thr;
     float *d_frames;
-    /* host copies of a pass's rows (pinned when small) and the raw ring */
+    /* host copies of two passes' rows (pinned when small) and the raw ring */
     int pinned;
     double *h_X, *h_noise, *h_raw;
     uint8_t *h_hits;
@@ -559,6 +559,8 @@ ATKDSP_API void atkdsp_cfar_destroy(atkdsp_cfar *c) {
     atkb_free(c->d_thr);
     atkb_free(c->d_frames);
     if (c->ev_in) atkb_event_destroy(c->ev_in);
+    if (c->ev_pass[0]) atkb_event_destroy(c->ev_pass[0]);
+    if (c->ev_pass[1]) atkb_event_destroy(c->ev_pass[1]);
     if (c->stream) atkb_stream_destroy(c->stream);
     free(c);
 }
@@ -592,9 +594,9 @@ ATKDSP_API atkdsp_cfar *atkdsp_cfar_create(size_t nbins, const atkdsp_cfar_confi
     if (fc < 1) fc = 1;
     if (fc > CF_PASS_FRAMES) fc = CF_PASS_FRAMES;
     c->fc = (int)fc;
-    c->ring = c->fc + k - 1;
+    c->ring = 2 * c->fc + k - 1;
     const size_t nb = nbins, rows = (size_t)c->fc, ring = (size_t)c->ring;
-    c->pinned = (rows * nb * 17 + (k > 1 ? ring * nb * 8 : 0)) <= CF_PINNED_MAX;
+    c->pinned = (2 * rows * nb * 17 + (k > 1 ? ring * nb * 8 : 0)) <= CF_PINNED_MAX;
     c->next_id = 1;
     c->mask = (uint8_t *)calloc(nb, 1);
     c->ok = (uint8_t *)calloc(nb, 1);
@@ -612,14 +614,16 @@ ATKDSP_API atkdsp_cfar *atkdsp_cfar_create(size_t nbins, const atkdsp_cfar_confi
                  ? ATKB_OK
                  : ATKB_E_NOMEM;
     if (rc == ATKB_OK) {
-        c->h_X = (double *)host_buf(c, rows * nb * sizeof(double));
-        c->h_noise = (double *)host_buf(c, rows * nb * sizeof(double));
-        c->h_hits = (uint8_t *)host_buf(c, rows * nb);
+        c->h_X = (double *)host_buf(c, 2 * rows * nb * sizeof(double));
+        c->h_noise = (double *)host_buf(c, 2 * rows * nb * sizeof(double));
+        c->h_hits = (uint8_t *)host_buf(c, 2 * rows * nb);
         if (k > 1) c->h_raw = (double *)host_buf(c, ring * nb * sizeof(double));
         if (!c->h_X || !c->h_noise || !c->h_hits || (k > 1 && !c->h_raw)) rc = ATKB_E_NOMEM;
     }
     if (rc == ATKB_OK) rc = atkb_stream_create(&c->stream);
     if (rc == ATKB_OK) rc = atkb_event_create(&c->ev_in);
+    if (rc == ATKB_OK) rc = atkb_event_create(&c->ev_pass[0]);
+    if (rc == ATKB_OK) rc = atkb_event_create(&c->ev_pass[1]);
     if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_ok, nb);
     if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_sided, nb);
     if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_idx, nb * (size_t)c->N * sizeof(int32_t));
@@ -739,6 +743,23 @@ static int popcount64(uint64_t x) {
     return n;
 }
 
+/* the first hit at or after i (nb if none), eight bins at a time */
+static long next_hit(const uint8_t *h, long i, long nb) {
+    for (; i < nb && (i & 7); ++i)
+        if (h[i]) return i;
+    for (; i + 8 <= nb; i += 8) {
+        uint64_t w;
+        memcpy(&w, h + i, 8);
+        if (w) {
+            while (!h[i]) ++i;
+            return i;
+        }
+    }
+    for (; i < nb; ++i)
+        if (h[i]) return i;
+    return nb;
+}
+
 /* One tested frame F (absolute), its rows from the device: X, noise, hits;
  * raw rows by ring row. Returns the events written. */
 static size_t track_frame(atkdsp_cfar *c, int64_t F, const double *X, const double *noise, const uint8_t *hits,
@@ -754,11 +775,7 @@ static size_t track_frame(atkdsp_cfar *c, int64_t F, const double *X, const doub
     size_t nblob = 0;
     uint64_t nhit = 0;
     long i = 0;
-    while (i < nb) {
-        if (!hits[i]) {
-            ++i;
-            continue;
-        }
+    while ((i = next_hit(hits, i, nb)) < nb) {
         long lo = i, hi = i, prev = i;
         for (long j = i + 1; j < nb; ++j) {
             if (j - prev - 1 > g) break;
@@ -935,8 +952,58 @@ static size_t track_frame(atkdsp_cfar *c, int64_t F, const double *X, const doub
 
 /* ================================================= a call */
 
+/* One pass: frames [done, done + nf) of a call whose first frame is F_start
+ * with seen_start frames seen before it. Enqueues the conversion, the test
+ * and the copies of the pass's rows into host set `set`; nothing waits. */
+typedef struct {
+    size_t done;
+    int nf;
+    int64_t F0, j0;
+} cf_pass;
+
+static int pass_enqueue(atkdsp_cfar *c, const cf_pass *ps, const float *frames, int on_device, int units, int set,
+                        uint8_t *d_hits_out) {
+    const size_t nb = c->nbins, hs = (size_t)set * (size_t)c->fc * nb;
+    const int k = c->cfg.k_frames, nf = ps->nf;
+    const int64_t F0 = ps->F0, j0 = ps->j0;
+    const float *src = frames + ps->done * nb;
+    int rc = ATKB_OK;
+    if (!on_device) {
+        rc = atkb_h2d(c->d_frames, src, (size_t)nf * nb * sizeof(float), c->stream);
+        src = c->d_frames;
+    }
+    if (rc == ATKB_OK) rc = atkb_cfar_raw(src, units, F0, nf, (long long)nb, c->d_raw, c->ring, c->stream);
+    if (rc == ATKB_OK && j0 < nf)
+        rc = atkb_cfar_test(c->d_raw, c->ring, F0, F0 + j0, nf, (long long)nb, k, c->cfg.mode, c->cfg.n_ref, c->N,
+                            c->cfg.os_k, c->alpha, c->alpha_ca, c->et, c->d_ok, c->d_sided, c->d_idx, c->d_X,
+                            c->d_noise, c->d_thr, c->d_hits, c->stream);
+    if (rc == ATKB_OK && j0 < nf) {
+        const size_t off = (size_t)j0 * nb, rows = (size_t)(nf - j0) * nb;
+        rc = atkb_d2h(c->h_hits + hs + off, c->d_hits + off, rows, c->stream);
+        if (rc == ATKB_OK) rc = atkb_d2h(c->h_X + hs + off, c->d_X + off, rows * sizeof(double), c->stream);
+        if (rc == ATKB_OK) rc = atkb_d2h(c->h_noise + hs + off, c->d_noise + off, rows * sizeof(double), c->stream);
+        if (rc == ATKB_OK && d_hits_out)
+            rc = atkb_d2d(d_hits_out + (ps->done + (size_t)j0) * nb, c->d_hits + off, rows, c->stream);
+    }
+    if (rc == ATKB_OK && d_hits_out && j0 > 0)
+        rc = atkb_memset(d_hits_out + ps->done * nb, 0, (size_t)(j0 < nf ? j0 : nf) * nb, c->stream);
+    if (rc == ATKB_OK && k > 1) {
+        /* the pass's raw rows into the host ring, in at most two runs */
+        const size_t r0 = (size_t)(F0 % c->ring);
+        const size_t first = (size_t)nf < (size_t)c->ring - r0 ? (size_t)nf : (size_t)c->ring - r0;
+        rc = atkb_d2h(c->h_raw + r0 * nb, c->d_raw + r0 * nb, first * nb * sizeof(double), c->stream);
+        if (rc == ATKB_OK && first < (size_t)nf)
+            rc = atkb_d2h(c->h_raw, c->d_raw, ((size_t)nf - first) * nb * sizeof(double), c->stream);
+    }
+    if (rc == ATKB_OK) rc = atkb_event_record(c->ev_pass[set], c->stream);
+    return rc;
+}
+
 /* frames: host (on_device 0) or device floats, nframes x nbins; d_hits_out:
- * device, nframes x nbins, or NULL */
+ * device, nframes x nbins, or NULL. The call runs in passes of at most fc
+ * frames; while the host tracks pass i, the GPU converts, tests and copies
+ * pass i + 1 into the other host set (the raw ring holds both passes and the
+ * k - 1 frames before them). */
 static ptrdiff_t cfar_run(atkdsp_cfar *c, const float *frames, int on_device, int units, size_t nframes,
                           double frame_t0, double frame_dt, atkdsp_cfar_event *ev, size_t cap, uint8_t *d_hits_out,
                           void *stream) {
@@ -953,47 +1020,36 @@ static ptrdiff_t cfar_run(atkdsp_cfar *c, const float *frames, int on_device, in
         if (rc == ATKB_OK) rc = atkb_stream_wait(c->stream, c->ev_in);
         if (rc != ATKB_OK) return atkb_map_rc(rc);
     }
+    const int64_t F_start = c->frame, seen_start = c->seen;
+    cf_pass cur, next;
     size_t nev = 0;
-    for (size_t done = 0; done < nframes;) {
-        const int nf = (int)((nframes - done) < (size_t)c->fc ? (nframes - done) : (size_t)c->fc);
-        const int64_t F0 = c->frame;
-        /* frames of this pass tested once k frames have been seen since reset */
-        int64_t j0 = (int64_t)k - 1 - c->seen;
-        if (j0 < 0) j0 = 0;
-        const float *src = frames + done * nb;
-        if (!on_device) {
-            rc = atkb_h2d(c->d_frames, src, (size_t)nf * nb * sizeof(float), c->stream);
-            src = c->d_frames;
+    int last_set = -1, last_row = -1;
+    for (size_t at = 0, i = 0; at < nframes; ++i) {
+        cur.done = at;
+        cur.nf = (int)((nframes - at) < (size_t)c->fc ? (nframes - at) : (size_t)c->fc);
+        cur.F0 = F_start + (int64_t)at;
+        cur.j0 = (int64_t)k - 1 - (seen_start + (int64_t)at);
+        if (cur.j0 < 0) cur.j0 = 0;
+        if (i == 0) rc = pass_enqueue(c, &cur, frames, on_device, units, 0, d_hits_out);
+        at += (size_t)cur.nf;
+        if (rc == ATKB_OK && at < nframes) {
+            next.done = at;
+            next.nf = (int)((nframes - at) < (size_t)c->fc ? (nframes - at) : (size_t)c->fc);
+            next.F0 = F_start + (int64_t)at;
+            next.j0 = (int64_t)k - 1 - (seen_start + (int64_t)at);
+            if (next.j0 < 0) next.j0 = 0;
+            rc = pass_enqueue(c, &next, frames, on_device, units, (int)((i + 1) & 1), d_hits_out);
         }
-        if (rc == ATKB_OK) rc = atkb_cfar_raw(src, units, F0, nf, (long long)nb, c->d_raw, c->ring, c->stream);
-        if (rc == ATKB_OK && j0 < nf)
-            rc = atkb_cfar_test(c->d_raw, c->ring, F0, F0 + j0, nf, (long long)nb, k, c->cfg.mode, c->cfg.n_ref,
-                                c->N, c->cfg.os_k, c->alpha, c->alpha_ca, c->et, c->d_ok, c->d_sided, c->d_idx,
-                                c->d_X, c->d_noise, c->d_thr, c->d_hits, c->stream);
-        if (rc == ATKB_OK && j0 < nf) {
-            const size_t off = (size_t)j0 * nb, rows = (size_t)(nf - j0) * nb;
-            rc = atkb_d2h(c->h_hits + off, c->d_hits + off, rows, c->stream);
-            if (rc == ATKB_OK) rc = atkb_d2h(c->h_X + off, c->d_X + off, rows * sizeof(double), c->stream);
-            if (rc == ATKB_OK) rc = atkb_d2h(c->h_noise + off, c->d_noise + off, rows * sizeof(double), c->stream);
-            if (rc == ATKB_OK && d_hits_out)
-                rc = atkb_d2d(d_hits_out + (done + (size_t)j0) * nb, c->d_hits + off, rows, c->stream);
+        const int set = (int)(i & 1);
+        if (rc == ATKB_OK) rc = atkb_event_sync(c->ev_pass[set]);
+        if (rc != ATKB_OK) {
+            atkb_stream_sync(c->stream);
+            return atkb_map_rc(rc);
         }
-        if (rc == ATKB_OK && d_hits_out && j0 > 0)
-            rc = atkb_memset(d_hits_out + done * nb, 0, (size_t)(j0 < nf ? j0 : nf) * nb, c->stream);
-        if (rc == ATKB_OK && k > 1) {
-            /* the pass's raw rows into the host ring, in at most two runs */
-            const size_t r0 = (size_t)(F0 % c->ring);
-            const size_t first = (size_t)nf < (size_t)c->ring - r0 ? (size_t)nf : (size_t)c->ring - r0;
-            rc = atkb_d2h(c->h_raw + r0 * nb, c->d_raw + r0 * nb, first * nb * sizeof(double), c->stream);
-            if (rc == ATKB_OK && first < (size_t)nf)
-                rc = atkb_d2h(c->h_raw, c->d_raw, ((size_t)nf - first) * nb * sizeof(double), c->stream);
-        }
-        if (rc == ATKB_OK) rc = atkb_stream_sync(c->stream);
-        if (rc != ATKB_OK) return atkb_map_rc(rc);
-        int last = -1;
-        for (int j = 0; j < nf; ++j) {
-            const int64_t F = F0 + j;
-            const double tf = frame_t0 + (double)(done + (size_t)j) * frame_dt;
+        const size_t hs = (size_t)set * (size_t)c->fc * nb;
+        for (int j = 0; j < cur.nf; ++j) {
+            const int64_t F = cur.F0 + j;
+            const double tf = frame_t0 + (double)(cur.done + (size_t)j) * frame_dt;
             const size_t row = (size_t)(F % c->ring);
             c->st.frames++;
             c->ht[row] = tf;
@@ -1004,20 +1060,24 @@ static ptrdiff_t cfar_run(atkdsp_cfar *c, const float *frames, int on_device, in
                 c->st.warmup++;
                 continue;
             }
-            const size_t o = (size_t)j * nb;
+            const size_t o = hs + (size_t)j * nb;
             nev += track_frame(c, F, c->h_X + o, c->h_noise + o, c->h_hits + o, tf, frame_dt, ev + nev);
-            last = j;
+            last_set = set;
+            last_row = j;
         }
-        if (last >= 0) {
-            const size_t o = (size_t)last * nb;
-            memcpy(c->last_X, c->h_X + o, nb * sizeof(double));
-            memcpy(c->last_hits, c->h_hits + o, nb);
-            rc = atkb_d2h(c->last_thr, c->d_thr + o, nb * sizeof(double), c->stream);
-            if (rc == ATKB_OK) rc = atkb_stream_sync(c->stream);
-            if (rc != ATKB_OK) return atkb_map_rc(rc);
-            c->has_last = 1;
-        }
-        done += (size_t)nf;
+    }
+    if (last_row >= 0) {
+        /* the last tested frame is in the last pass, whose rows d_thr still holds */
+        const size_t o = (size_t)last_set * (size_t)c->fc * nb + (size_t)last_row * nb;
+        memcpy(c->last_X, c->h_X + o, nb * sizeof(double));
+        memcpy(c->last_hits, c->h_hits + o, nb);
+        rc = atkb_d2h(c->last_thr, c->d_thr + (size_t)last_row * nb, nb * sizeof(double), c->stream);
+        if (rc == ATKB_OK) rc = atkb_stream_sync(c->stream);
+        if (rc != ATKB_OK) return atkb_map_rc(rc);
+        c->has_last = 1;
+    } else if (d_hits_out) {
+        rc = atkb_stream_sync(c->stream);
+        if (rc != ATKB_OK) return atkb_map_rc(rc);
     }
     return (ptrdiff_t)nev;
 }

@@ -33,6 +33,10 @@ def _cfar(nbins, **cfg):
     return ak.Cfar(nbins, **cfg)
 
 
+def _arr(events) -> np.ndarray:
+    return np.array([[e[k] for k in EVENT_KEYS] for e in events], np.float64).reshape(-1, len(EVENT_KEYS))
+
+
 def _same_events(got: np.ndarray, ref: np.ndarray, what):
     assert got.shape == ref.shape, (what, got.shape, ref.shape)
     if not len(ref):
@@ -72,9 +76,9 @@ def test_golden_cases_match_the_reference(golden_cfar, name):
 
 @pytest.mark.parametrize("name", ["ca_default", "os_k3_looks4", "go_mask_hann", "ca_k8_long"])
 def test_events_do_not_depend_on_how_frames_are_split(golden_cfar, name):
-    """One call, one frame per call, and uneven calls give the same events,
-    counters and last frame: the raw ring carries the k - 1 frames before a
-    call."""
+    """One call, one frame per call, and uneven calls give the same events
+    (times to the rounding of each call's own start time), counters and last
+    frame: the raw ring carries the k - 1 frames before a call."""
     xs = golden_cfar[f"{name}/in"]
     outs = []
     for pattern in ([len(xs)], [1] * len(xs), [5, 1, 2, 17, 1000]):
@@ -91,8 +95,14 @@ def test_events_do_not_depend_on_how_frames_are_split(golden_cfar, name):
             pos += len(blk)
         rows += [[0] + [e[k] for k in EVENT_KEYS] for e in c.flush()]
         outs.append((np.array(rows).reshape(-1, 1 + len(EVENT_KEYS)), c.stats(), c.last()))
+    times = [1 + EVENT_KEYS.index("t0"), 1 + EVENT_KEYS.index("t1")]
+    rest = [c for c in range(1 + len(EVENT_KEYS)) if c not in times]
     for ev, st, last in outs[1:]:
-        assert np.array_equal(ev, outs[0][0], equal_nan=True), name
+        # a call's frame times start from its own frame_t0 (t0 + pos dt, then
+        # + j dt), so they round differently from one call's t0 + (pos + j) dt
+        assert ev.shape == outs[0][0].shape, name
+        assert np.array_equal(ev[:, rest], outs[0][0][:, rest], equal_nan=True), name
+        assert np.allclose(ev[:, times], outs[0][0][:, times], rtol=1e-12, atol=0, equal_nan=True), name
         assert st == outs[0][1], name
         for g, r in zip(last, outs[0][2]):
             assert np.array_equal(g, r, equal_nan=True), name
@@ -125,7 +135,7 @@ def test_device_frames_many_passes_against_the_oracle():
     assert h_or.sum() > 100
     c2 = _cfar(nb, **cfg)
     ev2 = c2.process(xs, FRAME_T0, FRAME_DT)
-    assert ev == ev2
+    assert np.array_equal(_arr(ev), _arr(ev2), equal_nan=True) and len(ev) > 10
     assert c.stats() == c2.stats()
 
 
@@ -208,8 +218,8 @@ def test_reset_mask_and_argument_rules():
     assert c.last() is None and c.stats()["resets"] == 1
     e2 = c.process(xs, 0.0, 1.0)
     assert len(e1) == len(e2) and e2[0]["id"] > e1[-1]["id"]       # ids keep counting
-    for a, b in zip(e1, e2):
-        assert {k: v for k, v in a.items() if k != "id"} == {k: v for k, v in b.items() if k != "id"}
+    keep = [i for i, k in enumerate(EVENT_KEYS) if k != "id"]
+    assert np.array_equal(_arr(e1)[:, keep], _arr(e2)[:, keep], equal_nan=True)
     # masking a bin takes it out of the test and out of every window
     c2 = _cfar(1024)
     mask = np.zeros(1024, np.uint8)

@@ -47,11 +47,14 @@ info = atkdsp.build_info()
 assert "abi 26" in info and "b200" in info, info
 ours = ctypes.CDLL({str(OUR_SO)!r})
 for name in ("atkdsp_pfb_create", "atkdsp_pfb_process_n", "atkdsp_unpack_dc",
-             "atkdsp_pfb_cov_accumulate", "atkdsp_pfb_channel_power"):
+             "atkdsp_pfb_cov_accumulate", "atkdsp_pfb_channel_power", "atkdsp_osx_process_n",
+             "atkdsp_cfar_create", "atkdsp_cfar_process", "atkdsp_cfar_alpha"):
     a = ctypes.cast(getattr(lib, name), ctypes.c_void_p).value
     b = ctypes.cast(getattr(ours, name), ctypes.c_void_p).value
     assert a == b, name
 assert lib.atkdsp_nco_mix is not None            # outside the path: the reference's
+a, et = atkdsp.cfar_alpha("ca", 16, 1e-6)        # the binding's solver call, answered by this library
+assert abs(a - 17.27764883379317) < 1e-12, a
 print("ok", info)
 """
     env = dict(os.environ, ATKDSP_LIB=str(composite))
