@@ -4,6 +4,7 @@
     python -m atkdsp_b200.microbench --sweep
     python -m atkdsp_b200.microbench --osx --nfft 4096 --channels 64
     python -m atkdsp_b200.microbench --kernels
+    python -m atkdsp_b200.microbench --cfar --nbins 4096 --frames 1024
 
 Each configuration channelizes one device-resident block of 2^log2n cf32
 samples (seeded noise, larger than L2 at the default 2^24) through a
@@ -24,6 +25,11 @@ algorithmic bytes (read + written once) per second.
 --osx times the overlap-save extractor instead: one device-resident cf32
 stream through atkdsp_gpu_osx_process_n with the extractor_channels plan of
 workloads.py (CUDA events on the handle's stream around the whole call).
+
+--cfar times the CFAR detector and tracker on device frames (nbins dB lines
+of exponential noise with 64 bursts, CA 16 + 16 cells, 4 guard, k_frames 4)
+through atkdsp_gpu_cfar_process: the whole synchronous call, host clock,
+median of the repetitions. {"nbins", "frames", "ms", "mcells_s", "events"}.
 """
 
 from __future__ import annotations
@@ -95,6 +101,35 @@ def run_osx(nfft: int = 4096, channels: int = 64, log2n: int = 24, reps: int = 5
             "msps": round(nel * n / t / 1e3, 1), "out_samples": int(sum(counts)) * nel}
 
 
+def run_cfar(nbins: int = 4096, frames: int = 1024, reps: int = 5) -> dict:
+    import time
+
+    import torch
+
+    from . import Cfar
+    from .gpu import cfar_process
+
+    g = torch.Generator(device="cuda").manual_seed(21)
+    u = torch.rand((frames, nbins), dtype=torch.float64, device="cuda", generator=g)
+    p = -torch.log1p(-u) * torch.linspace(1.0, 2.0, nbins, dtype=torch.float64, device="cuda")
+    rng = np.random.default_rng(21)
+    for _ in range(64):
+        lo, f0 = int(rng.integers(0, nbins - 8)), int(rng.integers(0, frames - 8))
+        p[f0:f0 + int(rng.integers(4, 200)), lo:lo + int(rng.integers(1, 8))] += 10 ** rng.uniform(1, 3)
+    x = (10.0 * torch.log10(p)).to(torch.float32).contiguous()
+    c = Cfar(nbins, k_frames=4)
+    for _ in range(2):
+        cfar_process(c, x, 0.0, 1e-3)
+    ts, nev = [], 0
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        nev = len(cfar_process(c, x, 0.0, 1e-3)[0])
+        ts.append((time.perf_counter() - t0) * 1e3)
+    ms = float(np.median(ts))
+    return {"nbins": nbins, "frames": frames, "ms": round(ms, 3),
+            "mcells_s": round(nbins * frames / ms / 1e3, 1), "events": nev}
+
+
 def run_kernels(reps: int = 5) -> list:
     import torch
 
@@ -162,8 +197,13 @@ def main(argv=None):
     ap.add_argument("--nfft", type=int, default=4096)
     ap.add_argument("--channels", type=int, default=64)
     ap.add_argument("--elements", type=int, default=1)
+    ap.add_argument("--cfar", action="store_true", help="the CFAR detector and tracker")
+    ap.add_argument("--nbins", type=int, default=4096)
+    ap.add_argument("--frames", type=int, default=1024)
     a = ap.parse_args(argv)
-    if a.kernels:
+    if a.cfar:
+        print(json.dumps(run_cfar(a.nbins, a.frames, a.reps)), flush=True)
+    elif a.kernels:
         for r in run_kernels(a.reps):
             print(json.dumps(r), flush=True)
     elif a.osx:
