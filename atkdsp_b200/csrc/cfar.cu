@@ -11,7 +11,9 @@
  *
  * The reference-cell table is cell-major (idx[q * nbins + i]), so the threads
  * of a warp, one bin each, read one table row with coalesced loads; the
- * frame's X row they index stays in L1 / L2.
+ * frame's X row they index stays in L1 / L2. Each hit row is written twice:
+ * as bytes (the W1 gate's layout) and as a bitmask from one warp ballot per
+ * 32 bins, which is what the host tracker reads.
  */
 #include <cuda_runtime.h>
 #include <math.h>
@@ -55,24 +57,12 @@ __global__ void __launch_bounds__(kThreads) cfar_mean_kernel(const double *__res
     X[(f - f0) * nbins + i] = __ddiv_rn(s, (double)k);
 }
 
-__global__ void __launch_bounds__(kThreads) cfar_cell_kernel(long long f0, long long t0, long long nbins, int mode,
-                                                             int n_ref, int N, int os_k, double alpha,
-                                                             double alpha_ca, double et,
-                                                             const uint8_t *__restrict__ ok,
-                                                             const uint8_t *__restrict__ sided,
-                                                             const int32_t *__restrict__ idx,
-                                                             const double *__restrict__ X,
-                                                             double *__restrict__ noise, double *__restrict__ thr,
-                                                             uint8_t *__restrict__ hits) {
-    const long long i = (long long)blockIdx.x * kThreads + threadIdx.x;
-    const long long row = (t0 - f0 + blockIdx.y) * nbins;
-    if (i >= nbins) return;
-    if (!ok[i]) {
-        noise[row + i] = CUDART_NAN;
-        thr[row + i] = CUDART_NAN;
-        hits[row + i] = 0;
-        return;
-    }
+/* one testable bin's statistic, threshold and hit */
+__device__ __forceinline__ bool cell_test(long long i, long long row, long long nbins, int mode, int n_ref, int N,
+                                          int os_k, double alpha, double alpha_ca, double et,
+                                          const uint8_t *__restrict__ sided, const int32_t *__restrict__ idx,
+                                          const double *__restrict__ X, double *__restrict__ noise,
+                                          double *__restrict__ thr) {
     const double *Xr = X + row;
     double Z, a = alpha, scale = et;
     if (mode == 1) {
@@ -117,7 +107,60 @@ __global__ void __launch_bounds__(kThreads) cfar_cell_kernel(long long f0, long 
     const double t = __dmul_rn(a, Z);
     thr[row + i] = t;
     noise[row + i] = __ddiv_rn(Z, scale);
-    hits[row + i] = Xr[i] > t;
+    return Xr[i] > t;
+}
+
+__global__ void __launch_bounds__(kThreads) cfar_cell_kernel(long long f0, long long t0, long long nbins, int mode,
+                                                             int n_ref, int N, int os_k, double alpha,
+                                                             double alpha_ca, double et,
+                                                             const uint8_t *__restrict__ ok,
+                                                             const uint8_t *__restrict__ sided,
+                                                             const int32_t *__restrict__ idx,
+                                                             const double *__restrict__ X,
+                                                             double *__restrict__ noise, double *__restrict__ thr,
+                                                             uint8_t *__restrict__ hits, uint32_t *__restrict__ bits,
+                                                             long long words) {
+    const long long i = (long long)blockIdx.x * kThreads + threadIdx.x;
+    const long long f = t0 - f0 + blockIdx.y;
+    const long long row = f * nbins;
+    bool hit = false;
+    if (i < nbins && !ok[i]) {
+        noise[row + i] = CUDART_NAN;
+        thr[row + i] = CUDART_NAN;
+        hits[row + i] = 0;
+    } else if (i < nbins) {
+        hit = cell_test(i, row, nbins, mode, n_ref, N, os_k, alpha, alpha_ca, et, sided, idx, X, noise, thr);
+        hits[row + i] = hit;
+    }
+    /* the row as a bitmask too: bin i is bit i % 32 of word i / 32 */
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    if ((threadIdx.x & 31) == 0 && (i >> 5) < words) bits[f * words + (i >> 5)] = m;
+}
+
+
+
+/* a pass's rows at its columns: rows of X and noise (row r of X / noise to
+ * row r of Xc / Nc), then nraw raw rows from frame rf0 on (to Rc) */
+__global__ void __launch_bounds__(kThreads) cfar_gather_kernel(const double *__restrict__ X,
+                                                               const double *__restrict__ noise, long long nbins,
+                                                               int rows, const double *__restrict__ raw, int ring,
+                                                               long long rf0, int nraw,
+                                                               const int32_t *__restrict__ cols, int ncol,
+                                                               double *__restrict__ Xc, double *__restrict__ Nc,
+                                                               double *__restrict__ Rc) {
+    const long long total = (long long)(rows + nraw) * ncol;
+    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < total;
+         e += (long long)gridDim.x * kThreads) {
+        const long long r = e / ncol, q = e - r * ncol;
+        const long long b = cols[q];
+        if (r < rows) {
+            Xc[e] = X[r * nbins + b];
+            Nc[e] = noise[r * nbins + b];
+        } else {
+            const long long rr = r - rows;
+            Rc[rr * ncol + q] = raw[((rf0 + rr) % ring) * nbins + b];
+        }
+    }
 }
 
 int grid_for(long long work) {
@@ -138,7 +181,8 @@ extern "C" int atkb_cfar_raw(const float *frames, int units, long long f0, int n
 extern "C" int atkb_cfar_test(const double *raw, int ring, long long f0, long long t0, int nf, long long nbins,
                               int k, int mode, int n_ref, int n_cells, int os_k, double alpha, double alpha_ca,
                               double et, const uint8_t *ok, const uint8_t *sided, const int32_t *idx, double *X,
-                              double *noise, double *thr, uint8_t *hits, void *stream) {
+                              double *noise, double *thr, uint8_t *hits, uint32_t *bits, long long words,
+                              void *stream) {
     const long long ntest = f0 + nf - t0;
     if (ntest <= 0) return ATKB_OK;
     if (ntest > 65535 || nbins <= 0) return ATKB_E_ARG;
@@ -146,6 +190,15 @@ extern "C" int atkb_cfar_test(const double *raw, int ring, long long f0, long lo
     cudaStream_t s = (cudaStream_t)stream;
     cfar_mean_kernel<<<grid, kThreads, 0, s>>>(raw, ring, f0, t0, nbins, k, X);
     cfar_cell_kernel<<<grid, kThreads, 0, s>>>(f0, t0, nbins, mode, n_ref, n_cells, os_k, alpha, alpha_ca, et, ok,
-                                               sided, idx, X, noise, thr, hits);
+                                               sided, idx, X, noise, thr, hits, bits, words);
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
+extern "C" int atkb_cfar_gather(const double *X, const double *noise, long long nbins, int rows, const double *raw,
+                                int ring, long long rf0, int nraw, const int32_t *cols, int ncol, double *Xc,
+                                double *Nc, double *Rc, void *stream) {
+    if (ncol <= 0 || rows + nraw <= 0) return ATKB_OK;
+    cfar_gather_kernel<<<grid_for((long long)(rows + nraw) * ncol), kThreads, 0, (cudaStream_t)stream>>>(
+        X, noise, nbins, rows, raw, ring, rf0, nraw, cols, ncol, Xc, Nc, Rc);
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }

@@ -385,6 +385,10 @@ typedef struct {
     int track;
 } cf_blob;
 
+typedef struct {
+    int32_t lo, hi;
+} cf_span;
+
 struct atkdsp_cfar {
     atkdsp_cfar_config cfg;
     size_t nbins;
@@ -402,17 +406,28 @@ struct atkdsp_cfar {
     int has_last;
     double *last_X, *last_thr;
     uint8_t *last_hits;
-    /* device: tables, the raw ring (frame F in row F % ring), a pass's rows */
+    /* device: tables; the raw ring (frame F in row F % ring); two sets of a
+     * pass's rows (hits, X, noise, thr); a pass's rows at its columns */
     int fc, ring;
-    void *stream, *ev_in, *ev_pass[2];
+    void *stream, *gstream, *ev_in, *ev_pass[2];
     uint8_t *d_ok, *d_sided, *d_hits;
-    int32_t *d_idx;
+    uint32_t *d_bits;             /* hit rows as bits, `words` per row */
+    size_t words;
+    int32_t *d_idx, *d_cols;
     double *d_raw, *d_X, *d_noise, *d_thr;
+    double *d_Xc, *d_Nc, *d_Rc;
     float *d_frames;
-    /* host copies of two passes' rows (pinned when small) and the raw ring */
+    /* host (pinned when small): two sets of hit bit rows; the gathered rows of
+     * the pass being tracked: X and noise of its tested frames, raw of those
+     * frames and the k - 1 before them, all at the pass's columns */
     int pinned;
-    double *h_X, *h_noise, *h_raw;
-    uint8_t *h_hits;
+    uint32_t *h_bits;
+    double *h_Xc, *h_Nc, *h_Rc;
+    int32_t *h_cols, *colmap;     /* colmap[bin]: its column, -1 outside */
+    int ncol;
+    int64_t rc_f0;                /* the frame of h_Rc's row 0 */
+    cf_span *spans;
+    size_t spans_cap;
     double *ht, *hd;              /* frame start and duration by ring row */
 };
 
@@ -545,23 +560,32 @@ ATKDSP_API void atkdsp_cfar_destroy(atkdsp_cfar *c) {
     free(c->last_hits);
     free(c->ht);
     free(c->hd);
-    host_buf_free(c, c->h_X);
-    host_buf_free(c, c->h_noise);
-    host_buf_free(c, c->h_raw);
-    host_buf_free(c, c->h_hits);
+    host_buf_free(c, c->h_bits);
+    host_buf_free(c, c->h_Xc);
+    host_buf_free(c, c->h_Nc);
+    host_buf_free(c, c->h_Rc);
+    host_buf_free(c, c->h_cols);
+    free(c->colmap);
+    free(c->spans);
     atkb_free(c->d_ok);
     atkb_free(c->d_sided);
     atkb_free(c->d_idx);
     atkb_free(c->d_hits);
+    atkb_free(c->d_bits);
     atkb_free(c->d_raw);
     atkb_free(c->d_X);
     atkb_free(c->d_noise);
     atkb_free(c->d_thr);
+    atkb_free(c->d_cols);
+    atkb_free(c->d_Xc);
+    atkb_free(c->d_Nc);
+    atkb_free(c->d_Rc);
     atkb_free(c->d_frames);
     if (c->ev_in) atkb_event_destroy(c->ev_in);
     if (c->ev_pass[0]) atkb_event_destroy(c->ev_pass[0]);
     if (c->ev_pass[1]) atkb_event_destroy(c->ev_pass[1]);
     if (c->stream) atkb_stream_destroy(c->stream);
+    if (c->gstream) atkb_stream_destroy(c->gstream);
     free(c);
 }
 
@@ -596,7 +620,10 @@ ATKDSP_API atkdsp_cfar *atkdsp_cfar_create(size_t nbins, const atkdsp_cfar_confi
     c->fc = (int)fc;
     c->ring = 2 * c->fc + k - 1;
     const size_t nb = nbins, rows = (size_t)c->fc, ring = (size_t)c->ring;
-    c->pinned = (2 * rows * nb * 17 + (k > 1 ? ring * nb * 8 : 0)) <= CF_PINNED_MAX;
+    const size_t rrows = rows + (size_t)k - 1;     /* raw rows a pass's tracker reads */
+    c->words = (nb + 31) / 32;
+    const size_t W = c->words;
+    c->pinned = (2 * rows * W * 4 + 2 * rows * nb * 8 + (k > 1 ? rrows * nb * 8 : 0) + nb * 4) <= CF_PINNED_MAX;
     c->next_id = 1;
     c->mask = (uint8_t *)calloc(nb, 1);
     c->ok = (uint8_t *)calloc(nb, 1);
@@ -609,18 +636,22 @@ ATKDSP_API atkdsp_cfar *atkdsp_cfar_create(size_t nbins, const atkdsp_cfar_confi
     c->last_hits = (uint8_t *)calloc(nb, 1);
     c->ht = (double *)calloc(ring, sizeof(double));
     c->hd = (double *)calloc(ring, sizeof(double));
+    c->colmap = (int32_t *)malloc(nb * sizeof(int32_t));
     int rc = (c->mask && c->ok && c->sided && c->beta && c->tracks && c->blobs && c->last_X && c->last_thr &&
-              c->last_hits && c->ht && c->hd)
+              c->last_hits && c->ht && c->hd && c->colmap)
                  ? ATKB_OK
                  : ATKB_E_NOMEM;
     if (rc == ATKB_OK) {
-        c->h_X = (double *)host_buf(c, 2 * rows * nb * sizeof(double));
-        c->h_noise = (double *)host_buf(c, 2 * rows * nb * sizeof(double));
-        c->h_hits = (uint8_t *)host_buf(c, 2 * rows * nb);
-        if (k > 1) c->h_raw = (double *)host_buf(c, ring * nb * sizeof(double));
-        if (!c->h_X || !c->h_noise || !c->h_hits || (k > 1 && !c->h_raw)) rc = ATKB_E_NOMEM;
+        for (size_t i = 0; i < nb; ++i) c->colmap[i] = -1;
+        c->h_bits = (uint32_t *)host_buf(c, 2 * rows * W * sizeof(uint32_t));
+        c->h_Xc = (double *)host_buf(c, rows * nb * sizeof(double));
+        c->h_Nc = (double *)host_buf(c, rows * nb * sizeof(double));
+        if (k > 1) c->h_Rc = (double *)host_buf(c, rrows * nb * sizeof(double));
+        c->h_cols = (int32_t *)host_buf(c, nb * sizeof(int32_t));
+        if (!c->h_bits || !c->h_Xc || !c->h_Nc || (k > 1 && !c->h_Rc) || !c->h_cols) rc = ATKB_E_NOMEM;
     }
     if (rc == ATKB_OK) rc = atkb_stream_create(&c->stream);
+    if (rc == ATKB_OK) rc = atkb_stream_create(&c->gstream);
     if (rc == ATKB_OK) rc = atkb_event_create(&c->ev_in);
     if (rc == ATKB_OK) rc = atkb_event_create(&c->ev_pass[0]);
     if (rc == ATKB_OK) rc = atkb_event_create(&c->ev_pass[1]);
@@ -628,10 +659,15 @@ ATKDSP_API atkdsp_cfar *atkdsp_cfar_create(size_t nbins, const atkdsp_cfar_confi
     if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_sided, nb);
     if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_idx, nb * (size_t)c->N * sizeof(int32_t));
     if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_raw, ring * nb * sizeof(double));
-    if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_X, rows * nb * sizeof(double));
-    if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_noise, rows * nb * sizeof(double));
-    if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_thr, rows * nb * sizeof(double));
-    if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_hits, rows * nb);
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_X, 2 * rows * nb * sizeof(double));
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_noise, 2 * rows * nb * sizeof(double));
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_thr, 2 * rows * nb * sizeof(double));
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_hits, 2 * rows * nb);
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_bits, 2 * rows * W * sizeof(uint32_t));
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_cols, nb * sizeof(int32_t));
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_Xc, rows * nb * sizeof(double));
+    if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_Nc, rows * nb * sizeof(double));
+    if (rc == ATKB_OK && k > 1) rc = atkb_malloc((void **)&c->d_Rc, rrows * nb * sizeof(double));
     if (rc == ATKB_OK) rc = atkb_malloc((void **)&c->d_frames, rows * nb * sizeof(float));
     if (rc == ATKB_OK) rc = tables_build(c);
     if (rc != ATKB_OK) {
@@ -669,14 +705,16 @@ static double band_beta(atkdsp_cfar *c, int nb) {
 }
 
 /* the single-frame band test: the raw power over the testable bins of
- * [lo, hi] against beta x their noise (this frame's estimate) */
+ * [lo, hi] against beta x their noise (this frame's estimate); raw and
+ * noise are rows at the pass's columns */
 static int band_pass(atkdsp_cfar *c, const double *raw, const double *noise, int32_t lo, int32_t hi) {
+    const int32_t *cm = c->colmap;
     double sr = 0.0, sz = 0.0;
     int nb = 0;
     for (int32_t b = lo; b <= hi; ++b) {
         if (c->ok[b]) {
-            sr += raw[b];
-            sz += noise[b];
+            sr += raw[cm[b]];
+            sz += noise[cm[b]];
             ++nb;
         }
     }
@@ -743,30 +781,34 @@ static int popcount64(uint64_t x) {
     return n;
 }
 
-/* the first hit at or after i (nb if none), eight bins at a time */
-static long next_hit(const uint8_t *h, long i, long nb) {
-    for (; i < nb && (i & 7); ++i)
-        if (h[i]) return i;
-    for (; i + 8 <= nb; i += 8) {
-        uint64_t w;
-        memcpy(&w, h + i, 8);
-        if (w) {
-            while (!h[i]) ++i;
-            return i;
-        }
+/* hit rows are bitmasks: bin b is bit b % 32 of word b / 32 */
+static int bit_at(const uint32_t *w, long b) { return (int)((w[b >> 5] >> (b & 31)) & 1u); }
+
+/* the first hit at or after i (nb if none), 32 bins a word */
+static long next_hit(const uint32_t *w, long i, long nb) {
+    if (i >= nb) return nb;
+    const long nw = (nb + 31) >> 5;
+    long q = i >> 5;
+    uint32_t m = w[q] & (0xffffffffu << (i & 31));
+    while (!m) {
+        if (++q >= nw) return nb;
+        m = w[q];
     }
-    for (; i < nb; ++i)
-        if (h[i]) return i;
-    return nb;
+    const long r = (q << 5) + __builtin_ctz(m);
+    return r < nb ? r : nb;
 }
 
-/* One tested frame F (absolute), its rows from the device: X, noise, hits;
- * raw rows by ring row. Returns the events written. */
-static size_t track_frame(atkdsp_cfar *c, int64_t F, const double *X, const double *noise, const uint8_t *hits,
+/* One tested frame F (absolute): its hit row (every bin) and its X and noise
+ * rows at the pass's columns (colmap), the raw rows at the same columns
+ * from h_Rc. Every bin the tracker reads is a column: the pass's blobs and
+ * every span a track can take during the pass lie in them (pass_columns).
+ * Returns the events written. */
+static size_t track_frame(atkdsp_cfar *c, int64_t F, const double *X, const double *noise, const uint32_t *hits,
                           double tf, double dt, atkdsp_cfar_event *ev) {
     const long nb = (long)c->nbins;
     const int k = c->cfg.k_frames;
-    const double *raw = k > 1 ? c->h_raw + (size_t)(F % c->ring) * (size_t)nb : NULL;
+    const int32_t *cm = c->colmap;
+    const double *raw = k > 1 ? c->h_Rc + (size_t)(F - c->rc_f0) * (size_t)c->ncol : NULL;
     c->st.cells_tested += c->n_ok;
     c->st.untestable += c->n_untestable;
 
@@ -777,14 +819,11 @@ static size_t track_frame(atkdsp_cfar *c, int64_t F, const double *X, const doub
     long i = 0;
     while ((i = next_hit(hits, i, nb)) < nb) {
         long lo = i, hi = i, prev = i;
-        for (long j = i + 1; j < nb; ++j) {
-            if (j - prev - 1 > g) break;
-            if (hits[j]) {
-                hi = j;
-                prev = j;
-            }
+        for (long j; (j = next_hit(hits, prev + 1, nb)) < nb && j - prev - 1 <= g;) {
+            hi = j;
+            prev = j;
         }
-        for (long b = lo; b <= hi; ++b) nhit += hits[b];
+        for (long b = lo; b <= hi; ++b) nhit += (uint64_t)bit_at(hits, b);
         i = hi + 1;
         if (hi - lo + 1 < c->cfg.min_bins) continue;
         cf_blob *o = &c->blobs[nblob++];
@@ -793,17 +832,18 @@ static size_t track_frame(atkdsp_cfar *c, int64_t F, const double *X, const doub
         o->sbe = o->se = o->sx = o->sn = 0.0;
         long pk = -1;
         for (long b = lo; b <= hi; ++b) {
-            if (!hits[b]) continue;
-            double e = X[b] - noise[b];
+            if (!bit_at(hits, b)) continue;
+            const double xb = X[cm[b]], nz = noise[cm[b]];
+            double e = xb - nz;
             if (e < 0.0) e = 0.0;
             o->sbe += (double)b * e;
             o->se += e;
-            o->sx += X[b];
-            o->sn += noise[b];
-            if (pk < 0 || X[b] > X[pk]) pk = b;
+            o->sx += xb;
+            o->sn += nz;
+            if (pk < 0 || xb > X[cm[pk]]) pk = b;
         }
-        o->px = X[pk];
-        o->pn = noise[pk];
+        o->px = X[cm[pk]];
+        o->pn = noise[cm[pk]];
         o->track = -1;
     }
     c->st.cell_hits += nhit;
@@ -907,7 +947,7 @@ static size_t track_frame(atkdsp_cfar *c, int64_t F, const double *X, const doub
                     for (int r = 0; r < k; ++r) {
                         const int64_t Fr = F - k + 1 + r;
                         const size_t row = (size_t)(Fr % c->ring);
-                        if (band_pass(c, c->h_raw + row * (size_t)nb, noise, lo, hi)) {
+                        if (band_pass(c, c->h_Rc + (size_t)(Fr - c->rc_f0) * (size_t)c->ncol, noise, lo, hi)) {
                             tr->t0 = c->ht[row];
                             found = 1;
                             break;
@@ -952,18 +992,21 @@ static size_t track_frame(atkdsp_cfar *c, int64_t F, const double *X, const doub
 
 /* ================================================= a call */
 
-/* One pass: frames [done, done + nf) of a call whose first frame is F_start
- * with seen_start frames seen before it. Enqueues the conversion, the test
- * and the copies of the pass's rows into host set `set`; nothing waits. */
+/* One pass: frames [done, done + nf) of a call; F0 the absolute frame of its
+ * first, j0 its first tested frame (earlier ones are warm-up). */
 typedef struct {
     size_t done;
     int nf;
     int64_t F0, j0;
 } cf_pass;
 
+/* Enqueue a pass on the handle's stream: conversion into the raw ring, the
+ * test into device row set `set`, the hit rows into host set `set`, the
+ * caller's device hit masks. Nothing waits. */
 static int pass_enqueue(atkdsp_cfar *c, const cf_pass *ps, const float *frames, int on_device, int units, int set,
                         uint8_t *d_hits_out) {
-    const size_t nb = c->nbins, hs = (size_t)set * (size_t)c->fc * nb;
+    const size_t nb = c->nbins, hs = (size_t)set * (size_t)c->fc * nb, W = c->words;
+    const size_t bs = (size_t)set * (size_t)c->fc * W;
     const int k = c->cfg.k_frames, nf = ps->nf;
     const int64_t F0 = ps->F0, j0 = ps->j0;
     const float *src = frames + ps->done * nb;
@@ -975,35 +1018,94 @@ static int pass_enqueue(atkdsp_cfar *c, const cf_pass *ps, const float *frames, 
     if (rc == ATKB_OK) rc = atkb_cfar_raw(src, units, F0, nf, (long long)nb, c->d_raw, c->ring, c->stream);
     if (rc == ATKB_OK && j0 < nf)
         rc = atkb_cfar_test(c->d_raw, c->ring, F0, F0 + j0, nf, (long long)nb, k, c->cfg.mode, c->cfg.n_ref, c->N,
-                            c->cfg.os_k, c->alpha, c->alpha_ca, c->et, c->d_ok, c->d_sided, c->d_idx, c->d_X,
-                            c->d_noise, c->d_thr, c->d_hits, c->stream);
+                            c->cfg.os_k, c->alpha, c->alpha_ca, c->et, c->d_ok, c->d_sided, c->d_idx, c->d_X + hs,
+                            c->d_noise + hs, c->d_thr + hs, c->d_hits + hs, c->d_bits + bs, (long long)W,
+                            c->stream);
     if (rc == ATKB_OK && j0 < nf) {
         const size_t off = (size_t)j0 * nb, rows = (size_t)(nf - j0) * nb;
-        rc = atkb_d2h(c->h_hits + hs + off, c->d_hits + off, rows, c->stream);
-        if (rc == ATKB_OK) rc = atkb_d2h(c->h_X + hs + off, c->d_X + off, rows * sizeof(double), c->stream);
-        if (rc == ATKB_OK) rc = atkb_d2h(c->h_noise + hs + off, c->d_noise + off, rows * sizeof(double), c->stream);
+        rc = atkb_d2h(c->h_bits + bs + (size_t)j0 * W, c->d_bits + bs + (size_t)j0 * W,
+                      (size_t)(nf - j0) * W * sizeof(uint32_t), c->stream);
         if (rc == ATKB_OK && d_hits_out)
-            rc = atkb_d2d(d_hits_out + (ps->done + (size_t)j0) * nb, c->d_hits + off, rows, c->stream);
+            rc = atkb_d2d(d_hits_out + (ps->done + (size_t)j0) * nb, c->d_hits + hs + off, rows, c->stream);
     }
     if (rc == ATKB_OK && d_hits_out && j0 > 0)
         rc = atkb_memset(d_hits_out + ps->done * nb, 0, (size_t)(j0 < nf ? j0 : nf) * nb, c->stream);
-    if (rc == ATKB_OK && k > 1) {
-        /* the pass's raw rows into the host ring, in at most two runs */
-        const size_t r0 = (size_t)(F0 % c->ring);
-        const size_t first = (size_t)nf < (size_t)c->ring - r0 ? (size_t)nf : (size_t)c->ring - r0;
-        rc = atkb_d2h(c->h_raw + r0 * nb, c->d_raw + r0 * nb, first * nb * sizeof(double), c->stream);
-        if (rc == ATKB_OK && first < (size_t)nf)
-            rc = atkb_d2h(c->h_raw, c->d_raw, ((size_t)nf - first) * nb * sizeof(double), c->stream);
-    }
     if (rc == ATKB_OK) rc = atkb_event_record(c->ev_pass[set], c->stream);
     return rc;
 }
 
+static int span_cmp(const void *a, const void *b) {
+    const cf_span *x = (const cf_span *)a, *y = (const cf_span *)b;
+    return x->lo < y->lo ? -1 : x->lo > y->lo;
+}
+
+static int span_push(atkdsp_cfar *c, size_t *n, int32_t lo, int32_t hi) {
+    if (*n == c->spans_cap) {
+        const size_t cap = c->spans_cap ? 2 * c->spans_cap : 1024;
+        cf_span *p = (cf_span *)realloc(c->spans, cap * sizeof(cf_span));
+        if (!p) return ATKB_E_NOMEM;
+        c->spans = p;
+        c->spans_cap = cap;
+    }
+    c->spans[*n].lo = lo;
+    c->spans[*n].hi = hi;
+    ++*n;
+    return ATKB_OK;
+}
+
+/* The bins the tracker can read while it walks a pass, as columns (h_cols,
+ * colmap): the runs of hits of the pass's tested frames (bit rows j0..nf-1
+ * of `hits`) and the spans of the tracks alive before it, joined whenever two
+ * lie within merge_gap + 1 bins of each other. A blob joins a track only
+ * within that reach of the track's span, and the track's next span is the
+ * hull of its blobs, so by induction every span a track takes during the
+ * pass stays inside one joined interval; so do the blobs and their hits. */
+static int pass_columns(atkdsp_cfar *c, const uint32_t *hits, int j0, int nf) {
+    const long nb = (long)c->nbins, g = c->cfg.merge_gap, reach = g + 1;
+    size_t n = 0;
+    for (int j = j0; j < nf; ++j) {
+        const uint32_t *row = hits + (size_t)j * c->words;
+        long i = 0;
+        while ((i = next_hit(row, i, nb)) < nb) {
+            long hi = i, prev = i;
+            for (long q; (q = next_hit(row, prev + 1, nb)) < nb && q - prev - 1 <= g;) {
+                hi = q;
+                prev = q;
+            }
+            if (span_push(c, &n, (int32_t)i, (int32_t)hi) != ATKB_OK) return ATKB_E_NOMEM;
+            i = hi + 1;
+        }
+    }
+    for (int t = 0; t < c->ntracks; ++t)
+        if (span_push(c, &n, c->tracks[t].cur_lo, c->tracks[t].cur_hi) != ATKB_OK) return ATKB_E_NOMEM;
+    qsort(c->spans, n, sizeof(cf_span), span_cmp);
+    int ncol = 0;
+    for (size_t q = 0; q < n;) {
+        long lo = c->spans[q].lo, hi = c->spans[q].hi;
+        for (++q; q < n && (long)c->spans[q].lo <= hi + reach; ++q)
+            if ((long)c->spans[q].hi > hi) hi = c->spans[q].hi;
+        if (lo < 0) lo = 0;
+        if (hi > nb - 1) hi = nb - 1;
+        for (long b = lo; b <= hi; ++b) {
+            c->colmap[b] = ncol;
+            c->h_cols[ncol++] = (int32_t)b;
+        }
+    }
+    c->ncol = ncol;
+    return ATKB_OK;
+}
+
+static void columns_clear(atkdsp_cfar *c) {
+    for (int q = 0; q < c->ncol; ++q) c->colmap[c->h_cols[q]] = -1;
+    c->ncol = 0;
+}
+
 /* frames: host (on_device 0) or device floats, nframes x nbins; d_hits_out:
  * device, nframes x nbins, or NULL. The call runs in passes of at most fc
- * frames; while the host tracks pass i, the GPU converts, tests and copies
- * pass i + 1 into the other host set (the raw ring holds both passes and the
- * k - 1 frames before them). */
+ * frames. While the host tracks pass i, the GPU converts and tests pass
+ * i + 1 into the other row set and copies its hit rows. For the pass it
+ * tracks, the host then fetches X, noise and raw at that pass's columns
+ * only (a gather on a second stream), not the whole rows. */
 static ptrdiff_t cfar_run(atkdsp_cfar *c, const float *frames, int on_device, int units, size_t nframes,
                           double frame_t0, double frame_dt, atkdsp_cfar_event *ev, size_t cap, uint8_t *d_hits_out,
                           void *stream) {
@@ -1041,12 +1143,33 @@ static ptrdiff_t cfar_run(atkdsp_cfar *c, const float *frames, int on_device, in
             rc = pass_enqueue(c, &next, frames, on_device, units, (int)((i + 1) & 1), d_hits_out);
         }
         const int set = (int)(i & 1);
+        const size_t hs = (size_t)set * (size_t)c->fc * nb, bs = (size_t)set * (size_t)c->fc * c->words;
         if (rc == ATKB_OK) rc = atkb_event_sync(c->ev_pass[set]);
+        const int j0 = (int)cur.j0;
+        if (rc == ATKB_OK && j0 < cur.nf) {
+            rc = pass_columns(c, c->h_bits + bs, j0, cur.nf);
+            c->rc_f0 = cur.F0 + j0 - (k - 1);
+            if (rc == ATKB_OK && c->ncol > 0) {
+                const int rows = cur.nf - j0, nraw = k > 1 ? rows + k - 1 : 0;
+                const size_t nc = (size_t)c->ncol;
+                rc = atkb_h2d(c->d_cols, c->h_cols, nc * sizeof(int32_t), c->gstream);
+                if (rc == ATKB_OK)
+                    rc = atkb_cfar_gather(c->d_X + hs + (size_t)j0 * nb, c->d_noise + hs + (size_t)j0 * nb,
+                                          (long long)nb, rows, c->d_raw, c->ring, c->rc_f0, nraw, c->d_cols,
+                                          c->ncol, c->d_Xc, c->d_Nc, c->d_Rc, c->gstream);
+                if (rc == ATKB_OK) rc = atkb_d2h(c->h_Xc, c->d_Xc, (size_t)rows * nc * sizeof(double), c->gstream);
+                if (rc == ATKB_OK) rc = atkb_d2h(c->h_Nc, c->d_Nc, (size_t)rows * nc * sizeof(double), c->gstream);
+                if (rc == ATKB_OK && nraw)
+                    rc = atkb_d2h(c->h_Rc, c->d_Rc, (size_t)nraw * nc * sizeof(double), c->gstream);
+                if (rc == ATKB_OK) rc = atkb_stream_sync(c->gstream);
+            }
+        }
         if (rc != ATKB_OK) {
+            columns_clear(c);
             atkb_stream_sync(c->stream);
+            atkb_stream_sync(c->gstream);
             return atkb_map_rc(rc);
         }
-        const size_t hs = (size_t)set * (size_t)c->fc * nb;
         for (int j = 0; j < cur.nf; ++j) {
             const int64_t F = cur.F0 + j;
             const double tf = frame_t0 + (double)(cur.done + (size_t)j) * frame_dt;
@@ -1060,22 +1183,25 @@ static ptrdiff_t cfar_run(atkdsp_cfar *c, const float *frames, int on_device, in
                 c->st.warmup++;
                 continue;
             }
-            const size_t o = hs + (size_t)j * nb;
-            nev += track_frame(c, F, c->h_X + o, c->h_noise + o, c->h_hits + o, tf, frame_dt, ev + nev);
+            const size_t oc = (size_t)(j - j0) * (size_t)c->ncol;
+            nev += track_frame(c, F, c->h_Xc + oc, c->h_Nc + oc, c->h_bits + bs + (size_t)j * c->words, tf,
+                               frame_dt, ev + nev);
             last_set = set;
             last_row = j;
         }
+        columns_clear(c);
     }
     if (last_row >= 0) {
-        /* the last tested frame is in the last pass, whose rows d_thr still holds */
+        /* the last tested frame is in the last pass, whose rows nothing overwrote */
         const size_t o = (size_t)last_set * (size_t)c->fc * nb + (size_t)last_row * nb;
-        memcpy(c->last_X, c->h_X + o, nb * sizeof(double));
-        memcpy(c->last_hits, c->h_hits + o, nb);
-        rc = atkb_d2h(c->last_thr, c->d_thr + (size_t)last_row * nb, nb * sizeof(double), c->stream);
+        const uint32_t *lb = c->h_bits + ((size_t)last_set * (size_t)c->fc + (size_t)last_row) * c->words;
+        for (size_t b = 0; b < nb; ++b) c->last_hits[b] = (uint8_t)bit_at(lb, (long)b);
+        rc = atkb_d2h(c->last_X, c->d_X + o, nb * sizeof(double), c->stream);
+        if (rc == ATKB_OK) rc = atkb_d2h(c->last_thr, c->d_thr + o, nb * sizeof(double), c->stream);
         if (rc == ATKB_OK) rc = atkb_stream_sync(c->stream);
         if (rc != ATKB_OK) return atkb_map_rc(rc);
         c->has_last = 1;
-    } else if (d_hits_out) {
+    } else {
         rc = atkb_stream_sync(c->stream);
         if (rc != ATKB_OK) return atkb_map_rc(rc);
     }

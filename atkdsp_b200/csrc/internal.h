@@ -273,13 +273,20 @@ int  atkb_spec_launch(int mode, const void *in, long long frames, long long hop,
  * raw rows f-k+1 .. f (oldest first), then each testable bin's statistic over
  * its n_cells reference cells (idx: n_cells x nbins, cell-major) and the
  * test; X, noise, thr (double) and hits (u8) rows go to row f - f0 of the
- * outputs (frames below t0 are left alone). */
+ * outputs, and the hits as bits (bin i: bit i % 32 of word i / 32, `words`
+ * words a row) to row f - f0 of `bits` (frames below t0 are left alone). */
 int  atkb_cfar_raw(const float *frames, int units, long long f0, int nf, long long nbins, double *raw, int ring,
                    void *stream);
 int  atkb_cfar_test(const double *raw, int ring, long long f0, long long t0, int nf, long long nbins, int k,
                     int mode, int n_ref, int n_cells, int os_k, double alpha, double alpha_ca, double et,
                     const uint8_t *ok, const uint8_t *sided, const int32_t *idx, double *X, double *noise,
-                    double *thr, uint8_t *hits, void *stream);
+                    double *thr, uint8_t *hits, uint32_t *bits, long long words, void *stream);
+/* the rows the tracker reads, at the columns `cols` (ncol bins) only: rows
+ * 0..rows-1 of X and noise (stride nbins) into Xc / Nc (stride ncol), and
+ * raw frames rf0 .. rf0+nraw-1 from the ring into Rc (stride ncol) */
+int  atkb_cfar_gather(const double *X, const double *noise, long long nbins, int rows, const double *raw, int ring,
+                      long long rf0, int nraw, const int32_t *cols, int ncol, double *Xc, double *Nc, double *Rc,
+                      void *stream);
 
 /* unpack ------------------------------------------------------------------- */
 /* device raw -> device cf32 (out may be NULL: mean only), (x - c) * k per component; the means (double,
