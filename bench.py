@@ -26,8 +26,8 @@ Arms printed in ONE JSON line (rank 0):
               stream (C ABI, uneven blocks), the unpack front end, the
               coherent array, the overlap-save extractor (64 channels from
               one 61.44 MS/s stream), Undertow's six-scale filterbank bank
-              (one launch per chunk), the spectrum reduction, the serving
-              loop
+              (one launch per chunk), the spectrum reduction, the CFAR
+              detector and tracker (W3's gate, Mcells/s), the serving loop
 
 --impl reference runs only the reference's CPU channelizer (all host threads)
 on the same workload and prints its line.
