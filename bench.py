@@ -513,6 +513,20 @@ def _c3_arm(torch, device, steps):
 OSX_N = 1 << 24
 
 
+def _osx_fold_rate(nch: int, nfft: int, n: int, sec: float) -> dict:
+    """What bounds the extractor: its exact fold, not HBM. Every block of
+    nfft / 2 new samples folds all nfft spectrum bins into each channel, one
+    complex product and add per bin, as 8 separately rounded FP32 operations
+    (4 multiplies, 2 adds, 2 accumulating adds: no FMA, for the reference's
+    rounding). Against the FP32 pipe's 128 operations per SM per clock (148
+    SMs at the 1965 MHz maximum: 37.2 T operations/s)."""
+    blocks = n / (nfft // 2)
+    ops = nch * nfft * 8 * blocks
+    peak = 148 * 128 * 1.965e9
+    return {"fp32_ops_per_step": int(ops), "tops": round(ops / sec / 1e12, 2), "peak_tops": round(peak / 1e12, 1),
+            "frac": round(ops / sec / peak, 3), "what": "rounded FP32 multiplies and adds of the fold"}
+
+
 def _osx_arm(torch, device, steps, cpu: bool):
     """The overlap-save extractor: one 61.44 MS/s cf32 stream (noise + tones),
     nfft 4096, 64 channels (workloads.extractor_channels). value: atkdsp_gpu_osx_process_n on
@@ -594,6 +608,7 @@ def _osx_arm(torch, device, steps, cpu: bool):
                    "path": "atkdsp_osx_process, pinned host buffers"},
            "dropin": {"value": round(OSX_N / te["pageable"] / 1e6, 2), "unit": "MSamples/s",
                       "path": "atkdsp_osx_process, pageable host buffers"},
+           "fold": _osx_fold_rate(len(slots), OSX_NFFT, OSX_N, dt / k),
            "out_samples_per_step": out_samples,
            "path": "atkdsp_gpu_osx_process_n: fused transform + 64 channel folds/inverses/rolls per block, "
                    "resampler, state carry"}
