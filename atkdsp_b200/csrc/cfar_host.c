@@ -26,7 +26,7 @@
 #define CF_PI 3.14159265358979323846
 #define CF_LN10 2.302585092994045684
 /* frames per device pass: at most this many cells, and at most 4096 frames */
-#define CF_PASS_CELLS ((size_t)1 << 19)
+#define CF_PASS_CELLS ((size_t)1 << 20)
 #define CF_PASS_FRAMES 4096
 /* host buffers up to this size are pinned */
 #define CF_PINNED_MAX ((size_t)256 << 20)

@@ -109,8 +109,8 @@ def test_events_do_not_depend_on_how_frames_are_split(golden_cfar, name):
 
 
 def test_device_frames_many_passes_against_the_oracle():
-    """65536 bins: 64 frames per device pass, so 150 frames take three passes
-    with k_frames = 3 spanning them. The device hit masks (every frame's, from
+    """65536 bins: 16 frames per device pass (2^20 cells), so 150 frames take
+    ten passes, with k_frames = 3 windows spanning their boundaries. The device hit masks (every frame's, from
     atkdsp_gpu_cfar_process) against the numpy oracle's, and the events
     against the host entry point's."""
     import torch

@@ -92,7 +92,7 @@ def _frames(rng, nb, nf):
 
 @pytest.mark.skipif(O.reference() is None, reason="reference library not built")
 def test_many_passes_and_random_configurations_against_the_reference(emu):
-    """Passes of 2^19 cells: 65,536 bins make 8-frame passes, so tracks,
+    """Passes of 2^20 cells: 70,000 bins make 14-frame passes, so tracks,
     k-frame windows and the column sets cross many pass boundaries; calls of
     random length split them again."""
     rng = np.random.default_rng(2027)
