@@ -51,7 +51,7 @@ def _build(tmp: Path, checked: bool) -> _Lib:
     out = tmp / ("libcfar_emu_chk.so" if checked else "libcfar_emu.so")
     subprocess.run([gcc, "-std=c99", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-DATKDSP_BUILD=1",
                     f"-I{ROOT / 'include'}", f"-I{ROOT / 'atkdsp_b200' / 'csrc'}", str(src), str(EMU),
-                    "-o", str(out), "-lm"], check=True)
+                    "-o", str(out), "-lm", "-lpthread"], check=True)
     return _Lib(out)
 
 
