@@ -57,7 +57,61 @@ __global__ void __launch_bounds__(kThreads) cfar_mean_kernel(const double *__res
     X[(f - f0) * nbins + i] = __ddiv_rn(s, (double)k);
 }
 
-/* one testable bin's statistic, threshold and hit */
+/* the k-th smallest (0-based) of a[0..n), NaN-free: Hoare's selection,
+ * partitioning around the middle element; i and j stay inside [lo, hi]
+ * because the pivot value stops both scans. The value is unique, whatever
+ * order the cells came in. */
+__device__ __forceinline__ double select_kth(double *a, int n, int k) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const double pivot = a[(lo + hi) >> 1];
+        int i = lo, j = hi;
+        while (i <= j) {
+            while (a[i] < pivot) ++i;
+            while (a[j] > pivot) --j;
+            if (i <= j) {
+                const double t = a[i];
+                a[i] = a[j];
+                a[j] = t;
+                ++i;
+                --j;
+            }
+        }
+        if (k <= j) hi = j;
+        else if (k >= i) lo = i;
+        else break;
+    }
+    return a[k];
+}
+
+/* a bitonic network over P registers (every index a compile-time constant
+ * once unrolled, so v stays in registers): ascending on return */
+template <int LOGP>
+__device__ __forceinline__ void bitonic_sort(double (&v)[1 << LOGP]) {
+    constexpr int P = 1 << LOGP;
+#pragma unroll
+    for (int kk = 1; kk <= LOGP; ++kk) {
+#pragma unroll
+        for (int jj = kk - 1; jj >= 0; --jj) {
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+                const int l = i ^ (1 << jj);
+                if (l > i) {
+                    const double a = v[i], b = v[l];
+                    const bool swap = ((i >> kk) & 1) == 0 ? (a > b) : (a < b);
+                    v[i] = swap ? b : a;
+                    v[l] = swap ? a : b;
+                }
+            }
+        }
+    }
+}
+
+/* one testable bin's statistic, threshold and hit. OSMAX > 0: the OS
+ * statistic over at most OSMAX cells: up to 32 sorted in registers (padded
+ * with +inf, which sorts after every cell), more gathered into a local array
+ * and selected. */
+template <int OSMAX>
 __device__ __forceinline__ bool cell_test(long long i, long long row, long long nbins, int mode, int n_ref, int N,
                                           int os_k, double alpha, double alpha_ca, double et,
                                           const uint8_t *__restrict__ sided, const int32_t *__restrict__ idx,
@@ -65,28 +119,31 @@ __device__ __forceinline__ bool cell_test(long long i, long long row, long long 
                                           double *__restrict__ thr) {
     const double *Xr = X + row;
     double Z, a = alpha, scale = et;
-    if (mode == 1) {
-        /* the os_k-th smallest: the value v with #(< v) <= os_k - 1 < #(<= v);
-         * a NaN among the cells makes T NaN */
+    if constexpr (OSMAX == 32) {
+        /* the os_k-th smallest; a NaN among the cells makes T NaN */
+        double v[32];
         bool has_nan = false;
-        for (int q = 0; q < N; ++q) has_nan |= isnan(Xr[idx[(long long)q * nbins + i]]);
-        Z = CUDART_NAN;
-        if (!has_nan) {
-            const int want = os_k - 1;
-            for (int q = 0; q < N; ++q) {
-                const double v = Xr[idx[(long long)q * nbins + i]];
-                int lt = 0, le = 0;
-                for (int p = 0; p < N; ++p) {
-                    const double w = Xr[idx[(long long)p * nbins + i]];
-                    lt += w < v;
-                    le += w <= v;
-                }
-                if (lt <= want && want < le) {
-                    Z = v;
-                    break;
-                }
-            }
+#pragma unroll
+        for (int q = 0; q < 32; ++q) {
+            v[q] = q < N ? Xr[idx[(long long)q * nbins + i]] : CUDART_INF;
+            has_nan |= isnan(v[q]);
         }
+        bitonic_sort<5>(v);
+        /* v[os_k - 1] by masks, not an index: a runtime index would move v
+         * to local memory */
+        unsigned long long pick = 0;
+#pragma unroll
+        for (int q = 0; q < 32; ++q)
+            pick |= (unsigned long long)__double_as_longlong(v[q]) & (0ull - (unsigned long long)(q == os_k - 1));
+        Z = has_nan ? CUDART_NAN : __longlong_as_double((long long)pick);
+    } else if constexpr (OSMAX > 0) {
+        double v[OSMAX];
+        bool has_nan = false;
+        for (int q = 0; q < N; ++q) {
+            v[q] = Xr[idx[(long long)q * nbins + i]];
+            has_nan |= isnan(v[q]);
+        }
+        Z = has_nan ? CUDART_NAN : select_kth(v, N, os_k - 1);
     } else if ((mode == 2 || mode == 3) && sided[i]) {
         double L = 0.0, R = 0.0;
         for (int q = 0; q < n_ref; ++q) L = __dadd_rn(L, Xr[idx[(long long)q * nbins + i]]);
@@ -110,6 +167,7 @@ __device__ __forceinline__ bool cell_test(long long i, long long row, long long 
     return Xr[i] > t;
 }
 
+template <int OSMAX>
 __global__ void __launch_bounds__(kThreads) cfar_cell_kernel(long long f0, long long t0, long long nbins, int mode,
                                                              int n_ref, int N, int os_k, double alpha,
                                                              double alpha_ca, double et,
@@ -129,7 +187,7 @@ __global__ void __launch_bounds__(kThreads) cfar_cell_kernel(long long f0, long 
         thr[row + i] = CUDART_NAN;
         hits[row + i] = 0;
     } else if (i < nbins) {
-        hit = cell_test(i, row, nbins, mode, n_ref, N, os_k, alpha, alpha_ca, et, sided, idx, X, noise, thr);
+        hit = cell_test<OSMAX>(i, row, nbins, mode, n_ref, N, os_k, alpha, alpha_ca, et, sided, idx, X, noise, thr);
         hits[row + i] = hit;
     }
     /* the row as a bitmask too: bin i is bit i % 32 of word i / 32 */
@@ -189,8 +247,20 @@ extern "C" int atkb_cfar_test(const double *raw, int ring, long long f0, long lo
     const dim3 grid((unsigned)((nbins + kThreads - 1) / kThreads), (unsigned)ntest);
     cudaStream_t s = (cudaStream_t)stream;
     cfar_mean_kernel<<<grid, kThreads, 0, s>>>(raw, ring, f0, t0, nbins, k, X);
-    cfar_cell_kernel<<<grid, kThreads, 0, s>>>(f0, t0, nbins, mode, n_ref, n_cells, os_k, alpha, alpha_ca, et, ok,
-                                               sided, idx, X, noise, thr, hits, bits, words);
+    if (mode != 1)
+        cfar_cell_kernel<0><<<grid, kThreads, 0, s>>>(f0, t0, nbins, mode, n_ref, n_cells, os_k, alpha, alpha_ca, et,
+                                                      ok, sided, idx, X, noise, thr, hits, bits, words);
+    else if (n_cells <= 32)
+        cfar_cell_kernel<32><<<grid, kThreads, 0, s>>>(f0, t0, nbins, mode, n_ref, n_cells, os_k, alpha, alpha_ca, et,
+                                                       ok, sided, idx, X, noise, thr, hits, bits, words);
+    else if (n_cells <= 64)
+        cfar_cell_kernel<64><<<grid, kThreads, 0, s>>>(f0, t0, nbins, mode, n_ref, n_cells, os_k, alpha, alpha_ca, et,
+                                                       ok, sided, idx, X, noise, thr, hits, bits, words);
+    else if (n_cells <= 512)
+        cfar_cell_kernel<512><<<grid, kThreads, 0, s>>>(f0, t0, nbins, mode, n_ref, n_cells, os_k, alpha, alpha_ca,
+                                                        et, ok, sided, idx, X, noise, thr, hits, bits, words);
+    else
+        return ATKB_E_ARG;
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }
 

@@ -27,7 +27,8 @@ stream through atkdsp_gpu_osx_process_n with the extractor_channels plan of
 workloads.py (CUDA events on the handle's stream around the whole call).
 
 --cfar times the CFAR detector and tracker on device frames (nbins dB lines
-of exponential noise with 64 bursts, CA 16 + 16 cells, 4 guard, k_frames 4)
+of exponential noise with 64 bursts, 16 + 16 cells, 4 guard, k_frames 4;
+--mode picks the statistic, CA by default)
 through atkdsp_gpu_cfar_process: the whole synchronous call, host clock,
 median of the repetitions. {"nbins", "frames", "ms", "mcells_s", "events"}.
 """
@@ -101,7 +102,7 @@ def run_osx(nfft: int = 4096, channels: int = 64, log2n: int = 24, reps: int = 5
             "msps": round(nel * n / t / 1e3, 1), "out_samples": int(sum(counts)) * nel}
 
 
-def run_cfar(nbins: int = 4096, frames: int = 1024, reps: int = 5) -> dict:
+def run_cfar(nbins: int = 4096, frames: int = 1024, reps: int = 5, mode: str = "ca") -> dict:
     import time
 
     import torch
@@ -117,7 +118,7 @@ def run_cfar(nbins: int = 4096, frames: int = 1024, reps: int = 5) -> dict:
         lo, f0 = int(rng.integers(0, nbins - 8)), int(rng.integers(0, frames - 8))
         p[f0:f0 + int(rng.integers(4, 200)), lo:lo + int(rng.integers(1, 8))] += 10 ** rng.uniform(1, 3)
     x = (10.0 * torch.log10(p)).to(torch.float32).contiguous()
-    c = Cfar(nbins, k_frames=4)
+    c = Cfar(nbins, k_frames=4, mode=mode)
     for _ in range(2):
         cfar_process(c, x, 0.0, 1e-3)
     ts, nev = [], 0
@@ -126,7 +127,7 @@ def run_cfar(nbins: int = 4096, frames: int = 1024, reps: int = 5) -> dict:
         nev = len(cfar_process(c, x, 0.0, 1e-3)[0])
         ts.append((time.perf_counter() - t0) * 1e3)
     ms = float(np.median(ts))
-    return {"nbins": nbins, "frames": frames, "ms": round(ms, 3),
+    return {"nbins": nbins, "frames": frames, "mode": mode, "ms": round(ms, 3),
             "mcells_s": round(nbins * frames / ms / 1e3, 1), "events": nev}
 
 
@@ -200,9 +201,10 @@ def main(argv=None):
     ap.add_argument("--cfar", action="store_true", help="the CFAR detector and tracker")
     ap.add_argument("--nbins", type=int, default=4096)
     ap.add_argument("--frames", type=int, default=1024)
+    ap.add_argument("--mode", default="ca", choices=["ca", "os", "go", "so"], help="the CFAR statistic")
     a = ap.parse_args(argv)
     if a.cfar:
-        print(json.dumps(run_cfar(a.nbins, a.frames, a.reps)), flush=True)
+        print(json.dumps(run_cfar(a.nbins, a.frames, a.reps, a.mode)), flush=True)
     elif a.kernels:
         for r in run_kernels(a.reps):
             print(json.dumps(r), flush=True)

@@ -139,6 +139,34 @@ def test_device_frames_many_passes_against_the_oracle():
     assert c.stats() == c2.stats()
 
 
+@pytest.mark.parametrize("n_ref,os_k", [(8, 0), (40, 0), (40, 1), (256, 300)])
+def test_os_selection_against_the_oracle(n_ref, os_k):
+    """The OS statistic gathers a bin's cells into a local array (64 or 512
+    entries) and selects the os_k-th smallest: every frame's hits against
+    the oracle's sort, for windows of 16 to 512 cells and ranks from the
+    smallest to past the middle, with masked bins making some windows
+    borrow."""
+    import torch
+    from atkdsp_b200.gpu import cfar_process
+    rng = np.random.default_rng(93 + n_ref)
+    nb, nf = 2048, 12
+    floor = rng.exponential(1.0, size=(nf, nb)) * np.linspace(1.0, 2.0, nb)[None, :]
+    floor[:, 700:702] += 1000.0          # narrower than the guard: the window sees only noise
+    floor[3:8, 1500:1503] += 50.0
+    xs = (10.0 * np.log10(floor)).astype(np.float32)
+    cfg = dict(mode="os", n_ref=n_ref, n_guard=2, pfa=1e-4, os_k=os_k)
+    mask = np.zeros(nb, np.uint8)
+    mask[100:140] = 1
+    c = _cfar(nb, **cfg)
+    c.set_mask(mask)
+    _ev, hits = cfar_process(c, torch.from_numpy(xs).cuda(), 0.0, 1.0, hits=True)
+    X, thr, h_or = CO.cell_test(xs, dict(cfg, os_k=c.cfg["os_k"]), c.alpha, c.alpha_ca, mask)
+    diff = hits.cpu().numpy() != h_or
+    near = np.abs(X - thr) <= 1e-12 * np.abs(thr)
+    assert not (diff & ~near).any(), int(diff.sum())
+    assert h_or[:, 700:702].any()         # os_k 1 (the minimum of 80 cells) needs a large alpha
+
+
 def test_linear_units_take_w2_powers_as_they_come():
     """units="linear": each value is the cell's linear power (clamped below
     at 1e-30); against the oracle fed the same linear values."""
