@@ -385,9 +385,6 @@ typedef struct {
     int track;
 } cf_blob;
 
-typedef struct {
-    int32_t lo, hi;
-} cf_span;
 
 struct atkdsp_cfar {
     atkdsp_cfar_config cfg;
@@ -426,8 +423,7 @@ struct atkdsp_cfar {
     int32_t *h_cols, *colmap;     /* colmap[bin]: its column, -1 outside */
     int ncol;
     int64_t rc_f0;                /* the frame of h_Rc's row 0 */
-    cf_span *spans;
-    size_t spans_cap;
+    uint32_t *orm;                /* a pass's hit rows and live spans, OR-ed */
     double *ht, *hd;              /* frame start and duration by ring row */
 };
 
@@ -566,7 +562,7 @@ ATKDSP_API void atkdsp_cfar_destroy(atkdsp_cfar *c) {
     host_buf_free(c, c->h_Rc);
     host_buf_free(c, c->h_cols);
     free(c->colmap);
-    free(c->spans);
+    free(c->orm);
     atkb_free(c->d_ok);
     atkb_free(c->d_sided);
     atkb_free(c->d_idx);
@@ -637,8 +633,9 @@ ATKDSP_API atkdsp_cfar *atkdsp_cfar_create(size_t nbins, const atkdsp_cfar_confi
     c->ht = (double *)calloc(ring, sizeof(double));
     c->hd = (double *)calloc(ring, sizeof(double));
     c->colmap = (int32_t *)malloc(nb * sizeof(int32_t));
+    c->orm = (uint32_t *)malloc(((nb + 31) / 32) * sizeof(uint32_t));
     int rc = (c->mask && c->ok && c->sided && c->beta && c->tracks && c->blobs && c->last_X && c->last_thr &&
-              c->last_hits && c->ht && c->hd && c->colmap)
+              c->last_hits && c->ht && c->hd && c->colmap && c->orm)
                  ? ATKB_OK
                  : ATKB_E_NOMEM;
     if (rc == ATKB_OK) {
@@ -1034,62 +1031,36 @@ static int pass_enqueue(atkdsp_cfar *c, const cf_pass *ps, const float *frames, 
     return rc;
 }
 
-static int span_cmp(const void *a, const void *b) {
-    const cf_span *x = (const cf_span *)a, *y = (const cf_span *)b;
-    return x->lo < y->lo ? -1 : x->lo > y->lo;
-}
-
-static int span_push(atkdsp_cfar *c, size_t *n, int32_t lo, int32_t hi) {
-    if (*n == c->spans_cap) {
-        const size_t cap = c->spans_cap ? 2 * c->spans_cap : 1024;
-        cf_span *p = (cf_span *)realloc(c->spans, cap * sizeof(cf_span));
-        if (!p) return ATKB_E_NOMEM;
-        c->spans = p;
-        c->spans_cap = cap;
-    }
-    c->spans[*n].lo = lo;
-    c->spans[*n].hi = hi;
-    ++*n;
-    return ATKB_OK;
-}
-
 /* The bins the tracker can read while it walks a pass, as columns (h_cols,
  * colmap): the runs of hits of the pass's tested frames (bit rows j0..nf-1
  * of `hits`) and the spans of the tracks alive before it, joined whenever two
  * lie within merge_gap + 1 bins of each other. A blob joins a track only
  * within that reach of the track's span, and the track's next span is the
  * hull of its blobs, so by induction every span a track takes during the
- * pass stays inside one joined interval; so do the blobs and their hits. */
+ * pass stays inside one joined interval; so do the blobs and their hits.
+ * The intervals come from the OR of the hit rows and the spans: a run's hits
+ * lie at most merge_gap apart, so joining set bins within the reach gives
+ * the same intervals as joining the runs. */
 static int pass_columns(atkdsp_cfar *c, const uint32_t *hits, int j0, int nf) {
-    const long nb = (long)c->nbins, g = c->cfg.merge_gap, reach = g + 1;
-    size_t n = 0;
+    const long nb = (long)c->nbins, reach = c->cfg.merge_gap + 1;
+    const size_t W = c->words;
+    uint32_t *m = c->orm;
+    memset(m, 0, W * sizeof(uint32_t));
     for (int j = j0; j < nf; ++j) {
-        const uint32_t *row = hits + (size_t)j * c->words;
-        long i = 0;
-        while ((i = next_hit(row, i, nb)) < nb) {
-            long hi = i, prev = i;
-            for (long q; (q = next_hit(row, prev + 1, nb)) < nb && q - prev - 1 <= g;) {
-                hi = q;
-                prev = q;
-            }
-            if (span_push(c, &n, (int32_t)i, (int32_t)hi) != ATKB_OK) return ATKB_E_NOMEM;
-            i = hi + 1;
-        }
+        const uint32_t *row = hits + (size_t)j * W;
+        for (size_t w = 0; w < W; ++w) m[w] |= row[w];
     }
     for (int t = 0; t < c->ntracks; ++t)
-        if (span_push(c, &n, c->tracks[t].cur_lo, c->tracks[t].cur_hi) != ATKB_OK) return ATKB_E_NOMEM;
-    qsort(c->spans, n, sizeof(cf_span), span_cmp);
+        for (long b = c->tracks[t].cur_lo; b <= c->tracks[t].cur_hi; ++b) m[b >> 5] |= 1u << (b & 31);
     int ncol = 0;
-    for (size_t q = 0; q < n;) {
-        long lo = c->spans[q].lo, hi = c->spans[q].hi;
-        for (++q; q < n && (long)c->spans[q].lo <= hi + reach; ++q)
-            if ((long)c->spans[q].hi > hi) hi = c->spans[q].hi;
-        if (lo < 0) lo = 0;
-        if (hi > nb - 1) hi = nb - 1;
-        for (long b = lo; b <= hi; ++b) {
+    for (long i = next_hit(m, 0, nb); i < nb; i = next_hit(m, i, nb)) {
+        long hi = i, q;
+        while ((q = next_hit(m, hi + 1, nb)) < nb && q <= hi + reach) hi = q;
+        for (long b = i; b <= hi; ++b) {
             c->colmap[b] = ncol;
             c->h_cols[ncol++] = (int32_t)b;
         }
+        i = hi + 1;
     }
     c->ncol = ncol;
     return ATKB_OK;
