@@ -17,9 +17,10 @@
  * group) pairs: each thread keeps a tile's TB*TB sums in registers over its
  * share of the hops, so one hop's 2*TB loads feed TB*TB products (the old
  * one-pair-per-thread split loaded both operands for every product). The
- * block of hops is staged through shared memory in chunks of CHUNK hops; the
- * hop groups' partial sums are then added in group order, so the results
- * are deterministic.
+ * block of hops is staged through shared memory in chunks of CHUNK hops,
+ * double-buffered: the next chunk's asynchronous copies (cp.async) fly while
+ * the current one is summed. The hop groups' partial sums are then added in
+ * group order, so the results are deterministic.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -31,12 +32,20 @@
 
 namespace {
 
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 template <int TB>
 __global__ void __launch_bounds__(W_NT)
 w12_kernel(const float2 *__restrict__ out, int nel, int nchan, long long m,
            const uint8_t *__restrict__ gate, float2 *__restrict__ R, uint32_t *__restrict__ counts,
            float *__restrict__ pwr, float *__restrict__ mean_pwr) {
-    __shared__ float2 ys[MAX_NEL][CHUNK];
+    __shared__ float2 ys[2][MAX_NEL][CHUNK];
     __shared__ double diag[MAX_NEL];
     extern __shared__ double red[];            /* [W_NT][TB*TB][2]: the groups' partial sums */
     const int nb = (nel + TB - 1) / TB;
@@ -58,12 +67,26 @@ w12_kernel(const float2 *__restrict__ out, int nel, int nchan, long long m,
         for (int r = 0; r < TB; ++r)
 #pragma unroll
             for (int c = 0; c < TB; ++c) sr[r][c] = si[r][c] = 0.0;
-        for (long long i0 = 0; i0 < m; i0 += CHUNK) {
+        /* chunk c's hops into buffer c & 1: copies for real samples, zeros
+         * for the padding rows and the tail */
+        auto stage = [&](long long i0, int buf) {
             const int cnt = (int)((m - i0) < CHUNK ? (m - i0) : CHUNK);
             for (int e = tid; e < nb * TB * CHUNK; e += W_NT) {
                 const int a = e / CHUNK, i = e - a * CHUNK;
-                ys[a][i] = (a < nel && i < cnt) ? out[((long long)a * nchan + k) * m + i0 + i]
-                                                : make_float2(0.f, 0.f);
+                if (a < nel && i < cnt) cp_async8(&ys[buf][a][i], out + ((long long)a * nchan + k) * m + i0 + i);
+                else ys[buf][a][i] = make_float2(0.f, 0.f);
+            }
+            cp_async_commit();
+        };
+        if (m > 0) stage(0, 0);
+        for (long long i0 = 0, c = 0; i0 < m; i0 += CHUNK, ++c) {
+            const int cnt = (int)((m - i0) < CHUNK ? (m - i0) : CHUNK);
+            const int buf = (int)(c & 1);
+            if (i0 + CHUNK < m) {
+                stage(i0 + CHUNK, buf ^ 1);
+                cp_async_wait<1>();            /* this chunk's group has landed */
+            } else {
+                cp_async_wait<0>();
             }
             __syncthreads();
             if (active && (w1 || A == B)) {
@@ -71,8 +94,8 @@ w12_kernel(const float2 *__restrict__ out, int nel, int nchan, long long m,
                     float2 ya[TB], yb[TB];
 #pragma unroll
                     for (int r = 0; r < TB; ++r) {
-                        ya[r] = ys[A * TB + r][i];
-                        yb[r] = ys[B * TB + r][i];
+                        ya[r] = ys[buf][A * TB + r][i];
+                        yb[r] = ys[buf][B * TB + r][i];
                     }
 #pragma unroll
                     for (int r = 0; r < TB; ++r)
