@@ -17,7 +17,8 @@
  * group) pairs: each thread keeps a tile's TB*TB sums in registers over its
  * share of the hops, so one hop's 2*TB loads feed TB*TB products (the old
  * one-pair-per-thread split loaded both operands for every product). The
- * block of hops is staged through shared memory in chunks of CHUNK hops,
+ * block of hops is staged through shared memory in chunks of CHUNK hops
+ * (2048 for one element, 256 otherwise), rows only for the elements present,
  * double-buffered: the next chunk's asynchronous copies (cp.async) fly while
  * the current one is summed. The hop groups' partial sums are then added in
  * group order, so the results are deterministic.
@@ -27,7 +28,10 @@
 #include "internal.h"
 
 #define W_NT 256
-#define CHUNK 64
+/* hops per staged chunk: one element's rows are short, so it takes longer
+ * chunks (more hops per thread between barriers) */
+template <int TB>
+struct chunk_of { static constexpr int value = TB == 1 ? 2048 : 256; };
 #define MAX_NEL 32
 
 namespace {
@@ -40,15 +44,18 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <int TB>
+template <int TB, int CHUNK = chunk_of<TB>::value>
 __global__ void __launch_bounds__(W_NT)
 w12_kernel(const float2 *__restrict__ out, int nel, int nchan, long long m,
            const uint8_t *__restrict__ gate, float2 *__restrict__ R, uint32_t *__restrict__ counts,
            float *__restrict__ pwr, float *__restrict__ mean_pwr) {
-    __shared__ float2 ys[2][MAX_NEL][CHUNK];
     __shared__ double diag[MAX_NEL];
-    extern __shared__ double red[];            /* [W_NT][TB*TB][2]: the groups' partial sums */
+    /* dynamic: the groups' partial sums [W_NT][TB*TB][2], then the two
+     * staging buffers [2][rows][CHUNK] of the hop chunks */
+    extern __shared__ double red[];
     const int nb = (nel + TB - 1) / TB;
+    const int rows = nb * TB;
+    float2 *ys = (float2 *)(red + (size_t)W_NT * TB * TB * 2);
     const int T = nb * (nb + 1) / 2;           /* tiles of the upper triangle */
     const int groups = T >= W_NT ? 1 : W_NT / T;
     const int tid = threadIdx.x;
@@ -73,8 +80,9 @@ w12_kernel(const float2 *__restrict__ out, int nel, int nchan, long long m,
             const int cnt = (int)((m - i0) < CHUNK ? (m - i0) : CHUNK);
             for (int e = tid; e < nb * TB * CHUNK; e += W_NT) {
                 const int a = e / CHUNK, i = e - a * CHUNK;
-                if (a < nel && i < cnt) cp_async8(&ys[buf][a][i], out + ((long long)a * nchan + k) * m + i0 + i);
-                else ys[buf][a][i] = make_float2(0.f, 0.f);
+                float2 *dst = ys + ((size_t)buf * rows + a) * CHUNK + i;
+                if (a < nel && i < cnt) cp_async8(dst, out + ((long long)a * nchan + k) * m + i0 + i);
+                else *dst = make_float2(0.f, 0.f);
             }
             cp_async_commit();
         };
@@ -93,9 +101,10 @@ w12_kernel(const float2 *__restrict__ out, int nel, int nchan, long long m,
                 for (int i = g; i < cnt; i += groups) {
                     float2 ya[TB], yb[TB];
 #pragma unroll
+                    const float2 *yc = ys + (size_t)buf * rows * CHUNK;
                     for (int r = 0; r < TB; ++r) {
-                        ya[r] = ys[buf][A * TB + r][i];
-                        yb[r] = ys[buf][B * TB + r][i];
+                        ya[r] = yc[(A * TB + r) * CHUNK + i];
+                        yb[r] = yc[(B * TB + r) * CHUNK + i];
                     }
 #pragma unroll
                     for (int r = 0; r < TB; ++r)
@@ -176,11 +185,18 @@ template <int TB>
 int w12_launch(const void *out, unsigned nel, unsigned nchan, size_t m, const uint8_t *gate, void *R,
                uint32_t *counts, float *pwr, float *mean_pwr, cudaStream_t s) {
     static bool configured[64];
-    const size_t smem = (size_t)W_NT * TB * TB * 2 * sizeof(double);
+    constexpr int CHUNK = chunk_of<TB>::value;
+    const size_t red = (size_t)W_NT * TB * TB * 2 * sizeof(double);
+    const size_t rows = ((nel + TB - 1) / TB) * TB;
+    const size_t smem = red + 2 * rows * CHUNK * sizeof(float2);
+    /* TB 1 and 2 serve one and two elements (atkb_w12), TB 4 up to MAX_NEL */
+    constexpr size_t rows_max = TB == 4 ? MAX_NEL : TB;
+    constexpr size_t smem_max = (size_t)W_NT * TB * TB * 2 * sizeof(double) + 2 * rows_max * CHUNK * sizeof(float2);
+    static_assert(smem_max <= 227 * 1024, "one CTA's shared memory fits an SM");
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
-        if (cudaFuncSetAttribute(w12_kernel<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        if (cudaFuncSetAttribute(w12_kernel<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max) !=
             cudaSuccess)
             return ATKB_E_KERNEL;
         configured[dev] = true;

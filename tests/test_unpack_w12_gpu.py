@@ -135,6 +135,28 @@ def test_w1_hermitian_and_matches_twin():
     assert cc[40] == oc.shape[2]
 
 
+@pytest.mark.parametrize("nel,m", [(1, 2048 * 3 + 77), (2, 256 * 5 + 3), (3, 255), (8, 257)])
+def test_w12_chunk_edges_against_float64(nel, m):
+    """The hops are staged in chunks (2048 for one element, 256 otherwise),
+    two buffers in flight: several full chunks plus a ragged tail, and
+    blocks just under and over one chunk, against float64 sums."""
+    rng = np.random.default_rng(40 + nel)
+    M = 24
+    y = (rng.standard_normal((nel, M, m)) + 1j * rng.standard_normal((nel, M, m))).astype(np.complex64)
+    R = np.zeros((M, nel, nel), np.complex64)
+    c = np.zeros(M, np.uint32)
+    ak.pfb_cov_accumulate(y, nel, M, None, R, c)
+    assert (c == m).all()
+    for k in range(M):
+        yk = y[:, k, :].astype(np.complex128)
+        Rt = yk @ yk.conj().T
+        assert np.max(np.abs(R[k] - Rt)) / np.max(np.abs(Rt)) < 1e-6, k
+    pwr, meanp = ak.pfb_channel_power(y, nel, M)
+    pt = (np.abs(y.astype(np.complex128)) ** 2).mean(axis=2)
+    assert np.max(np.abs(pwr - pt) / pt) < 1e-6
+    assert np.allclose(meanp, pt.mean(0), rtol=1e-6)
+
+
 def test_w12_many_elements_and_empty_block():
     rng = np.random.default_rng(12)
     nel, M, m = 32, 16, 300
