@@ -171,6 +171,7 @@ def _bind(lib) -> None:
         "atkdsp_cfar_stats": ([vp, P(_CfarCounters)], C.c_int),
         "atkdsp_gpu_cfar_process": ([vp, vp, C.c_int, sz, d, d, P(_CfarEvent), sz, vp, vp], ssz),
         "atkdsp_gpu_tune_set": ([u, u, u, C.c_int], C.c_int),
+        "atkdsp_gpu_fail_alloc_after": ([C.c_longlong], None),
         "atkdsp_gpu_tune_get": ([u, u, u], C.c_int),
     }
     for name, (args, res) in sigs.items():

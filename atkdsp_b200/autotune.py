@@ -4,14 +4,17 @@
     python -m atkdsp_b200.autotune --write    # ... and rewrite csrc/tune_table.h
 
 For every power-of-two nchan (16..2048), oversample (1, 2, 4) and
-taps/branch in the grid, the kernel has two tile shapes (include/atkdsp_gpu.h,
-atkdsp_gpu_tune_set): the paired fold and one hop per thread. Both are timed
-on one stream of 2^log2n cf32 samples through the batched kernel
-(atkdsp_b200.microbench.run_one, the kernel's own CUDA events, median of the
-repetitions), and the faster one goes into the table the library compiles in.
-A shape not in the grid keeps the paired fold. Outputs are identical either
-way; only speed differs. One JSON line per shape:
-{"nchan", "oversample", "taps", "paired_gsps", "single_gsps", "pair"}.
+taps/branch in the grid, the kernel has two or three tile shapes
+(include/atkdsp_gpu.h, atkdsp_gpu_tune_set): the paired fold (two hops per
+thread), one hop per thread, and -- at oversample 1 or 2 with nchan <= 1024 --
+the quad fold (four hops per thread). Each is timed on one stream of 2^log2n
+cf32 samples through the batched kernel (atkdsp_b200.microbench.run_one, the
+kernel's own CUDA events, median of the repetitions), and the fastest goes
+into the table the library compiles in (the paired fold unless another is
+faster by the margin). A shape not in the grid takes the quad fold where it
+exists, else the paired fold. Outputs are identical whichever is chosen; only
+speed differs. One JSON line per shape:
+{"nchan", "oversample", "taps", "paired_gsps", "single_gsps", "quad_gsps", "pair"}.
 """
 
 from __future__ import annotations
@@ -40,15 +43,18 @@ def tune(nchans=NCHANS, oversamples=OVERSAMPLES, taps=TAPS, log2n: int = 22, rep
                 continue
             for K in taps:
                 r = {}
-                for choice in (1, 0):
+                for choice in (1, 0, 2):
                     if lib.atkdsp_gpu_tune_set(M, os_, K, choice) != 0:
+                        if choice == 2:
+                            continue                     # no quad fold for this shape
                         raise RuntimeError(f"no tile-shape choice for nchan {M} os {os_}")
                     r[choice] = run_one(M, K, os_, log2n, reps)["gsps"]
                 lib.atkdsp_gpu_tune_set(M, os_, K, -1)
-                # the paired fold stays unless one hop per thread is faster by the margin
-                pair = 0 if r[0] > r[1] * (1.0 + margin) else 1
+                # the paired fold stays unless another shape is faster by the margin
+                best = max(r, key=lambda c: r[c])
+                pair = best if r[best] > r[1] * (1.0 + margin) else 1
                 row = {"nchan": M, "oversample": os_, "taps": K, "paired_gsps": r[1],
-                       "single_gsps": r[0], "pair": pair}
+                       "single_gsps": r[0], "quad_gsps": r.get(2), "pair": pair}
                 print(json.dumps(row), flush=True)
                 rows.append(row)
     return rows
@@ -56,14 +62,17 @@ def tune(nchans=NCHANS, oversamples=OVERSAMPLES, taps=TAPS, log2n: int = 22, rep
 
 def write_table(rows, path: Path = TABLE) -> None:
     lines = ["/* Tile-shape table: 1 = paired fold, 0 = one hop and 8 branches per thread,",
-             " * per (nchan, oversample, taps/branch). Written by",
+             " * 2 = quad fold (four hops per thread), per (nchan, oversample,",
+             " * taps/branch). Written by",
              " *   python -m atkdsp_b200.autotune --write",
-             " * from device measurements (GS/s paired / one hop per thread in each",
-             " * comment); shapes not listed use the paired fold. */",
+             " * from device measurements (GS/s paired / one hop per thread / quad in",
+             " * each comment); shapes not listed take the quad fold where it exists,",
+             " * else the paired fold. */",
              "static const tune_entry k_tune_table[] = {"]
     for r in rows:
+        q = f" / {r['quad_gsps']:.2f}" if r.get("quad_gsps") is not None else ""
         lines.append(f"    {{{r['nchan']}, {r['oversample']}, {r['taps']}, {r['pair']}}},"
-                     f"  /* {r['paired_gsps']:.2f} / {r['single_gsps']:.2f} */")
+                     f"  /* {r['paired_gsps']:.2f} / {r['single_gsps']:.2f}{q} */")
     lines.append("};")
     path.write_text("\n".join(lines) + "\n")
 
@@ -74,8 +83,15 @@ def main(argv=None):
     ap.add_argument("--out", default=None, help="write the table here instead")
     ap.add_argument("--log2n", type=int, default=22)
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--nchans", default=None, help="comma list (default: all)")
+    ap.add_argument("--oversamples", default=None, help="comma list (default: 1,2,4)")
+    ap.add_argument("--taps", default=None, help="comma list (default: all)")
     a = ap.parse_args(argv)
-    rows = tune(log2n=a.log2n, reps=a.reps)
+
+    def lst(v, d):
+        return tuple(int(t) for t in v.split(",")) if v else d
+    rows = tune(lst(a.nchans, NCHANS), lst(a.oversamples, OVERSAMPLES), lst(a.taps, TAPS),
+                log2n=a.log2n, reps=a.reps)
     if a.write or a.out:
         write_table(rows, Path(a.out) if a.out else TABLE)
 

@@ -31,7 +31,9 @@
 #include "host_internal.h"
 
 #define ATKB_PI 3.14159265358979323846
-#define MAX_NEL_SUPPORTED 32
+/* W1/W2 on device handle arrays up to this many elements (the wide kernel's
+ * shared-memory diagonal); the filterbank itself takes any max_nel */
+#define MAX_W12_NEL 6144
 #define MAX_POW2_NCHAN 4096
 #define MAX_GENERIC_NCHAN 6400
 
@@ -152,6 +154,13 @@ static int can_pair(unsigned M, unsigned os) {
     return ATKB_PTS == 8 && is_pow2(M) && M >= 16 && M <= 2048 && (os == 1 || os == 2 || os == 4);
 }
 
+/* the quad fold: four hops per thread over two branches (q, q + M/2), whose
+ * class mod M/8 a hop shift of M/os keeps for os 1 and 2; a tile must hold
+ * four hops (nchan <= 1024) */
+static int can_quad(unsigned M, unsigned os) {
+    return ATKB_PTS == 8 && is_pow2(M) && M >= 16 && M <= 1024 && (os == 1 || os == 2);
+}
+
 static int tune_choice(unsigned M, unsigned os, unsigned K) {
     unsigned i;
     int c = -1;
@@ -164,13 +173,14 @@ static int tune_choice(unsigned M, unsigned os, unsigned K) {
     for (i = 0; i < sizeof k_tune_table / sizeof k_tune_table[0]; ++i)
         if (k_tune_table[i].nchan == M && k_tune_table[i].os == os && k_tune_table[i].K == K)
             return k_tune_table[i].pair;
-    return 1;
+    return can_quad(M, os) ? 2 : 1;
 }
 
 ATKDSP_API int atkdsp_gpu_tune_set(unsigned nchan, unsigned oversample, unsigned taps_per_poly, int choice) {
     unsigned i;
     int rc = ATKDSP_OK;
-    if (!can_pair(nchan, oversample) || choice < -1 || choice > 1) return ATKDSP_E_ARG;
+    if (!can_pair(nchan, oversample) || choice < -1 || choice > 2) return ATKDSP_E_ARG;
+    if (choice == 2 && !can_quad(nchan, oversample)) return ATKDSP_E_ARG;
     pthread_mutex_lock(&g_tune_lock);
     for (i = 0; i < g_tune_novr; ++i)
         if (g_tune_ovr[i].nchan == nchan && g_tune_ovr[i].os == oversample && g_tune_ovr[i].K == taps_per_poly)
@@ -189,6 +199,8 @@ ATKDSP_API int atkdsp_gpu_tune_set(unsigned nchan, unsigned oversample, unsigned
     return rc;
 }
 
+ATKDSP_API void atkdsp_gpu_fail_alloc_after(long long n) { atkb_fail_alloc_after(n); }
+
 ATKDSP_API int atkdsp_gpu_tune_get(unsigned nchan, unsigned oversample, unsigned taps_per_poly) {
     if (!can_pair(nchan, oversample)) return ATKDSP_E_ARG;
     return tune_choice(nchan, oversample, taps_per_poly);
@@ -197,15 +209,17 @@ ATKDSP_API int atkdsp_gpu_tune_get(unsigned nchan, unsigned oversample, unsigned
 static int plan_fft(unsigned M, unsigned os, int want_pair, atkb_fft_plan *pl) {
     memset(pl, 0, sizeof *pl);
     if (is_pow2(M) && M >= 16 && M <= MAX_POW2_NCHAN) {
-        const int pair = want_pair && can_pair(M, os);
-        unsigned rem = M / (pair ? 4 : ATKB_PTS);
+        const int quad = want_pair == 2 && can_quad(M, os);
+        const int pair = !quad && want_pair && can_pair(M, os);
+        unsigned rem = M / (quad ? 2 : pair ? 4 : ATKB_PTS);
         pl->fast = 1;
         pl->pair = pair;
+        pl->quad = quad;
         /* nchan 4096 at oversample 1/2/4: one thread folds both parities of
          * both hops of its two-hop tile (paired loads), then radix-8 first
          * passes: the paired tap layout with the radix-8 plan */
         pl->ptaps = pair || (M == 4096 && (os == 1 || os == 2 || os == 4));
-        pl->radix[pl->npass++] = pair ? 4 : ATKB_PTS;
+        pl->radix[pl->npass++] = quad ? 2 : pair ? 4 : ATKB_PTS;
         while (rem >= ATKB_PTS) { pl->radix[pl->npass++] = ATKB_PTS; rem /= ATKB_PTS; }
         if (rem > 1) pl->radix[pl->npass++] = (int)rem;
     } else {
@@ -311,6 +325,7 @@ ATKDSP_API void atkdsp_pfb_destroy(atkdsp_pfb *p) {
     atkb_event_destroy(p->small_ev);
     atkb_event_destroy(p->tbl_event);
     atkb_stream_destroy(p->stream);
+    free((void *)p->dins);
     free(p);
 }
 
@@ -322,7 +337,7 @@ static int bank_build(bank_entry *be, void *stream) {
     const size_t taps_b = align16(L * sizeof(float));
     const size_t tab_b = (size_t)M * 2 * sizeof(double);
     const size_t pass_b = (size_t)pl.twlen * 2 * sizeof(double);
-    const size_t total = 2 * taps_b + 2 * tab_b + pass_b;
+    const size_t total = 3 * taps_b + 2 * tab_b + pass_b;
     char *h = (char *)calloc(1, total);
     double *proto = (double *)malloc(L * sizeof(double));
     if (!h || !proto) { free(h); free(proto); return ATKB_E_NOMEM; }
@@ -332,6 +347,7 @@ static int bank_build(bank_entry *be, void *stream) {
     double *twd = (double *)(h + 2 * taps_b);
     double *W = (double *)(h + 2 * taps_b + tab_b);
     double *wp = (double *)(h + 2 * taps_b + 2 * tab_b);
+    float *tapsQ = (float *)(h + 2 * taps_b + 2 * tab_b + pass_b);
     size_t q;
     unsigned j;
     for (q = 0; q < L; ++q) taps[q] = (float)proto[q];
@@ -347,6 +363,15 @@ static int bank_build(bank_entry *be, void *stream) {
                         const size_t r = pl.ptaps ? q2 + 2 * i : 4 * q2 + i;
                         tapsP[((k2 * (P / 4) + q2) * MP + jj) * 4 + i] = taps[k2 * M + jj + r * MP];
                     }
+    }
+    if (pl.quad) {
+        /* (c*2K + v)*MP + j holds the tap (4v + c)*MP + j: class c's 2K taps
+         * at stride MP, consecutive across a warp's branches j */
+        const size_t MP = M / 8, V = 2 * (size_t)be->K;
+        size_t c, v, jj;
+        for (c = 0; c < 4; ++c)
+            for (v = 0; v < V; ++v)
+                for (jj = 0; jj < MP; ++jj) tapsQ[(c * V + v) * MP + jj] = taps[(4 * v + c) * MP + jj];
     }
     for (j = 0; j < M; ++j) {
         /* the reference's rotation table, channelizer.c:164-170 */
@@ -391,6 +416,7 @@ static int bank_build(bank_entry *be, void *stream) {
     B->twd = (const char *)be->d_const + 2 * taps_b;
     B->wfull = (const char *)be->d_const + 2 * taps_b + tab_b;
     B->wpass = (const char *)be->d_const + 2 * taps_b + 2 * tab_b;
+    B->tapsQ = (const float *)((const char *)be->d_const + 2 * taps_b + 2 * tab_b + pass_b);
     B->plan = pl;
     B->logm = 0;
     if (pl.fast) {
@@ -472,7 +498,6 @@ atkdsp_pfb *atkb_pfb_create_internal(double fs, unsigned nchan, unsigned oversam
                                      int lean) {
     if (!(fs > 0.0) || nchan < 2 || oversample < 1 || nchan % oversample != 0) return NULL;
     if (taps_per_poly < 2 || max_nel < 1) return NULL;
-    if (max_nel > MAX_NEL_SUPPORTED) return NULL;
     if (is_pow2(nchan) ? nchan > MAX_POW2_NCHAN : nchan > MAX_GENERIC_NCHAN) return NULL;
     if (atten_db < 20.0) atten_db = 20.0;
     atkdsp_pfb *p = (atkdsp_pfb *)calloc(1, sizeof *p);
@@ -519,6 +544,7 @@ atkdsp_pfb *atkb_pfb_create_internal(double fs, unsigned nchan, unsigned oversam
         p->lc = 0; p->b = 0; p->cur = 0;
         return p;
     }
+    if (rc == ATKB_OK && !(p->dins = (const void **)calloc(max_nel, sizeof *p->dins))) rc = ATKB_E_NOMEM;
     /* host-path staging: about 2^20 samples per element, whole hops */
     if (rc == ATKB_OK) {
         size_t chunk = ((size_t)1 << 21) / max_nel;
@@ -779,7 +805,7 @@ static ptrdiff_t process_small(atkdsp_pfb *p, const atkdsp_cf32 *const *ins, uns
         p->lc = (unsigned)(p->lc + n);
         return 0;
     }
-    const void *dins[MAX_NEL_SUPPORTED];
+    const void **dins = p->dins;
     for (e = 0; e < nel; ++e) dins[e] = (const atkdsp_cf32 *)p->d_small_in + (size_t)e * ATKB_SMALL_N;
     /* outputs packed with stride m: [nel * nchan][m], the caller's layout */
     const size_t out_n = (size_t)nel * p->nchan * m;
@@ -817,7 +843,7 @@ ATKDSP_API ptrdiff_t atkdsp_pfb_process_n(atkdsp_pfb *p, const atkdsp_cf32 *cons
     }
     size_t pos = 0, col = 0;
     int rc = ATKB_OK;
-    const atkdsp_cf32 *dins[MAX_NEL_SUPPORTED];
+    const void **dins = p->dins;
     for (e = 0; e < nel; ++e) dins[e] = (const atkdsp_cf32 *)p->d_in_stage + (size_t)e * p->chunk;
     while (pos < n && rc == ATKB_OK) {
         const size_t nc = (n - pos < p->chunk) ? n - pos : p->chunk;
@@ -907,67 +933,93 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_n_raw(atkdsp_pfb *p, const void *con
     return rc == ATKB_OK ? (ptrdiff_t)m : map_rc(rc);
 }
 
-/* ============================================ per-device scratch for host calls
- * W1/W2 and unpack on HOST buffers stage through device memory. One scratch
- * area per device, grown when a larger call first needs it and then kept;
- * calls on one device are serialised by its lock. */
+/* ============================================ per-thread scratch for host calls
+ * W1/W2 and unpack on HOST buffers stage through device memory. Each calling
+ * thread has its own staging area and CUDA stream per device, so calls from
+ * different threads never wait on each other (the reference's callers run
+ * different handles and these stateless calls from several threads at once,
+ * src/undertow.c:252-257). A thread's area is allocated by its first such
+ * call on a device and grown only when a larger call comes; later calls of
+ * the same or a smaller size allocate nothing. A thread that exits releases
+ * its areas. The device-pointer unpack_dc / block_mean calls take their mean
+ * partials from a separate fixed per-thread buffer (never regrown, never
+ * shared with the staging), so host calls can't move memory that queued
+ * device work still uses. */
 #define MAX_DEV 16
+#define GPU_PARTIALS 4096                 /* atkb_unpack_partials bound, doubles x2 */
 typedef struct {
-    pthread_mutex_t lock;
-    void *d;
+    void *d;                              /* staging for host calls */
     size_t cap;
     void *stream;
-    int ready;
+    double *partials;                     /* device unpack_dc / block_mean */
 } scratch_t;
-static scratch_t g_scr[MAX_DEV];
-static pthread_mutex_t g_scr_init = PTHREAD_MUTEX_INITIALIZER;
+typedef struct { scratch_t dev[MAX_DEV]; } thread_scratch;
+static pthread_key_t g_scr_key;
+static pthread_once_t g_scr_once = PTHREAD_ONCE_INIT;
+static int g_scr_key_ok;
 
-static scratch_t *scratch_lock(size_t bytes, int *rc) {
+static void scratch_release(void *v) {
+    thread_scratch *t = (thread_scratch *)v;
+    int cur = -1, d;
+    if (!t) return;
+    atkb_get_device(&cur);
+    for (d = 0; d < MAX_DEV; ++d) {
+        scratch_t *s = &t->dev[d];
+        if (!s->d && !s->stream && !s->partials) continue;
+        atkb_set_device(d);
+        if (s->stream) atkb_stream_sync(s->stream);
+        atkb_free(s->d);
+        atkb_free(s->partials);
+        atkb_stream_destroy(s->stream);
+    }
+    if (cur >= 0) atkb_set_device(cur);
+    free(t);
+}
+static void scratch_key_init(void) { g_scr_key_ok = pthread_key_create(&g_scr_key, scratch_release) == 0; }
+
+/* this thread's scratch on the current device, with at least `bytes` of
+ * staging (0: staging untouched) */
+static scratch_t *thread_scratch_get(size_t bytes, int *rc) {
     int dev = 0;
     *rc = atkb_get_device(&dev);
     if (*rc != ATKB_OK) return NULL;
     if (dev < 0 || dev >= MAX_DEV) { *rc = ATKB_E_NODEV; return NULL; }
-    scratch_t *s = &g_scr[dev];
-    pthread_mutex_lock(&g_scr_init);
-    if (!s->ready) {
-        pthread_mutex_init(&s->lock, NULL);
-        s->ready = 1;
+    pthread_once(&g_scr_once, scratch_key_init);
+    if (!g_scr_key_ok) { *rc = ATKB_E_NOMEM; return NULL; }
+    thread_scratch *t = (thread_scratch *)pthread_getspecific(g_scr_key);
+    if (!t) {
+        t = (thread_scratch *)calloc(1, sizeof *t);
+        if (!t || pthread_setspecific(g_scr_key, t) != 0) { free(t); *rc = ATKB_E_NOMEM; return NULL; }
     }
-    pthread_mutex_unlock(&g_scr_init);
-    pthread_mutex_lock(&s->lock);
+    scratch_t *s = &t->dev[dev];
     if (!s->stream && (*rc = atkb_stream_create(&s->stream)) != ATKB_OK) {
         s->stream = NULL;
-        pthread_mutex_unlock(&s->lock);
         return NULL;
     }
     if (s->cap < bytes) {
+        atkb_stream_sync(s->stream);      /* the old area may still feed a copy */
         atkb_free(s->d);
         s->d = NULL;
         s->cap = 0;
-        size_t want = bytes + bytes / 4 + 4096;
-        if ((*rc = atkb_malloc(&s->d, want)) != ATKB_OK) {
-            s->d = NULL;
-            pthread_mutex_unlock(&s->lock);
-            return NULL;
-        }
+        const size_t want = bytes + bytes / 4 + 4096;
+        if ((*rc = atkb_malloc(&s->d, want)) != ATKB_OK) { s->d = NULL; return NULL; }
         s->cap = want;
     }
     *rc = ATKB_OK;
     return s;
 }
-static void scratch_unlock(scratch_t *s) { pthread_mutex_unlock(&s->lock); }
 
 /* ====================================================================== W1/W2 */
 ATKDSP_API void atkdsp_pfb_cov_accumulate(const atkdsp_cf32 *out, unsigned nel, unsigned nchan,
                                           size_t m, const uint8_t *gate, atkdsp_cf32 *R,
                                           uint32_t *counts) {
-    if (!out || !R || !counts || nel < 1 || nchan < 1 || nel > MAX_NEL_SUPPORTED) return;
+    if (!out || !R || !counts || nel < 1 || nchan < 1 || nel > MAX_W12_NEL) return;
     const size_t ob = align16((size_t)nel * nchan * m * sizeof(atkdsp_cf32));
     const size_t rb = align16((size_t)nchan * nel * nel * sizeof(atkdsp_cf32));
     const size_t cb = align16((size_t)nchan * sizeof(uint32_t));
     const size_t gb = align16(nchan);
     int rc;
-    scratch_t *s = scratch_lock(ob + rb + cb + gb, &rc);
+    scratch_t *s = thread_scratch_get(ob + rb + cb + gb, &rc);
     if (!s) return;
     char *d = (char *)s->d;
     rc = atkb_h2d(d, out, (size_t)nel * nchan * m * sizeof(atkdsp_cf32), s->stream);
@@ -980,7 +1032,6 @@ ATKDSP_API void atkdsp_pfb_cov_accumulate(const atkdsp_cf32 *out, unsigned nel, 
     if (rc == ATKB_OK) rc = atkb_d2h(R, d + ob, (size_t)nchan * nel * nel * sizeof(atkdsp_cf32), s->stream);
     if (rc == ATKB_OK) rc = atkb_d2h(counts, d + ob + rb, nchan * sizeof(uint32_t), s->stream);
     atkb_stream_sync(s->stream);
-    scratch_unlock(s);
 }
 
 ATKDSP_API void atkdsp_pfb_cov_reset(atkdsp_cf32 *R, uint32_t *counts, unsigned nel, unsigned nchan,
@@ -999,12 +1050,12 @@ ATKDSP_API void atkdsp_pfb_cov_reset(atkdsp_cf32 *R, uint32_t *counts, unsigned 
 
 ATKDSP_API void atkdsp_pfb_channel_power(const atkdsp_cf32 *out, unsigned nel, unsigned nchan,
                                          size_t m, float *pwr, float *mean_pwr) {
-    if (!out || nel < 1 || nchan < 1 || nel > MAX_NEL_SUPPORTED) return;
+    if (!out || nel < 1 || nchan < 1 || nel > MAX_W12_NEL) return;
     const size_t ob = align16((size_t)nel * nchan * m * sizeof(atkdsp_cf32));
     const size_t pb = align16((size_t)nel * nchan * sizeof(float));
     const size_t mb = align16((size_t)nchan * sizeof(float));
     int rc;
-    scratch_t *s = scratch_lock(ob + pb + mb, &rc);
+    scratch_t *s = thread_scratch_get(ob + pb + mb, &rc);
     if (!s) return;
     char *d = (char *)s->d;
     rc = atkb_h2d(d, out, (size_t)nel * nchan * m * sizeof(atkdsp_cf32), s->stream);
@@ -1014,13 +1065,12 @@ ATKDSP_API void atkdsp_pfb_channel_power(const atkdsp_cf32 *out, unsigned nel, u
     if (rc == ATKB_OK && pwr) rc = atkb_d2h(pwr, d + ob, (size_t)nel * nchan * sizeof(float), s->stream);
     if (rc == ATKB_OK && mean_pwr) rc = atkb_d2h(mean_pwr, d + ob + pb, nchan * sizeof(float), s->stream);
     atkb_stream_sync(s->stream);
-    scratch_unlock(s);
 }
 
 ATKDSP_API int atkdsp_gpu_pfb_cov_accumulate(const atkdsp_cf32 *d_out, unsigned nel, unsigned nchan,
                                              size_t m, const uint8_t *d_gate, atkdsp_cf32 *d_R,
                                              uint32_t *d_counts, void *stream) {
-    if (!d_out || !d_R || !d_counts || nel < 1 || nchan < 1 || nel > MAX_NEL_SUPPORTED) return ATKDSP_E_ARG;
+    if (!d_out || !d_R || !d_counts || nel < 1 || nchan < 1 || nel > MAX_W12_NEL) return ATKDSP_E_ARG;
     return map_rc(atkb_w12(d_out, nel, nchan, m, d_gate, d_R, d_counts, NULL, NULL, stream));
 }
 
@@ -1028,7 +1078,7 @@ ATKDSP_API int atkdsp_gpu_pfb_accumulate(const atkdsp_cf32 *d_out, unsigned nel,
                                          size_t m, const uint8_t *d_gate, atkdsp_cf32 *d_R,
                                          uint32_t *d_counts, float *d_pwr, float *d_mean_pwr,
                                          void *stream) {
-    if (!d_out || nel < 1 || nchan < 1 || nel > MAX_NEL_SUPPORTED) return ATKDSP_E_ARG;
+    if (!d_out || nel < 1 || nchan < 1 || nel > MAX_W12_NEL) return ATKDSP_E_ARG;
     if ((d_R == NULL) != (d_counts == NULL)) return ATKDSP_E_ARG;
     return map_rc(atkb_w12(d_out, nel, nchan, m, d_gate, d_R, d_counts, d_pwr, d_mean_pwr, stream));
 }
@@ -1041,7 +1091,7 @@ ATKDSP_API int atkdsp_gpu_pfb_cov_reset(atkdsp_cf32 *d_R, uint32_t *d_counts, un
 
 ATKDSP_API int atkdsp_gpu_pfb_channel_power(const atkdsp_cf32 *d_out, unsigned nel, unsigned nchan,
                                             size_t m, float *d_pwr, float *d_mean_pwr, void *stream) {
-    if (!d_out || nel < 1 || nchan < 1 || nel > MAX_NEL_SUPPORTED) return ATKDSP_E_ARG;
+    if (!d_out || nel < 1 || nchan < 1 || nel > MAX_W12_NEL) return ATKDSP_E_ARG;
     return map_rc(atkb_w12(d_out, nel, nchan, m, NULL, NULL, NULL, d_pwr, d_mean_pwr, stream));
 }
 
@@ -1098,7 +1148,7 @@ static ptrdiff_t unpack_host(const void *raw, size_t nbytes, int fmt, atkdsp_cf3
     const size_t ob = align16(n * sizeof(atkdsp_cf32));
     const size_t pb = align16((size_t)atkb_unpack_partials(n) * 2 * sizeof(double));
     int rc;
-    scratch_t *s = scratch_lock(rb + ob + pb + 64, &rc);
+    scratch_t *s = thread_scratch_get(rb + ob + pb + 64, &rc);
     if (!s) return map_rc(rc);
     char *d = (char *)s->d;
     double *d_mean = (double *)(d + rb + ob + pb);
@@ -1113,7 +1163,6 @@ static ptrdiff_t unpack_host(const void *raw, size_t nbytes, int fmt, atkdsp_cf3
     if (rc == ATKB_OK && want_mean) rc = atkb_d2h(hm, d_mean, sizeof hm, s->stream);
     if (rc == ATKB_OK && pole) rc = atkb_d2h(dc_state, d_mean + 2, sizeof(atkdsp_cf32), s->stream);
     if (rc == ATKB_OK) rc = atkb_stream_sync(s->stream);
-    scratch_unlock(s);
     if (rc != ATKB_OK) return map_rc(rc == ATKB_E_NOMEM ? rc : ATKB_E_KERNEL);
     if (mean_re) *mean_re = hm[0];
     if (mean_im) *mean_im = hm[1];
@@ -1133,13 +1182,18 @@ ATKDSP_API ptrdiff_t atkdsp_unpack_dc(const void *raw, size_t nbytes, int fmt, a
     return unpack_host(raw, nbytes, fmt, out, out_cap, off_re, off_im, mean_re, mean_im, 0.0f, NULL);
 }
 
-/* device-pointer unpack: a small per-device area holds the mean partials */
+/* device-pointer unpack: the calling thread's fixed partials buffer on the
+ * current device (allocated by its first such call, then reused) */
 static int gpu_partials(double **d) {
     int rc;
-    scratch_t *s = scratch_lock(4096 * 2 * sizeof(double), &rc);
+    scratch_t *s = thread_scratch_get(0, &rc);
     if (!s) return rc;
-    *d = (double *)s->d;
-    scratch_unlock(s);
+    if (!s->partials) {
+        void *p = NULL;
+        if ((rc = atkb_malloc(&p, GPU_PARTIALS * 2 * sizeof(double))) != ATKB_OK) return rc;
+        s->partials = (double *)p;
+    }
+    *d = s->partials;
     return ATKB_OK;
 }
 

@@ -64,6 +64,8 @@ struct atkdsp_pfb {
     size_t tbl_bytes;
     int *d_counters;
     int grid;
+    const void **dins;            /* max_nel staging input pointers (host array,
+                                   * filled per call; allocated at create) */
 };
 
 /* How a job's new samples are stored: cf32, or int16 I/Q converted in the

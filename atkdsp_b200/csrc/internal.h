@@ -28,7 +28,8 @@ extern "C" {
 /* ---- FFT plan --------------------------------------------------------------
  * nchan = radix[0] * radix[1] * ... * radix[npass-1], Stockham order. For a
  * power of two >= 16 the fast path is used: radix[0] == ATKB_PTS (4 when
- * `pair` is set) and every later radix is ATKB_PTS except a smaller last one.
+ * `pair` is set, 2 when `quad` is) and every later radix is ATKB_PTS except
+ * a smaller last one.
  * `pair`: the paired fold (two consecutive hops per thread, even or odd
  * branches), used for oversample 1, 2 or 4. */
 #define ATKB_MAX_PASS 24
@@ -41,6 +42,9 @@ typedef struct {
     int npass;
     int fast;                     /* 1: power-of-two fast path */
     int pair;                     /* 1: paired fold, first radix 4             */
+    int quad;                     /* 1: quad fold (four hops per thread over two
+                                   * branches), first radix 2; oversample 1 or
+                                   * 2, nchan <= 1024 */
     int ptaps;                    /* taps in the paired layout (pair, or the
                                    * nchan-4096 two-hop tile's paired fold) */
     int radix[ATKB_MAX_PASS];
@@ -60,6 +64,8 @@ typedef struct {
                                    * k*nchan + j + r*MP, r = 4q .. 4q+3; paired:
                                    * float4 (2k + c)*MP + j holds r = c + 2i,
                                    * i = 0..3 */
+    const float *tapsQ;           /* device: quad fold, (c*2K + v)*MP + j holds
+                                   * the tap (4v + c)*MP + j, c = 0..3 */
     const void *twd;              /* device: nchan double2 (cos, sin)(2 pi j/nchan) */
     const void *wfull;            /* device: nchan double2 W^j = (cos, -sin)  */
     const void *wpass;            /* device: per-pass twiddles (fast path)    */
@@ -115,6 +121,9 @@ size_t atkb_pool_idle_bytes(void *pool);
 int  atkb_malloc_pool(void **p, size_t bytes, void *pool, void *stream);
 void atkb_free_async(void *p, void *stream);
 int  atkb_host_alloc(void **p, size_t bytes);      /* pinned */
+/* fault injection: the n-th allocation (device, pool or pinned) from now
+ * fails with ATKB_E_NOMEM; 0 disarms */
+void atkb_fail_alloc_after(long long n);
 void atkb_host_free(void *p);
 int  atkb_h2d(void *dst, const void *src, size_t bytes, void *stream);
 int  atkb_d2h(void *dst, const void *src, size_t bytes, void *stream);
@@ -135,7 +144,10 @@ int  atkb_event_elapsed_ms(float *ms, void *start, void *stop);
 /* graphs: capture the work enqueued on `stream` between begin and end */
 int  atkb_graph_begin(void *stream);
 int  atkb_graph_end(void *stream, void **exec);
-int  atkb_graph_launch(void *exec, void *stream);
+int  atkb_graph_launch(void *exec, void *stream);       /* inside an NVTX range */
+/* NVTX ranges on the host timeline (no-ops unless a profiler is attached) */
+void atkb_range_push(const char *name);
+void atkb_range_pop(void);
 void atkb_graph_destroy(void *exec);
 
 /* filterbank --------------------------------------------------------------- */

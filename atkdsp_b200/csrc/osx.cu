@@ -20,6 +20,7 @@
  * reproduces the reference's per-block loop bit for bit.
  */
 #include <cuda_runtime.h>
+#include <atomic>
 #include <stdint.h>
 
 #include "fft_sm.cuh"
@@ -376,7 +377,8 @@ __global__ void osx_carry_kernel(const float2 *__restrict__ state, long long sta
     }
 }
 
-bool g_configured[64];
+/* the attributes are idempotent: concurrent first callers may both set them */
+std::atomic<bool> g_configured[64];
 
 int set_smem(const void *fn, int bytes) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
@@ -393,14 +395,14 @@ extern "C" int atkb_osx_launch(const atkb_osx_run *run, int m, int nel, void *st
     const atkb_osx_run &R = *run;
     cudaStream_t s = (cudaStream_t)stream;
     int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !g_configured[dev]) {
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return ATKB_E_NODEV;
+    if (!g_configured[dev].load(std::memory_order_acquire)) {
         const int big = (int)atkb_osx_group_smem(ATKB_OSX_FUSED_MAX);
         if (!set_smem((const void *)osx_group_kernel, big) || !set_smem((const void *)osx_group_chan_kernel, OSX_WORK * 16) ||
             !set_smem((const void *)osx_four_a<0>, 4096 * 16) || !set_smem((const void *)osx_four_a<1>, 4096 * 16) ||
             !set_smem((const void *)osx_four_b<0>, 4096 * 16) || !set_smem((const void *)osx_four_b<1>, 4096 * 16))
             return ATKB_E_KERNEL;
-        g_configured[dev] = true;
+        g_configured[dev].store(true, std::memory_order_release);
     }
     const dim3 groups((m + OSX_G - 1) / OSX_G, nel);
     if (R.nfft <= ATKB_OSX_FUSED_MAX) {

@@ -39,6 +39,7 @@
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <atomic>
 #include "internal.h"
 
 /* the fast path's tile: 4096 complex points, PTS per thread (ATKB_PTS in
@@ -722,6 +723,174 @@ __device__ __forceinline__ void write_tile(const atkb_job &J, long long h0, int 
     }
 }
 
+/* ---- the quad fold: oversample 1 or 2, nchan <= 1024 --------------------------
+ * Thread (quad g, class c, branch j) folds the four hops ta + t (ta = 4g,
+ * t = 0..3) of the tile over the two branches q0 = j + c*MP and q1 = q0 + M/2
+ * (MP = M/8, c = 0..3). In hop ta's frame its samples are the slots
+ * u = 4v + c (sample u*MP + j, tap u*MP + j), v = 0 .. 2K-1; hop ta + t sees
+ * the same sample at slot u - t*8/os, i.e. at v - t*D with D = 2/os, which
+ * keeps the class c. So every sample the thread loads feeds all four hops,
+ * and each tap it loads serves the four hops in turn through a window of
+ * W = 4*D taps held in registers: per input sample position one 8-byte
+ * sample load, one 4-byte tap load and four complex multiply-adds (against
+ * one tap load per two multiply-adds in the paired fold). Branch q_i of hop t
+ * sums its taps in slot order -- k ascending, a rounded multiply then a
+ * rounded add, from -0.0f -- like every other fold here, so all tile shapes
+ * give the reference's bits. The two branches feed a radix-2
+ * first Stockham pass (Ns = 1: points q0 and q0 + M/2 of each hop). */
+template <int LOGM>
+struct QuadLin {                       /* cf32, the quad's windows in one buffer */
+    const float2 *p;                   /* at slot c of hop ta, branch j */
+    __device__ __forceinline__ float2 at(int v) const { return __ldg(p + (long long)v * (1 << (LOGM - 1))); }
+};
+template <int LOGM>
+struct QuadLin16 {                     /* raw int16 I/Q, converted on the fly */
+    const short2 *p;
+    float cre, cim, ks;
+    __device__ __forceinline__ float2 at(int v) const {
+        return conv16(__ldg(p + (long long)v * (1 << (LOGM - 1))), cre, cim, ks);
+    }
+};
+template <int LOGM>
+struct QuadMixed {                     /* cf32 state / input by index */
+    const float2 *st, *in;
+    long long g, head;
+    __device__ __forceinline__ float2 at(int v) const {
+        const long long pos = g + (long long)v * (1 << (LOGM - 1));
+        return __ldg(pos < head ? st + pos : in + (pos - head));
+    }
+};
+template <int LOGM>
+struct QuadMixed16 {                   /* cf32 state / raw int16 input by index */
+    const float2 *st;
+    const short2 *in;
+    long long g, head;
+    float cre, cim, ks;
+    __device__ __forceinline__ float2 at(int v) const {
+        const long long pos = g + (long long)v * (1 << (LOGM - 1));
+        return pos < head ? __ldg(st + pos) : conv16(__ldg(in + (pos - head)), cre, cim, ks);
+    }
+};
+
+/* acc[t][i]: hop ta + t, branch q_i. tq: this thread's 2K taps at stride MP
+ * (tap v of class c, branch j). nq: valid hops of the quad (1..4). */
+template <int LOGOS, class LD>
+__device__ __forceinline__ void fold_quad(float2 (&acc)[4][2], const float *__restrict__ tq, int MP, int K,
+                                          int nq, const LD &ld) {
+    constexpr int D = 2 >> LOGOS;      /* v-shift per hop */
+    constexpr int W = 4 * D;           /* tap window (a power of two) */
+    const int V = 2 * K;               /* taps per class */
+    const int vend = V + (nq - 1) * D; /* one past the last sample position */
+#pragma unroll
+    for (int t = 0; t < 4; ++t) acc[t][0] = acc[t][1] = make_float2(-0.0f, -0.0f);
+    float T[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) T[w] = 0.0f;
+    for (int v0 = 0; v0 < vend; v0 += W) {
+        if (v0 >= W - D && v0 + W <= V && nq == 4) {
+            /* every hop in its window: no conditions */
+#pragma unroll
+            for (int s = 0; s < W; ++s) {
+                const int v = v0 + s;
+                T[s] = __ldg(tq + (long long)v * MP);
+                const float2 x = ld.at(v);
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const int sv = (s - t * D) & (W - 1);       /* slot of tap v - t*D */
+                    const int par = LOGOS ? ((s - t) & 1) : (s & 1);
+                    mac(acc[t][par], T[sv], x);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int s = 0; s < W; ++s) {
+                const int v = v0 + s;
+                if (v < V) T[s] = __ldg(tq + (long long)v * MP);
+                if (v < vend) {
+                    const float2 x = ld.at(v);
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) {
+                        const int vt = v - t * D;
+                        const int sv = (s - t * D) & (W - 1);
+                        const int par = LOGOS ? ((s - t) & 1) : (s & 1);
+                        if (t < nq && vt >= 0 && vt < V) mac(acc[t][par], T[sv], x);
+                    }
+                }
+            }
+        }
+    }
+}
+
+/* the radix-2 first pass (Ns = 1) of one hop: points q0 and q0 + M/2 in,
+ * 2*q0 + {0, 1} out */
+template <int LOGM>
+__device__ __forceinline__ void first_pass2(float2 a, float2 b, double2 *sm, int t, int q0) {
+    double2 x0 = make_double2((double)a.x, (double)a.y), x1 = make_double2((double)b.x, (double)b.y);
+    dft2(x0, x1);
+    sm[SW((t << LOGM) + 2 * q0)] = x0;
+    sm[SW((t << LOGM) + 2 * q0 + 1)] = x1;
+}
+
+template <int LOGM, int LOGOS>
+__device__ __forceinline__ void fold_tile_quad(const atkb_job &J, const atkb_bank &B, long long h0,
+                                               int nvalid, double2 *sm) {
+    constexpr int M = 1 << LOGM;
+    constexpr int LOGMP = LOGM - LOGP;
+    constexpr int MP = 1 << LOGMP;
+    constexpr int HOP = M >> LOGOS;
+    static_assert(PTS == 8 && LOGM <= 10 && LOGOS <= 1, "quad fold: PTS 8, four hops a tile");
+    const int tid = threadIdx.x;
+    const int j = tid & (MP - 1);
+    const int c = (tid >> LOGMP) & 3;
+    const int ta = (tid >> (LOGMP + 2)) * 4;
+    const int nq = min(4, nvalid - ta);
+    float2 acc[4][2];
+    if (nq > 0) {
+        const float *tq = B.tapsQ + (long long)c * (2 * B.K) * MP + j;
+        const long long w0 = h0 * (long long)HOP;
+        const long long w1 = (h0 + nvalid - 1) * (long long)HOP + B.L;
+        const long long off = (h0 + ta) * (long long)HOP + c * MP + j;
+        if (w0 >= J.head) {
+            if (J.in_kind) {
+                const QuadLin16<LOGM> ld{(const short2 *)J.in + (off - J.head), J.cre, J.cim, J.kscale};
+                fold_quad<LOGOS>(acc, tq, MP, B.K, nq, ld);
+            } else {
+                const QuadLin<LOGM> ld{(const float2 *)J.in + (off - J.head)};
+                fold_quad<LOGOS>(acc, tq, MP, B.K, nq, ld);
+            }
+        } else if (w1 <= J.head) {
+            const QuadLin<LOGM> ld{(const float2 *)J.state + off};
+            fold_quad<LOGOS>(acc, tq, MP, B.K, nq, ld);
+        } else if (J.in_kind) {
+            const QuadMixed16<LOGM> ld{(const float2 *)J.state, (const short2 *)J.in, off, J.head,
+                                       J.cre, J.cim, J.kscale};
+            fold_quad<LOGOS>(acc, tq, MP, B.K, nq, ld);
+        } else {
+            const QuadMixed<LOGM> ld{(const float2 *)J.state, (const float2 *)J.in, off, J.head};
+            fold_quad<LOGOS>(acc, tq, MP, B.K, nq, ld);
+        }
+    } else {
+#pragma unroll
+        for (int t = 0; t < 4; ++t) acc[t][0] = acc[t][1] = make_float2(0.0f, 0.0f);
+    }
+#pragma unroll
+    for (int t = 0; t < 4; ++t) first_pass2<LOGM>(acc[t][0], acc[t][1], sm, ta + t, j + c * MP);
+}
+
+template <int LOGM, int LOGOS>
+__device__ void tile_quad(const atkb_job &J, const atkb_bank &B, long long h0, int nvalid, double2 *sm,
+                          float2 *tile_out) {
+    constexpr int M = 1 << LOGM;
+    fold_tile_quad<LOGM, LOGOS>(J, B, h0, nvalid, sm);
+    /* a quad's M/2 threads hold its four hops' points through the passes
+     * before the last (bfly gives each hop M/8 consecutive threads) */
+    constexpr int G0 = M / 2;
+    constexpr int G = G0 < 32 ? 32 : G0 > NT ? NT : G0;
+    group_sync<G>();
+    fft_rest<LOGM, 1, 1, G>(sm, (const double2 *)B.wpass, B.plan.twoff, tile_out, B, J, h0);
+    write_tile<LOGM>(J, h0, nvalid, tile_out);
+}
+
 /* fold + first Stockham pass (Ns = 1, radix PTS, no twiddles) of one hop
  * and PTS branches per thread, into the tile's shared points */
 template <int LOGM>
@@ -1072,7 +1241,8 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
         const long long left = J.hops - h0;
         const int nvalid = (int)(left < SB.tile_hops ? left : SB.tile_hops);
         const int lm = SB.plan.fast ? SB.logm : 0;
-        int key = SB.plan.pair ? 16 * (1 + (SB.os == 1 ? 0 : SB.os == 2 ? 1 : 2)) + lm : lm;
+        int key = SB.plan.quad ? 80 + 16 * (SB.os == 1 ? 0 : 1) + lm
+                : SB.plan.pair ? 16 * (1 + (SB.os == 1 ? 0 : SB.os == 2 ? 1 : 2)) + lm : lm;
         /* a launch with less dynamic shared memory than the bank's tile needs
          * skips the tile (its outputs stay unwritten) instead of running off
          * the end of shared memory */
@@ -1093,8 +1263,13 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
             else tile_4096x2_pair<2>(J, SB, h0, nvalid, sm);
             break;
         PAIRED(4) PAIRED(5) PAIRED(6) PAIRED(7) PAIRED(8) PAIRED(9) PAIRED(10) PAIRED(11)
+#define QUAD(L)                                                                \
+        case 80 + L: tile_quad<L, 0>(J, SB, h0, nvalid, sm, to); break;    \
+        case 96 + L: tile_quad<L, 1>(J, SB, h0, nvalid, sm, to); break;
+        QUAD(4) QUAD(5) QUAD(6) QUAD(7) QUAD(8) QUAD(9) QUAD(10)
 #undef UNPAIRED
 #undef PAIRED
+#undef QUAD
         case -1: break;
         default: tile_generic(J, SB, h0, nvalid, sm); break;
         }
@@ -1132,12 +1307,14 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
 extern "C" int atkb_pfb_max_smem(void) { return 200 * 1024; }
 
 extern "C" int atkb_pfb_grid(int dev, int smem_bytes) {
-    static int configured[64];
-    if (dev >= 0 && dev < 64 && !configured[dev]) {
+    /* the attribute is idempotent: concurrent first callers may both set it */
+    static std::atomic<bool> configured[64];
+    if (dev < 0 || dev >= 64) return -1;
+    if (!configured[dev].load(std::memory_order_acquire)) {
         if (cudaFuncSetAttribute(pfb_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  atkb_pfb_max_smem()) != cudaSuccess)
             return -1;
-        configured[dev] = 1;
+        configured[dev].store(true, std::memory_order_release);
     }
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pfb_tiles_kernel, NT, smem_bytes) !=
@@ -1157,7 +1334,9 @@ extern "C" int atkb_pfb_launch_n(const atkb_job *d_jobs, const int *d_tile_start
                                  void *stream) {
     if (njobs <= 0) return ATKB_OK;
     if (grid < 1) grid = 1;
+    atkb_range_push("atkdsp tile kernel launch");
     pfb_tiles_kernel<<<grid, NT, smem_bytes, (cudaStream_t)stream>>>(d_jobs, d_tile_start, d_carry, njobs,
                                                                     d_njobs, d_counters);
+    atkb_range_pop();
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }

@@ -2,6 +2,8 @@
  * Every function returns an ATKB_* status; no CUDA type crosses into C. */
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <atomic>
+#include <nvtx3/nvToolsExt.h>
 #include "internal.h"
 
 static int st(cudaError_t e) {
@@ -32,8 +34,23 @@ extern "C" void atkb_stream_destroy(void *stream) {
 }
 extern "C" int atkb_stream_sync(void *stream) { return st(cudaStreamSynchronize((cudaStream_t)stream)); }
 
+/* Allocation fault injection (host side, no device fault): when armed with
+ * n > 0, the n-th device, pool or pinned allocation from then on fails with
+ * ATKB_E_NOMEM as a real out-of-memory would, and the hook disarms itself. */
+static std::atomic<long long> g_fail_countdown{0};
+static bool inject_alloc_failure() {
+    long long c = g_fail_countdown.load(std::memory_order_relaxed);
+    while (c > 0) {
+        if (g_fail_countdown.compare_exchange_weak(c, c - 1, std::memory_order_relaxed))
+            return c == 1;
+    }
+    return false;
+}
+extern "C" void atkb_fail_alloc_after(long long n) { g_fail_countdown.store(n > 0 ? n : 0); }
+
 extern "C" int atkb_malloc(void **p, size_t bytes) {
     *p = nullptr;
+    if (inject_alloc_failure()) return ATKB_E_NOMEM;
     return st(cudaMalloc(p, bytes ? bytes : 256));
 }
 extern "C" void atkb_free(void *p) {
@@ -71,6 +88,7 @@ extern "C" size_t atkb_pool_idle_bytes(void *pool) {
 }
 extern "C" int atkb_malloc_pool(void **p, size_t bytes, void *pool, void *stream) {
     *p = nullptr;
+    if (inject_alloc_failure()) return ATKB_E_NOMEM;
     return st(cudaMallocFromPoolAsync(p, bytes ? bytes : 256, (cudaMemPool_t)pool, (cudaStream_t)stream));
 }
 extern "C" void atkb_free_async(void *p, void *stream) {
@@ -78,6 +96,7 @@ extern "C" void atkb_free_async(void *p, void *stream) {
 }
 extern "C" int atkb_host_alloc(void **p, size_t bytes) {
     *p = nullptr;
+    if (inject_alloc_failure()) return ATKB_E_NOMEM;
     return st(cudaMallocHost(p, bytes ? bytes : 256));
 }
 extern "C" void atkb_host_free(void *p) {
@@ -140,8 +159,17 @@ extern "C" int atkb_graph_end(void *stream, void **exec) {
     *exec = (void *)x;
     return rc;
 }
+/* NVTX ranges (header-only NVTX 3: free unless a profiler injects itself) on
+ * the host timeline around every graph replay and tile-kernel launch, so a
+ * trace shows when each batch or server round was enqueued */
+extern "C" void atkb_range_push(const char *name) { nvtxRangePushA(name); }
+extern "C" void atkb_range_pop(void) { nvtxRangePop(); }
+
 extern "C" int atkb_graph_launch(void *exec, void *stream) {
-    return st(cudaGraphLaunch((cudaGraphExec_t)exec, (cudaStream_t)stream));
+    nvtxRangePushA("atkdsp graph launch");
+    const int rc = st(cudaGraphLaunch((cudaGraphExec_t)exec, (cudaStream_t)stream));
+    nvtxRangePop();
+    return rc;
 }
 extern "C" void atkb_graph_destroy(void *exec) {
     if (exec) cudaGraphExecDestroy((cudaGraphExec_t)exec);

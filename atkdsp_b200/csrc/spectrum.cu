@@ -14,6 +14,7 @@
  * only in their rounding sequence.
  */
 #include <cuda_runtime.h>
+#include <atomic>
 #include <stdint.h>
 
 #include "fft_sm.cuh"
@@ -148,7 +149,8 @@ int spec_launch(const void *in, long long frames, long long hop, int logn, const
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }
 
-bool g_configured[64];
+/* the attributes are idempotent: concurrent first callers may both set them */
+std::atomic<bool> g_configured[64];
 
 }  // namespace
 
@@ -156,15 +158,15 @@ extern "C" int atkb_spec_launch(int mode, const void *in, long long frames, long
                                 const void *tw, int nblk, int per, void *part, float *o0, float *o1, float *o2,
                                 float *o3, void *stream) {
     int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !g_configured[dev]) {
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return ATKB_E_NODEV;
+    if (!g_configured[dev].load(std::memory_order_acquire)) {
         const int b = ATKB_SPEC_NMAX * 16;
         if (cudaFuncSetAttribute(spec_frames_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess ||
             cudaFuncSetAttribute(spec_frames_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess ||
             cudaFuncSetAttribute(spec_frames_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess ||
             cudaFuncSetAttribute(spec_frames_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * b) != cudaSuccess)
             return ATKB_E_KERNEL;
-        g_configured[dev] = true;
+        g_configured[dev].store(true, std::memory_order_release);
     }
     cudaStream_t s = (cudaStream_t)stream;
     switch (mode) {

@@ -25,6 +25,7 @@
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <atomic>
 #include "internal.h"
 
 #define W_NT 256
@@ -100,8 +101,8 @@ w12_kernel(const float2 *__restrict__ out, int nel, int nchan, long long m,
             if (active && (w1 || A == B)) {
                 for (int i = g; i < cnt; i += groups) {
                     float2 ya[TB], yb[TB];
-#pragma unroll
                     const float2 *yc = ys + (size_t)buf * rows * CHUNK;
+#pragma unroll
                     for (int r = 0; r < TB; ++r) {
                         ya[r] = yc[(A * TB + r) * CHUNK + i];
                         yb[r] = yc[(B * TB + r) * CHUNK + i];
@@ -168,6 +169,65 @@ w12_kernel(const float2 *__restrict__ out, int nel, int nchan, long long m,
     }
 }
 
+/* W1 / W2 for arrays wider than MAX_NEL elements: one CTA per channel, one
+ * thread per (a, b) pair of the upper triangle (grid-stride), each summing
+ * its pair over the hops in hop order, in double, straight from global
+ * memory (a thread's loads of element a and b are strided by nchan*m, so
+ * this path trades bandwidth for generality; wide arrays are rare). The
+ * diagonal sums land in shared memory (nel doubles, dynamic) for W2. Same
+ * results as the tiled kernel's: every sum in double, rounded once. */
+__global__ void __launch_bounds__(W_NT)
+w12_wide_kernel(const float2 *__restrict__ out, int nel, int nchan, long long m,
+                const uint8_t *__restrict__ gate, float2 *__restrict__ R, uint32_t *__restrict__ counts,
+                float *__restrict__ pwr, float *__restrict__ mean_pwr) {
+    extern __shared__ double wdiag[];
+    const long long pairs = (long long)nel * (nel + 1) / 2;
+    for (int k = blockIdx.x; k < nchan; k += gridDim.x) {
+        const bool w1 = R && counts && (!gate || gate[k]);
+        const bool w2 = pwr || mean_pwr;
+        if (!w1 && !w2) continue;
+        for (long long t = threadIdx.x; t < pairs; t += W_NT) {
+            int a = 0;
+            long long rem = t;
+            while (rem >= nel - a) { rem -= nel - a; ++a; }
+            const int b = a + (int)rem;
+            if (!w1 && a != b) continue;
+            const float2 *ya = out + ((long long)a * nchan + k) * m;
+            const float2 *yb = out + ((long long)b * nchan + k) * m;
+            double tr = 0.0, ti = 0.0;
+            for (long long i = 0; i < m; ++i) {
+                const float2 u = __ldg(ya + i), v = __ldg(yb + i);
+                tr += (double)u.x * v.x + (double)u.y * v.y;
+                ti += (double)u.y * v.x - (double)u.x * v.y;
+            }
+            if (a == b) wdiag[a] = tr;
+            if (w1 && m > 0) {
+                float2 *Rk = R + (long long)k * nel * nel;
+                float2 q = Rk[(long long)a * nel + b];
+                Rk[(long long)a * nel + b] = make_float2((float)((double)q.x + tr), (float)((double)q.y + ti));
+                if (a != b) {
+                    q = Rk[(long long)b * nel + a];
+                    Rk[(long long)b * nel + a] = make_float2((float)((double)q.x + tr), (float)((double)q.y - ti));
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (w1) counts[k] += (uint32_t)m;
+            if (w2) {
+                const double inv = m ? 1.0 / (double)m : 0.0;
+                double across = 0.0;
+                for (int a = 0; a < nel; ++a) {
+                    if (pwr) pwr[(long long)a * nchan + k] = (float)(wdiag[a] * inv);
+                    across += wdiag[a] * inv;
+                }
+                if (mean_pwr) mean_pwr[k] = (float)(across / (double)nel);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void cov_reset_kernel(float2 *R, uint32_t *counts, int nel, int nchan,
                                  const uint8_t *__restrict__ gate) {
     const long long per = (long long)nel * nel;
@@ -184,7 +244,8 @@ __global__ void cov_reset_kernel(float2 *R, uint32_t *counts, int nel, int nchan
 template <int TB>
 int w12_launch(const void *out, unsigned nel, unsigned nchan, size_t m, const uint8_t *gate, void *R,
                uint32_t *counts, float *pwr, float *mean_pwr, cudaStream_t s) {
-    static bool configured[64];
+    /* the attribute is idempotent: concurrent first callers may both set it */
+    static std::atomic<bool> configured[64];
     constexpr int CHUNK = chunk_of<TB>::value;
     const size_t red = (size_t)W_NT * TB * TB * 2 * sizeof(double);
     const size_t rows = ((nel + TB - 1) / TB) * TB;
@@ -194,12 +255,12 @@ int w12_launch(const void *out, unsigned nel, unsigned nchan, size_t m, const ui
     constexpr size_t smem_max = (size_t)W_NT * TB * TB * 2 * sizeof(double) + 2 * rows_max * CHUNK * sizeof(float2);
     static_assert(smem_max <= 227 * 1024, "one CTA's shared memory fits an SM");
     int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !configured[dev]) {
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return ATKB_E_NODEV;
+    if (!configured[dev].load(std::memory_order_acquire)) {
         if (cudaFuncSetAttribute(w12_kernel<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max) !=
             cudaSuccess)
             return ATKB_E_KERNEL;
-        configured[dev] = true;
+        configured[dev].store(true, std::memory_order_release);
     }
     const int grid = (int)(nchan < 4096 ? nchan : 4096);
     w12_kernel<TB><<<grid, W_NT, smem, s>>>((const float2 *)out, (int)nel, (int)nchan, (long long)m, gate,
@@ -211,8 +272,16 @@ int w12_launch(const void *out, unsigned nel, unsigned nchan, size_t m, const ui
 
 extern "C" int atkb_w12(const void *out, unsigned nel, unsigned nchan, size_t m, const uint8_t *gate,
                         void *R, uint32_t *counts, float *pwr, float *mean_pwr, void *stream) {
-    if (nel < 1 || nel > MAX_NEL || nchan < 1) return ATKB_E_ARG;
+    if (nel < 1 || nchan < 1) return ATKB_E_ARG;
     cudaStream_t s = (cudaStream_t)stream;
+    if (nel > MAX_NEL) {
+        const size_t smem = (size_t)nel * sizeof(double);
+        if (smem > 48 * 1024) return ATKB_E_ARG;          /* 6144 elements */
+        const int grid = (int)(nchan < 4096 ? nchan : 4096);
+        w12_wide_kernel<<<grid, W_NT, smem, s>>>((const float2 *)out, (int)nel, (int)nchan, (long long)m, gate,
+                                                 (float2 *)R, counts, pwr, mean_pwr);
+        return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+    }
     if (nel == 1) return w12_launch<1>(out, nel, nchan, m, gate, R, counts, pwr, mean_pwr, s);
     if (nel == 2) return w12_launch<2>(out, nel, nchan, m, gate, R, counts, pwr, mean_pwr, s);
     return w12_launch<4>(out, nel, nchan, m, gate, R, counts, pwr, mean_pwr, s);

@@ -202,7 +202,14 @@ def main(argv=None):
     ap.add_argument("--nbins", type=int, default=4096)
     ap.add_argument("--frames", type=int, default=1024)
     ap.add_argument("--mode", default="ca", choices=["ca", "os", "go", "so"], help="the CFAR statistic")
+    ap.add_argument("--choice", type=int, default=-1,
+                    help="tile shape for the filterbank run (atkdsp_gpu_tune_set: 1 paired, 0 one hop "
+                         "per thread, 2 quad; -1 the table's)")
     a = ap.parse_args(argv)
+    if a.choice >= 0:
+        from . import load
+        if load().atkdsp_gpu_tune_set(a.nchan, a.oversample, a.taps, a.choice) != 0:
+            raise SystemExit(f"no tile shape {a.choice} for nchan {a.nchan} oversample {a.oversample}")
     if a.cfar:
         print(json.dumps(run_cfar(a.nbins, a.frames, a.reps, a.mode)), flush=True)
     elif a.kernels:

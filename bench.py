@@ -212,9 +212,13 @@ def _cpu_reference_rate(specs, budget_s: float = 8.0, threads: int | None = None
 
 
 def run_reference(args, rank, world):
+    """The reference's own CPU channelizer (oracle/_ref, built from its
+    sources) on this arm's workload: every one of the 256 streams, one block
+    each per step through atkdsp_pfb_process_n with its own handle (state
+    carried from step to step), all host threads. Rank 0 only."""
     if rank != 0:
         return
-    specs = _specs(0)
+    specs = _specs(0, args)
     from oracle import oracle as O
     ref = O.reference()
     if ref is None:
@@ -223,22 +227,17 @@ def run_reference(args, rank, world):
     from atkdsp_b200 import workloads as W
     nth = os.cpu_count() or 1
     ref.lib.atkdsp_set_threads(nth)
-    # a bounded sample per step: streams taken in order up to ~3e7 samples
-    sample, tot = [], 0
-    for s in specs:
-        sample.append(s)
-        tot += s.length
-        if tot > 3e7:
-            break
-    xs = [W.stream_samples(s, 0) for s in sample]
-    handles = [ref.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1) for s in sample]
-    outs = [np.zeros(s.nchan * (s.length // (s.nchan // 2) + 2), np.complex64) for s in sample]
+    xs = [W.stream_samples(s, 0) for s in specs]
+    tot = sum(x.size for x in xs)
+    handles = [ref.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1) for s in specs]
+    outs = [np.zeros(s.nchan * (s.length // (s.nchan // s.oversample) + 2), np.complex64) for s in specs]
+    fn = handles[0]._o._f("pfb_process_n")
+    arrs = [(O._pcf * 1)(O._cfp(x)) for x in xs]
 
     def step():
-        for p, x, o in zip(handles, xs, outs):
-            m = p.out_hops(x.size)
-            arr = (O._pcf * 1)(O._cfp(x))
-            p._o._f("pfb_process_n")(p._p, arr, 1, x.size, O._cfp(o), o.size)
+        for p, a, x, o in zip(handles, arrs, xs, outs):
+            if fn(p._p, a, 1, x.size, O._cfp(o), o.size) < 0:
+                raise RuntimeError("reference atkdsp_pfb_process_n failed")
 
     for _ in range(args.warmup):
         step()
@@ -247,19 +246,105 @@ def run_reference(args, rank, world):
         step()
     dt = time.perf_counter() - t0
     v = tot * args.steps / dt / 1e6
-    desc = f"first {len(sample)} of 256 streams, one block each, {tot} samples per step"
+    desc = f"all {len(specs)} streams, one block each per step ({tot} samples per step)"
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "MSamples/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 fold + f64 fft (CPU)",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "streams": 256, "oversample": 2,
-                                        "sample": desc},
+        "data": "synthetic", "config": _config(args, world),
         "cpu_baseline": {"value": round(v, 3), "unit": "MSamples/s", "cores": nth,
                          "kind": "reference", "sample": desc},
         "e2e": {"value": round(v, 3), "unit": "MSamples/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "native_so": _native_maps(),
     }))
+
+
+def _config(args, world):
+    """The workload description both arms print."""
+    name = WORKLOAD if args.streams == 256 and args.min_log2 == 14 and args.max_log2 == 22 else \
+        f"uneven_streams_{args.streams}_2^{args.min_log2:g}-2^{args.max_log2:g}"
+    return {"workload": name, "streams": args.streams, "nchan": [64, 256, 1024, 4096],
+            "taps_per_branch": [8, 12, 16], "oversample": 2, "blocks": 3,
+            "parallelism": f"replicas x{world} (stream-sharded)",
+            "l2": "inputs larger than L2 (~1.5 GB per step)"}
+
+
+# ------------------------------------------- accuracy checks (outside timing)
+def _rel_err(y, r):
+    """Worst channel's RMS error and largest single error, each divided by
+    that channel's RMS (the parity bar's metric)."""
+    y = np.asarray(y).reshape(-1, np.asarray(y).shape[-1]).astype(np.complex128)
+    r = np.asarray(r).reshape(-1, np.asarray(r).shape[-1]).astype(np.complex128)
+    rms = np.sqrt(np.mean(np.abs(r) ** 2, axis=1))
+    rms = np.where(rms > 0, rms, 1.0)
+    e = np.abs(y - r)
+    return float(np.max(np.sqrt(np.mean(e ** 2, axis=1)) / rms)), float(np.max(np.max(e, axis=1) / rms))
+
+
+def _accuracy(cases, what: str) -> dict:
+    """cases: (ours, reference, float64 or None) output triples of the same
+    inputs, (..., nchan, m) each (the float64 one may cover fewer hops).
+    Returns the worst channel over all cases."""
+    vr = vm = v64 = r64 = 0.0
+    have64 = False
+    for y, r, y64 in cases:
+        a, b = _rel_err(y, r)
+        vr, vm = max(vr, a), max(vm, b)
+        if y64 is not None:
+            m = y64.shape[-1]
+            have64 = True
+            v64 = max(v64, _rel_err(np.asarray(y)[..., :m], y64)[0])
+            r64 = max(r64, _rel_err(np.asarray(r)[..., :m], y64)[0])
+    out = {"vs_reference_rms": float(f"{vr:.3g}"), "vs_reference_max": float(f"{vm:.3g}"), "checked": what,
+           "bar": 1e-5}
+    if have64:
+        out["vs_fp64_rms"] = float(f"{v64:.3g}")
+        out["reference_vs_fp64_rms"] = float(f"{r64:.3g}")
+    return out
+
+
+def _fp64(nchan, os_, taps, atten, xs):
+    """The float64 restatement of the filterbank over element arrays xs."""
+    from oracle import fp64
+    from oracle import oracle as O
+    t = fp64.Fp64Pfb(O.oracle().prototype(nchan, taps, atten), nchan, os_, len(xs))
+    return t.process_n(xs, len(xs))
+
+
+def _batched_accuracy(specs, torch, device) -> dict | None:
+    """One stream of each (nchan, taps) pair of the workload, through a fresh
+    batch of the same kernel and through the reference library, same input
+    (the stream's first block, at most 2^18 samples); float64 on 2^15."""
+    from oracle import oracle as O
+    ref = O.reference()
+    if ref is None:
+        return None
+    import atkdsp_b200 as ak
+    from atkdsp_b200 import gpu
+    from atkdsp_b200 import workloads as W
+    pick = {}
+    for s in specs:
+        pick.setdefault((s.nchan, s.taps), s)
+    chosen = [pick[k] for k in sorted(pick)]
+    xs = [W.stream_samples(s, 0)[: 1 << 18] for s in chosen]
+    hs = [ak.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1) for s in chosen]
+    b = gpu.Batch(hs, use_graph=False)
+    din = [torch.from_numpy(x).to(device) for x in xs]
+    dout = [torch.empty(max(1, s.nchan * h.out_hops(x.size)), dtype=torch.complex64, device=device)
+            for s, h, x in zip(chosen, hs, xs)]
+    ms = b.process(din, dout)
+    torch.cuda.synchronize()
+    cases = []
+    for s, x, o, m in zip(chosen, xs, dout, ms):
+        y = o[: s.nchan * m].view(s.nchan, m).cpu().numpy()
+        r = np.asarray(ref.Pfb(FS, s.nchan, s.oversample, s.taps, 80.0, 1).process(x))
+        y64 = _fp64(s.nchan, s.oversample, s.taps, 80.0, [x[: 1 << 15]])[0]
+        cases.append((y, r, y64))
+    del b, hs
+    return _accuracy(cases, f"{len(chosen)} streams, one per (nchan, taps) pair, first block "
+                            f"(<= 2^18 samples; float64 on 2^15)")
 
 
 # -------------------------------------------------------------- our arms
@@ -379,11 +464,13 @@ def _cabi_arm(specs, sets, torch, barrier, max_over_ranks, pinned: bool, steps: 
 
 
 # --------------------------------------------------- the other configurations
-def _c1_arm(torch):
+def _c1_arm(torch, cpu: bool):
     """Single stream, M=64 critically sampled, 16 taps/branch, beta 8, 2^20 cf32
     samples fed in blocks 1, 999, 4096, 7 (cycling) through the drop-in C ABI
     with host buffers -- each call is synchronous, so this measures per-call
-    latency as much as the kernel."""
+    latency as much as the kernel. The CPU baseline is the reference library
+    on one thread over the same calls (its OpenMP start-up makes more threads
+    slower on blocks this small)."""
     import atkdsp_b200 as ak
     from atkdsp_b200 import workloads as W
     x = W.single_stream(1 << 20)
@@ -391,21 +478,45 @@ def _c1_arm(torch):
     p = ak.Pfb(FS, 64, 1, 16, W.ATTEN_BETA8, 1)
     p.process(x[:5000])
     p.reset()
+    outs = []
     t0 = time.perf_counter()
     pos, i, calls = 0, 0, 0
     while pos < x.size:
         b = blocks[i % len(blocks)]
-        p.process(x[pos:pos + b])
+        outs.append(p.process(x[pos:pos + b]))
         pos += b
         i += 1
         calls += 1
     dt = time.perf_counter() - t0
-    return {"workload": "single_stream_m64_blocks_1_999_4096_7", "value": round(x.size / dt / 1e6, 2),
-            "unit": "MSamples/s", "calls": calls, "us_per_call": round(dt / calls * 1e6, 2),
-            "path": "atkdsp_pfb_process (host buffers)"}
+    res = {"workload": "single_stream_m64_blocks_1_999_4096_7", "value": round(x.size / dt / 1e6, 2),
+           "unit": "MSamples/s", "calls": calls, "us_per_call": round(dt / calls * 1e6, 2),
+           "path": "atkdsp_pfb_process (host buffers)"}
+    if cpu:
+        from oracle import oracle as O
+        ref = O.reference()
+        if ref is not None:
+            ref.lib.atkdsp_set_threads(1)
+            rp = ref.Pfb(FS, 64, 1, 16, W.ATTEN_BETA8, 1)
+            routs = []
+            t0 = time.perf_counter()
+            pos, i = 0, 0
+            while pos < x.size:
+                b = blocks[i % len(blocks)]
+                routs.append(rp.process(x[pos:pos + b]))
+                pos += b
+                i += 1
+            rdt = time.perf_counter() - t0
+            ref.lib.atkdsp_set_threads(os.cpu_count() or 1)
+            res["cpu_baseline"] = {"value": round(x.size / rdt / 1e6, 2), "unit": "MSamples/s", "cores": 1,
+                                   "kind": "reference", "sample": "the whole workload, same calls"}
+            y = np.concatenate([o for o in outs if o.shape[1]], axis=1)
+            r = np.concatenate([o for o in routs if np.asarray(o).shape[1]], axis=1)
+            y64 = _fp64(64, 1, 16, W.ATTEN_BETA8, [x])[0]
+            res["accuracy"] = _accuracy([(y, r, y64)], "the whole stream")
+    return res
 
 
-def _c2_arm(torch, device, steps):
+def _c2_arm(torch, device, steps, cpu: bool):
     """40 MS/s front end: ci16q11 with noise + 8 tones + a constant DC offset,
     2,000,000-sample (50 ms) blocks; per block the running DC estimate (the
     previous block's mean) is the offset, the filterbank (M=1024, 2x, 12 taps)
@@ -458,13 +569,64 @@ def _c2_arm(torch, device, steps):
     ev1.record(st)
     torch.cuda.synchronize()
     dt = ev0.elapsed_time(ev1) / 1e3
-    return {"workload": "front_end_ci16q11_m1024_os2_k12_blocks_2e6", "value": round(nb * blk / dt / 1e6, 2),
-            "unit": "MSamples/s", "x_real_time_at_40msps": round(nb * blk / dt / 40e6, 1),
-            "bytes_per_sample": 4 + 4 + 16 + 16,
-            "path": "block_mean + fused unpack/filterbank + one-pass W1/W2, per 50 ms block"}
+    res = {"workload": "front_end_ci16q11_m1024_os2_k12_blocks_2e6", "value": round(nb * blk / dt / 1e6, 2),
+           "unit": "MSamples/s", "x_real_time_at_40msps": round(nb * blk / dt / 40e6, 1),
+           "bytes_per_sample": 4 + 4 + 16 + 16,
+           "path": "block_mean + fused unpack/filterbank + one-pass W1/W2, per 50 ms block"}
+    if cpu:
+        res.update(_c2_check(raw[: 3 * blk].cpu().numpy(), blk, torch, device))
+    return res
 
 
-def _c3_arm(torch, device, steps):
+def _c2_check(raw, blk, torch, device) -> dict:
+    """The front end's first three blocks through a fresh handle and through
+    the reference library (unpack_dc with the previous block's mean as the
+    offset, then the filterbank, then W1 and W2), the same offsets fed to
+    both: output and W2 power accuracy, and the reference's rate on all host
+    threads for the same work."""
+    from oracle import oracle as O
+    ref = O.reference()
+    if ref is None:
+        return {}
+    import atkdsp_b200 as ak
+    from atkdsp_b200 import gpu
+    nth = os.cpu_count() or 1
+    ref.lib.atkdsp_set_threads(nth)
+    rp = ref.Pfb(FS, 1024, 2, 12, 80.0, 1)
+    R = np.zeros((1024, 1, 1), np.complex64)
+    cnt = np.zeros(1024, np.uint32)
+    blocks = [raw[b * blk:(b + 1) * blk] for b in range(3)]
+    offs, refs, pw_ref = [0j], [], []
+    t0 = time.perf_counter()
+    for b in range(3):
+        x, mean = ref.unpack_dc(blocks[b].tobytes(), "ci16q11", offs[-1])
+        y = rp.process_n([x], 1)
+        ref.pfb_cov_accumulate(y, 1, 1024, None, R, cnt)
+        pw_ref.append(ref.pfb_channel_power(y, 1, 1024)[0])
+        refs.append(y)
+        offs.append(complex(np.float32(mean.real), np.float32(mean.imag)))
+    rdt = time.perf_counter() - t0
+    p = ak.Pfb(FS, 1024, 2, 12, 80.0, 1)
+    st = torch.cuda.ExternalStream(ak.load().atkdsp_gpu_pfb_stream(p.handle), device=device)
+    cases, pw_err = [], 0.0
+    for b in range(3):
+        r = torch.from_numpy(blocks[b].reshape(-1).copy()).to(device)
+        torch.cuda.synchronize()
+        y = gpu.process_n_raw(p, [r], 1, "ci16q11", offs[b], stream=st)
+        pwr, _mp = gpu.channel_power(y, 1, 1024, stream=st)
+        torch.cuda.synchronize()
+        cases.append((y.cpu().numpy(), refs[b], None))
+        pw = pwr.cpu().numpy().reshape(-1).astype(np.float64)
+        pw_err = max(pw_err, float(np.max(np.abs(pw - pw_ref[b].reshape(-1)) / pw_ref[b].reshape(-1))))
+    acc = _accuracy(cases, "the first three 2,000,000-sample blocks (same offsets on both sides)")
+    acc["w2_power_max_rel"] = float(f"{pw_err:.3g}")
+    return {"accuracy": acc,
+            "cpu_baseline": {"value": round(3 * blk / rdt / 1e6, 2), "unit": "MSamples/s", "cores": nth,
+                             "kind": "reference", "sample": "three 2,000,000-sample blocks: unpack_dc, "
+                                                            "filterbank, W1, W2"}}
+
+
+def _c3_arm(torch, device, steps, cpu: bool):
     """Coherent array: 8 cf32 element streams, M=2048, 1x, 16 taps, 2^24 samples
     each, 4 common tones with per-element phases + noise at 10 dB; one
     process_n call per step, then W1 (8x8 per channel) and W2 in one pass."""
@@ -506,8 +668,56 @@ def _c3_arm(torch, device, steps):
     ev1.record(st)
     torch.cuda.synchronize()
     dt = ev0.elapsed_time(ev1) / 1e3
-    return {"workload": "coherent_8el_m2048_os1_k16_2^24", "value": round(nel * n * max(steps, 1) / dt / 1e6, 2),
-            "unit": "MSamples/s (aggregate over elements)", "path": "process_n (device) + one-pass W1/W2"}
+    res = {"workload": "coherent_8el_m2048_os1_k16_2^24", "value": round(nel * n * max(steps, 1) / dt / 1e6, 2),
+           "unit": "MSamples/s (aggregate over elements)", "path": "process_n (device) + one-pass W1/W2"}
+    if cpu:
+        res.update(_c3_check([x[: 1 << 20].cpu().numpy() for x in xs], torch, device))
+    return res
+
+
+def _c3_check(xs, torch, device) -> dict:
+    """The coherent array's first 2^20 samples of each element through a
+    fresh handle and through the reference library (process_n, W1, W2):
+    accuracy of the outputs, W1 and W2, float64 on 2^16, and the reference's
+    rate on all host threads for the same work."""
+    from oracle import oracle as O
+    ref = O.reference()
+    if ref is None:
+        return {}
+    import atkdsp_b200 as ak
+    from atkdsp_b200 import gpu
+    from atkdsp_b200 import workloads as W
+    nel, M = len(xs), 2048
+    nth = os.cpu_count() or 1
+    ref.lib.atkdsp_set_threads(nth)
+    rp = ref.Pfb(FS, M, 1, 16, W.ATTEN_BETA8, nel)
+    R = np.zeros((M, nel, nel), np.complex64)
+    cnt = np.zeros(M, np.uint32)
+    t0 = time.perf_counter()
+    yr = rp.process_n(xs, nel)
+    ref.pfb_cov_accumulate(yr, nel, M, None, R, cnt)
+    pr, _ = ref.pfb_channel_power(yr, nel, M)
+    rdt = time.perf_counter() - t0
+    p = ak.Pfb(FS, M, 1, 16, W.ATTEN_BETA8, nel)
+    st = torch.cuda.ExternalStream(ak.load().atkdsp_gpu_pfb_stream(p.handle), device=device)
+    din = [torch.from_numpy(x).to(device) for x in xs]
+    Rd = torch.zeros((M, nel, nel), dtype=torch.complex64, device=device)
+    cd = torch.zeros(M, dtype=torch.int32, device=device)
+    pd = torch.zeros((nel, M), dtype=torch.float32, device=device)
+    md = torch.zeros(M, dtype=torch.float32, device=device)
+    torch.cuda.synchronize()
+    y = gpu.process_n(p, din, nel, stream=st)
+    gpu.accumulate(y, nel, M, Rd, cd, pd, md, stream=st)
+    torch.cuda.synchronize()
+    y64 = _fp64(M, 1, 16, W.ATTEN_BETA8, [x[: 1 << 16] for x in xs])
+    acc = _accuracy([(y.cpu().numpy(), yr, y64)], "2^20 samples of each of the 8 elements (float64 on 2^16)")
+    Rg = Rd.cpu().numpy()
+    acc["w1_max_rel"] = float(f"{float(np.max(np.abs(Rg - R)) / np.max(np.abs(R))):.3g}")
+    acc["w2_power_max_rel"] = float(f"{float(np.max(np.abs(pd.cpu().numpy() - pr) / pr)):.3g}")
+    return {"accuracy": acc,
+            "cpu_baseline": {"value": round(nel * xs[0].size / rdt / 1e6, 2),
+                             "unit": "MSamples/s (aggregate over elements)", "cores": nth, "kind": "reference",
+                             "sample": "2^20 samples of each element: process_n, W1, W2"}}
 
 
 OSX_N = 1 << 24
@@ -701,12 +911,12 @@ def _spectrum_arm(torch, device, steps, cpu: bool):
     stats lines in one pass; cpu: the reference's atkdsp_spectrum_reduce on
     2^22 samples with every host thread."""
     from atkdsp_b200.gpu import Spectrum
-    from oracle import oracle as O
     n, hop, N = 4096, 2048, 1 << 24
     g = torch.Generator(device=device)
     g.manual_seed(13)
     x = torch.randn(N, dtype=torch.complex64, device=device, generator=g)
-    w = torch.from_numpy(O.oracle().window("hann", n)).to(device)
+    k = np.arange(n)
+    w = torch.from_numpy((0.5 - 0.5 * np.cos(2.0 * np.pi * k / (n - 1))).astype(np.float32)).to(device)
     sp = Spectrum(n)
     res = {"workload": "spectrum_n4096_hop2048_hann_2^24", "unit": "MSamples/s",
            "path": "atkdsp_gpu_spectrum_reduce (average detector) / atkdsp_gpu_spectrum_stats"}
@@ -723,6 +933,7 @@ def _spectrum_arm(torch, device, steps, cpu: bool):
         res[name] = round(N * max(steps, 1) / (e0.elapsed_time(e1) / 1e3) / 1e6, 2)
     res["frames_per_call"] = (N - n) // hop + 1
     if cpu:
+        from oracle import oracle as O
         ref = O.reference()
         if ref is not None:
             nth = os.cpu_count() or 1
@@ -788,7 +999,7 @@ def _cfar_arm(torch, device, steps, cpu: bool):
     return res
 
 
-def _served_arm(torch, device, duration_s):
+def _served_arm(torch, device, duration_s, cpu: bool):
     """Serving: 4096 live streams at {2.4, 10, 40} MS/s delivering 1.6 ms ci16
     blocks with Poisson arrivals, nchan {256, 1024}, 16 taps, 2x, churn 20/s,
     admission by free HBM. Then the largest stream count whose p99 block
@@ -822,7 +1033,57 @@ def _served_arm(torch, device, duration_s):
         n, r = best
         res["within_p99_1.6ms"] = {"streams": n, "value": round(r["samples_done"] / r["wall_s"] / 1e6, 2),
                                    "p50_ms": round(r["lat_p50_ms"], 3), "p99_ms": round(r["lat_p99_ms"], 3)}
+    if cpu:
+        res.update(_served_check(torch, device))
     return res
+
+
+def _served_check(torch, device) -> dict:
+    """Served streams' blocks (ci16, nchan 256 / 1024, 16 taps, 2x): eight
+    streams' first four 1.6 ms blocks through the fused int16 device path and
+    through the reference library (unpack to cf32, then the filterbank) for
+    accuracy; and the reference's rate over one block of each of the first
+    512 streams of the trace, one call pair per block, all host threads."""
+    from oracle import oracle as O
+    ref = O.reference()
+    if ref is None:
+        return {}
+    import atkdsp_b200 as ak
+    from atkdsp_b200 import gpu
+    from atkdsp_b200 import workloads as W
+    specs = W.served_streams(4096)
+    nth = os.cpu_count() or 1
+    ref.lib.atkdsp_set_threads(nth)
+    cases = []
+    for sp in specs[:8]:
+        rp = ref.Pfb(FS, sp.nchan, 2, 16, 80.0, 1)
+        p = ak.Pfb(FS, sp.nchan, 2, 16, 80.0, 1)
+        st = torch.cuda.ExternalStream(ak.load().atkdsp_gpu_pfb_stream(p.handle), device=device)
+        ys, rs = [], []
+        for b in range(4):
+            raw = W.ci16_block(sp.block, sp.seed, b)
+            x, _ = ref.unpack_dc(raw.tobytes(), "ci16", 0j)
+            rs.append(rp.process_n([x], 1))
+            d = torch.from_numpy(raw.reshape(-1).copy()).to(device)
+            torch.cuda.synchronize()
+            ys.append(gpu.process_n_raw(p, [d], 1, "ci16", 0j, stream=st).cpu().numpy())
+        cases.append((np.concatenate(ys, axis=-1), np.concatenate(rs, axis=-1), None))
+    acc = _accuracy(cases, "eight served streams, four blocks each")
+    blocks = [(sp, W.ci16_block(sp.block, sp.seed, 0).tobytes()) for sp in specs[:512]]
+    handles = {}
+    n = 0
+    t0 = time.perf_counter()
+    for sp, raw in blocks:
+        h = handles.get(sp.nchan) or handles.setdefault(sp.nchan, ref.Pfb(FS, sp.nchan, 2, 16, 80.0, 1))
+        x, _ = ref.unpack_dc(raw, "ci16", 0j)
+        h.process_n([x], 1)
+        n += x.size
+    rdt = time.perf_counter() - t0
+    return {"accuracy": acc,
+            "cpu_baseline": {"value": round(n / rdt / 1e6, 2), "unit": "MSamples/s", "cores": nth,
+                             "kind": "reference",
+                             "sample": "one block of each of the first 512 streams of the trace (unpack_dc + "
+                                       "filterbank per block)"}}
 
 
 def run_ours(args, rep):
@@ -894,9 +1155,9 @@ def run_ours(args, rep):
     del batch, handles, bstream
     torch.cuda.synchronize()
     if rank == 0:
-        for name, fn in (("single_stream", lambda: _c1_arm(torch)),
-                         ("front_end", lambda: _c2_arm(torch, device, 1)),
-                         ("coherent_array", lambda: _c3_arm(torch, device, args.steps)),
+        for name, fn in (("single_stream", lambda: _c1_arm(torch, "cpu" in arms and not args.no_cpu)),
+                         ("front_end", lambda: _c2_arm(torch, device, 1, "cpu" in arms and not args.no_cpu)),
+                         ("coherent_array", lambda: _c3_arm(torch, device, args.steps, "cpu" in arms and not args.no_cpu)),
                          ("extractor", lambda: _osx_arm(torch, device, args.steps,
                                                         "cpu" in arms and not args.no_cpu)),
                          ("scale_bank", lambda: _bank_arm(torch, device, args.steps,
@@ -905,7 +1166,7 @@ def run_ours(args, rep):
                                                             "cpu" in arms and not args.no_cpu)),
                          ("cfar", lambda: _cfar_arm(torch, device, args.steps,
                                                     "cpu" in arms and not args.no_cpu)),
-                         ("served", lambda: _served_arm(torch, device, 3.0))):
+                         ("served", lambda: _served_arm(torch, device, 3.0, "cpu" in arms and not args.no_cpu))):
             if name in arms:
                 try:
                     extra[name] = fn()
@@ -917,11 +1178,20 @@ def run_ours(args, rep):
         return
     peak, peak_kind = _peaks()
     achieved = alg / (k_ms / 1e3) / 1e9
-    traffic = None
+    # DRAM traffic per launch: the traffic / algorithmic-bytes ratio of an ncu
+    # capture of this kernel on a smaller version of the workload (the full
+    # launch is too large for a multi-pass capture), scaled to this launch
+    traffic, traffic_src = None, None
     prof = ROOT / "profiles" / "pfb_tiles_uneven256.json"
     if prof.exists():
-        traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+        pj = json.loads(prof.read_text())
+        if pj.get("ratio_traffic_over_algorithmic"):
+            traffic = int(round(pj["ratio_traffic_over_algorithmic"] * alg))
+            traffic_src = (f"ratio {pj['ratio_traffic_over_algorithmic']} from "
+                           f"profiles/pfb_tiles_uneven256.json ({pj.get('captured', 'capture')}) x this launch's "
+                           f"algorithmic bytes")
     cpu = _cpu_reference_rate(specs) if "cpu" in arms and not args.no_cpu else None
+    acc = _batched_accuracy(specs, torch, device) if "cpu" in arms and not args.no_cpu else None
     total = S * world
     value = total * args.steps / t_batch / 1e6
     line = {
@@ -929,12 +1199,7 @@ def run_ours(args, rep):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_batch / args.steps * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 fold + f64 fft", "data": "synthetic (seeded noise + tones, generated on device)",
-        "config": {"workload": WORKLOAD if args.streams == 256 and args.min_log2 == 14 and
-                   args.max_log2 == 22 else f"uneven_streams_{args.streams}_2^{args.min_log2:g}-2^{args.max_log2:g}",
-                   "streams": args.streams, "nchan": [64, 256, 1024, 4096],
-                   "taps_per_branch": [8, 12, 16], "oversample": 2, "blocks": 3,
-                   "samples_per_step_per_gpu": S, "parallelism": f"replicas x{world} (stream-sharded)",
-                   "l2": "inputs larger than L2 (~1.5 GB per step)"},
+        "config": dict(_config(args, world), samples_per_step_per_gpu=S),
         "plain": None if t_plain is None else {
             "value": round(total * args.steps / t_plain / 1e6, 2), "unit": "MSamples/s",
             "what": "one device-pointer call per stream"},
@@ -952,17 +1217,51 @@ def run_ours(args, rep):
             "value": round(total / t_dropin[0] / 1e6, 2), "unit": "MSamples/s",
             "what": f"atkdsp_pfb_process per stream, pageable host buffers, {CABI_THREADS} host threads"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_source": traffic_src,
                      "kernel": "pfb_tiles_kernel", "kernel_ms": round(k_ms, 4),
                      "alg_bytes_per_launch": alg, "peak_kind": peak_kind},
         "configs": extra,
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
+        "native_so": _native_maps(),
     }
+    if acc:
+        line["accuracy"] = acc
     if cpu:
         line["cpu_baseline"] = {"value": round(cpu[0], 2), "unit": "MSamples/s", "cores": cpu[1],
                                 "kind": "reference", "sample": cpu[2]}
     print(json.dumps(line))
+
+
+def _native_maps() -> list:
+    """The shared objects of this repository mapped into this process (read
+    from /proc/self/maps): the evidence of which native code ran."""
+    seen = []
+    try:
+        with open("/proc/self/maps") as f:
+            for ln in f:
+                parts = ln.split()
+                if len(parts) >= 6 and parts[-1].endswith(".so") and parts[-1].startswith(str(ROOT)):
+                    rel = os.path.relpath(parts[-1], ROOT)
+                    if rel not in seen:
+                        seen.append(rel)
+    except OSError:
+        pass
+    return seen
+
+
+def _spawn_ranks(n: int) -> int:
+    """`--gpus N` without a launcher: start N ranks under torch.distributed.run
+    (one process per GPU, rendezvous on 127.0.0.1) and pass their output and
+    exit status through."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve())]
+    cmd += sys.argv[1:]
+    return subprocess.call(cmd)
 
 
 def main():
@@ -980,10 +1279,14 @@ def main():
     ap.add_argument("--max-log2", type=float, default=22.0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(_spawn_ranks(args.gpus))
     from atkdsp_b200.replicas import Replicas
 
     # one process per GPU; the group exists only for the timing reductions
     rep = Replicas(backend="gloo" if args.impl == "reference" else None, timeout_s=120)
+    if rep.world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but the launcher started {rep.world} ranks")
     try:
         if args.impl == "reference":
             run_reference(args, rep.rank, rep.world)
@@ -991,17 +1294,7 @@ def main():
             run_ours(args, rep)
     finally:
         rep.close()
-    import gc
-    gc.collect()
-    if args.impl != "reference":
-        import torch
-        torch.cuda.synchronize()
     sys.stdout.flush()
-    sys.stderr.flush()
-    # Leave without interpreter teardown: the process holds two CUDA runtimes
-    # (torch's and the library's static one) whose exit-time destructors run
-    # in an order neither controls; every result is already printed.
-    os._exit(0)
 
 
 if __name__ == "__main__":

@@ -106,21 +106,36 @@ ATKDSP_API int         atkdsp_gpu_pfb_channel_power(const atkdsp_cf32 *d_out, un
                                                     float *d_mean_pwr, void *stream);
 
 /* ---- tile shape (no reference counterpart) ------------------------------
- * For a power-of-two nchan <= 2048 at oversample 1, 2 or 4 the kernel has two
- * tile shapes: the paired fold (each thread folds two consecutive hops over
- * the even or odd branches: half the sample and tap loads, one more FFT pass)
- * or one hop and 8 branches per thread. Filterbanks take the choice for their
- * (nchan, oversample, taps/branch) from the table compiled into the library
- * (written by `python -m atkdsp_b200.autotune --write` from measurements on
- * the device), else the paired fold. atkdsp_gpu_tune_set overrides it for
- * filterbanks created afterwards in this process (choice 1: paired, 0: one
- * hop per thread, -1: back to the table); ATKDSP_E_ARG for a shape with only
- * one tile shape. atkdsp_gpu_tune_get returns the choice such a filterbank
- * gets now (1 or 0), or ATKDSP_E_ARG. Outputs are the same either way. */
+ * For a power-of-two nchan <= 2048 at oversample 1, 2 or 4 the kernel has
+ * several tile shapes, i.e. hops per thread in the fold: the paired fold
+ * (each thread folds two consecutive hops over the even or odd branches:
+ * half the sample and tap loads, one more FFT pass), one hop and 8 branches
+ * per thread, and -- at oversample 1 or 2 with nchan <= 1024 -- the quad fold
+ * (four hops per thread over two branches, a radix-2 first pass).
+ * Filterbanks take the choice for their (nchan, oversample, taps/branch) from
+ * the table compiled into the library (written by `python -m
+ * atkdsp_b200.autotune --write` from measurements on the device), else the
+ * quad fold where it exists and the paired fold elsewhere.
+ * atkdsp_gpu_tune_set overrides it for filterbanks created afterwards in this
+ * process (choice 1: paired, 0: one hop per thread, 2: quad, -1: back to the
+ * table); ATKDSP_E_ARG for a shape without that choice.
+ * atkdsp_gpu_tune_get returns the choice such a filterbank gets now (0, 1 or
+ * 2), or ATKDSP_E_ARG. Every shape meets the same parity bar; they differ
+ * only in speed (and, through their FFT plans, in the last bit of a few
+ * outputs). */
 ATKDSP_API int         atkdsp_gpu_tune_set(unsigned nchan, unsigned oversample,
                                            unsigned taps_per_poly, int choice);
 ATKDSP_API int         atkdsp_gpu_tune_get(unsigned nchan, unsigned oversample,
                                            unsigned taps_per_poly);
+
+/* ---- allocation fault injection (no reference counterpart) --------------
+ * A test hook for callers' out-of-memory handling, acting on the host only:
+ * with n > 0 the n-th device, pool or pinned-host allocation this library
+ * makes from now on fails as a real out-of-memory would (create returns
+ * NULL, the server's open ATKDSP_E_NOMEM, the host W1/W2/unpack calls leave
+ * their outputs untouched), and the hook disarms itself; n <= 0 disarms it.
+ * No kernel is involved and no device fault is raised. */
+ATKDSP_API void        atkdsp_gpu_fail_alloc_after(long long n);
 
 /* ---- batches: many independent handles in one persistent launch --------
  * A batch groups handles (each single-element, any nchan / taps / oversample)

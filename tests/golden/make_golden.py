@@ -3,8 +3,10 @@
 Run in a container that has the reference sources (it reads them; nothing on
 the GPU machine does):
 
-    make -C oracle            # builds oracle/_ref/libatkdsp_ref.so from the sources
+    make -C oracle REF=<reference tree>     # builds oracle/_ref/libatkdsp_ref.so
     python tests/golden/make_golden.py [REF_ROOT] [--only NAME ...]
+
+REF_ROOT defaults to the ATKDSP_REFERENCE environment variable.
 
 Every output here is produced by the REFERENCE: its C library (compiled from
 its own sources by oracle/Makefile) for float32 results, and its numpy twin
@@ -34,6 +36,7 @@ Fixture files (tests/golden/*.npz):
 from __future__ import annotations
 
 import hashlib
+import os
 import sys
 from pathlib import Path
 
@@ -53,7 +56,7 @@ import cfar_cases                              # noqa: E402
 _ARGS = [a for a in sys.argv[1:] if not a.startswith("--")]
 ONLY = sys.argv[sys.argv.index("--only") + 1:] if "--only" in sys.argv else None
 REF_ROOT = Path(_ARGS[0]) if _ARGS and (ONLY is None or sys.argv.index(_ARGS[0]) < sys.argv.index("--only")) \
-    else Path("/root/reference")
+    else Path(os.environ["ATKDSP_REFERENCE"])
 sys.path.insert(0, str(REF_ROOT / "python"))
 from atkdsp import reference as twin           # noqa: E402
 

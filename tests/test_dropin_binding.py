@@ -4,10 +4,12 @@ The binding binds ~300 symbols eagerly, most outside the channelizer path,
 so the drop-in is a link-only composite: this library first, the reference
 library (built from its sources into oracle/_ref) second. The dynamic loader
 then resolves the channelizer path from this library and everything else
-from the reference. INTEGRATION.md section 2(a) gives the same recipe.
+from the reference.
 
-Skipped where the reference sources (its binding) are absent. No GPU call is
-made: load(), the ABI check and symbol binding need none.
+The reference's source tree (for its binding, python/atkdsp) is named by the
+ATKDSP_REFERENCE environment variable; the test is skipped where it is not
+set or the binding is absent. No GPU call is made: load(), the ABI check and
+symbol binding need none.
 """
 
 from __future__ import annotations
@@ -22,7 +24,7 @@ import pytest
 
 from conftest import ROOT
 
-REF_PY = Path("/root/reference/python")
+REF_PY = Path(os.environ.get("ATKDSP_REFERENCE", "/nonexistent")) / "python"
 REF_SO = ROOT / "oracle" / "_ref" / "libatkdsp_ref.so"
 OUR_SO = ROOT / "atkdsp_b200" / "lib" / "libatkdsp_b200.so"
 

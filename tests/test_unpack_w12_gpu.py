@@ -215,3 +215,41 @@ def test_w2_powers_gate_w1_on_the_device():
     assert np.all(Rd[gh == 0] == 0)
     assert np.array_equal(cnt.cpu().numpy().astype(np.uint32), co)
     assert np.all(co[gh == 0] == 0) and np.all(co[gh == 1] == y.shape[-1])
+
+
+def test_host_w1_w2_and_unpack_from_two_threads_at_once():
+    """The host-pointer W1/W2 and unpack calls stage through a per-thread
+    device area on their own stream, so calls from different threads run at
+    the same time and never share memory: each thread's results equal the
+    same calls made one after the other."""
+    import threading
+    rng = np.random.default_rng(11)
+    nel, M, m = 3, 256, 700
+    blocks = [(rng.standard_normal((nel, M, m)) + 1j * rng.standard_normal((nel, M, m))).astype(np.complex64)
+              for _ in range(2)]
+    raws = [rng.integers(-2048, 2048, 2 * 300_001, dtype=np.int64).astype("<i2").tobytes() for _ in range(2)]
+
+    def work(i, res):
+        R = np.zeros((M, nel, nel), np.complex64)
+        c = np.zeros(M, np.uint32)
+        for _ in range(20):
+            ak.pfb_cov_accumulate(blocks[i], nel, M, None, R, c)
+            pw, mp = ak.pfb_channel_power(blocks[i], nel, M)
+            x, mean = ak.unpack_dc(raws[i], "ci16q11", 0.01j)
+        res[i] = (R, c, pw, mp, x, mean)
+
+    serial = [None, None]
+    for i in range(2):
+        work(i, serial)
+    par = [None, None]
+    ts = [threading.Thread(target=work, args=(i, par)) for i in range(2)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    for i in range(2):
+        for a, b in zip(serial[i], par[i]):
+            if isinstance(a, np.ndarray):
+                assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), i
+            else:
+                assert a == b, i

@@ -87,3 +87,50 @@ def test_no_alloc_unpack_dc_refuses_calls_beyond_its_scratch():
     m = mean.cpu().numpy()                     # raw zeros: the mean before the offset is 0
     assert abs(m[0]) < 1e-12 and abs(m[1]) < 1e-12
     assert torch.all(out[:MAX_SAMPLES] == complex(-0.5, -0.5)).item()
+
+
+def _call_ptr(f, ptr, nbytes, fmt, out, n, off, mean):
+    return f(C.c_void_p(ptr), nbytes, ak.FMT[fmt], C.c_void_p(out.data_ptr()), n, float(off.real),
+             float(off.imag), None if mean is None else C.c_void_p(mean.data_ptr()), None)
+
+
+@pytest.mark.parametrize("case", ["empty", "unaligned_ci16", "cf32_copy_no_mean"])
+def test_no_alloc_unpack_dc_edge_paths(case):
+    """The paths where the entry point's code differs from the allocating
+    one's: an empty block (the mean is the offset), a raw pointer 4 bytes
+    past a 16-byte boundary (the scalar conversion kernel), and cf32 with a
+    zero offset and no mean (a plain copy). Each is run twice in a row, and
+    must give the allocating entry point's samples and mean."""
+    lib = ak.load()
+    noalloc = _entry(lib, "atkdsp_gpu_unpack_dc_noalloc")
+    alloc = _entry(lib, "atkdsp_gpu_unpack_dc")
+    rng = np.random.default_rng(7)
+    if case == "empty":
+        fmt, off, n = "ci16q11", 0.25 - 0.5j, 0
+        buf = torch.zeros(16, dtype=torch.int16, device="cuda")
+        ptr, nbytes = buf.data_ptr(), 0
+    elif case == "unaligned_ci16":
+        fmt, off, n = "ci16", -0.125 + 0.0625j, 50_001
+        buf = torch.from_numpy(rng.integers(-32768, 32768, 2 * n + 2, dtype=np.int64).astype("<i2")).cuda()
+        ptr, nbytes = buf.data_ptr() + 4, 4 * n
+        assert ptr % 16 == 4
+    else:
+        fmt, off, n = "cf32", 0j, 70_003
+        x = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+        buf = torch.from_numpy(x).cuda()
+        ptr, nbytes = buf.data_ptr(), 8 * n
+    want_mean = case != "cf32_copy_no_mean"
+    for _ in range(2):
+        out_a = torch.full((max(n, 1),), complex(7.0, 7.0), dtype=torch.complex64, device="cuda")
+        out_b = out_a.clone()
+        mean_a = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda") if want_mean else None
+        mean_b = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda") if want_mean else None
+        assert _call_ptr(noalloc, ptr, nbytes, fmt, out_a, n, off, mean_a) == n
+        assert _call_ptr(alloc, ptr, nbytes, fmt, out_b, n, off, mean_b) == n
+        torch.cuda.synchronize()
+        assert np.array_equal(out_a.cpu().numpy().view(np.uint32), out_b.cpu().numpy().view(np.uint32)), case
+        if want_mean:
+            ma, mb = mean_a.cpu().numpy(), mean_b.cpu().numpy()
+            assert np.all(np.abs(ma - mb) <= 1e-12 * np.maximum(1.0, np.abs(mb))), (case, ma, mb)
+            if n == 0:
+                assert np.allclose(ma, [np.float32(off.real), np.float32(off.imag)], rtol=0, atol=0)
