@@ -121,6 +121,9 @@ def _bind(lib) -> None:
         "atkdsp_gpu_pfb_sync": ([vp], C.c_int),
         "atkdsp_gpu_pfb_process_n": ([vp, P(vp), u, sz, vp, sz, vp], ssz),
         "atkdsp_gpu_pfb_process_n_raw": ([vp, P(vp), u, sz, C.c_int, C.c_float, C.c_float, vp, sz, vp], ssz),
+        "atkdsp_gpu_pfb_w12_scratch_bytes": ([vp, sz], sz),
+        "atkdsp_gpu_pfb_process_w12": ([vp, vp, sz, C.c_int, C.c_float, C.c_float, vp, sz, vp, vp, vp, vp, vp,
+                                        vp, sz, vp], ssz),
         "atkdsp_gpu_batch_process_raw": ([vp, P(vp), P(sz), C.c_int, P(C.c_float), P(vp), P(ssz), vp], ssz),
         "atkdsp_gpu_unpack_dc_noalloc": ([vp, sz, C.c_int, vp, sz, C.c_float, C.c_float, vp, vp], ssz),
         "atkdsp_gpu_unpack_dc": ([vp, sz, C.c_int, vp, sz, C.c_float, C.c_float, vp, vp], ssz),
@@ -172,6 +175,10 @@ def _bind(lib) -> None:
         "atkdsp_gpu_cfar_process": ([vp, vp, C.c_int, sz, d, d, P(_CfarEvent), sz, vp, vp], ssz),
         "atkdsp_gpu_tune_set": ([u, u, u, C.c_int], C.c_int),
         "atkdsp_gpu_fail_alloc_after": ([C.c_longlong], None),
+        "atkdsp_gpu_pfb_faults": ([vp], C.c_int),
+        "atkdsp_gpu_batch_faults": ([vp], C.c_int),
+        "atkdsp_gpu_debug_build": ([], C.c_int),
+        "atkdsp_gpu_inject_short_window": ([C.c_longlong], None),
         "atkdsp_gpu_tune_get": ([u, u, u], C.c_int),
     }
     for name, (args, res) in sigs.items():

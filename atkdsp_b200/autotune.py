@@ -11,9 +11,8 @@ the quad fold (four hops per thread). Each is timed on one stream of 2^log2n
 cf32 samples through the batched kernel (atkdsp_b200.microbench.run_one, the
 kernel's own CUDA events, median of the repetitions), and the fastest goes
 into the table the library compiles in (the paired fold unless another is
-faster by the margin). A shape not in the grid takes the quad fold where it
-exists, else the paired fold. Outputs are identical whichever is chosen; only
-speed differs. One JSON line per shape:
+faster by the margin). A shape not in the grid takes the paired fold. Every
+shape meets the same parity bar; only speed differs. One JSON line per shape:
 {"nchan", "oversample", "taps", "paired_gsps", "single_gsps", "quad_gsps", "pair"}.
 """
 
@@ -66,8 +65,7 @@ def write_table(rows, path: Path = TABLE) -> None:
              " * taps/branch). Written by",
              " *   python -m atkdsp_b200.autotune --write",
              " * from device measurements (GS/s paired / one hop per thread / quad in",
-             " * each comment); shapes not listed take the quad fold where it exists,",
-             " * else the paired fold. */",
+             " * each comment); shapes not listed take the paired fold. */",
              "static const tune_entry k_tune_table[] = {"]
     for r in rows:
         q = f" / {r['quad_gsps']:.2f}" if r.get("quad_gsps") is not None else ""

@@ -135,10 +135,11 @@ static void design_prototype(unsigned nchan, unsigned K, double atten_db, double
 static int is_pow2(unsigned v) { return v && !(v & (v - 1)); }
 
 /* ---- the tile-shape choice -----------------------------------------------
- * Where both exist (can_pair), a bank uses the paired fold (two hops per
- * thread over even or odd branches: half the loads, one more FFT pass) or
- * one hop and 8 branches per thread. The choice comes from a runtime
- * override (atkdsp_gpu_tune_set), else from the table the autotuner wrote
+ * Where several exist (can_pair, can_quad), a bank uses the paired fold (two
+ * hops per thread over even or odd branches: half the loads, one more FFT
+ * pass), one hop and 8 branches per thread, or the quad fold (four hops per
+ * thread over two branches). The choice comes from a runtime override
+ * (atkdsp_gpu_tune_set), else from the table the autotuner wrote
  * (tune_table.h, measured on B200), else the paired fold. */
 typedef struct { unsigned nchan, os, K; int pair; } tune_entry;
 #include "tune_table.h"
@@ -173,7 +174,7 @@ static int tune_choice(unsigned M, unsigned os, unsigned K) {
     for (i = 0; i < sizeof k_tune_table / sizeof k_tune_table[0]; ++i)
         if (k_tune_table[i].nchan == M && k_tune_table[i].os == os && k_tune_table[i].K == K)
             return k_tune_table[i].pair;
-    return can_quad(M, os) ? 2 : 1;
+    return 1;
 }
 
 ATKDSP_API int atkdsp_gpu_tune_set(unsigned nchan, unsigned oversample, unsigned taps_per_poly, int choice) {
@@ -241,6 +242,8 @@ static int plan_fft(unsigned M, unsigned os, int want_pair, atkb_fft_plan *pl) {
             }
         }
     }
+    /* beyond one CTA's shared memory: the separate-kernel path */
+    pl->big = !pl->fast && (M > MAX_GENERIC_NCHAN || (is_pow2(M) && M > MAX_POW2_NCHAN));
     /* per-pass twiddles (fast path): pass p >= 1 holds W_{Ns R}^{k} at k,
      * k in [0, Ns); the kernel forms the powers r = 2 .. R-1 by complex
      * multiplication */
@@ -322,10 +325,12 @@ ATKDSP_API void atkdsp_pfb_destroy(atkdsp_pfb *p) {
     atkb_free(p->d_counters);
     atkb_host_free(p->h_tables);           /* h_small_in lives inside it */
     atkb_host_free(p->h_small_out);
+    atkb_host_free(p->h_pend);
     atkb_event_destroy(p->small_ev);
     atkb_event_destroy(p->tbl_event);
     atkb_stream_destroy(p->stream);
     free((void *)p->dins);
+    atkb_free(p->d_big);
     free(p);
 }
 
@@ -423,7 +428,10 @@ static int bank_build(bank_entry *be, void *stream) {
         unsigned v = M;
         while (v > 1) { v >>= 1; ++B->logm; }
     }
-    if (pl.fast && M == 4096) {
+    if (pl.big) {
+        B->tile_hops = 1;                /* no tiles: separate kernels per hop chunk */
+        B->smem_bytes = 0;
+    } else if (pl.fast && M == 4096) {
         /* two hops a tile, computed in turn: the FFT tile plus the first
          * hop's 4096 outputs (so the write covers two hops per channel) */
         B->tile_hops = 2;
@@ -498,7 +506,7 @@ atkdsp_pfb *atkb_pfb_create_internal(double fs, unsigned nchan, unsigned oversam
                                      int lean) {
     if (!(fs > 0.0) || nchan < 2 || oversample < 1 || nchan % oversample != 0) return NULL;
     if (taps_per_poly < 2 || max_nel < 1) return NULL;
-    if (is_pow2(nchan) ? nchan > MAX_POW2_NCHAN : nchan > MAX_GENERIC_NCHAN) return NULL;
+    if (lean && (is_pow2(nchan) ? nchan > MAX_POW2_NCHAN : nchan > MAX_GENERIC_NCHAN)) return NULL;
     if (atten_db < 20.0) atten_db = 20.0;
     atkdsp_pfb *p = (atkdsp_pfb *)calloc(1, sizeof *p);
     if (!p) return NULL;
@@ -545,6 +553,8 @@ atkdsp_pfb *atkb_pfb_create_internal(double fs, unsigned nchan, unsigned oversam
         return p;
     }
     if (rc == ATKB_OK && !(p->dins = (const void **)calloc(max_nel, sizeof *p->dins))) rc = ATKB_E_NOMEM;
+    if (rc == ATKB_OK && p->bank.plan.big)          /* two double2 buffers of a hop chunk */
+        rc = atkb_malloc(&p->d_big, 2 * (size_t)atkb_pfb_big_hops((int)nchan) * nchan * 16);
     /* host-path staging: about 2^20 samples per element, whole hops */
     if (rc == ATKB_OK) {
         size_t chunk = ((size_t)1 << 21) / max_nel;
@@ -572,6 +582,7 @@ atkdsp_pfb *atkb_pfb_create_internal(double fs, unsigned nchan, unsigned oversam
             p->h_small_in = (char *)p->h_tables + p->tbl_bytes;
             p->d_small_in = (char *)p->d_tables + p->tbl_bytes;
             rc = atkb_host_alloc(&p->h_small_out, (size_t)max_nel * nchan * m_small * sizeof(atkdsp_cf32));
+            if (rc == ATKB_OK) rc = atkb_host_alloc(&p->h_pend, (size_t)max_nel * p->hop * sizeof(atkdsp_cf32));
             if (rc == ATKB_OK) rc = atkb_event_create(&p->small_ev);
         }
     }
@@ -635,6 +646,7 @@ ATKDSP_API void atkdsp_pfb_reset(atkdsp_pfb *p) {
                 p->stream);
     atkb_stream_sync(p->stream);
     p->small_live = 0;
+    p->npend = 0;
     p->lc = 0;
     p->b = 0;
     p->cur = 0;
@@ -700,6 +712,47 @@ void atkb_job_conv(atkb_job *J, atkb_carry *C, const conv_t *cv) {
     }
 }
 
+/* Bounds-check injection (a test hook, host side only): the next step's
+ * jobs claim `n` fewer samples than they have, so the kernel's window check
+ * must catch the last tiles and the carry and skip them; the buffers still
+ * hold every sample, so nothing can be read out of bounds even if the check
+ * failed. */
+static long long g_short_window;
+static pthread_mutex_t g_short_lock = PTHREAD_MUTEX_INITIALIZER;
+static long long take_short_window(void) {
+    pthread_mutex_lock(&g_short_lock);
+    const long long v = g_short_window;
+    g_short_window = 0;
+    pthread_mutex_unlock(&g_short_lock);
+    return v;
+}
+ATKDSP_API void atkdsp_gpu_inject_short_window(long long n) {
+    pthread_mutex_lock(&g_short_lock);
+    g_short_window = n > 0 ? n : 0;
+    pthread_mutex_unlock(&g_short_lock);
+}
+
+/* The fault bits the handle's launches set since the last query (0: none),
+ * cleared by the query; the debug build adds its per-thread index checks. */
+ATKDSP_API int atkdsp_gpu_pfb_faults(atkdsp_pfb *p) {
+    unsigned v = 0;
+    const unsigned z = 0;
+    if (!p) return ATKDSP_E_ARG;
+    if (atkb_set_device(p->dev) != ATKB_OK) return ATKDSP_E_FFT;
+    if (p->stream && atkb_stream_sync(p->stream) != ATKB_OK) return ATKDSP_E_FFT;
+    if (p->d_counters) {
+        if (atkb_d2h(&v, p->d_counters + ATKB_FAULT_WORD, sizeof v, p->stream) != ATKB_OK ||
+            atkb_stream_sync(p->stream) != ATKB_OK)
+            return ATKDSP_E_FFT;
+        if (v && (atkb_h2d(p->d_counters + ATKB_FAULT_WORD, &z, sizeof z, p->stream) != ATKB_OK ||
+                  atkb_stream_sync(p->stream) != ATKB_OK))
+            return ATKDSP_E_FFT;
+    }
+    return (int)(v | atkb_pfb_debug_fault());
+}
+
+ATKDSP_API int atkdsp_gpu_debug_build(void) { return atkb_pfb_debug_build(); }
+
 /* One step: nel elements, n new samples each at ins[e] (device), m hops
  * written to outs + e * nchan * ldo (device, row stride ldo). Builds the job
  * and carry tables, uploads them, launches the tile kernel and the carry,
@@ -719,6 +772,7 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
     const unsigned nxt = (unsigned)(p->cur ^ 1);
     int rc;
     unsigned e;
+    const long long short_window = take_short_window();
     if (p->tbl_event_live) {
         rc = atkb_event_sync(p->tbl_event);
         if (rc != ATKB_OK) return rc;
@@ -726,7 +780,8 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
     atkb_job *J = tbl_jobs(p->h_tables);
     atkb_carry *C = tbl_carry(p->h_tables, p->max_nel);
     int *T = tbl_tiles(p->h_tables, p->max_nel);
-    const int tiles = (int)((m + (size_t)p->bank.tile_hops - 1) / (size_t)p->bank.tile_hops);
+    const int big = p->bank.plan.big;
+    const int tiles = big ? 0 : (int)((m + (size_t)p->bank.tile_hops - 1) / (size_t)p->bank.tile_hops);
     for (e = 0; e < nel; ++e) {
         memset(&J[e], 0, sizeof J[e]);
         J[e].state = state_buf(p, p->cur, e);
@@ -748,6 +803,9 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
         C[e].head = (long long)head;
         C[e].from = (long long)(m * p->hop);
         C[e].len = (long long)(head + n - m * p->hop);
+        J[e].nsrc = C[e].nsrc = (long long)(head + n) - short_window;
+        C[e].cap = (long long)p->cap_state;
+        J[e].w2 = e == 0 ? p->w2_next : NULL;
         job_conv(&J[e], &C[e], cv);
     }
     T[nel] = (int)nel * tiles;
@@ -756,6 +814,19 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
     if (rc == ATKB_OK) rc = atkb_event_record(p->tbl_event, stream);
     if (rc != ATKB_OK) return rc;
     p->tbl_event_live = 1;
+    if (big) {
+        /* the hops through the separate kernels, a chunk at a time; after the
+         * upload (which carries a small call's block), before the tile kernel,
+         * which then only copies the state carries */
+        const long long H = atkb_pfb_big_hops((int)p->nchan);
+        long long h0;
+        for (e = 0; e < nel; ++e)
+            for (h0 = 0; h0 < (long long)m; h0 += H) {
+                const int nh = (int)((long long)m - h0 < H ? (long long)m - h0 : H);
+                rc = atkb_pfb_big(&J[e], &p->bank, h0, nh, p->d_big, p->grid, stream);
+                if (rc != ATKB_OK) return rc;
+            }
+    }
     {
         /* nel jobs: tile_start[nel] is their total (the kernel reads
          * tile_start[njobs]); the same launch copies the nel carries */
@@ -771,15 +842,53 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
     return ATKB_OK;
 }
 
-/* A small host call through the handle's pinned staging: one memcpy in, one
- * DMA each way, one memcpy out. A block that completes no hop only extends
- * the state (s = state ++ in): one copy into the current state buffer, left
- * in flight -- the call returns 0 at once, and every later use of the handle
- * is ordered after that copy (same stream, or atkb_pfb_order_after_small). */
+/* Pending samples (small calls that completed no hop) into the device state,
+ * right after the samples it already holds: one copy per element, left in
+ * flight and marked by small_ev. Every path other than the small-call path
+ * calls this before it reads or writes the state. */
+int atkb_pfb_flush_pending(atkdsp_pfb *p) {
+    int rc = ATKB_OK;
+    unsigned e;
+    if (!p->npend) return ATKB_OK;
+    if (p->small_live) {                 /* one copy in flight at a time */
+        rc = atkb_event_sync(p->small_ev);
+        if (rc != ATKB_OK) return rc;
+        p->small_live = 0;
+    }
+    const size_t at = p->ov + p->lc - p->npend;      /* the device state's head */
+    for (e = 0; e < p->pend_nel && rc == ATKB_OK; ++e)
+        rc = atkb_h2d(state_buf(p, p->cur, e) + at, (atkdsp_cf32 *)p->h_pend + (size_t)e * p->hop,
+                      p->npend * sizeof(atkdsp_cf32), p->stream);
+    if (rc == ATKB_OK) rc = atkb_event_record(p->small_ev, p->stream);
+    if (rc != ATKB_OK) return rc;
+    p->small_live = 1;
+    p->npend = 0;
+    return ATKB_OK;
+}
+
+/* A small host call through the handle's pinned staging. A block that
+ * completes no hop is only appended to the pending samples on the host (no
+ * device work at all); a block that completes hops travels with the pending
+ * samples and the job tables in one host->device copy, then one launch, one
+ * device->host copy of the outputs and one synchronisation. */
 static ptrdiff_t process_small(atkdsp_pfb *p, const atkdsp_cf32 *const *ins, unsigned nel, size_t n,
                                atkdsp_cf32 *out, size_t m) {
     int rc = ATKB_OK;
     unsigned e;
+    if (p->npend && (p->pend_nel != nel || (m > 0 && p->npend + n > ATKB_SMALL_N))) {
+        rc = atkb_pfb_flush_pending(p);
+        if (rc != ATKB_OK) return map_rc(rc);
+    }
+    if (m == 0) {                        /* lc + n < hop: the pending samples stay < hop */
+        for (e = 0; e < nel && n; ++e)
+            memcpy((atkdsp_cf32 *)p->h_pend + (size_t)e * p->hop + p->npend, ins[e], n * sizeof(atkdsp_cf32));
+        if (n) {
+            p->npend += (unsigned)n;
+            p->pend_nel = nel;
+        }
+        p->lc = (unsigned)(p->lc + n);
+        return 0;
+    }
     if (p->small_live) {                 /* h_small_in may still feed that copy */
         rc = atkb_event_sync(p->small_ev);
         if (rc != ATKB_OK) return map_rc(rc);
@@ -789,28 +898,22 @@ static ptrdiff_t process_small(atkdsp_pfb *p, const atkdsp_cf32 *const *ins, uns
         rc = atkb_event_sync(p->tbl_event);
         if (rc != ATKB_OK) return map_rc(rc);
     }
+    /* each element's pending samples, then its new block */
+    const size_t np = p->npend, nt = np + n;
     atkdsp_cf32 *hin = (atkdsp_cf32 *)p->h_small_in;
-    if (n)
-        for (e = 0; e < nel; ++e) memcpy(hin + (size_t)e * ATKB_SMALL_N, ins[e], n * sizeof(atkdsp_cf32));
-    if (m == 0) {
-        const size_t head = p->ov + p->lc;      /* head + n < ov + hop: within the buffer */
-        for (e = 0; e < nel && n && rc == ATKB_OK; ++e)
-            rc = atkb_h2d(state_buf(p, p->cur, e) + head, hin + (size_t)e * ATKB_SMALL_N,
-                          n * sizeof(atkdsp_cf32), p->stream);
-        if (rc == ATKB_OK && n) {
-            rc = atkb_event_record(p->small_ev, p->stream);
-            if (rc == ATKB_OK) p->small_live = 1;
-        }
-        if (rc != ATKB_OK) return map_rc(rc);
-        p->lc = (unsigned)(p->lc + n);
-        return 0;
+    for (e = 0; e < nel; ++e) {
+        if (np) memcpy(hin + (size_t)e * ATKB_SMALL_N, (atkdsp_cf32 *)p->h_pend + (size_t)e * p->hop,
+                       np * sizeof(atkdsp_cf32));
+        if (n) memcpy(hin + (size_t)e * ATKB_SMALL_N + np, ins[e], n * sizeof(atkdsp_cf32));
     }
     const void **dins = p->dins;
     for (e = 0; e < nel; ++e) dins[e] = (const atkdsp_cf32 *)p->d_small_in + (size_t)e * ATKB_SMALL_N;
     /* outputs packed with stride m: [nel * nchan][m], the caller's layout */
     const size_t out_n = (size_t)nel * p->nchan * m;
-    const size_t up = ((size_t)(nel - 1) * ATKB_SMALL_N + n) * sizeof(atkdsp_cf32);
-    rc = run_step_up(p, nel, dins, n, (atkdsp_cf32 *)p->d_out_stage, m, m, p->stream, &CONV_CF32, up);
+    const size_t up = ((size_t)(nel - 1) * ATKB_SMALL_N + nt) * sizeof(atkdsp_cf32);
+    p->lc -= (unsigned)np;               /* the device state holds lc - npend of the leftover */
+    p->npend = 0;
+    rc = run_step_up(p, nel, dins, nt, (atkdsp_cf32 *)p->d_out_stage, m, m, p->stream, &CONV_CF32, up);
     if (rc == ATKB_OK)
         rc = atkb_d2h(p->h_small_out, p->d_out_stage, out_n * sizeof(atkdsp_cf32), p->stream);
     if (rc == ATKB_OK) rc = atkb_stream_sync(p->stream);
@@ -820,6 +923,8 @@ static ptrdiff_t process_small(atkdsp_pfb *p, const atkdsp_cf32 *const *ins, uns
 }
 
 int atkb_pfb_order_after_small(atkdsp_pfb *p, void *stream) {
+    const int rc = atkb_pfb_flush_pending(p);
+    if (rc != ATKB_OK) return rc;
     if (!p->small_live) return ATKB_OK;
     if (!stream || stream == p->stream) return ATKB_OK;
     return atkb_stream_wait(stream, p->small_ev);
@@ -836,6 +941,7 @@ ATKDSP_API ptrdiff_t atkdsp_pfb_process_n(atkdsp_pfb *p, const atkdsp_cf32 *cons
     if (m > 0 && (!out || cap < (size_t)nel * p->nchan * m)) return ATKDSP_E_CAP;
     if (atkb_set_device(p->dev) != ATKB_OK) return ATKDSP_E_FFT;
     if (p->h_small_in && n <= ATKB_SMALL_N) return process_small(p, ins, nel, n, out, m);
+    if (p->npend && atkb_pfb_flush_pending(p) != ATKB_OK) return ATKDSP_E_FFT;
     if (p->small_live) {
         const int rs = atkb_event_sync(p->small_ev);
         if (rs != ATKB_OK) return map_rc(rs);
@@ -930,6 +1036,57 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_n_raw(atkdsp_pfb *p, const void *con
     if (atkb_set_device(p->dev) != ATKB_OK) return ATKDSP_E_FFT;
     if (atkb_pfb_order_after_small(p, stream) != ATKB_OK) return ATKDSP_E_FFT;
     const int rc = run_step(p, nel, d_raws, n, d_out, m, m, stream ? stream : p->stream, &cv);
+    return rc == ATKB_OK ? (ptrdiff_t)m : map_rc(rc);
+}
+
+/* ---- the filterbank with W1 / W2 fused into its epilogue (one element) ---- */
+static int w2_fusable(const atkdsp_pfb *p) {
+    return p->bank.plan.fast && p->nchan <= 2048;
+}
+
+ATKDSP_API size_t atkdsp_gpu_pfb_w12_scratch_bytes(const atkdsp_pfb *p, size_t n) {
+    if (!p) return 0;
+    const size_t m = ((size_t)p->lc + n) / p->hop;
+    const size_t th = (size_t)p->bank.tile_hops;
+    return w2_fusable(p) ? ((m + th - 1) / th) * p->nchan * sizeof(double) : 0;
+}
+
+ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_w12(atkdsp_pfb *p, const void *d_in, size_t n, int fmt,
+                                                float off_re, float off_im, atkdsp_cf32 *d_out, size_t cap,
+                                                const uint8_t *d_gate, atkdsp_cf32 *d_R, uint32_t *d_counts,
+                                                float *d_pwr, float *d_mean_pwr, void *d_scratch,
+                                                size_t scratch_bytes, void *stream) {
+    conv_t cv = CONV_CF32;
+    if (!p || (n && !d_in)) return ATKDSP_E_ARG;
+    if (fmt != ATKDSP_FMT_CF32 && !raw_conv(fmt, off_re, off_im, &cv)) return ATKDSP_E_ARG;
+    if (fmt == ATKDSP_FMT_CF32 && (off_re != 0.0f || off_im != 0.0f)) return ATKDSP_E_ARG;
+    if (n && ((size_t)d_in & (fmt == ATKDSP_FMT_CF32 ? 7 : 3))) return ATKDSP_E_ARG;
+    if ((d_R == NULL) != (d_counts == NULL)) return ATKDSP_E_ARG;
+    if ((size_t)p->lc + n >= ((size_t)1 << 62)) return ATKDSP_E_ARG;
+    const size_t m = ((size_t)p->lc + n) / p->hop;
+    if (m > 0 && (!d_out || cap < (size_t)p->nchan * m)) return ATKDSP_E_CAP;
+    if (m > (size_t)0x7fffffff / 4) return ATKDSP_E_ARG;
+    const int fused = w2_fusable(p);
+    const size_t need = atkdsp_gpu_pfb_w12_scratch_bytes(p, n);
+    if (fused && m > 0 && (!d_scratch || scratch_bytes < need || ((size_t)d_scratch & 7))) return ATKDSP_E_CAP;
+    if (atkb_set_device(p->dev) != ATKB_OK) return ATKDSP_E_FFT;
+    if (atkb_pfb_order_after_small(p, stream) != ATKB_OK) return ATKDSP_E_FFT;
+    void *st = stream ? stream : p->stream;
+    const void *ins[1];
+    ins[0] = d_in;
+    p->w2_next = (fused && m > 0) ? (double *)d_scratch : NULL;
+    int rc = run_step(p, 1, ins, n, d_out, m, m, st, &cv);
+    p->w2_next = NULL;
+    if (rc == ATKB_OK) {
+        if (fused) {
+            const size_t th = (size_t)p->bank.tile_hops;
+            rc = m > 0 ? atkb_w2_finish((const double *)d_scratch, (int)((m + th - 1) / th), (int)p->nchan,
+                                        (long long)m, d_gate, d_R, d_counts, d_pwr, d_mean_pwr, st)
+                       : atkb_w12(d_out, 1, p->nchan, 0, d_gate, d_R, d_counts, d_pwr, d_mean_pwr, st);
+        } else {
+            rc = atkb_w12(d_out, 1, p->nchan, m, d_gate, d_R, d_counts, d_pwr, d_mean_pwr, st);
+        }
+    }
     return rc == ATKB_OK ? (ptrdiff_t)m : map_rc(rc);
 }
 
@@ -1308,7 +1465,7 @@ ATKDSP_API atkdsp_gpu_batch *atkdsp_gpu_batch_create(atkdsp_pfb *const *handles,
     if (!handles || count < 1) return NULL;
     unsigned i;
     for (i = 0; i < count; ++i)
-        if (!handles[i] || handles[i]->dev != handles[0]->dev) return NULL;
+        if (!handles[i] || handles[i]->dev != handles[0]->dev || handles[i]->bank.plan.big) return NULL;
     atkdsp_gpu_batch *b = (atkdsp_gpu_batch *)calloc(1, sizeof *b);
     if (!b) return NULL;
     b->count = count;
@@ -1339,6 +1496,21 @@ ATKDSP_API atkdsp_gpu_batch *atkdsp_gpu_batch_create(atkdsp_pfb *const *handles,
 
 ATKDSP_API void *atkdsp_gpu_batch_stream(atkdsp_gpu_batch *b) { return b ? b->stream : NULL; }
 
+/* the fault bits of the batch's launches since the last query (cleared) */
+ATKDSP_API int atkdsp_gpu_batch_faults(atkdsp_gpu_batch *b) {
+    unsigned v = 0;
+    const unsigned z = 0;
+    if (!b) return ATKDSP_E_ARG;
+    if (atkb_set_device(b->dev) != ATKB_OK || atkb_stream_sync(b->stream) != ATKB_OK) return ATKDSP_E_FFT;
+    if (atkb_d2h(&v, b->d_counters + ATKB_FAULT_WORD, sizeof v, b->stream) != ATKB_OK ||
+        atkb_stream_sync(b->stream) != ATKB_OK)
+        return ATKDSP_E_FFT;
+    if (v && (atkb_h2d(b->d_counters + ATKB_FAULT_WORD, &z, sizeof z, b->stream) != ATKB_OK ||
+              atkb_stream_sync(b->stream) != ATKB_OK))
+        return ATKDSP_E_FFT;
+    return (int)(v | atkb_pfb_debug_fault());
+}
+
 ATKDSP_API float atkdsp_gpu_batch_kernel_ms(atkdsp_gpu_batch *b) {
     float ms = -1.0f;
     if (!b) return -1.0f;
@@ -1368,8 +1540,9 @@ static ptrdiff_t batch_process(atkdsp_gpu_batch *b, const void *const *d_ins, co
     int rc;
     unsigned i;
     if (b->ev_live[slot] && atkb_event_sync(b->ev[slot]) != ATKB_OK) return ATKDSP_E_FFT;
-    for (i = 0; i < b->count; ++i) {     /* a handle's pending small-call copy lands first */
+    for (i = 0; i < b->count; ++i) {     /* a handle's pending small-call samples land first */
         atkdsp_pfb *h = b->h[i];
+        if (h->npend && atkb_pfb_flush_pending(h) != ATKB_OK) return ATKDSP_E_FFT;
         if (h->small_live) {
             if (atkb_event_sync(h->small_ev) != ATKB_OK) return ATKDSP_E_FFT;
             h->small_live = 0;
@@ -1411,6 +1584,8 @@ static ptrdiff_t batch_process(atkdsp_gpu_batch *b, const void *const *d_ins, co
         C[i].head = (long long)head;
         C[i].from = (long long)(m * p->hop);
         C[i].len = (long long)(head + n - m * p->hop);
+        J[i].nsrc = C[i].nsrc = (long long)(head + n);
+        C[i].cap = (long long)p->cap_state;
         job_conv(&J[i], &C[i], &cv);
         total += (long long)m;
         if (tiles > 0x3fffffff) return ATKDSP_E_ARG;

@@ -24,6 +24,7 @@ atkdsp_pfb *atkb_pfb_create_served(double fs, unsigned nchan, unsigned oversampl
 /* order `stream` (NULL: the handle's) after the handle's pending small-call
  * copy, if any; the device-pointer and batch paths call it first */
 int atkb_pfb_order_after_small(atkdsp_pfb *p, void *stream);
+int atkb_pfb_flush_pending(atkdsp_pfb *p);
 
 /* a device bank shared by every handle with the same (device, nchan,
  * oversample, taps, attenuation): taps, tables and the device atkb_bank */
@@ -61,9 +62,21 @@ struct atkdsp_pfb {
                                        * carries a small call's tables and block */
     void *small_ev;
     int small_live;
+    /* blocks of small calls that completed no hop wait here, in pinned host
+     * memory, instead of costing a copy each: h_pend holds npend (< hop)
+     * samples per element for the pend_nel elements of those calls, the tail
+     * of the stream past the device state's head. They travel with the next
+     * call that produces hops, or are uploaded (atkb_pfb_flush_pending)
+     * before any other path reads the state. */
+    void *h_pend;
+    unsigned npend, pend_nel;
     size_t tbl_bytes;
     int *d_counters;
     int grid;
+    double *w2_next;              /* the next step's fused W2 partials (element
+                                   * 0), set only inside atkdsp_gpu_pfb_process_w12 */
+    void *d_big;                  /* large filterbanks: fold / FFT scratch, two
+                                   * double2 buffers of atkb_pfb_big_hops hops */
     const void **dins;            /* max_nel staging input pointers (host array,
                                    * filled per call; allocated at create) */
 };

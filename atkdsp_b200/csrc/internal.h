@@ -45,6 +45,8 @@ typedef struct {
     int quad;                     /* 1: quad fold (four hops per thread over two
                                    * branches), first radix 2; oversample 1 or
                                    * 2, nchan <= 1024 */
+    int big;                      /* 1: nchan beyond one CTA's shared memory:
+                                   * separate fold / pass / epilogue kernels */
     int ptaps;                    /* taps in the paired layout (pair, or the
                                    * nchan-4096 two-hop tile's paired fold) */
     int radix[ATKB_MAX_PASS];
@@ -92,6 +94,11 @@ typedef struct {
                                    * held as cre/cim = -(c * k), kscale = k (a
                                    * power of two): fma(float(v), k, cre) */
     int tiles;                    /* ceil(hops / bank->tile_hops)              */
+    long long nsrc;               /* samples of s = state ++ in there are (head
+                                   * + n): every window must end within them */
+    double *w2;                   /* device, or NULL: the fused W2 partials, one
+                                   * row of nchan doubles per tile of the job
+                                   * (power-of-two nchan <= 2048 banks only) */
 } atkb_job;
 
 /* ---- state carry: dst[0, len) = s[from, from + len) -------------------- */
@@ -104,7 +111,23 @@ typedef struct {
     long long len;
     int in_kind;                  /* as atkb_job: int16 input is converted   */
     float cre, cim, kscale;
+    long long nsrc;               /* samples of s there are (head + n)       */
+    long long cap;                /* capacity of dst in samples              */
 } atkb_carry;
+
+/* ---- the tile kernel's fault word (counters[ATKB_FAULT_WORD]) -------------
+ * Before touching a tile or a carry the kernel checks, uniformly across the
+ * CTA, that every window it will read ends within the job's nsrc samples,
+ * that its output columns lie within the row stride and that a carry fits its
+ * destination; a violation sets a bit here and the tile or carry is skipped
+ * (nothing is read or written for it), so the launch completes and the host
+ * reports ATKDSP_E_FFT. Built with ATKB_DEBUG_BOUNDS, every thread also checks
+ * each shared-memory and output index it computes. */
+#define ATKB_FAULT_WORD 3
+#define ATKB_FAULT_WINDOW 1u
+#define ATKB_FAULT_OUTPUT 2u
+#define ATKB_FAULT_CARRY  4u
+#define ATKB_FAULT_INDEX  8u
 
 /* device / memory ---------------------------------------------------------- */
 int  atkb_get_device(int *dev);
@@ -171,11 +194,30 @@ int  atkb_pfb_launch_n(const atkb_job *d_jobs, const int *d_tile_start, const at
                        int njobs_max, const int *d_njobs, int *d_counters, int grid, int smem_bytes,
                        void *stream);
 int  atkb_event_query(void *ev);        /* ATKB_OK when complete, 1 when pending */
+/* large filterbanks (plan.big: nchan beyond one CTA's shared memory): hops
+ * [h0, h0 + nh) of job J (a host copy; its pointers are device pointers)
+ * through fold, FFT-pass and epilogue kernels in `scratch`, 2 * nh * nchan
+ * double2 of device memory. At most atkb_pfb_big_hops(nchan) hops a call
+ * with the scratch the host sizes by it. The state carry is left to a
+ * tile-kernel launch with no tiles. */
+long long atkb_pfb_big_hops(int nchan);
+/* the debug build's per-thread index-check word (read and cleared), and
+ * whether this library is that build */
+unsigned atkb_pfb_debug_fault(void);
+int  atkb_pfb_debug_build(void);
+int  atkb_pfb_big(const atkb_job *J, const atkb_bank *B, long long h0, int nh, void *scratch, int grid,
+                  void *stream);
 
 /* W1 + W2 over a device [nel][nchan][m] block. R, counts, pwr, mean_pwr are
  * device pointers (any may be NULL to skip that output). */
 int  atkb_w12(const void *out, unsigned nel, unsigned nchan, size_t m, const uint8_t *gate,
               void *R, uint32_t *counts, float *pwr, float *mean_pwr, void *stream);
+/* the fused W2 partials (tiles rows of nchan doubles, tile order) of one
+ * single-element block of m hops: W2 power per channel and, for one
+ * element, W1 (R[k] += S, counts += m, gated) -- the same sums atkb_w12
+ * computes over the block's outputs */
+int  atkb_w2_finish(const double *part, int tiles, int nchan, long long m, const uint8_t *gate, void *R,
+                    uint32_t *counts, float *pwr, float *mean_pwr, void *stream);
 int  atkb_cov_reset(void *R, uint32_t *counts, unsigned nel, unsigned nchan,
                     const uint8_t *gate, void *stream);
 

@@ -145,6 +145,21 @@ __device__ __forceinline__ void dftR(double2 *v) {
     else if (R == 16) dft16(v);
 }
 
+/* Per-thread index checks of the debug build (ATKB_DEBUG_BOUNDS): an index
+ * outside its buffer sets a bit of g_atkb_debug_fault and the access is
+ * skipped; atkb_pfb_debug_fault reads and clears the word. In the normal
+ * build IDX_OK is constant true and costs nothing. */
+#ifdef ATKB_DEBUG_BOUNDS
+__device__ unsigned g_atkb_debug_fault;
+__device__ __forceinline__ bool idx_ok(bool ok) {
+    if (!ok) atomicOr(&g_atkb_debug_fault, ATKB_FAULT_INDEX);
+    return ok;
+}
+#define IDX_OK(c) idx_ok(c)
+#else
+#define IDX_OK(c) true
+#endif
+
 /* one element of the stream s = state[0, head) ++ in[0, ...) */
 /* int16 I/Q -> cf32 exactly as the unpack front end does, (float(v) - c) * k
  * with rounded operations (reference src/convert.c:64-73), in the fused form
@@ -456,7 +471,7 @@ __device__ __forceinline__ void stage_window(float2 *xs, const atkb_job &J, long
     for (int i = threadIdx.x; i < W; i += NT) {
         const long long g = g0 + i;
         const float2 *src = g < J.head ? st + g : in + (g - J.head);
-        cp_async8(xs + i + (i >> logs) * MR, src);
+        if (IDX_OK(i + (i >> logs) * MR < 8192 && g < J.nsrc)) cp_async8(xs + i + (i >> logs) * MR, src);
     }
     cp_async_wait_all();
     __syncthreads();
@@ -603,7 +618,8 @@ __device__ __forceinline__ void first_pass4(const float2 (&f)[4], double2 *sm, i
     for (int i = 0; i < 4; ++i) v[i] = make_double2((double)f[i].x, (double)f[i].y);
     dft4(v[0], v[1], v[2], v[3]);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) sm[SW((t << LOGM) + jp * 4 + i)] = v[i];
+    for (int i = 0; i < 4; ++i)
+        if (IDX_OK((t << LOGM) + jp * 4 + i < TILE_POINTS)) sm[SW((t << LOGM) + jp * 4 + i)] = v[i];
 }
 
 /* the paired fold of hops ta, ta + 1 (parity c, branch j) from global memory;
@@ -717,9 +733,33 @@ __device__ __forceinline__ void write_tile(const atkb_job &J, long long h0, int 
         const long long step = (long long)MP * J.ldo;
 #pragma unroll 4
         for (int u = 0; u < PTS; ++u) {
-            *o = tile_out[(kb0 + u * MP) * (NH + 1) + t2];
+            const int row = kb0 + u * MP;
+            if (IDX_OK(row < (1 << LOGM) && J.out_col + h0 + t2 < J.ldo &&
+                       row * (NH + 1) + t2 < TILE_POINTS * 2))
+                *o = tile_out[row * (NH + 1) + t2];
             o += step;
         }
+    }
+}
+
+/* W2 fused into the epilogue: the tile's power per channel, sum over its
+ * valid hops t of |y|^2 in double from the rounded outputs (the reference's
+ * W2 sum, src/channelizer.c:459-461, for these hops), written to the job's
+ * partial buffer at row h0 / tile_hops. A second kernel adds the tiles' rows
+ * in tile order (atkb_w2_finish). tile_out stays intact until the barrier
+ * that opens the next tile. */
+template <int LOGM>
+__device__ __forceinline__ void w2_partial(const atkb_job &J, long long h0, int nvalid, const float2 *tile_out) {
+    constexpr int M = 1 << LOGM;
+    constexpr int NH = 1 << (12 - LOGM);
+    double *row = J.w2 + (h0 / NH) * M;
+    for (int kb = threadIdx.x; kb < M; kb += NT) {
+        double s = 0.0;
+        for (int t = 0; t < nvalid; ++t) {
+            const float2 y = tile_out[kb * (NH + 1) + t];
+            s += (double)y.x * y.x + (double)y.y * y.y;
+        }
+        row[kb] = s;
     }
 }
 
@@ -827,8 +867,10 @@ template <int LOGM>
 __device__ __forceinline__ void first_pass2(float2 a, float2 b, double2 *sm, int t, int q0) {
     double2 x0 = make_double2((double)a.x, (double)a.y), x1 = make_double2((double)b.x, (double)b.y);
     dft2(x0, x1);
-    sm[SW((t << LOGM) + 2 * q0)] = x0;
-    sm[SW((t << LOGM) + 2 * q0 + 1)] = x1;
+    if (IDX_OK((t << LOGM) + 2 * q0 + 1 < TILE_POINTS)) {
+        sm[SW((t << LOGM) + 2 * q0)] = x0;
+        sm[SW((t << LOGM) + 2 * q0 + 1)] = x1;
+    }
 }
 
 template <int LOGM, int LOGOS>
@@ -889,6 +931,7 @@ __device__ void tile_quad(const atkb_job &J, const atkb_bank &B, long long h0, i
     group_sync<G>();
     fft_rest<LOGM, 1, 1, G>(sm, (const double2 *)B.wpass, B.plan.twoff, tile_out, B, J, h0);
     write_tile<LOGM>(J, h0, nvalid, tile_out);
+    if (J.w2) w2_partial<LOGM>(J, h0, nvalid, tile_out);
 }
 
 /* fold + first Stockham pass (Ns = 1, radix PTS, no twiddles) of one hop
@@ -1072,6 +1115,7 @@ __device__ void tile_fast(const atkb_job &J, const atkb_bank &B, long long h0, i
                                                    J, h0);
 
     write_tile<LOGM>(J, h0, nvalid, tile_out);
+    if (J.w2) w2_partial<LOGM>(J, h0, nvalid, tile_out);
 }
 
 /* ---- generic path: any nchan >= 2 ----------------------------------------- */
@@ -1247,6 +1291,17 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
          * skips the tile (its outputs stay unwritten) instead of running off
          * the end of shared memory */
         if ((unsigned)SB.smem_bytes > dyn_smem) key = -1;
+        /* bounds, uniform across the CTA: the tile's last window must end
+         * within the job's samples and its columns within the output rows */
+        {
+            unsigned bad = 0;
+            if ((h0 + nvalid - 1) * (long long)SB.hop + SB.L > J.nsrc || h0 + nvalid > J.hops) bad |= ATKB_FAULT_WINDOW;
+            if (J.out_col + h0 + nvalid > J.ldo) bad |= ATKB_FAULT_OUTPUT;
+            if (bad) {
+                if (threadIdx.x == 0) atomicOr((unsigned *)&counters[ATKB_FAULT_WORD], bad);
+                key = -1;
+            }
+        }
         float2 *to = (float2 *)sm;
         switch (key) {
 #define UNPAIRED(L) case L: tile_fast<L, -1>(J, SB, h0, nvalid, sm, to); break;
@@ -1289,6 +1344,10 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
         const Src src{(const float2 *)C.state, C.in, C.head, C.in_kind, C.cre, C.cim, C.kscale};
         float2 *dst = (float2 *)C.dst;
         const long long from = C.from, len = C.len;
+        if (from < 0 || len < 0 || from + len > C.nsrc || len > C.cap) {   /* uniform: skip it */
+            if (threadIdx.x == 0) atomicOr((unsigned *)&counters[ATKB_FAULT_WORD], ATKB_FAULT_CARRY);
+            continue;
+        }
         for (long long i = threadIdx.x; i < len; i += NT) dst[i] = src.at(from + i);
     }
     if (threadIdx.x == 0) {
@@ -1299,6 +1358,108 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
             atomicExch(&counters[2], 0);
             atomicExch(&counters[1], 0);
         }
+    }
+}
+
+/* ---- large filterbanks: nchan beyond one CTA's shared memory --------------
+ * A power of two above 4096 or any other nchan above 6400 has no in-CTA tile:
+ * a hop's M points (16 M bytes in double) do not fit beside a second buffer.
+ * Such a filterbank runs one hop chunk at a time through device scratch:
+ *   fold      one thread per (hop, branch), the reference's operation order
+ *             (a rounded multiply, then a rounded add, k ascending);
+ *   FFT       the plan's Stockham passes, each one kernel over the chunk,
+ *             ping-ponging between the two scratch halves (mixed radix 2, 3,
+ *             4, 8, 16, and a direct DFT for any other prime factor);
+ *   epilogue  rotation, cal and rounding as the tile kernel does them, written
+ *             channel-major (a warp's lanes on consecutive hops of a channel).
+ * Slower than the tile kernel (every pass goes through HBM), but any nchan
+ * the reference accepts runs, with the same results. */
+__global__ void __launch_bounds__(256)
+big_fold_kernel(const atkb_job J, const float *__restrict__ taps, int M, int K, int hop, long long h0, int nh,
+                double2 *__restrict__ F) {
+    const Src src{(const float2 *)J.state, J.in, J.head, J.in_kind, J.cre, J.cim, J.kscale};
+    const long long total = (long long)nh * M;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int t = (int)(e / M);
+        const int q = (int)(e - (long long)t * M);
+        const long long base = (h0 + t) * (long long)hop + q;
+        float h = __ldg(taps + q);
+        float2 x = src.at(base);
+        float fr = __fmul_rn(h, x.x), fi = __fmul_rn(h, x.y);
+        for (int k = 1; k < K; ++k) {
+            h = __ldg(taps + (long long)k * M + q);
+            x = src.at(base + (long long)k * M);
+            fr = __fadd_rn(fr, __fmul_rn(h, x.x));
+            fi = __fadd_rn(fi, __fmul_rn(h, x.y));
+        }
+        F[e] = make_double2((double)fr, (double)fi);
+    }
+}
+
+__global__ void __launch_bounds__(256)
+big_pass_kernel(const double2 *__restrict__ src, double2 *__restrict__ dst, int M, int Ns, int R, int nh,
+                const double2 *__restrict__ W) {
+    const int MR = M / R;
+    const int NsR = Ns * R;
+    const int stride = M / NsR;
+    const long long total = (long long)nh * MR;
+    for (long long bi = (long long)blockIdx.x * blockDim.x + threadIdx.x; bi < total;
+         bi += (long long)gridDim.x * blockDim.x) {
+        const int tt = (int)(bi / MR);
+        const int j = (int)(bi - (long long)tt * MR);
+        const int k = j % Ns;
+        const double2 *s = src + (long long)tt * M + j;
+        double2 *d = dst + (long long)tt * M + (long long)(j - k) * R + k;
+        if (R == 2 || R == 3 || R == 4 || R == 8 || R == 16) {
+            double2 v[16];
+            for (int r = 0; r < R; ++r) {
+                v[r] = s[(long long)r * MR];
+                if (r) v[r] = cmul(v[r], __ldg(W + (long long)r * k * stride));
+            }
+            if (R == 2) dft2(v[0], v[1]);
+            else if (R == 3) dft3(v[0], v[1], v[2]);
+            else if (R == 4) dft4(v[0], v[1], v[2], v[3]);
+            else if (R == 8) dft8(v);
+            else dft16(v);
+            for (int r = 0; r < R; ++r) d[(long long)r * Ns] = v[r];
+        } else {
+            /* direct DFT with the twiddle folded in: W_{NsR}^{r (k + o Ns)} */
+            for (int o = 0; o < R; ++o) {
+                double2 acc = make_double2(0.0, 0.0);
+                for (int r = 0; r < R; ++r) {
+                    const long long ex = ((long long)r * (k + (long long)o * Ns)) % NsR;
+                    const double2 w = __ldg(W + ex * stride);
+                    const double2 x = s[(long long)r * MR];
+                    acc.x += x.x * w.x - x.y * w.y;
+                    acc.y += x.x * w.y + x.y * w.x;
+                }
+                d[(long long)o * Ns] = acc;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256)
+big_out_kernel(const double2 *__restrict__ X, const atkb_job J, const double2 *__restrict__ twd, int M, int os,
+               int hop, long long h0, int nh) {
+    const float2 *cal = (const float2 *)J.cal;
+    float2 *out = (float2 *)J.out;
+    const long long total = (long long)nh * M;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int kb = (int)(e / nh);
+        const int tt = (int)(e - (long long)kb * nh);
+        double2 v = X[(long long)tt * M + kb];
+        const long long b = J.b0 + h0 + tt;
+        const int s = (int)((b + 1) % os);
+        const int jr = (int)(((long long)kb * s) % os);
+        v = cmul_rn(v, __ldg(twd + (jr ? M - jr * hop : 0)));
+        if (cal) {
+            const float2 c = __ldg(cal + kb);
+            v = cmul_rn(v, make_double2((double)c.x, (double)c.y));
+        }
+        out[(long long)kb * J.ldo + J.out_col + h0 + tt] = make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
     }
 }
 
@@ -1338,5 +1499,82 @@ extern "C" int atkb_pfb_launch_n(const atkb_job *d_jobs, const int *d_tile_start
     pfb_tiles_kernel<<<grid, NT, smem_bytes, (cudaStream_t)stream>>>(d_jobs, d_tile_start, d_carry, njobs,
                                                                     d_njobs, d_counters);
     atkb_range_pop();
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
+extern "C" long long atkb_pfb_big_hops(int nchan) {
+    const long long h = (1LL << 20) / nchan;
+    return h < 1 ? 1 : h;
+}
+
+extern "C" int atkb_pfb_big(const atkb_job *J, const atkb_bank *B, long long h0, int nh, void *scratch,
+                            int grid, void *stream) {
+    if (nh <= 0) return ATKB_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int M = B->nchan;
+    double2 *A = (double2 *)scratch, *Bf = A + (size_t)nh * M;
+    if (grid < 1) grid = 1;
+    atkb_range_push("atkdsp large-filterbank chunk");
+    big_fold_kernel<<<grid, 256, 0, st>>>(*J, B->taps, M, B->K, B->hop, h0, nh, A);
+    int Ns = 1;
+    double2 *cur = A, *nxt = Bf;
+    for (int p = 0; p < B->plan.npass; ++p) {
+        const int R = B->plan.radix[p];
+        big_pass_kernel<<<grid, 256, 0, st>>>(cur, nxt, M, Ns, R, nh, (const double2 *)B->wfull);
+        Ns *= R;
+        double2 *t = cur; cur = nxt; nxt = t;
+    }
+    big_out_kernel<<<grid, 256, 0, st>>>(cur, *J, (const double2 *)B->twd, M, B->os, B->hop, h0, nh);
+    atkb_range_pop();
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
+extern "C" unsigned atkb_pfb_debug_fault(void) {
+#ifdef ATKB_DEBUG_BOUNDS
+    unsigned v = 0, z = 0;
+    if (cudaMemcpyFromSymbol(&v, g_atkb_debug_fault, sizeof v) != cudaSuccess) return ATKB_FAULT_INDEX;
+    if (v) cudaMemcpyToSymbol(g_atkb_debug_fault, &z, sizeof z);
+    return v;
+#else
+    return 0;
+#endif
+}
+
+extern "C" int atkb_pfb_debug_build(void) {
+#ifdef ATKB_DEBUG_BOUNDS
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+namespace {
+/* the tiles' W2 partials of one single-element job, per channel added in tile
+ * order: W2 power (S / m), and W1 for one element (R[k] += S, counts += m),
+ * gated like atkb_w12 */
+__global__ void w2_finish_kernel(const double *__restrict__ part, int tiles, int M, long long m,
+                                 const uint8_t *__restrict__ gate, float2 *__restrict__ R,
+                                 uint32_t *__restrict__ counts, float *__restrict__ pwr, float *__restrict__ mean_pwr) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= M) return;
+    double S = 0.0;
+    for (int t = 0; t < tiles; ++t) S += part[(long long)t * M + k];
+    const double inv = m ? 1.0 / (double)m : 0.0;
+    if (pwr) pwr[k] = (float)(S * inv);
+    if (mean_pwr) mean_pwr[k] = (float)((S * inv) / 1.0);
+    if (R && counts && (!gate || gate[k])) {
+        if (m > 0) {
+            const float2 v = R[k];
+            R[k] = make_float2((float)((double)v.x + S), (float)((double)v.y + 0.0));
+        }
+        counts[k] += (uint32_t)m;
+    }
+}
+}  // namespace
+
+extern "C" int atkb_w2_finish(const double *part, int tiles, int nchan, long long m, const uint8_t *gate, void *R,
+                              uint32_t *counts, float *pwr, float *mean_pwr, void *stream) {
+    w2_finish_kernel<<<(nchan + 255) / 256, 256, 0, (cudaStream_t)stream>>>(part, tiles, nchan, m, gate, (float2 *)R,
+                                                                          counts, pwr, mean_pwr);
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }

@@ -50,7 +50,8 @@ typedef struct {
 } sstream;
 
 typedef struct {
-    void *ev;
+    void *ev;                     /* the round's end (timed) */
+    void *ev0;                    /* the round's start on the stream (timed) */
     int nrec;
     atkdsp_server_done *rec;
 } round_t;
@@ -80,6 +81,8 @@ struct atkdsp_server {
     atkdsp_pfb **parked;
     unsigned nparked;
     void *pool;                   /* stream-ordered pool for the streams' state */
+    double gpu_ms;                /* device time of the completed rounds */
+    uint64_t gpu_rounds;
 };
 
 static double now_s(void) {
@@ -104,6 +107,7 @@ ATKDSP_API void atkdsp_server_destroy(atkdsp_server *s) {
     atkb_pool_destroy(s->pool);
     for (r = 0; r < NROUNDS; ++r) {
         atkb_event_destroy(s->rounds[r].ev);
+        atkb_event_destroy(s->rounds[r].ev0);
         free(s->rounds[r].rec);
     }
     for (r = 0; r < 2; ++r) {
@@ -139,7 +143,8 @@ ATKDSP_API atkdsp_server *atkdsp_server_create(unsigned max_streams, size_t hbm_
         if (rc == ATKB_OK) rc = atkb_event_create(&s->tbl_ev[r]);
     }
     for (r = 0; r < NROUNDS && rc == ATKB_OK; ++r) {
-        rc = atkb_event_create(&s->rounds[r].ev);
+        rc = atkb_event_create_timed(&s->rounds[r].ev);
+        if (rc == ATKB_OK) rc = atkb_event_create_timed(&s->rounds[r].ev0);
         s->rounds[r].rec = (atkdsp_server_done *)malloc(max_streams * sizeof(atkdsp_server_done));
         if (rc == ATKB_OK && !s->rounds[r].rec) rc = ATKB_E_NOMEM;
     }
@@ -325,6 +330,8 @@ ATKDSP_API int atkdsp_server_launch(atkdsp_server *s) {
         C[n].head = (long long)head;
         C[n].from = (long long)(m * p->hop);
         C[n].len = (long long)(head + b->n - m * p->hop);
+        J[n].nsrc = C[n].nsrc = (long long)(head + b->n);
+        C[n].cap = (long long)p->cap_state;
         atkb_job_conv(&J[n], &C[n], &t->cv);
         R->rec[n].id = (int)i;
         R->rec[n].tag = b->tag;
@@ -338,6 +345,8 @@ ATKDSP_API int atkdsp_server_launch(atkdsp_server *s) {
     if (tiles > 0x3fffffff) return ATKDSP_E_ARG;
     T[n] = (int)tiles;
     *tbl_count(base, s->cap) = n;
+    rc = atkb_event_record(R->ev0, s->stream);
+    if (rc != ATKB_OK) return atkb_map_rc(rc);
     if (s->use_graph) {
         if (!s->graph[slot]) {
             rc = atkb_graph_begin(s->stream);
@@ -399,6 +408,13 @@ ATKDSP_API int atkdsp_server_poll(atkdsp_server *s, atkdsp_server_done *done, in
             if (--st->inflight == 0 && st->state == 2) stream_free(s, (unsigned)d->id);
         }
         s->stats.blocks_done += (uint64_t)R->nrec;
+        {
+            float ms = 0.0f;
+            if (atkb_event_elapsed_ms(&ms, R->ev0, R->ev) == ATKB_OK) {
+                s->gpu_ms += ms;
+                ++s->gpu_rounds;
+            }
+        }
         s->r_head = (s->r_head + 1) % NROUNDS;
         --s->r_len;
         wait = 0;
@@ -490,6 +506,10 @@ ATKDSP_API int atkdsp_server_simulate(atkdsp_server *s, const atkdsp_sim_config 
     int rc = ATKDSP_OK;
     size_t nlat = 0, out_used = 0;
     unsigned i;
+    double launch_ms = 0.0;
+    uint64_t launches = 0;
+    s->gpu_ms = 0.0;
+    s->gpu_rounds = 0;
     if (!rate || !nch || !blk || !sid || !ooff || !ocap || !heap || !lat || !done) { rc = ATKDSP_E_NOMEM; goto out; }
     for (i = 0; i < ns; ++i) {
         rate[i] = cfg->rates[rng_next(&seed) % (uint64_t)cfg->nrates];
@@ -563,6 +583,10 @@ ATKDSP_API int atkdsp_server_simulate(atkdsp_server *s, const atkdsp_sim_config 
                 if (got < 0) { rc = got; goto out; }
                 const double dl = (now_s() - l0) * 1e3;
                 if (dl > res->max_launch_ms) res->max_launch_ms = dl;
+                if (got > 0) {
+                    launch_ms += dl;
+                    ++launches;
+                }
             }
             const double p0 = now_s();
             const int nd = atkdsp_server_poll(s, done, dcap, 0);
@@ -594,6 +618,9 @@ ATKDSP_API int atkdsp_server_simulate(atkdsp_server *s, const atkdsp_sim_config 
         atkdsp_server_get_stats(s, &st);
         res->rounds = st.rounds;
         res->blocks_per_round = st.rounds ? (double)st.blocks_launched / (double)st.rounds : 0.0;
+        res->mean_launch_ms = launches ? launch_ms / (double)launches : 0.0;
+        res->mean_round_gpu_ms = s->gpu_rounds ? s->gpu_ms / (double)s->gpu_rounds : 0.0;
+        res->gpu_busy = res->wall_s > 0 ? s->gpu_ms / 1e3 / (res->wall_s + cfg->warmup_s) : 0.0;
     }
     for (i = 0; i < ns; ++i)
         if (sid[i] >= 0) atkdsp_server_close(s, sid[i]);

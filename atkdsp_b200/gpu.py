@@ -15,7 +15,7 @@ import torch
 
 from . import AtkDspError, Cfar, Pfb, _cfar_event_dict, _check, _fmt, bytes_per_sample, load
 
-__all__ = ["Spectrum", "cfar_process", "process_n", "process_n_raw", "unpack_dc", "unpack", "block_mean", "accumulate",
+__all__ = ["Spectrum", "cfar_process", "process_n", "process_n_raw", "process_w12", "unpack_dc", "unpack", "block_mean", "accumulate",
            "cov_accumulate", "channel_power", "Batch", "sync"]
 
 
@@ -74,6 +74,30 @@ def process_n_raw(p: Pfb, raws, nel: int, fmt, offset: complex = 0j,
                                            float(offset.imag), _ptr(out), out.numel(), _stream(stream))
     _check(int(got), "gpu_pfb_process_n_raw")
     return out[: nel * p.nchan * got].view(nel, p.nchan, got)
+
+
+def process_w12(p: Pfb, x: torch.Tensor, fmt="cf32", offset: complex = 0j, out: torch.Tensor | None = None,
+                R: torch.Tensor | None = None, counts: torch.Tensor | None = None,
+                pwr: torch.Tensor | None = None, mean_pwr: torch.Tensor | None = None,
+                gate: torch.Tensor | None = None, scratch: torch.Tensor | None = None,
+                stream=None) -> torch.Tensor:
+    """atkdsp_gpu_pfb_process_w12: one element's block through the filterbank
+    with W1 / W2 fused into its epilogue. x: complex64 samples (fmt "cf32") or
+    int16 I/Q pairs (fmt "ci16" / "ci16q11"). Returns (1, nchan, m)."""
+    lib = load()
+    n = int(x.numel()) if x.dtype == torch.complex64 else int(x.numel()) // 2
+    m = p.out_hops(n)
+    if out is None:
+        out = torch.empty(p.nchan * max(m, 1), dtype=torch.complex64, device=x.device)
+    need = int(lib.atkdsp_gpu_pfb_w12_scratch_bytes(p.handle, n))
+    if scratch is None or scratch.numel() * scratch.element_size() < need:
+        scratch = torch.empty(max(need, 8), dtype=torch.uint8, device=x.device)
+    got = lib.atkdsp_gpu_pfb_process_w12(p.handle, _ptr(x), n, _fmt(fmt), float(offset.real), float(offset.imag),
+                                         _ptr(out), out.numel(), _ptr(gate), _ptr(R), _ptr(counts), _ptr(pwr),
+                                         _ptr(mean_pwr), _ptr(scratch), scratch.numel() * scratch.element_size(),
+                                         _stream(stream))
+    _check(int(got), "gpu_pfb_process_w12")
+    return out[: p.nchan * got].view(1, p.nchan, got)
 
 
 def unpack_dc(raw: torch.Tensor, fmt, offset: complex = 0j, out: torch.Tensor | None = None,

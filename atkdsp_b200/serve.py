@@ -45,7 +45,8 @@ class SimResult(C.Structure):
                 ("wall_s", C.c_double), ("lat_p50_ms", C.c_double), ("lat_p90_ms", C.c_double),
                 ("lat_p99_ms", C.c_double), ("lat_max_ms", C.c_double), ("max_open_ms", C.c_double),
                 ("max_close_ms", C.c_double), ("max_launch_ms", C.c_double), ("max_poll_ms", C.c_double),
-                ("max_loop_ms", C.c_double)]
+                ("max_loop_ms", C.c_double), ("mean_launch_ms", C.c_double), ("mean_round_gpu_ms", C.c_double),
+                ("gpu_busy", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

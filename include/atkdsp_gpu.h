@@ -73,6 +73,28 @@ ATKDSP_API ptrdiff_t   atkdsp_gpu_unpack_dc_noalloc(const void *d_raw, size_t nb
                                                     atkdsp_cf32 *d_out, size_t out_cap,
                                                     float off_re, float off_im, double *d_mean,
                                                     void *stream);
+/* One element's block through the filterbank with W2 (per-channel power)
+ * and W1 (per-channel covariance, one element: the power sum) fused into the
+ * filterbank's epilogue (no reference counterpart as one call: it is
+ * atkdsp_pfb_process, then atkdsp_pfb_cov_accumulate and
+ * atkdsp_pfb_channel_power of reference include/atkdsp.h:3209, 3239, 3248 on
+ * the block's output). Each tile of the filterbank adds up its channels'
+ * power in double as it writes them; a small second kernel adds the tiles in
+ * order, so the block's outputs are not read again. d_in: n cf32 samples
+ * (fmt ATKDSP_FMT_CF32, zero offset) or int16 I/Q (ATKDSP_FMT_CI16 /
+ * CI16Q11, converted with the offset as atkdsp_gpu_pfb_process_n_raw does).
+ * d_R / d_counts (W1) and d_pwr / d_mean_pwr (W2) may each be NULL, d_gate
+ * gates W1 as in atkdsp_pfb_cov_accumulate. d_scratch: device memory of at
+ * least atkdsp_gpu_pfb_w12_scratch_bytes(p, n) bytes (0 where the filterbank
+ * does not fuse -- nchan 4096 or not a power of two -- and W1/W2 run as a
+ * separate pass instead). Returns m, ATKDSP_E_CAP for too small a d_out or
+ * scratch, ATKDSP_E_ARG. */
+ATKDSP_API size_t      atkdsp_gpu_pfb_w12_scratch_bytes(const atkdsp_pfb *p, size_t n);
+ATKDSP_API ptrdiff_t   atkdsp_gpu_pfb_process_w12(atkdsp_pfb *p, const void *d_in, size_t n, int fmt,
+                                                  float off_re, float off_im, atkdsp_cf32 *d_out,
+                                                  size_t cap, const uint8_t *d_gate, atkdsp_cf32 *d_R,
+                                                  uint32_t *d_counts, float *d_pwr, float *d_mean_pwr,
+                                                  void *d_scratch, size_t scratch_bytes, void *stream);
 /* The mean that atkdsp_unpack_dc (reference include/atkdsp.h:270) returns --
  * of the samples before the offset (off_re, off_im) is taken out -- without
  * writing the samples: for a caller whose filterbank reads the raw samples
@@ -115,7 +137,7 @@ ATKDSP_API int         atkdsp_gpu_pfb_channel_power(const atkdsp_cf32 *d_out, un
  * Filterbanks take the choice for their (nchan, oversample, taps/branch) from
  * the table compiled into the library (written by `python -m
  * atkdsp_b200.autotune --write` from measurements on the device), else the
- * quad fold where it exists and the paired fold elsewhere.
+ * paired fold.
  * atkdsp_gpu_tune_set overrides it for filterbanks created afterwards in this
  * process (choice 1: paired, 0: one hop per thread, 2: quad, -1: back to the
  * table); ATKDSP_E_ARG for a shape without that choice.
@@ -137,6 +159,26 @@ ATKDSP_API int         atkdsp_gpu_tune_get(unsigned nchan, unsigned oversample,
  * No kernel is involved and no device fault is raised. */
 ATKDSP_API void        atkdsp_gpu_fail_alloc_after(long long n);
 
+/* ---- bounds checks (no reference counterpart) ----------------------------
+ * The tile kernel checks, before it touches a tile or a state carry, that
+ * every window it reads ends within the samples the job has and that its
+ * outputs and the carry fit their buffers; a violation sets a fault bit and
+ * the tile or carry is skipped -- nothing out of bounds is read or written,
+ * and the launch completes. atkdsp_gpu_pfb_faults returns the bits the
+ * handle's launches set since the last call (atkdsp_gpu_batch_faults, below,
+ * those of a batch's launches) (1 window, 2 output, 4 carry,
+ * 8 an index caught by the debug build's per-thread checks; 0: none) and
+ * clears them. The library built with ATKB_DEBUG_BOUNDS
+ * (lib/libatkdsp_b200_debug.so, `make -C atkdsp_b200 debug`) also checks each
+ * shared-memory and output index per thread; atkdsp_gpu_debug_build returns
+ * 1 in that build. atkdsp_gpu_inject_short_window(n) is a test hook: the next
+ * filterbank step's jobs claim n fewer samples than they hold (the buffers
+ * hold them all, so even a missed check could read nothing out of bounds),
+ * which the window check must report. */
+ATKDSP_API int         atkdsp_gpu_pfb_faults(atkdsp_pfb *p);
+ATKDSP_API int         atkdsp_gpu_debug_build(void);
+ATKDSP_API void        atkdsp_gpu_inject_short_window(long long n);
+
 /* ---- batches: many independent handles in one persistent launch --------
  * A batch groups handles (each single-element, any nchan / taps / oversample)
  * so that one call channelizes one new block of every handle with a single
@@ -147,6 +189,9 @@ ATKDSP_API void        atkdsp_gpu_fail_alloc_after(long long n);
 typedef struct atkdsp_gpu_batch atkdsp_gpu_batch;
 ATKDSP_API atkdsp_gpu_batch *atkdsp_gpu_batch_create(atkdsp_pfb *const *handles, unsigned count,
                                                      int use_graph);
+/* the fault bits of the batch's launches since the last call, cleared (as
+ * atkdsp_gpu_pfb_faults) */
+ATKDSP_API int         atkdsp_gpu_batch_faults(atkdsp_gpu_batch *b);
 ATKDSP_API void        atkdsp_gpu_batch_destroy(atkdsp_gpu_batch *b);
 /* d_ins[i]: ns[i] new samples of handle i (device); d_outs[i]: its
  * [nchan][m_i] output (device), at least nchan * out_hops(handle i, ns[i])

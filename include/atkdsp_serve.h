@@ -96,6 +96,11 @@ typedef struct {
     /* the longest single host call of each kind during the run, and the
      * longest pass of the driver loop (where a stall on the host shows) */
     double max_open_ms, max_close_ms, max_launch_ms, max_poll_ms, max_loop_ms;
+    /* where a round's time goes: the host's launch call (tables for every
+     * pending block, graph replay) and the round's device time (its events on
+     * the server's stream, table upload + tile kernel + carries), both
+     * averaged over rounds; gpu_busy: device time / run time */
+    double mean_launch_ms, mean_round_gpu_ms, gpu_busy;
 } atkdsp_sim_result;
 
 ATKDSP_API int           atkdsp_server_simulate(atkdsp_server *s, const atkdsp_sim_config *cfg,

@@ -251,3 +251,59 @@ def test_nan_samples_keep_their_meaning(ref, M, os_, K):
     ak.pfb_cov_accumulate(y, 1, M, None, R, c)
     ref.pfb_cov_accumulate(r, 1, M, None, Rr, cr)
     assert np.array_equal(np.isnan(R), np.isnan(Rr)) and np.array_equal(c, cr)
+
+
+@pytest.mark.parametrize("M,os_,K,nel", [(8192, 2, 8, 1), (16384, 1, 4, 1), (6401, 1, 3, 2), (7919, 1, 2, 1),
+                                         (12000, 3, 4, 1)])
+def test_large_filterbanks_match_the_reference(ref, M, os_, K, nel):
+    """nchan beyond one CTA's shared memory (a power of two above 4096, any
+    other value above 6400, primes included) runs through the separate fold,
+    FFT-pass and epilogue kernels: the reference accepts these, and so does
+    this library, with the same parity bar and streaming continuity."""
+    rng = np.random.default_rng(M + K)
+    n = M * K + 9 * (M // os_) + 17
+    xs = [W.tones_noise(n, 2, 20.0, rng) for _ in range(nel)]
+    blocks = [n // 3, 1, 999, n]
+    y = run_blocks(ak.Pfb(FS, M, os_, K, 80.0, nel), xs, blocks)
+    r = run_blocks(ref.Pfb(FS, M, os_, K, 80.0, nel), xs, blocks)
+    assert y.shape[-1] >= 8
+    _parity(y, r, (M, os_, K))
+
+
+def test_wide_arrays_match_the_reference(ref):
+    """More than 32 elements (the reference has no limit): the filterbank and
+    W1 / W2 (the wide-array kernel) against the reference."""
+    nel, M = 40, 64
+    rng = np.random.default_rng(40)
+    xs = [W.tones_noise(64 * 50 + 5, 1, 15.0, rng) for _ in range(nel)]
+    y = np.asarray(ak.Pfb(FS, M, 2, 8, 80.0, nel).process_n(xs, nel))
+    r = np.asarray(ref.Pfb(FS, M, 2, 8, 80.0, nel).process_n(xs, nel))
+    _parity(y, r, "wide array")
+    R, c = np.zeros((M, nel, nel), np.complex64), np.zeros(M, np.uint32)
+    Rr, cr = np.zeros((M, nel, nel), np.complex64), np.zeros(M, np.uint32)
+    ak.pfb_cov_accumulate(y, nel, M, None, R, c)
+    ref.pfb_cov_accumulate(r, nel, M, None, Rr, cr)
+    assert np.array_equal(c, cr)
+    _w1_holds(R, Rr, _w1_exact([y]), "wide array")
+    pw, mp = ak.pfb_channel_power(y, nel, M)
+    pwr, mpr = ref.pfb_channel_power(r, nel, M)
+    assert np.max(np.abs(pw - pwr) / pwr) <= TOL and np.max(np.abs(mp - mpr) / mpr) <= TOL
+
+
+def test_small_calls_then_the_device_api():
+    """Blocks that complete no hop wait on the host until the next call that
+    produces hops; any other path (the device API here, a batch) first moves
+    them into the device state: the result equals one unbroken call."""
+    from atkdsp_b200 import gpu
+    rng = np.random.default_rng(5)
+    x = W.tones_noise(256 * 40 + 3, 2, 20.0, rng)
+    whole = np.asarray(ak.Pfb(FS, 256, 2, 12).process(x))
+    p = ak.Pfb(FS, 256, 2, 12)
+    parts = [np.asarray(p.process(x[:5])), np.asarray(p.process(x[5:40]))]      # no hops yet
+    d = torch.from_numpy(x[40:]).cuda()
+    torch.cuda.synchronize()
+    y = gpu.process_n(p, [d], 1)
+    gpu.sync(p)
+    parts.append(y[0].cpu().numpy())
+    got = np.concatenate([a for a in parts if a.shape[-1]], axis=-1)
+    assert np.array_equal(got, whole)

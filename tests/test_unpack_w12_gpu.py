@@ -253,3 +253,47 @@ def test_host_w1_w2_and_unpack_from_two_threads_at_once():
                 assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), i
             else:
                 assert a == b, i
+
+
+@pytest.mark.parametrize("M,os_,K,fmt", [(1024, 2, 12, "cf32"), (1024, 2, 12, "ci16q11"), (256, 2, 16, "ci16"),
+                                         (64, 1, 8, "cf32"), (4096, 2, 8, "cf32"), (192, 2, 6, "cf32")])
+def test_fused_w12_equals_the_separate_pass(M, os_, K, fmt):
+    """atkdsp_gpu_pfb_process_w12 (W2 power sums taken in the filterbank's
+    epilogue, tile by tile, then added in tile order) against the filterbank
+    followed by the separate W1/W2 pass: the same outputs bit for bit, the
+    same counts, and W1 / W2 within a few float roundings (only the order of
+    the double additions differs); across three blocks, gated W1. Shapes the
+    epilogue does not fuse (nchan 4096, not a power of two) take the separate
+    pass inside the same call."""
+    import torch
+    from atkdsp_b200 import gpu
+    rng = np.random.default_rng(M + K)
+    p1, p2 = ak.Pfb(2.4e6, M, os_, K), ak.Pfb(2.4e6, M, os_, K)
+    s1 = torch.cuda.ExternalStream(ak.load().atkdsp_gpu_pfb_stream(p1.handle))
+    s2 = torch.cuda.ExternalStream(ak.load().atkdsp_gpu_pfb_stream(p2.handle))
+    gate = torch.from_numpy((rng.random(M) < 0.7).astype(np.uint8)).cuda()
+    R1 = torch.zeros((M, 1, 1), dtype=torch.complex64, device="cuda"); R2 = R1.clone()
+    c1 = torch.zeros(M, dtype=torch.int32, device="cuda"); c2 = c1.clone()
+    w1 = torch.zeros((1, M), dtype=torch.float32, device="cuda"); w2 = w1.clone()
+    m1 = torch.zeros(M, dtype=torch.float32, device="cuda"); m2 = m1.clone()
+    off = 0.0123 - 0.0456j if fmt != "cf32" else 0j
+    for b in range(3):
+        n = int(rng.integers(M * K, M * K + 50 * M))
+        if fmt == "cf32":
+            x = torch.from_numpy(((rng.standard_normal(n) + 1j * rng.standard_normal(n)) * 3).astype(np.complex64)).cuda()
+        else:
+            x = torch.from_numpy(rng.integers(-2000, 2000, 2 * n, dtype=np.int64).astype("<i2")).cuda()
+        torch.cuda.synchronize()
+        y1 = gpu.process_w12(p1, x, fmt, off, R=R1, counts=c1, pwr=w1, mean_pwr=m1, gate=gate, stream=s1)
+        y2 = gpu.process_n(p2, [x], 1, stream=s2) if fmt == "cf32" else \
+            gpu.process_n_raw(p2, [x], 1, fmt, off, stream=s2)
+        gpu.accumulate(y2, 1, M, R2, c2, w2, m2, gate=gate, stream=s2)
+        torch.cuda.synchronize()
+        assert np.array_equal(y1.cpu().numpy(), y2.cpu().numpy()), b
+        a, r = w1.cpu().numpy(), w2.cpu().numpy()
+        assert np.max(np.abs(a - r) / np.maximum(r, 1e-30)) <= 1e-6, b
+        assert np.max(np.abs(m1.cpu().numpy() - m2.cpu().numpy()) / np.maximum(m2.cpu().numpy(), 1e-30)) <= 1e-6
+    assert np.array_equal(c1.cpu().numpy(), c2.cpu().numpy())
+    Ra, Rb = R1.cpu().numpy().reshape(-1), R2.cpu().numpy().reshape(-1)
+    assert np.max(np.abs(Ra - Rb) / np.maximum(np.abs(Rb), 1e-30)) <= 1e-6
+    assert np.all(Ra[gate.cpu().numpy() == 0] == 0)
