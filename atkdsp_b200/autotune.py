@@ -7,13 +7,16 @@ For every power-of-two nchan (16..2048), oversample (1, 2, 4) and
 taps/branch in the grid, the kernel has two or three tile shapes
 (include/atkdsp_gpu.h, atkdsp_gpu_tune_set): the paired fold (two hops per
 thread), one hop per thread, and -- at oversample 1 or 2 with nchan <= 1024 --
-the quad fold (four hops per thread). Each is timed on one stream of 2^log2n
+the quad fold (four hops per thread); at nchan <= 512 the paired and
+one-hop shapes also run with the tile window read through L1 instead of
+staged in shared memory. Each is timed on one stream of 2^log2n
 cf32 samples through the batched kernel (atkdsp_b200.microbench.run_one, the
 kernel's own CUDA events, median of the repetitions), and the fastest goes
 into the table the library compiles in (the paired fold unless another is
 faster by the margin). A shape not in the grid takes the paired fold. Every
 shape meets the same parity bar; only speed differs. One JSON line per shape:
-{"nchan", "oversample", "taps", "paired_gsps", "single_gsps", "quad_gsps", "pair"}.
+{"nchan", "oversample", "taps", "paired_gsps", "single_gsps", "quad_gsps",
+"paired_unstaged_gsps", "single_unstaged_gsps", "pair"} ("pair": the chosen code).
 """
 
 from __future__ import annotations
@@ -42,10 +45,10 @@ def tune(nchans=NCHANS, oversamples=OVERSAMPLES, taps=TAPS, log2n: int = 22, rep
                 continue
             for K in taps:
                 r = {}
-                for choice in (1, 0, 2):
+                for choice in (1, 0, 2, 5, 4):
                     if lib.atkdsp_gpu_tune_set(M, os_, K, choice) != 0:
-                        if choice == 2:
-                            continue                     # no quad fold for this shape
+                        if choice > 1:
+                            continue                     # not offered for this shape
                         raise RuntimeError(f"no tile-shape choice for nchan {M} os {os_}")
                     r[choice] = run_one(M, K, os_, log2n, reps)["gsps"]
                 lib.atkdsp_gpu_tune_set(M, os_, K, -1)
@@ -53,7 +56,8 @@ def tune(nchans=NCHANS, oversamples=OVERSAMPLES, taps=TAPS, log2n: int = 22, rep
                 best = max(r, key=lambda c: r[c])
                 pair = best if r[best] > r[1] * (1.0 + margin) else 1
                 row = {"nchan": M, "oversample": os_, "taps": K, "paired_gsps": r[1],
-                       "single_gsps": r[0], "quad_gsps": r.get(2), "pair": pair}
+                       "single_gsps": r[0], "quad_gsps": r.get(2), "paired_unstaged_gsps": r.get(5),
+                       "single_unstaged_gsps": r.get(4), "pair": pair}
                 print(json.dumps(row), flush=True)
                 rows.append(row)
     return rows
@@ -61,14 +65,16 @@ def tune(nchans=NCHANS, oversamples=OVERSAMPLES, taps=TAPS, log2n: int = 22, rep
 
 def write_table(rows, path: Path = TABLE) -> None:
     lines = ["/* Tile-shape table: 1 = paired fold, 0 = one hop and 8 branches per thread,",
-             " * 2 = quad fold (four hops per thread), per (nchan, oversample,",
-             " * taps/branch). Written by",
+             " * 2 = quad fold (four hops per thread), +4 = tile window read through L1",
+             " * rather than staged, per (nchan, oversample, taps/branch). Written by",
              " *   python -m atkdsp_b200.autotune --write",
-             " * from device measurements (GS/s paired / one hop per thread / quad in",
-             " * each comment); shapes not listed take the paired fold. */",
+             " * from device measurements (GS/s paired / one hop per thread / quad /",
+             " * paired unstaged / one hop unstaged in each comment); shapes not listed",
+             " * take the paired fold. */",
              "static const tune_entry k_tune_table[] = {"]
     for r in rows:
-        q = f" / {r['quad_gsps']:.2f}" if r.get("quad_gsps") is not None else ""
+        q = "".join(f" / {r[k]:.2f}" if r.get(k) is not None else " / -"
+                    for k in ("quad_gsps", "paired_unstaged_gsps", "single_unstaged_gsps"))
         lines.append(f"    {{{r['nchan']}, {r['oversample']}, {r['taps']}, {r['pair']}}},"
                      f"  /* {r['paired_gsps']:.2f} / {r['single_gsps']:.2f}{q} */")
     lines.append("};")

@@ -162,6 +162,19 @@ static int can_quad(unsigned M, unsigned os) {
     return ATKB_PTS == 8 && is_pow2(M) && M >= 16 && M <= 1024 && (os == 1 || os == 2);
 }
 
+/* a tile-shape choice: the fold in the low two bits (0 one hop per thread,
+ * 1 paired, 2 quad), bit 2 set to keep a small nchan's tile window out of
+ * shared memory (the fold then reads it through L1) */
+#define TUNE_NOSTAGE 4
+static int can_nostage(unsigned M, unsigned os) { return can_pair(M, os) && M <= 512; }
+static int choice_ok(unsigned M, unsigned os, int choice) {
+    const int shape = choice & 3, ns = choice & TUNE_NOSTAGE;
+    if (choice < 0 || choice > 6 || shape == 3) return 0;
+    if (shape == 2 && (!can_quad(M, os) || ns)) return 0;
+    if (ns && !can_nostage(M, os)) return 0;
+    return can_pair(M, os);
+}
+
 static int tune_choice(unsigned M, unsigned os, unsigned K) {
     unsigned i;
     int c = -1;
@@ -180,8 +193,8 @@ static int tune_choice(unsigned M, unsigned os, unsigned K) {
 ATKDSP_API int atkdsp_gpu_tune_set(unsigned nchan, unsigned oversample, unsigned taps_per_poly, int choice) {
     unsigned i;
     int rc = ATKDSP_OK;
-    if (!can_pair(nchan, oversample) || choice < -1 || choice > 2) return ATKDSP_E_ARG;
-    if (choice == 2 && !can_quad(nchan, oversample)) return ATKDSP_E_ARG;
+    if (!can_pair(nchan, oversample) || (choice != -1 && !choice_ok(nchan, oversample, choice)))
+        return ATKDSP_E_ARG;
     pthread_mutex_lock(&g_tune_lock);
     for (i = 0; i < g_tune_novr; ++i)
         if (g_tune_ovr[i].nchan == nchan && g_tune_ovr[i].os == oversample && g_tune_ovr[i].K == taps_per_poly)
@@ -210,8 +223,9 @@ ATKDSP_API int atkdsp_gpu_tune_get(unsigned nchan, unsigned oversample, unsigned
 static int plan_fft(unsigned M, unsigned os, int want_pair, atkb_fft_plan *pl) {
     memset(pl, 0, sizeof *pl);
     if (is_pow2(M) && M >= 16 && M <= MAX_POW2_NCHAN) {
-        const int quad = want_pair == 2 && can_quad(M, os);
-        const int pair = !quad && want_pair && can_pair(M, os);
+        const int quad = (want_pair & 3) == 2 && can_quad(M, os);
+        const int pair = !quad && (want_pair & 3) && can_pair(M, os);
+        pl->nostage = (want_pair & TUNE_NOSTAGE) && can_nostage(M, os);
         unsigned rem = M / (quad ? 2 : pair ? 4 : ATKB_PTS);
         pl->fast = 1;
         pl->pair = pair;
@@ -327,6 +341,7 @@ ATKDSP_API void atkdsp_pfb_destroy(atkdsp_pfb *p) {
     atkb_host_free(p->h_small_out);
     atkb_host_free(p->h_pend);
     atkb_event_destroy(p->small_ev);
+    atkb_event_destroy(p->small_done);
     atkb_event_destroy(p->tbl_event);
     atkb_stream_destroy(p->stream);
     free((void *)p->dins);
@@ -584,6 +599,7 @@ atkdsp_pfb *atkb_pfb_create_internal(double fs, unsigned nchan, unsigned oversam
             rc = atkb_host_alloc(&p->h_small_out, (size_t)max_nel * nchan * m_small * sizeof(atkdsp_cf32));
             if (rc == ATKB_OK) rc = atkb_host_alloc(&p->h_pend, (size_t)max_nel * p->hop * sizeof(atkdsp_cf32));
             if (rc == ATKB_OK) rc = atkb_event_create(&p->small_ev);
+            if (rc == ATKB_OK) rc = atkb_event_create(&p->small_done);
         }
     }
     if (rc == ATKB_OK) rc = atkb_malloc((void **)&p->d_counters, ATKB_NCOUNTERS * sizeof(int));
@@ -810,6 +826,7 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
     }
     T[nel] = (int)nel * tiles;
     /* the tables as laid out for max_nel, uploaded whole (they are small) */
+    void *tb = p->d_tables;
     rc = atkb_h2d(p->d_tables, p->h_tables, p->tbl_bytes + up_extra, stream);
     if (rc == ATKB_OK) rc = atkb_event_record(p->tbl_event, stream);
     if (rc != ATKB_OK) return rc;
@@ -831,8 +848,8 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
         /* nel jobs: tile_start[nel] is their total (the kernel reads
          * tile_start[njobs]); the same launch copies the nel carries */
         const int work = (int)nel * tiles + (int)nel;
-        rc = atkb_pfb_launch(tbl_jobs(p->d_tables), tbl_tiles(p->d_tables, p->max_nel),
-                             tbl_carry(p->d_tables, p->max_nel), (int)nel, p->d_counters,
+        rc = atkb_pfb_launch(tbl_jobs(tb), tbl_tiles(tb, p->max_nel),
+                             tbl_carry(tb, p->max_nel), (int)nel, p->d_counters,
                              p->grid < work ? p->grid : work, p->bank.smem_bytes, stream);
         if (rc != ATKB_OK) return rc;
     }
@@ -916,7 +933,8 @@ static ptrdiff_t process_small(atkdsp_pfb *p, const atkdsp_cf32 *const *ins, uns
     rc = run_step_up(p, nel, dins, nt, (atkdsp_cf32 *)p->d_out_stage, m, m, p->stream, &CONV_CF32, up);
     if (rc == ATKB_OK)
         rc = atkb_d2h(p->h_small_out, p->d_out_stage, out_n * sizeof(atkdsp_cf32), p->stream);
-    if (rc == ATKB_OK) rc = atkb_stream_sync(p->stream);
+    if (rc == ATKB_OK) rc = atkb_event_record(p->small_done, p->stream);
+    if (rc == ATKB_OK) rc = atkb_event_spin(p->small_done);
     if (rc != ATKB_OK) return map_rc(rc);
     memcpy(out, p->h_small_out, out_n * sizeof(atkdsp_cf32));
     return (ptrdiff_t)m;

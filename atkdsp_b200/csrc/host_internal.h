@@ -70,6 +70,7 @@ struct atkdsp_pfb {
      * before any other path reads the state. */
     void *h_pend;
     unsigned npend, pend_nel;
+    void *small_done;             /* the end of a small call's work (polled) */
     size_t tbl_bytes;
     int *d_counters;
     int grid;

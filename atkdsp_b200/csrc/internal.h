@@ -45,6 +45,9 @@ typedef struct {
     int quad;                     /* 1: quad fold (four hops per thread over two
                                    * branches), first radix 2; oversample 1 or
                                    * 2, nchan <= 1024 */
+    int nostage;                  /* 1: nchan <= 512 folds read global memory
+                                   * even where the tile window would fit in
+                                   * shared memory (the autotuner's choice) */
     int big;                      /* 1: nchan beyond one CTA's shared memory:
                                    * separate fold / pass / epilogue kernels */
     int ptaps;                    /* taps in the paired layout (pair, or the
@@ -194,6 +197,7 @@ int  atkb_pfb_launch_n(const atkb_job *d_jobs, const int *d_tile_start, const at
                        int njobs_max, const int *d_njobs, int *d_counters, int grid, int smem_bytes,
                        void *stream);
 int  atkb_event_query(void *ev);        /* ATKB_OK when complete, 1 when pending */
+int  atkb_event_spin(void *ev);         /* wait for an event by polling it */
 /* large filterbanks (plan.big: nchan beyond one CTA's shared memory): hops
  * [h0, h0 + nh) of job J (a host copy; its pointers are device pointers)
  * through fold, FFT-pass and epilogue kernels in `scratch`, 2 * nh * nchan

@@ -486,7 +486,7 @@ __device__ __forceinline__ bool fold_tile_staged(double2 *v, const atkb_job &J, 
         return false;
     } else {
         const int os = B.os;
-        if (J.in_kind || (os != 1 && os != 2 && os != 4)) return false;
+        if (J.in_kind || B.plan.nostage || (os != 1 && os != 2 && os != 4)) return false;
         const int logs = LOGM - (os == 1 ? 0 : os == 2 ? 1 : 2);
         const long long Wl = (long long)(nvalid - 1) * B.hop + B.L;
         if (Wl > 8192) return false;
@@ -675,7 +675,7 @@ __device__ __forceinline__ void fold_tile_pair(const atkb_job &J, const atkb_ban
         /* small nchan: the whole tile window through shared memory (as in
          * fold_tile_staged; logical sample i at i + (i / hop) * MP) */
         const long long Wl = (long long)(nvalid - 1) * HOP + B.L;
-        if (!J.in_kind && Wl <= 8192 && staged_size((int)Wl, LOGM - LOGOS, MP) <= 8192) {
+        if (!J.in_kind && !B.plan.nostage && Wl <= 8192 && staged_size((int)Wl, LOGM - LOGOS, MP) <= 8192) {
             float2 *xs = (float2 *)sm;
             stage_window(xs, J, h0 * (long long)HOP, (int)Wl, LOGM - LOGOS, MP);
             if (ta_ok) {
@@ -1549,16 +1549,37 @@ extern "C" int atkb_pfb_debug_build(void) {
 }
 
 namespace {
-/* the tiles' W2 partials of one single-element job, per channel added in tile
- * order: W2 power (S / m), and W1 for one element (R[k] += S, counts += m),
- * gated like atkb_w12 */
-__global__ void w2_finish_kernel(const double *__restrict__ part, int tiles, int M, long long m,
-                                 const uint8_t *__restrict__ gate, float2 *__restrict__ R,
-                                 uint32_t *__restrict__ counts, float *__restrict__ pwr, float *__restrict__ mean_pwr) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= M) return;
+/* the tiles' W2 partials of one single-element job, per channel: W2 power
+ * (S / m), and W1 for one element (R[k] += S, counts += m), gated like
+ * atkb_w12. A block of W2F_WARPS warps takes 32 channels, one per lane; warp
+ * w adds the tiles t = w, w + W2F_WARPS, ... in order (eight loads in flight
+ * per lane), then lane k's W2F_WARPS partials are added in warp order: a
+ * fixed order, so the result is deterministic. */
+#define W2F_WARPS 16
+__global__ void __launch_bounds__(32 * W2F_WARPS)
+w2_finish_kernel(const double *__restrict__ part, int tiles, int M, long long m, const uint8_t *__restrict__ gate,
+                 float2 *__restrict__ R, uint32_t *__restrict__ counts, float *__restrict__ pwr,
+                 float *__restrict__ mean_pwr) {
+    __shared__ double red[W2F_WARPS][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int k = blockIdx.x * 32 + lane;
     double S = 0.0;
-    for (int t = 0; t < tiles; ++t) S += part[(long long)t * M + k];
+    if (k < M) {
+        int t = w;
+        for (; t + 7 * W2F_WARPS < tiles; t += 8 * W2F_WARPS) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = __ldg(part + (long long)(t + u * W2F_WARPS) * M + k);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) S += v[u];
+        }
+        for (; t < tiles; t += W2F_WARPS) S += __ldg(part + (long long)t * M + k);
+    }
+    red[w][lane] = S;
+    __syncthreads();
+    if (w != 0 || k >= M) return;
+    S = 0.0;
+    for (int g = 0; g < W2F_WARPS; ++g) S += red[g][lane];
     const double inv = m ? 1.0 / (double)m : 0.0;
     if (pwr) pwr[k] = (float)(S * inv);
     if (mean_pwr) mean_pwr[k] = (float)((S * inv) / 1.0);
@@ -1574,7 +1595,7 @@ __global__ void w2_finish_kernel(const double *__restrict__ part, int tiles, int
 
 extern "C" int atkb_w2_finish(const double *part, int tiles, int nchan, long long m, const uint8_t *gate, void *R,
                               uint32_t *counts, float *pwr, float *mean_pwr, void *stream) {
-    w2_finish_kernel<<<(nchan + 255) / 256, 256, 0, (cudaStream_t)stream>>>(part, tiles, nchan, m, gate, (float2 *)R,
-                                                                          counts, pwr, mean_pwr);
+    w2_finish_kernel<<<(nchan + 31) / 32, 32 * W2F_WARPS, 0, (cudaStream_t)stream>>>(part, tiles, nchan, m, gate,
+                                                                                    (float2 *)R, counts, pwr, mean_pwr);
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }

@@ -194,6 +194,15 @@ extern "C" int atkb_event_elapsed_ms(float *ms, void *start, void *stop) {
     return st(cudaEventElapsedTime(ms, (cudaEvent_t)start, (cudaEvent_t)stop));
 }
 
+/* wait for an event by polling it: no sleep-and-wake in the driver's
+ * synchronisation, for the short waits of small synchronous calls */
+extern "C" int atkb_event_spin(void *ev) {
+    for (;;) {
+        const cudaError_t e = cudaEventQuery((cudaEvent_t)ev);
+        if (e == cudaSuccess) return ATKB_OK;
+        if (e != cudaErrorNotReady) return st(e);
+    }
+}
 extern "C" int atkb_event_query(void *ev) {
     const cudaError_t e = cudaEventQuery((cudaEvent_t)ev);
     if (e == cudaSuccess) return ATKB_OK;

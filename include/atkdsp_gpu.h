@@ -140,9 +140,11 @@ ATKDSP_API int         atkdsp_gpu_pfb_channel_power(const atkdsp_cf32 *d_out, un
  * paired fold.
  * atkdsp_gpu_tune_set overrides it for filterbanks created afterwards in this
  * process (choice 1: paired, 0: one hop per thread, 2: quad, -1: back to the
- * table); ATKDSP_E_ARG for a shape without that choice.
- * atkdsp_gpu_tune_get returns the choice such a filterbank gets now (0, 1 or
- * 2), or ATKDSP_E_ARG. Every shape meets the same parity bar; they differ
+ * table; add 4 to 1 or 0 for nchan <= 512 to have the fold read the tile
+ * window through L1 instead of staging it in shared memory); ATKDSP_E_ARG
+ * for a shape without that choice.
+ * atkdsp_gpu_tune_get returns the choice such a filterbank gets now (0, 1,
+ * 2, 4 or 5), or ATKDSP_E_ARG. Every shape meets the same parity bar; they differ
  * only in speed (and, through their FFT plans, in the last bit of a few
  * outputs). */
 ATKDSP_API int         atkdsp_gpu_tune_set(unsigned nchan, unsigned oversample,

@@ -6,7 +6,9 @@ sums are the same bits in every shape (each branch sums its taps in the same
 order); the shapes' FFT plans differ in their first radix, so outputs may
 differ from shape to shape by the last bit, as they may from the reference.
 Choices: 1 the paired fold, 0 one hop per thread, 2 the quad fold (four hops
-per thread; oversample 1 or 2, nchan <= 1024)."""
+per thread; oversample 1 or 2, nchan <= 1024); plus 4 for the fold to read a
+small nchan's tile window through L1 instead of staging it in shared memory
+(5 paired, 4 one hop per thread; nchan <= 512)."""
 
 from __future__ import annotations
 
@@ -35,7 +37,10 @@ def test_override_table_set_get_and_reset():
     # the quad fold needs oversample 1 or 2 and nchan <= 1024
     assert lib.atkdsp_gpu_tune_set(256, 4, 12, 2) < 0
     assert lib.atkdsp_gpu_tune_set(2048, 2, 12, 2) < 0
-    assert lib.atkdsp_gpu_tune_set(256, 2, 12, 3) < 0
+    assert lib.atkdsp_gpu_tune_set(256, 2, 12, 3) < 0 and lib.atkdsp_gpu_tune_set(256, 2, 12, 6) < 0
+    assert lib.atkdsp_gpu_tune_set(256, 2, 12, 5) == 0 and lib.atkdsp_gpu_tune_get(256, 2, 12) == 5
+    assert lib.atkdsp_gpu_tune_set(256, 2, 12, -1) == 0
+    assert lib.atkdsp_gpu_tune_set(1024, 2, 12, 5) < 0          # nothing staged above 512 channels
 
 
 @pytest.mark.gpu
@@ -51,7 +56,10 @@ def test_both_tile_shapes_match_the_oracle(M, os_, K):
     x = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
     blocks = [1, 999, 4096, 7]
     ref = run_blocks(O.oracle().Pfb(FS, M, os_, K, 80.0, 1), [x], blocks)
-    choices = (1, 0, 2) if os_ in (1, 2) and M <= 1024 else (1, 0)
+    # every shape the library offers for this filterbank (tune_set refuses the rest)
+    choices = [c for c in (1, 0, 2, 5, 4) if lib.atkdsp_gpu_tune_set(M, os_, K, c) == 0]
+    assert choices[:2] == [1, 0] and (2 in choices) == (os_ in (1, 2) and M <= 1024)
+    assert (5 in choices) == (M <= 512)
     try:
         ys = []
         for choice in choices:
