@@ -24,7 +24,7 @@ FS = 2.4e6
 def test_override_table_set_get_and_reset():
     lib = ak.load()
     before = lib.atkdsp_gpu_tune_get(256, 2, 12)
-    assert before in (0, 1, 2)
+    assert before in (0, 1, 2, 4, 5)
     assert lib.atkdsp_gpu_tune_set(256, 2, 12, 0) == 0 and lib.atkdsp_gpu_tune_get(256, 2, 12) == 0
     assert lib.atkdsp_gpu_tune_set(256, 2, 12, 1) == 0 and lib.atkdsp_gpu_tune_get(256, 2, 12) == 1
     assert lib.atkdsp_gpu_tune_set(256, 2, 12, -1) == 0 and lib.atkdsp_gpu_tune_get(256, 2, 12) == before
