@@ -1195,9 +1195,8 @@ def run_ours(args, rep):
         pj = json.loads(prof.read_text())
         if pj.get("ratio_traffic_over_algorithmic"):
             traffic = int(round(pj["ratio_traffic_over_algorithmic"] * alg))
-            traffic_src = (f"ratio {pj['ratio_traffic_over_algorithmic']} from "
-                           f"profiles/pfb_tiles_uneven256.json ({pj.get('captured', 'capture')}) x this launch's "
-                           f"algorithmic bytes")
+            traffic_src = (f"ratio {pj['ratio_traffic_over_algorithmic']} (profiles/pfb_tiles_uneven256.json: "
+                           f"{pj.get('captured', 'ncu capture')}) x this launch's algorithmic bytes")
     cpu = _cpu_reference_rate(specs) if "cpu" in arms and not args.no_cpu else None
     acc = _batched_accuracy(specs, torch, device) if "cpu" in arms and not args.no_cpu else None
     total = S * world
