@@ -185,6 +185,14 @@ def _bind(lib) -> None:
         f = getattr(lib, name)
         f.argtypes = args
         f.restype = res
+    # second function objects for the per-block calls, taking addresses as
+    # ints: numpy's ctypes.data_as costs more than the call itself
+    for attr, name, args, res in (("_lean_pfb_process", "atkdsp_pfb_process", [vp, vp, sz, vp, sz], ssz),
+                                  ("_lean_pfb_process_n", "atkdsp_pfb_process_n", [vp, vp, u, sz, vp, sz], ssz)):
+        f = lib._FuncPtr((name, lib))
+        f.argtypes = args
+        f.restype = res
+        setattr(lib, attr, f)
 
 
 def load(path: str | os.PathLike | None = None):
@@ -360,10 +368,14 @@ class Pfb:
         for a in arrs:
             if a.size != n:
                 raise AtkDspError("pfb: elements must be equal length")
-        m = self._lib.atkdsp_pfb_out_hops(self._p, n)
-        out = np.zeros(nel * self.nchan * m, np.complex64)
-        inarr = (C.POINTER(_Cf32) * nel)(*[_cfp(a) for a in arrs])
-        got = self._lib.atkdsp_pfb_process_n(self._p, inarr, nel, n, _cfp(out), out.size)
+        lib = self._lib
+        m = lib.atkdsp_pfb_out_hops(self._p, n)
+        out = np.empty(nel * self.nchan * m, np.complex64)     # every entry is written
+        if nel == 1:
+            got = lib._lean_pfb_process(self._p, arrs[0].ctypes.data, n, out.ctypes.data, out.size)
+        else:
+            inarr = (C.c_void_p * nel)(*[a.ctypes.data for a in arrs])
+            got = lib._lean_pfb_process_n(self._p, inarr, nel, n, out.ctypes.data, out.size)
         _check(int(got), "pfb_process_n")
         return out[: nel * self.nchan * got].reshape(nel, self.nchan, got)
 

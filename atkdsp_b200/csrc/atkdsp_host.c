@@ -597,6 +597,8 @@ atkdsp_pfb *atkb_pfb_create_internal(double fs, unsigned nchan, unsigned oversam
             p->h_small_in = (char *)p->h_tables + p->tbl_bytes;
             p->d_small_in = (char *)p->d_tables + p->tbl_bytes;
             rc = atkb_host_alloc(&p->h_small_out, (size_t)max_nel * nchan * m_small * sizeof(atkdsp_cf32));
+            if (rc == ATKB_OK && atkb_host_dev_ptr(p->h_small_out, &p->dz_small_out) != ATKB_OK)
+                p->dz_small_out = NULL;       /* then the outputs come back by copy */
             if (rc == ATKB_OK) rc = atkb_host_alloc(&p->h_pend, (size_t)max_nel * p->hop * sizeof(atkdsp_cf32));
             if (rc == ATKB_OK) rc = atkb_event_create(&p->small_ev);
             if (rc == ATKB_OK) rc = atkb_event_create(&p->small_done);
@@ -774,16 +776,17 @@ ATKDSP_API int atkdsp_gpu_debug_build(void) { return atkb_pfb_debug_build(); }
  * and carry tables, uploads them, launches the tile kernel and the carry,
  * and advances the host mirror of the state. Asynchronous on `stream`. */
 static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size_t n, atkdsp_cf32 *outs,
-                       size_t ldo, size_t m, void *stream, const conv_t *cv, size_t up_extra);
+                       size_t ldo, size_t m, void *stream, const conv_t *cv, size_t up_extra, int per_hop);
 
 static int run_step(atkdsp_pfb *p, unsigned nel, const void *const *ins, size_t n,
                     atkdsp_cf32 *outs, size_t ldo, size_t m, void *stream, const conv_t *cv) {
-    return run_step_up(p, nel, ins, n, outs, ldo, m, stream, cv, 0);
+    return run_step_up(p, nel, ins, n, outs, ldo, m, stream, cv, 0, 0);
 }
 
-/* up_extra: bytes after the tables (a small call's block) in the same upload */
+/* up_extra: bytes after the tables (a small call's block) in the same upload;
+ * per_hop: run the hops through the one-CTA-per-hop kernel (small calls) */
 static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size_t n, atkdsp_cf32 *outs,
-                       size_t ldo, size_t m, void *stream, const conv_t *cv, size_t up_extra) {
+                       size_t ldo, size_t m, void *stream, const conv_t *cv, size_t up_extra, int per_hop) {
     const size_t head = p->ov + p->lc;
     const unsigned nxt = (unsigned)(p->cur ^ 1);
     int rc;
@@ -848,9 +851,12 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
         /* nel jobs: tile_start[nel] is their total (the kernel reads
          * tile_start[njobs]); the same launch copies the nel carries */
         const int work = (int)nel * tiles + (int)nel;
-        rc = atkb_pfb_launch(tbl_jobs(tb), tbl_tiles(tb, p->max_nel),
-                             tbl_carry(tb, p->max_nel), (int)nel, p->d_counters,
-                             p->grid < work ? p->grid : work, p->bank.smem_bytes, stream);
+        if (per_hop && !big)
+            rc = atkb_pfb_hops(tbl_jobs(tb), tbl_carry(tb, p->max_nel), (int)nel, (int)m, p->d_counters, stream);
+        else
+            rc = atkb_pfb_launch(tbl_jobs(tb), tbl_tiles(tb, p->max_nel),
+                                 tbl_carry(tb, p->max_nel), (int)nel, p->d_counters,
+                                 p->grid < work ? p->grid : work, p->bank.smem_bytes, stream);
         if (rc != ATKB_OK) return rc;
     }
     p->cur = (int)nxt;
@@ -930,8 +936,15 @@ static ptrdiff_t process_small(atkdsp_pfb *p, const atkdsp_cf32 *const *ins, uns
     const size_t up = ((size_t)(nel - 1) * ATKB_SMALL_N + nt) * sizeof(atkdsp_cf32);
     p->lc -= (unsigned)np;               /* the device state holds lc - npend of the leftover */
     p->npend = 0;
-    rc = run_step_up(p, nel, dins, nt, (atkdsp_cf32 *)p->d_out_stage, m, m, p->stream, &CONV_CF32, up);
-    if (rc == ATKB_OK)
+    /* a few hops: one CTA each (a tile's latency is ~20 us, a hop's a few) */
+    const int per_hop = !p->w2_next && (size_t)nel * m <= ATKB_PER_HOP_MAX && atkb_pfb_hops_ok(&p->bank);
+    /* the per-hop kernel writes up to ATKB_DIRECT_OUT outputs straight into
+     * the pinned buffer (each an 8-byte write over the bus: beyond that one
+     * device->host copy of the packed outputs is faster) */
+    const int direct = per_hop && p->dz_small_out != NULL && out_n <= ATKB_DIRECT_OUT;
+    rc = run_step_up(p, nel, dins, nt, (atkdsp_cf32 *)(direct ? p->dz_small_out : p->d_out_stage), m, m,
+                     p->stream, &CONV_CF32, up, per_hop);
+    if (rc == ATKB_OK && !direct)
         rc = atkb_d2h(p->h_small_out, p->d_out_stage, out_n * sizeof(atkdsp_cf32), p->stream);
     if (rc == ATKB_OK) rc = atkb_event_record(p->small_done, p->stream);
     if (rc == ATKB_OK) rc = atkb_event_spin(p->small_done);
@@ -1332,7 +1345,7 @@ static ptrdiff_t unpack_host(const void *raw, size_t nbytes, int fmt, atkdsp_cf3
     if (rc == ATKB_OK && pole) rc = atkb_h2d(d_mean + 2, dc_state, sizeof(atkdsp_cf32), s->stream);
     if (rc == ATKB_OK)
         rc = atkb_unpack(d, fmt, n, d + rb, cre, cim, k, off_re, off_im, want_mean ? d_mean : NULL,
-                         (double *)(d + rb + ob), s->stream);
+                         (double *)(d + rb + ob), NULL, s->stream);
     if (rc == ATKB_OK && pole) rc = atkb_dc_pole(d + rb, n, dc_alpha, d_mean + 2, s->stream);
     if (rc == ATKB_OK) rc = atkb_d2h(out, d + rb, n * sizeof(atkdsp_cf32), s->stream);
     if (rc == ATKB_OK && want_mean) rc = atkb_d2h(hm, d_mean, sizeof hm, s->stream);
@@ -1358,17 +1371,24 @@ ATKDSP_API ptrdiff_t atkdsp_unpack_dc(const void *raw, size_t nbytes, int fmt, a
 }
 
 /* device-pointer unpack: the calling thread's fixed partials buffer on the
- * current device (allocated by its first such call, then reused) */
-static int gpu_partials(double **d) {
+ * current device (allocated by its first such call, then reused), and the
+ * fused mean's block counter after the partials (zeroed on the caller's
+ * stream when allocated; every launch leaves it at 0) */
+static int gpu_partials(double **d, unsigned **done, void *stream) {
     int rc;
     scratch_t *s = thread_scratch_get(0, &rc);
     if (!s) return rc;
     if (!s->partials) {
         void *p = NULL;
-        if ((rc = atkb_malloc(&p, GPU_PARTIALS * 2 * sizeof(double))) != ATKB_OK) return rc;
+        if ((rc = atkb_malloc(&p, GPU_PARTIALS * 2 * sizeof(double) + 256)) != ATKB_OK) return rc;
+        if ((rc = atkb_memset((char *)p + GPU_PARTIALS * 2 * sizeof(double), 0, 256, stream)) != ATKB_OK) {
+            atkb_free(p);
+            return rc;
+        }
         s->partials = (double *)p;
     }
     *d = s->partials;
+    *done = (unsigned *)(s->partials + GPU_PARTIALS * 2);
     return ATKB_OK;
 }
 
@@ -1388,11 +1408,12 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_unpack_dc(const void *d_raw, size_t nbytes, int 
     size_t n = nbytes / (size_t)bps;
     if (n > out_cap) n = out_cap;
     double *part = NULL;
+    unsigned *done = NULL;
     if (d_mean) {
-        const int rc = gpu_partials(&part);
+        const int rc = gpu_partials(&part, &done, stream);
         if (rc != ATKB_OK) return map_rc(rc);
     }
-    const int rc = atkb_unpack(d_raw, fmt, n, d_out, cre, cim, k, off_re, off_im, d_mean, part, stream);
+    const int rc = atkb_unpack(d_raw, fmt, n, d_out, cre, cim, k, off_re, off_im, d_mean, part, done, stream);
     return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
 }
 
@@ -1422,8 +1443,10 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_block_mean(const void *d_raw, size_t nbytes, int
     unpack_consts(fmt, off_re, off_im, &cre, &cim, &k);
     const size_t n = nbytes / (size_t)bps;
     double *part = NULL;
-    int rc = gpu_partials(&part);
-    if (rc == ATKB_OK) rc = atkb_unpack(d_raw, fmt, n, NULL, cre, cim, k, off_re, off_im, d_mean, part, stream);
+    unsigned *done = NULL;
+    int rc = gpu_partials(&part, &done, stream);
+    if (rc == ATKB_OK)
+        rc = atkb_unpack(d_raw, fmt, n, NULL, cre, cim, k, off_re, off_im, d_mean, part, done, stream);
     return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
 }
 
@@ -1437,7 +1460,7 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_unpack(const void *d_raw, size_t nbytes, int fmt
     unpack_consts(fmt, 0.0f, 0.0f, &cre, &cim, &k);
     size_t n = nbytes / (size_t)bps;
     if (n > out_cap) n = out_cap;
-    int rc = atkb_unpack(d_raw, fmt, n, d_out, cre, cim, k, 0.0f, 0.0f, NULL, NULL, stream);
+    int rc = atkb_unpack(d_raw, fmt, n, d_out, cre, cim, k, 0.0f, 0.0f, NULL, NULL, NULL, stream);
     if (rc == ATKB_OK && dc_alpha > 0.0f && d_dc_state) rc = atkb_dc_pole(d_out, n, dc_alpha, d_dc_state, stream);
     return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
 }

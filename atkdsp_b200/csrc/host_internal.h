@@ -20,6 +20,11 @@ atkdsp_pfb *atkb_pfb_create_served(double fs, unsigned nchan, unsigned oversampl
 /* host calls of at most this many samples per element stage through pinned
  * memory owned by the handle */
 #define ATKB_SMALL_N ((size_t)1 << 15)
+/* small calls of at most this many hops (over all elements) run one CTA per
+ * hop; beyond it the tile kernel's throughput wins */
+#define ATKB_PER_HOP_MAX 1024
+/* ... and write at most this many outputs straight into pinned host memory */
+#define ATKB_DIRECT_OUT 2048
 
 /* order `stream` (NULL: the handle's) after the handle's pending small-call
  * copy, if any; the device-pointer and batch paths call it first */
@@ -58,6 +63,8 @@ struct atkdsp_pfb {
      * its output; `small_ev` marks the last copy out of h_small_in, which a
      * call that completes no hop leaves in flight (small_live) */
     void *h_small_in, *h_small_out;  /* h_small_in: right after the pinned tables */
+    void *dz_small_out;               /* h_small_out's device address, or NULL:
+                                       * the per-hop kernel writes there */
     void *d_small_in;                 /* right after the device tables: one copy
                                        * carries a small call's tables and block */
     void *small_ev;

@@ -151,6 +151,8 @@ int  atkb_host_alloc(void **p, size_t bytes);      /* pinned */
  * fails with ATKB_E_NOMEM; 0 disarms */
 void atkb_fail_alloc_after(long long n);
 void atkb_host_free(void *p);
+/* the device address of pinned host memory (kernels write it over the bus) */
+int  atkb_host_dev_ptr(void *h, void **d);
 int  atkb_h2d(void *dst, const void *src, size_t bytes, void *stream);
 int  atkb_d2h(void *dst, const void *src, size_t bytes, void *stream);
 int  atkb_d2d(void *dst, const void *src, size_t bytes, void *stream);
@@ -209,6 +211,12 @@ long long atkb_pfb_big_hops(int nchan);
  * whether this library is that build */
 unsigned atkb_pfb_debug_fault(void);
 int  atkb_pfb_debug_build(void);
+/* small calls: one CTA per hop of njobs jobs of m hops each (the bank a
+ * power of two 16..1024 on the fast plan, atkb_pfb_hops_ok), then one CTA per
+ * carry; the same outputs and fault word as atkb_pfb_launch */
+int  atkb_pfb_hops(const atkb_job *d_jobs, const atkb_carry *d_carry, int njobs, int m, int *d_counters,
+                   void *stream);
+int  atkb_pfb_hops_ok(const atkb_bank *B);
 int  atkb_pfb_big(const atkb_job *J, const atkb_bank *B, long long h0, int nh, void *scratch, int grid,
                   void *stream);
 
@@ -350,10 +358,13 @@ int  atkb_cfar_gather(const double *X, const double *noise, long long nbins, int
 /* device raw -> device cf32 (out may be NULL: mean only), (x - c) * k per component; the means (double,
  * BEFORE subtraction of the offset, i.e. sum(out)/n + off) go to d_mean[0..1]
  * when d_mean != NULL, using d_partial (>= 2 * atkb_unpack_partials(n)
- * doubles) as scratch. */
+ * doubles) as scratch. d_done (may be NULL): a device counter that is 0
+ * between calls; with it the unpack launch's last block computes the mean
+ * (no second launch) and puts the counter back to 0. */
 int  atkb_unpack_partials(size_t n);
 int  atkb_unpack(const void *raw, int fmt, size_t n, void *out, float cre, float cim, float k,
-                 float off_re, float off_im, double *d_mean, double *d_partial, void *stream);
+                 float off_re, float off_im, double *d_mean, double *d_partial, unsigned *d_done,
+                 void *stream);
 /* the same conversion and mean with the partial sums in a static device
  * array instead of caller scratch; at most atkb_unpack_noalloc_max_samples()
  * samples per call (ATKB_E_ARG beyond) */

@@ -1254,6 +1254,26 @@ __device__ __forceinline__ void fetch_tile(const atkb_job *__restrict__ jobs, co
     if (lane == 0) s_local[slot] = tile - tile_start[lo];
 }
 
+/* dst[0, len) = s[from, from + len), eight loads in flight per thread before
+ * their stores (a load-store loop would wait one memory round trip per
+ * step: the compiler cannot tell dst from the sources) */
+template <int T>
+__device__ __forceinline__ void carry_copy(const Src &src, float2 *dst, long long from, long long len) {
+    for (long long i0 = threadIdx.x; i0 < len; i0 += 8LL * T) {
+        float2 v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const long long i = i0 + (long long)u * T;
+            if (i < len) v[u] = src.at(from + i);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const long long i = i0 + (long long)u * T;
+            if (i < len) dst[i] = v[u];
+        }
+    }
+}
+
 #ifndef ATKB_TILE_MINB
 #define ATKB_TILE_MINB (PTS == 8 ? 2 : 2)
 #endif
@@ -1348,7 +1368,7 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
             if (threadIdx.x == 0) atomicOr((unsigned *)&counters[ATKB_FAULT_WORD], ATKB_FAULT_CARRY);
             continue;
         }
-        for (long long i = threadIdx.x; i < len; i += NT) dst[i] = src.at(from + i);
+        carry_copy<NT>(src, dst, from, len);
     }
     if (threadIdx.x == 0) {
         __threadfence();
@@ -1463,6 +1483,169 @@ big_out_kernel(const double2 *__restrict__ X, const atkb_job J, const double2 *_
     }
 }
 
+
+/* ---- small calls: one CTA per hop ------------------------------------------
+ * A host call of a few thousand samples completes a few dozen hops; the tile
+ * kernel would run them as one tile in one CTA, whose fold and passes take
+ * ~20 us of latency. Here every hop of every job gets its own CTA of
+ * HOPS_NT threads (power-of-two nchan 16..1024 on the fast plan), and the
+ * jobs' state carries one CTA each after them:
+ *   fold    thread per branch q, k ascending, a rounded multiply then a
+ *           rounded add: the bits of every tile shape's fold;
+ *   FFT     the bank's own plan, pass by pass between two shared-memory
+ *           buffers: the first pass (radix plan.radix[0], Ns = 1) without
+ *           twiddles, the others with tw_powers of the bank's per-pass table
+ *           and cmul, the last fused with finish_bin -- the arithmetic of the
+ *           tile kernel's passes, so the outputs equal the tile path's bits.
+ * The uniform bounds checks are the tile kernel's (window, output, carry). */
+#define HOPS_NT 128
+#define HOPS_MAXM 1024
+
+template <int R>
+__device__ __forceinline__ void hop_pass(const double2 *__restrict__ src, double2 *__restrict__ dst, int M, int Ns,
+                                         const double2 *__restrict__ tw, bool first) {
+    const int MR = M / R;
+    for (int j = threadIdx.x; j < MR; j += HOPS_NT) {
+        const int k = j & (Ns - 1);
+        double2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = src[j + r * MR];
+        if (!first) {
+            double2 w[R];
+            tw_powers<R>(__ldg(tw + k), w);
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
+        }
+        dftR<R>(v);
+        const int d = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[d + r * Ns] = v[r];
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void hop_pass_last(const double2 *__restrict__ src, int M, int Ns,
+                                              const double2 *__restrict__ tw, bool first, const atkb_bank &B,
+                                              const atkb_job &J, long long t) {
+    const int MR = M / R;                       /* == Ns */
+    const double2 *twd = (const double2 *)B.twd;
+    const float2 *cal = (const float2 *)J.cal;
+    float2 *out = (float2 *)J.out;
+    const int osm = B.os - 1;
+    const int s = (int)(J.b0 + t + 1) & osm;
+    for (int j = threadIdx.x; j < MR; j += HOPS_NT) {
+        double2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = src[j + r * MR];
+        if (!first) {
+            double2 w[R];
+            tw_powers<R>(__ldg(tw + j), w);
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
+        }
+        dftR<R>(v);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int kb = j + r * Ns;
+            out[(long long)kb * J.ldo + J.out_col + t] = finish_bin(v[r], kb, s, M, osm + 1, B.hop, true, twd, cal);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(HOPS_NT)
+pfb_hops_kernel(const atkb_job *__restrict__ jobs, const atkb_carry *__restrict__ carries, int njobs, int m,
+                int *counters) {
+    __shared__ double2 buf[2][HOPS_MAXM];
+    __shared__ atkb_bank SB;
+    const int b = blockIdx.x;
+    if (b >= njobs * m) {                       /* a state carry */
+        const int ci = b - njobs * m;
+        if (ci >= njobs) return;
+        const atkb_carry &C = carries[ci];
+        const long long from = C.from, len = C.len;
+        if (from < 0 || len < 0 || from + len > C.nsrc || len > C.cap) {
+            if (threadIdx.x == 0) atomicOr((unsigned *)&counters[ATKB_FAULT_WORD], ATKB_FAULT_CARRY);
+            return;
+        }
+        const Src src{(const float2 *)C.state, C.in, C.head, C.in_kind, C.cre, C.cim, C.kscale};
+        float2 *dst = (float2 *)C.dst;
+        carry_copy<HOPS_NT>(src, dst, from, len);
+        return;
+    }
+    const atkb_job &J = jobs[b / m];
+    const long long t = b % m;
+    {
+        static_assert(sizeof(atkb_bank) % 4 == 0, "word copies");
+        const int *bs = (const int *)J.bank;
+        int *bd = (int *)&SB;
+        for (int w = threadIdx.x; w < (int)(sizeof(atkb_bank) / 4); w += HOPS_NT) bd[w] = bs[w];
+    }
+    __syncthreads();
+    const int M = SB.nchan;
+    /* uniform across the CTA: a shape this kernel does not run, a window past
+     * the job's samples or a column past the row stride skips the hop */
+    {
+        unsigned bad = 0;
+        if (t >= J.hops || t * SB.hop + SB.L > J.nsrc) bad |= ATKB_FAULT_WINDOW;
+        if (J.out_col + t + 1 > J.ldo) bad |= ATKB_FAULT_OUTPUT;
+        if (!SB.plan.fast || M > HOPS_MAXM || M < 16) bad |= ATKB_FAULT_INDEX;
+        for (int p = 0; p < SB.plan.npass; ++p)
+            if (SB.plan.radix[p] != 2 && SB.plan.radix[p] != 4 && SB.plan.radix[p] != 8) bad |= ATKB_FAULT_INDEX;
+        if (bad) {
+            if (threadIdx.x == 0) atomicOr((unsigned *)&counters[ATKB_FAULT_WORD], bad);
+            return;
+        }
+    }
+    /* the fold, one branch per thread and step, eight taps' loads in flight */
+    {
+        const Src src{(const float2 *)J.state, J.in, J.head, J.in_kind, J.cre, J.cim, J.kscale};
+        const float *taps = SB.taps;
+        const int K = SB.K;
+        const long long base = t * SB.hop;
+        for (int q = threadIdx.x; q < M; q += HOPS_NT) {
+            float fr = -0.0f, fi = -0.0f;
+            for (int k0 = 0; k0 < K; k0 += 8) {
+                float h[8];
+                float2 x[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (k0 + u < K) {
+                        h[u] = __ldg(taps + (long long)(k0 + u) * M + q);
+                        x[u] = src.at(base + (long long)(k0 + u) * M + q);
+                    }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (k0 + u < K) {
+                        fr = __fadd_rn(fr, __fmul_rn(h[u], x[u].x));
+                        fi = __fadd_rn(fi, __fmul_rn(h[u], x[u].y));
+                    }
+            }
+            buf[0][q] = make_double2((double)fr, (double)fi);
+        }
+    }
+    __syncthreads();
+    /* the plan's passes */
+    const double2 *wp = (const double2 *)SB.wpass;
+    int Ns = 1, cur = 0;
+    for (int p = 0; p < SB.plan.npass; ++p) {
+        const int R = SB.plan.radix[p];
+        const double2 *tw = wp + SB.plan.twoff[p];
+        const bool first = p == 0;
+        if (p == SB.plan.npass - 1) {
+            if (R == 8) hop_pass_last<8>(buf[cur], M, Ns, tw, first, SB, J, t);
+            else if (R == 4) hop_pass_last<4>(buf[cur], M, Ns, tw, first, SB, J, t);
+            else hop_pass_last<2>(buf[cur], M, Ns, tw, first, SB, J, t);
+        } else {
+            if (R == 8) hop_pass<8>(buf[cur], buf[cur ^ 1], M, Ns, tw, first);
+            else if (R == 4) hop_pass<4>(buf[cur], buf[cur ^ 1], M, Ns, tw, first);
+            else hop_pass<2>(buf[cur], buf[cur ^ 1], M, Ns, tw, first);
+            __syncthreads();
+            cur ^= 1;
+        }
+        Ns *= R;
+    }
+}
+
 }  // namespace
 
 extern "C" int atkb_pfb_max_smem(void) { return 200 * 1024; }
@@ -1529,6 +1712,25 @@ extern "C" int atkb_pfb_big(const atkb_job *J, const atkb_bank *B, long long h0,
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }
 
+/* the small-call kernel: njobs jobs of m hops each, then their carries */
+extern "C" int atkb_pfb_hops(const atkb_job *d_jobs, const atkb_carry *d_carry, int njobs, int m, int *d_counters,
+                             void *stream) {
+    if (njobs < 1 || m < 0) return ATKB_E_ARG;
+    const long long grid = (long long)njobs * m + njobs;
+    if (grid > 0x7fffffffLL) return ATKB_E_ARG;
+    atkb_range_push("atkdsp small call");
+    pfb_hops_kernel<<<(unsigned)grid, HOPS_NT, 0, (cudaStream_t)stream>>>(d_jobs, d_carry, njobs, m, d_counters);
+    atkb_range_pop();
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
+extern "C" int atkb_pfb_hops_ok(const atkb_bank *B) {
+    if (!B->plan.fast || B->plan.big || B->nchan < 16 || B->nchan > HOPS_MAXM) return 0;
+    for (int p = 0; p < B->plan.npass; ++p)
+        if (B->plan.radix[p] != 2 && B->plan.radix[p] != 4 && B->plan.radix[p] != 8) return 0;
+    return 1;
+}
+
 extern "C" unsigned atkb_pfb_debug_fault(void) {
 #ifdef ATKB_DEBUG_BOUNDS
     unsigned v = 0, z = 0;
@@ -1551,35 +1753,53 @@ extern "C" int atkb_pfb_debug_build(void) {
 namespace {
 /* the tiles' W2 partials of one single-element job, per channel: W2 power
  * (S / m), and W1 for one element (R[k] += S, counts += m), gated like
- * atkb_w12. A block of W2F_WARPS warps takes 32 channels, one per lane; warp
- * w adds the tiles t = w, w + W2F_WARPS, ... in order (eight loads in flight
- * per lane), then lane k's W2F_WARPS partials are added in warp order: a
- * fixed order, so the result is deterministic. */
+ * atkb_w12. A block of W2F_WARPS warps takes W2F_CH = 8 channels: lane l of
+ * warp w reads channel l % 8 of the tiles t = s, s + 64, ... (s = 4w + l / 8,
+ * 64 tile streams; sixteen loads in flight, each quarter-warp one 64-byte
+ * row segment). The 64 stream sums of a channel are then added by a fixed tree
+ * (eight groups of eight in stream order, then the eight group sums in
+ * order), so the result is deterministic. Eight channels a block spread the
+ * reads of nchan 1024 over 128 SMs. */
 #define W2F_WARPS 16
+#define W2F_CH 8
+#define W2F_STREAMS (W2F_WARPS * 32 / W2F_CH)
 __global__ void __launch_bounds__(32 * W2F_WARPS)
 w2_finish_kernel(const double *__restrict__ part, int tiles, int M, long long m, const uint8_t *__restrict__ gate,
                  float2 *__restrict__ R, uint32_t *__restrict__ counts, float *__restrict__ pwr,
                  float *__restrict__ mean_pwr) {
-    __shared__ double red[W2F_WARPS][32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int k = blockIdx.x * 32 + lane;
+    __shared__ double red[W2F_STREAMS][W2F_CH];
+    __shared__ double grp[W2F_STREAMS / 8][W2F_CH];
+    const int c = threadIdx.x % W2F_CH, sidx = threadIdx.x / W2F_CH;
+    const int k = blockIdx.x * W2F_CH + c;
     double S = 0.0;
     if (k < M) {
-        int t = w;
-        for (; t + 7 * W2F_WARPS < tiles; t += 8 * W2F_WARPS) {
-            double v[8];
+        /* sixteen loads in flight, the ones past the last tile read as +0.0
+         * (S >= +0.0, so adding it is exact and the order is unchanged) */
+        for (int t = sidx; t < tiles; t += 16 * W2F_STREAMS) {
+            double v[16];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) v[u] = __ldg(part + (long long)(t + u * W2F_WARPS) * M + k);
+            for (int u = 0; u < 16; ++u) {
+                const int r = t + u * W2F_STREAMS;
+                v[u] = r < tiles ? __ldg(part + (long long)r * M + k) : 0.0;
+            }
 #pragma unroll
-            for (int u = 0; u < 8; ++u) S += v[u];
+            for (int u = 0; u < 16; ++u) S += v[u];
         }
-        for (; t < tiles; t += W2F_WARPS) S += __ldg(part + (long long)t * M + k);
     }
-    red[w][lane] = S;
+    red[sidx][c] = S;
     __syncthreads();
-    if (w != 0 || k >= M) return;
+    if (threadIdx.x < (W2F_STREAMS / 8) * W2F_CH) {
+        const int g = threadIdx.x / W2F_CH;
+        double G = 0.0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) G += red[8 * g + j][c];
+        grp[g][c] = G;
+    }
+    __syncthreads();
+    if (threadIdx.x >= W2F_CH || k >= M) return;
     S = 0.0;
-    for (int g = 0; g < W2F_WARPS; ++g) S += red[g][lane];
+#pragma unroll
+    for (int g = 0; g < W2F_STREAMS / 8; ++g) S += grp[g][c];
     const double inv = m ? 1.0 / (double)m : 0.0;
     if (pwr) pwr[k] = (float)(S * inv);
     if (mean_pwr) mean_pwr[k] = (float)((S * inv) / 1.0);
@@ -1595,7 +1815,7 @@ w2_finish_kernel(const double *__restrict__ part, int tiles, int M, long long m,
 
 extern "C" int atkb_w2_finish(const double *part, int tiles, int nchan, long long m, const uint8_t *gate, void *R,
                               uint32_t *counts, float *pwr, float *mean_pwr, void *stream) {
-    w2_finish_kernel<<<(nchan + 31) / 32, 32 * W2F_WARPS, 0, (cudaStream_t)stream>>>(part, tiles, nchan, m, gate,
-                                                                                    (float2 *)R, counts, pwr, mean_pwr);
+    w2_finish_kernel<<<(nchan + W2F_CH - 1) / W2F_CH, 32 * W2F_WARPS, 0, (cudaStream_t)stream>>>(
+        part, tiles, nchan, m, gate, (float2 *)R, counts, pwr, mean_pwr);
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }

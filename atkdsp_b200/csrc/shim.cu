@@ -102,6 +102,15 @@ extern "C" int atkb_host_alloc(void **p, size_t bytes) {
 extern "C" void atkb_host_free(void *p) {
     if (p) cudaFreeHost(p);
 }
+extern "C" int atkb_host_dev_ptr(void *h, void **d) {
+    *d = nullptr;
+    const cudaError_t e = cudaHostGetDevicePointer(d, h, 0);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();        /* not sticky: leave no error for the next launch check */
+        *d = nullptr;
+    }
+    return st(e);
+}
 extern "C" int atkb_h2d(void *dst, const void *src, size_t bytes, void *stream) {
     if (!bytes) return ATKB_OK;
     return st(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream));

@@ -64,19 +64,29 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-__global__ void __launch_bounds__(UNPACK_NT)
-unpack_kernel(const void *__restrict__ raw, int fmt, size_t n, float2 *__restrict__ out, float cre,
-              float cim, float k, float offr, float offi, double *__restrict__ partial) {
-    double sr = 0.0, si = 0.0;
-    const size_t stride = (size_t)gridDim.x * UNPACK_NT;
-    for (size_t i = (size_t)blockIdx.x * UNPACK_NT + threadIdx.x; i < n; i += stride) {
-        const float2 y = convert_one(raw, fmt, i, cre, cim, k, offr, offi);
-        if (out) out[i] = y;
-        sr += (double)y.x;
-        si += (double)y.y;
-    }
-    if (!partial) return;
+/* The mean from the blocks' partial sums, by one block of UNPACK_NT threads:
+ * thread t adds partials t, t + UNPACK_NT, ... in order, then the warps and
+ * the warp sums reduce in a fixed order. The loads bypass L1: in the fused
+ * form the partials were written by other blocks of the same launch. */
+__device__ void mean_finish(const double *partial, int nblocks, size_t n, float offr, float offi,
+                            double *mean) {
     __shared__ double red[2][UNPACK_NT / 32];
+    double sr = 0.0, si = 0.0;
+    /* eight partials in flight per thread; past the last block +0.0, which
+     * leaves the sums exact (they never hold -0.0) and in the same order */
+    for (int b0 = threadIdx.x; b0 < nblocks; b0 += 8 * UNPACK_NT) {
+        double2 v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int b = b0 + u * UNPACK_NT;
+            v[u] = b < nblocks ? __ldcg((const double2 *)partial + b) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            sr += v[u].x;
+            si += v[u].y;
+        }
+    }
     sr = warp_sum(sr);
     si = warp_sum(si);
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -87,8 +97,62 @@ unpack_kernel(const void *__restrict__ raw, int fmt, size_t n, float2 *__restric
         si = l < UNPACK_NT / 32 ? red[1][l] : 0.0;
         sr = warp_sum(sr);
         si = warp_sum(si);
-        if (l == 0) { partial[2 * blockIdx.x] = sr; partial[2 * blockIdx.x + 1] = si; }
+        if (l == 0) {
+            const double inv = n ? 1.0 / (double)n : 0.0;
+            mean[0] = sr * inv + (double)offr;
+            mean[1] = si * inv + (double)offi;
+        }
     }
+}
+
+/* This block's partial sums into partial[2 * blockIdx.x]. With done set, the
+ * block that finishes last (a ticket on *done after a fence on its partial)
+ * also computes the mean, exactly as unpack_mean_kernel would, and puts
+ * *done back to 0 for the next launch: one launch instead of two. */
+__device__ __forceinline__ void block_partial(double sr, double si, double *partial, double *mean,
+                                              unsigned *done, size_t n, float offr, float offi) {
+    __shared__ double red[2][UNPACK_NT / 32];
+    __shared__ int last;
+    sr = warp_sum(sr);
+    si = warp_sum(si);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { red[0][w] = sr; red[1][w] = si; }
+    __syncthreads();
+    if (w == 0) {
+        sr = l < UNPACK_NT / 32 ? red[0][l] : 0.0;
+        si = l < UNPACK_NT / 32 ? red[1][l] : 0.0;
+        sr = warp_sum(sr);
+        si = warp_sum(si);
+        if (l == 0) {
+            partial[2 * blockIdx.x] = sr;
+            partial[2 * blockIdx.x + 1] = si;
+            if (done) {
+                __threadfence();
+                last = atomicAdd(done, 1u) == gridDim.x - 1;
+            }
+        }
+    }
+    if (!done) return;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    mean_finish(partial, (int)gridDim.x, n, offr, offi, mean);
+    if (threadIdx.x == 0) *done = 0u;
+}
+
+__global__ void __launch_bounds__(UNPACK_NT)
+unpack_kernel(const void *__restrict__ raw, int fmt, size_t n, float2 *__restrict__ out, float cre,
+              float cim, float k, float offr, float offi, double *__restrict__ partial, double *mean,
+              unsigned *done) {
+    double sr = 0.0, si = 0.0;
+    const size_t stride = (size_t)gridDim.x * UNPACK_NT;
+    for (size_t i = (size_t)blockIdx.x * UNPACK_NT + threadIdx.x; i < n; i += stride) {
+        const float2 y = convert_one(raw, fmt, i, cre, cim, k, offr, offi);
+        if (out) out[i] = y;
+        sr += (double)y.x;
+        si += (double)y.y;
+    }
+    if (partial) block_partial(sr, si, partial, mean, done, n, offr, offi);
 }
 
 /* The same conversion and partial sums with 16-byte accesses: four samples
@@ -121,7 +185,7 @@ __device__ __forceinline__ void load4(const void *raw, size_t q, float (&a)[4], 
 template <int FMT>
 __global__ void __launch_bounds__(UNPACK_NT)
 unpack_kernel_v4(const void *__restrict__ raw, size_t n, float2 *__restrict__ out, float cre, float cim, float k,
-                 float offr, float offi, double *__restrict__ partial) {
+                 float offr, float offi, double *__restrict__ partial, double *mean, unsigned *done) {
     double sr = 0.0, si = 0.0;
     const size_t nq = n >> 2;
     const size_t stride = (size_t)gridDim.x * UNPACK_NT;
@@ -157,64 +221,32 @@ unpack_kernel_v4(const void *__restrict__ raw, size_t n, float2 *__restrict__ ou
         sr += (double)y.x;
         si += (double)y.y;
     }
-    if (!partial) return;
-    __shared__ double red[2][UNPACK_NT / 32];
-    sr = warp_sum(sr);
-    si = warp_sum(si);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) { red[0][w] = sr; red[1][w] = si; }
-    __syncthreads();
-    if (w == 0) {
-        sr = l < UNPACK_NT / 32 ? red[0][l] : 0.0;
-        si = l < UNPACK_NT / 32 ? red[1][l] : 0.0;
-        sr = warp_sum(sr);
-        si = warp_sum(si);
-        if (l == 0) { partial[2 * blockIdx.x] = sr; partial[2 * blockIdx.x + 1] = si; }
-    }
+    if (partial) block_partial(sr, si, partial, mean, done, n, offr, offi);
 }
 
-/* unpack_kernel_v4 when both pointers allow 16-byte accesses, else unpack_kernel */
+/* unpack_kernel_v4 when both pointers allow 16-byte accesses, else unpack_kernel.
+ * done (with partial and mean) fuses the mean into the launch. */
 void launch_unpack(const void *raw, int fmt, size_t n, float2 *out, float cre, float cim, float k, float offr,
-                   float offi, double *partial, int nb, cudaStream_t s) {
+                   float offi, double *partial, int nb, cudaStream_t s, double *mean = nullptr,
+                   unsigned *done = nullptr) {
     const bool v4 = ((uintptr_t)raw & 15) == 0 && ((uintptr_t)out & 15) == 0 && fmt >= 0 && fmt <= 4;
     if (!v4) {
-        unpack_kernel<<<nb, UNPACK_NT, 0, s>>>(raw, fmt, n, out, cre, cim, k, offr, offi, partial);
+        unpack_kernel<<<nb, UNPACK_NT, 0, s>>>(raw, fmt, n, out, cre, cim, k, offr, offi, partial, mean, done);
         return;
     }
     switch (fmt) {
-    case 0: unpack_kernel_v4<0><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial); break;
-    case 1: unpack_kernel_v4<1><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial); break;
-    case 2: unpack_kernel_v4<2><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial); break;
-    case 3: unpack_kernel_v4<3><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial); break;
-    default: unpack_kernel_v4<4><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial); break;
+    case 0: unpack_kernel_v4<0><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done); break;
+    case 1: unpack_kernel_v4<1><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done); break;
+    case 2: unpack_kernel_v4<2><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done); break;
+    case 3: unpack_kernel_v4<3><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done); break;
+    default: unpack_kernel_v4<4><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done); break;
     }
 }
 
 __global__ void __launch_bounds__(UNPACK_NT)
 unpack_mean_kernel(const double *__restrict__ partial, int nblocks, size_t n, float offr, float offi,
                    double *__restrict__ mean) {
-    double sr = 0.0, si = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += UNPACK_NT) {
-        sr += partial[2 * b];
-        si += partial[2 * b + 1];
-    }
-    __shared__ double red[2][UNPACK_NT / 32];
-    sr = warp_sum(sr);
-    si = warp_sum(si);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) { red[0][w] = sr; red[1][w] = si; }
-    __syncthreads();
-    if (w == 0) {
-        sr = l < UNPACK_NT / 32 ? red[0][l] : 0.0;
-        si = l < UNPACK_NT / 32 ? red[1][l] : 0.0;
-        sr = warp_sum(sr);
-        si = warp_sum(si);
-        if (l == 0) {
-            const double inv = n ? 1.0 / (double)n : 0.0;
-            mean[0] = sr * inv + (double)offr;
-            mean[1] = si * inv + (double)offi;
-        }
-    }
+    mean_finish(partial, nblocks, n, offr, offi, mean);
 }
 
 /* s += alpha (x - s); y = x - s, in order, one thread per component */
@@ -254,7 +286,7 @@ extern "C" int atkb_unpack_partials(size_t n) {
 
 extern "C" int atkb_unpack(const void *raw, int fmt, size_t n, void *out, float cre, float cim,
                            float k, float off_re, float off_im, double *d_mean, double *d_partial,
-                           void *stream) {
+                           unsigned *d_done, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
     const int nb = atkb_unpack_partials(n);
     if (n) {
@@ -264,7 +296,7 @@ extern "C" int atkb_unpack(const void *raw, int fmt, size_t n, void *out, float 
                 return ATKB_E_KERNEL;
         } else {
             launch_unpack(raw, fmt, n, (float2 *)out, cre, cim, k, off_re, off_im, d_mean ? d_partial : nullptr,
-                          nb, s);
+                          nb, s, d_mean, d_mean ? d_done : nullptr);
         }
     }
     if (d_mean) {
@@ -274,7 +306,7 @@ extern "C" int atkb_unpack(const void *raw, int fmt, size_t n, void *out, float 
             if (cudaMemcpyAsync(d_mean, z, sizeof z, cudaMemcpyHostToDevice, s) != cudaSuccess)
                 return ATKB_E_KERNEL;
             if (cudaStreamSynchronize(s) != cudaSuccess) return ATKB_E_KERNEL;
-        } else {
+        } else if (!d_done) {               /* with d_done the unpack launch computed it */
             unpack_mean_kernel<<<1, UNPACK_NT, 0, s>>>(d_partial, nb, n, off_re, off_im, d_mean);
         }
     }

@@ -87,8 +87,9 @@ ATKDSP_API ptrdiff_t atkdsp_unpack_dc(const void *raw, size_t nbytes, int fmt,
 typedef struct atkdsp_pfb atkdsp_pfb;
 /* reference include/atkdsp.h:3191-3193. NULL on bad arguments (fs <= 0,
  * nchan < 2, nchan % oversample, taps_per_poly < 2, max_nel < 1), when no GPU
- * is usable, when device memory runs out, or when nchan is beyond what the
- * device kernels support (power of two up to 4096, any other value up to 6400). */
+ * is usable, or when device memory runs out. Any nchan is accepted: a power of
+ * two up to 4096 or any other value up to 6400 runs through the tile kernel,
+ * a larger one through the large-filterbank kernels. */
 ATKDSP_API atkdsp_pfb *atkdsp_pfb_create(double fs, unsigned nchan, unsigned oversample,
                                          unsigned taps_per_poly, double atten_db,
                                          unsigned max_nel);
