@@ -129,6 +129,8 @@ def _bind(lib) -> None:
         "atkdsp_gpu_unpack_dc": ([vp, sz, C.c_int, vp, sz, C.c_float, C.c_float, vp, vp], ssz),
         "atkdsp_gpu_unpack": ([vp, sz, C.c_int, vp, sz, C.c_float, vp, vp], ssz),
         "atkdsp_gpu_block_mean": ([vp, sz, C.c_int, C.c_float, C.c_float, vp, vp], ssz),
+        "atkdsp_gpu_block_mean_dev": ([vp, sz, C.c_int, vp, vp, vp], ssz),
+        "atkdsp_gpu_pfb_process_w12_dev": ([vp, vp, sz, C.c_int, vp, vp, sz, vp, vp, vp, vp, vp, vp, sz, vp], ssz),
         "atkdsp_gpu_pfb_accumulate": ([vp, u, u, sz, vp, vp, vp, vp, vp, vp], C.c_int),
         "atkdsp_gpu_pfb_cov_accumulate": ([vp, u, u, sz, vp, vp, vp, vp], C.c_int),
         "atkdsp_gpu_pfb_cov_reset": ([vp, vp, u, u, vp, vp], C.c_int),

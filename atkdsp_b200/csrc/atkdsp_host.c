@@ -708,7 +708,7 @@ ATKDSP_API int atkdsp_pfb_describe(const atkdsp_pfb *p, char *buf, size_t cap) {
                     atkdsp_pfb_out_rate(p) / 1e3, p->L, p->K, p->atten, p->max_nel);
 }
 
-const conv_t ATKB_CONV_CF32 = {0, 0.0f, 0.0f, 1.0f};
+const conv_t ATKB_CONV_CF32 = {0, 0.0f, 0.0f, 1.0f, NULL};
 #define CONV_CF32 ATKB_CONV_CF32
 
 void atkb_job_conv(atkb_job *J, atkb_carry *C, const conv_t *cv);
@@ -721,6 +721,7 @@ void atkb_job_conv(atkb_job *J, atkb_carry *C, const conv_t *cv);
 void atkb_job_conv(atkb_job *J, atkb_carry *C, const conv_t *cv) {
     J->in_kind = C->in_kind = cv->kind;
     J->kscale = C->kscale = cv->k;
+    J->doff = C->doff = cv->kind ? cv->doff : NULL;
     if (cv->kind) {
         J->cre = C->cre = -(cv->cre * cv->k);
         J->cim = C->cim = -(cv->cim * cv->k);
@@ -834,6 +835,10 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
     if (rc == ATKB_OK) rc = atkb_event_record(p->tbl_event, stream);
     if (rc != ATKB_OK) return rc;
     p->tbl_event_live = 1;
+    if (cv->doff) {                      /* the int16 offset lives on the device */
+        rc = atkb_pfb_conv_from_offset(tbl_jobs(tb), tbl_carry(tb, p->max_nel), (int)nel, stream);
+        if (rc != ATKB_OK) return rc;
+    }
     if (big) {
         /* the hops through the separate kernels, a chunk at a time; after the
          * upload (which carries a small call's block), before the tile kernel,
@@ -853,6 +858,10 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
         const int work = (int)nel * tiles + (int)nel;
         if (per_hop && !big)
             rc = atkb_pfb_hops(tbl_jobs(tb), tbl_carry(tb, p->max_nel), (int)nel, (int)m, p->d_counters, stream);
+        else if (cv->doff && !big)       /* right after the constants kernel */
+            rc = atkb_pfb_launch_pdl(tbl_jobs(tb), tbl_tiles(tb, p->max_nel), tbl_carry(tb, p->max_nel),
+                                     (int)nel, p->d_counters, p->grid < work ? p->grid : work,
+                                     p->bank.smem_bytes, stream);
         else
             rc = atkb_pfb_launch(tbl_jobs(tb), tbl_tiles(tb, p->max_nel),
                                  tbl_carry(tb, p->max_nel), (int)nel, p->d_counters,
@@ -1046,6 +1055,7 @@ static int unpack_consts(int fmt, float off_re, float off_im, float *cre, float 
 int atkb_raw_conv(int fmt, float off_re, float off_im, conv_t *cv) {
     if (fmt != ATKDSP_FMT_CI16 && fmt != ATKDSP_FMT_CI16Q11) return 0;
     cv->kind = 1;
+    cv->doff = NULL;
     unpack_consts(fmt, off_re, off_im, &cv->cre, &cv->cim, &cv->k);
     return 1;
 }
@@ -1082,15 +1092,14 @@ ATKDSP_API size_t atkdsp_gpu_pfb_w12_scratch_bytes(const atkdsp_pfb *p, size_t n
     return w2_fusable(p) ? ((m + th - 1) / th) * p->nchan * sizeof(double) : 0;
 }
 
-ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_w12(atkdsp_pfb *p, const void *d_in, size_t n, int fmt,
-                                                float off_re, float off_im, atkdsp_cf32 *d_out, size_t cap,
-                                                const uint8_t *d_gate, atkdsp_cf32 *d_R, uint32_t *d_counts,
-                                                float *d_pwr, float *d_mean_pwr, void *d_scratch,
-                                                size_t scratch_bytes, void *stream) {
+static ptrdiff_t process_w12(atkdsp_pfb *p, const void *d_in, size_t n, int fmt, float off_re, float off_im,
+                             const double *d_off, atkdsp_cf32 *d_out, size_t cap, const uint8_t *d_gate,
+                             atkdsp_cf32 *d_R, uint32_t *d_counts, float *d_pwr, float *d_mean_pwr,
+                             void *d_scratch, size_t scratch_bytes, void *stream) {
     conv_t cv = CONV_CF32;
     if (!p || (n && !d_in)) return ATKDSP_E_ARG;
     if (fmt != ATKDSP_FMT_CF32 && !raw_conv(fmt, off_re, off_im, &cv)) return ATKDSP_E_ARG;
-    if (fmt == ATKDSP_FMT_CF32 && (off_re != 0.0f || off_im != 0.0f)) return ATKDSP_E_ARG;
+    if (fmt == ATKDSP_FMT_CF32 && (off_re != 0.0f || off_im != 0.0f || d_off)) return ATKDSP_E_ARG;
     if (n && ((size_t)d_in & (fmt == ATKDSP_FMT_CF32 ? 7 : 3))) return ATKDSP_E_ARG;
     if ((d_R == NULL) != (d_counts == NULL)) return ATKDSP_E_ARG;
     if ((size_t)p->lc + n >= ((size_t)1 << 62)) return ATKDSP_E_ARG;
@@ -1106,6 +1115,7 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_w12(atkdsp_pfb *p, const void *d_in,
     const void *ins[1];
     ins[0] = d_in;
     p->w2_next = (fused && m > 0) ? (double *)d_scratch : NULL;
+    cv.doff = d_off;
     int rc = run_step(p, 1, ins, n, d_out, m, m, st, &cv);
     p->w2_next = NULL;
     if (rc == ATKB_OK) {
@@ -1119,6 +1129,28 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_w12(atkdsp_pfb *p, const void *d_in,
         }
     }
     return rc == ATKB_OK ? (ptrdiff_t)m : map_rc(rc);
+}
+
+ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_w12(atkdsp_pfb *p, const void *d_in, size_t n, int fmt,
+                                                float off_re, float off_im, atkdsp_cf32 *d_out, size_t cap,
+                                                const uint8_t *d_gate, atkdsp_cf32 *d_R, uint32_t *d_counts,
+                                                float *d_pwr, float *d_mean_pwr, void *d_scratch,
+                                                size_t scratch_bytes, void *stream) {
+    return process_w12(p, d_in, n, fmt, off_re, off_im, NULL, d_out, cap, d_gate, d_R, d_counts, d_pwr,
+                       d_mean_pwr, d_scratch, scratch_bytes, stream);
+}
+
+/* the same with the int16 offset in device memory (the previous block's
+ * atkdsp_gpu_block_mean output, rounded to float on the device): a running
+ * DC estimate that never visits the host */
+ATKDSP_API ptrdiff_t atkdsp_gpu_pfb_process_w12_dev(atkdsp_pfb *p, const void *d_in, size_t n, int fmt,
+                                                    const double *d_offset, atkdsp_cf32 *d_out, size_t cap,
+                                                    const uint8_t *d_gate, atkdsp_cf32 *d_R,
+                                                    uint32_t *d_counts, float *d_pwr, float *d_mean_pwr,
+                                                    void *d_scratch, size_t scratch_bytes, void *stream) {
+    if (!d_offset || ((size_t)d_offset & 7) || fmt == ATKDSP_FMT_CF32) return ATKDSP_E_ARG;
+    return process_w12(p, d_in, n, fmt, 0.0f, 0.0f, d_offset, d_out, cap, d_gate, d_R, d_counts, d_pwr,
+                       d_mean_pwr, d_scratch, scratch_bytes, stream);
 }
 
 /* ============================================ per-thread scratch for host calls
@@ -1345,7 +1377,7 @@ static ptrdiff_t unpack_host(const void *raw, size_t nbytes, int fmt, atkdsp_cf3
     if (rc == ATKB_OK && pole) rc = atkb_h2d(d_mean + 2, dc_state, sizeof(atkdsp_cf32), s->stream);
     if (rc == ATKB_OK)
         rc = atkb_unpack(d, fmt, n, d + rb, cre, cim, k, off_re, off_im, want_mean ? d_mean : NULL,
-                         (double *)(d + rb + ob), NULL, s->stream);
+                         (double *)(d + rb + ob), NULL, NULL, s->stream);
     if (rc == ATKB_OK && pole) rc = atkb_dc_pole(d + rb, n, dc_alpha, d_mean + 2, s->stream);
     if (rc == ATKB_OK) rc = atkb_d2h(out, d + rb, n * sizeof(atkdsp_cf32), s->stream);
     if (rc == ATKB_OK && want_mean) rc = atkb_d2h(hm, d_mean, sizeof hm, s->stream);
@@ -1413,7 +1445,8 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_unpack_dc(const void *d_raw, size_t nbytes, int 
         const int rc = gpu_partials(&part, &done, stream);
         if (rc != ATKB_OK) return map_rc(rc);
     }
-    const int rc = atkb_unpack(d_raw, fmt, n, d_out, cre, cim, k, off_re, off_im, d_mean, part, done, stream);
+    const int rc = atkb_unpack(d_raw, fmt, n, d_out, cre, cim, k, off_re, off_im, d_mean, part, done, NULL,
+                               stream);
     return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
 }
 
@@ -1446,7 +1479,25 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_block_mean(const void *d_raw, size_t nbytes, int
     unsigned *done = NULL;
     int rc = gpu_partials(&part, &done, stream);
     if (rc == ATKB_OK)
-        rc = atkb_unpack(d_raw, fmt, n, NULL, cre, cim, k, off_re, off_im, d_mean, part, done, stream);
+        rc = atkb_unpack(d_raw, fmt, n, NULL, cre, cim, k, off_re, off_im, d_mean, part, done, NULL, stream);
+    return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
+}
+
+/* atkdsp_gpu_block_mean with the offset in device memory (two doubles,
+ * rounded to float on the device; d_offset may equal d_mean) */
+ATKDSP_API ptrdiff_t atkdsp_gpu_block_mean_dev(const void *d_raw, size_t nbytes, int fmt, const double *d_offset,
+                                               double *d_mean, void *stream) {
+    if (!d_raw || !d_mean || !d_offset || ((size_t)d_offset & 7)) return ATKDSP_E_ARG;
+    const int bps = atkdsp_bytes_per_sample(fmt);
+    if (!bps || !aligned_for(d_raw, fmt)) return ATKDSP_E_ARG;
+    float cre, cim, k;
+    unpack_consts(fmt, 0.0f, 0.0f, &cre, &cim, &k);
+    const size_t n = nbytes / (size_t)bps;
+    double *part = NULL;
+    unsigned *done = NULL;
+    int rc = gpu_partials(&part, &done, stream);
+    if (rc == ATKB_OK)
+        rc = atkb_unpack(d_raw, fmt, n, NULL, cre, cim, k, 0.0f, 0.0f, d_mean, part, done, d_offset, stream);
     return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
 }
 
@@ -1460,7 +1511,7 @@ ATKDSP_API ptrdiff_t atkdsp_gpu_unpack(const void *d_raw, size_t nbytes, int fmt
     unpack_consts(fmt, 0.0f, 0.0f, &cre, &cim, &k);
     size_t n = nbytes / (size_t)bps;
     if (n > out_cap) n = out_cap;
-    int rc = atkb_unpack(d_raw, fmt, n, d_out, cre, cim, k, 0.0f, 0.0f, NULL, NULL, NULL, stream);
+    int rc = atkb_unpack(d_raw, fmt, n, d_out, cre, cim, k, 0.0f, 0.0f, NULL, NULL, NULL, NULL, stream);
     if (rc == ATKB_OK && dc_alpha > 0.0f && d_dc_state) rc = atkb_dc_pole(d_out, n, dc_alpha, d_dc_state, stream);
     return rc == ATKB_OK ? (ptrdiff_t)n : map_rc(rc);
 }

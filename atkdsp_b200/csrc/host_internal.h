@@ -94,6 +94,8 @@ struct atkdsp_pfb {
 typedef struct {
     int kind;                     /* 0 cf32, 1 int16 pairs */
     float cre, cim, k;
+    const double *doff;           /* int16: the offset in device memory, or NULL
+                                   * (then cre / cim hold it) */
 } conv_t;
 
 extern const conv_t ATKB_CONV_CF32;

@@ -102,6 +102,12 @@ typedef struct {
     double *w2;                   /* device, or NULL: the fused W2 partials, one
                                    * row of nchan doubles per tile of the job
                                    * (power-of-two nchan <= 2048 banks only) */
+    const double *doff;           /* device, or NULL: the int16 offset (two
+                                   * doubles, rounded to float); when set,
+                                   * cre/cim are derived from it on the device
+                                   * as atkb_job_conv does on the host (the
+                                   * table by atkb_pfb_conv_from_offset, the
+                                   * large-filterbank fold by itself) */
 } atkb_job;
 
 /* ---- state carry: dst[0, len) = s[from, from + len) -------------------- */
@@ -116,6 +122,7 @@ typedef struct {
     float cre, cim, kscale;
     long long nsrc;               /* samples of s there are (head + n)       */
     long long cap;                /* capacity of dst in samples              */
+    const double *doff;           /* as atkb_job                             */
 } atkb_carry;
 
 /* ---- the tile kernel's fault word (counters[ATKB_FAULT_WORD]) -------------
@@ -198,6 +205,11 @@ int  atkb_pfb_launch(const atkb_job *d_jobs, const int *d_tile_start, const atkb
 int  atkb_pfb_launch_n(const atkb_job *d_jobs, const int *d_tile_start, const atkb_carry *d_carry,
                        int njobs_max, const int *d_njobs, int *d_counters, int grid, int smem_bytes,
                        void *stream);
+/* atkb_pfb_launch as a programmatic dependent of the kernel before it on the
+ * stream (which triggers early; the tile kernel waits for its completion
+ * before reading the tables) */
+int  atkb_pfb_launch_pdl(const atkb_job *d_jobs, const int *d_tile_start, const atkb_carry *d_carry,
+                         int njobs, int *d_counters, int grid, int smem_bytes, void *stream);
 int  atkb_event_query(void *ev);        /* ATKB_OK when complete, 1 when pending */
 int  atkb_event_spin(void *ev);         /* wait for an event by polling it */
 /* large filterbanks (plan.big: nchan beyond one CTA's shared memory): hops
@@ -217,6 +229,10 @@ int  atkb_pfb_debug_build(void);
 int  atkb_pfb_hops(const atkb_job *d_jobs, const atkb_carry *d_carry, int njobs, int m, int *d_counters,
                    void *stream);
 int  atkb_pfb_hops_ok(const atkb_bank *B);
+/* the int16 constants of nel device jobs and carries whose doff is set, from
+ * that device-held offset (after the table upload, before the tile kernel) */
+int  atkb_pfb_conv_from_offset(atkb_job *d_jobs, atkb_carry *d_carry, int nel, void *stream);
+
 int  atkb_pfb_big(const atkb_job *J, const atkb_bank *B, long long h0, int nh, void *scratch, int grid,
                   void *stream);
 
@@ -360,11 +376,13 @@ int  atkb_cfar_gather(const double *X, const double *noise, long long nbins, int
  * when d_mean != NULL, using d_partial (>= 2 * atkb_unpack_partials(n)
  * doubles) as scratch. d_done (may be NULL): a device counter that is 0
  * between calls; with it the unpack launch's last block computes the mean
- * (no second launch) and puts the counter back to 0. */
+ * (no second launch) and puts the counter back to 0. d_off (may be NULL): the
+ * offset as two doubles in device memory, rounded to float and turned into
+ * the constants on the device (cre, cim, off_re, off_im are then unused). */
 int  atkb_unpack_partials(size_t n);
 int  atkb_unpack(const void *raw, int fmt, size_t n, void *out, float cre, float cim, float k,
                  float off_re, float off_im, double *d_mean, double *d_partial, unsigned *d_done,
-                 void *stream);
+                 const double *d_off, void *stream);
 /* the same conversion and mean with the partial sums in a static device
  * array instead of caller scratch; at most atkb_unpack_noalloc_max_samples()
  * samples per call (ATKB_E_ARG beyond) */

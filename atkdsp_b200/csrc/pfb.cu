@@ -183,6 +183,14 @@ struct Src {
     }
 };
 
+/* The int16 constants from an offset held in device memory (a job's or a
+ * carry's doff): atkb_job_conv's -((off / k) * k), off the double rounded to
+ * float, by the same IEEE float operations as the host. */
+__device__ __forceinline__ void doff_consts(const double *doff, float k, float &cre, float &cim) {
+    cre = -__fmul_rn(__fdiv_rn(__double2float_rn(__ldg(doff)), k), k);
+    cim = -__fmul_rn(__fdiv_rn(__double2float_rn(__ldg(doff + 1)), k), k);
+}
+
 /* ---- fast path: nchan = 2^n, 16 <= nchan <= 4096 ------------------------- */
 /* Shared-memory index swizzle for the 16-byte complex doubles: the low LOGP
  * index bits are XORed with the next LOGP. The first pass stores at a stride
@@ -1282,6 +1290,10 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
                  const atkb_carry *__restrict__ carries, int njobs, const int *__restrict__ d_njobs,
                  int *counters) {
     extern __shared__ double2 sm[];
+    /* launched as a programmatic dependent of the kernel that fills the job
+     * table (atkb_pfb_launch_pdl): wait for it before the first read; a no-op
+     * for an ordinary launch */
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if (d_njobs) njobs = min(njobs, *d_njobs);      /* a server round: count set per launch */
     unsigned dyn_smem;
     asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_smem));
@@ -1397,7 +1409,9 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
 __global__ void __launch_bounds__(256)
 big_fold_kernel(const atkb_job J, const float *__restrict__ taps, int M, int K, int hop, long long h0, int nh,
                 double2 *__restrict__ F) {
-    const Src src{(const float2 *)J.state, J.in, J.head, J.in_kind, J.cre, J.cim, J.kscale};
+    float cre = J.cre, cim = J.cim;
+    if (J.doff) doff_consts(J.doff, J.kscale, cre, cim);
+    const Src src{(const float2 *)J.state, J.in, J.head, J.in_kind, cre, cim, J.kscale};
     const long long total = (long long)nh * M;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
@@ -1685,6 +1699,31 @@ extern "C" int atkb_pfb_launch_n(const atkb_job *d_jobs, const int *d_tile_start
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }
 
+/* atkb_pfb_launch as a programmatic dependent launch: its CTAs may start
+ * while the previous kernel on the stream (conv_from_offset_kernel) runs,
+ * and wait for that kernel's completion before reading the table */
+extern "C" int atkb_pfb_launch_pdl(const atkb_job *d_jobs, const int *d_tile_start, const atkb_carry *d_carry,
+                                   int njobs, int *d_counters, int grid, int smem_bytes, void *stream) {
+    if (njobs <= 0) return ATKB_OK;
+    if (grid < 1) grid = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = (size_t)smem_bytes;
+    cfg.stream = (cudaStream_t)stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const int *no_count = nullptr;
+    atkb_range_push("atkdsp tile kernel launch");
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, pfb_tiles_kernel, d_jobs, d_tile_start, d_carry, njobs, no_count,
+                                             d_counters);
+    atkb_range_pop();
+    return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
 extern "C" long long atkb_pfb_big_hops(int nchan) {
     const long long h = (1LL << 20) / nchan;
     return h < 1 ? 1 : h;
@@ -1709,6 +1748,27 @@ extern "C" int atkb_pfb_big(const atkb_job *J, const atkb_bank *B, long long h0,
     }
     big_out_kernel<<<grid, 256, 0, st>>>(cur, *J, (const double2 *)B->twd, M, B->os, B->hop, h0, nh);
     atkb_range_pop();
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
+/* The constants of nel device jobs (and their carries) whose int16 offset
+ * lives in device memory, written into the job table after its upload and
+ * before the tile kernel reads it: the tile kernel itself stays unchanged. */
+__global__ void conv_from_offset_kernel(atkb_job *jobs, atkb_carry *carries, int nel) {
+    /* let the tile kernel launch now: it waits for this grid's completion
+     * (griddepcontrol.wait) before it reads the table */
+    asm volatile("griddepcontrol.launch_dependents;");
+    const int e = threadIdx.x;
+    if (e >= nel || !jobs[e].doff) return;
+    float cre, cim;
+    doff_consts(jobs[e].doff, jobs[e].kscale, cre, cim);
+    jobs[e].cre = carries[e].cre = cre;
+    jobs[e].cim = carries[e].cim = cim;
+}
+
+extern "C" int atkb_pfb_conv_from_offset(atkb_job *d_jobs, atkb_carry *d_carry, int nel, void *stream) {
+    if (nel < 1 || nel > 1024) return ATKB_E_ARG;
+    conv_from_offset_kernel<<<1, nel, 0, (cudaStream_t)stream>>>(d_jobs, d_carry, nel);
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }
 

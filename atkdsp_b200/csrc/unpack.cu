@@ -58,6 +58,25 @@ __device__ __forceinline__ float2 convert_one(const void *raw, int fmt, size_t i
     return make_float2(__fmul_rn(__fsub_rn(a, cre), k), __fmul_rn(__fsub_rn(b, cim), k));
 }
 
+/* With the offset in device memory (the previous block's mean, rounded to
+ * float as a host caller would round it): the same constants unpack_consts
+ * computes on the host, by the same IEEE float operations. */
+__device__ __forceinline__ void offset_consts(const double *doff, int fmt, float k, float &cre, float &cim,
+                                              float &offr, float &offi) {
+    offr = __double2float_rn(__ldg(doff));
+    offi = __double2float_rn(__ldg(doff + 1));
+    if (fmt == 4) {
+        cre = offr;
+        cim = offi;
+    } else if (fmt == 0) {
+        cre = __fadd_rn(127.5f, __fdiv_rn(offr, k));
+        cim = __fadd_rn(127.5f, __fdiv_rn(offi, k));
+    } else {
+        cre = __fdiv_rn(offr, k);
+        cim = __fdiv_rn(offi, k);
+    }
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -143,7 +162,8 @@ __device__ __forceinline__ void block_partial(double sr, double si, double *part
 __global__ void __launch_bounds__(UNPACK_NT)
 unpack_kernel(const void *__restrict__ raw, int fmt, size_t n, float2 *__restrict__ out, float cre,
               float cim, float k, float offr, float offi, double *__restrict__ partial, double *mean,
-              unsigned *done) {
+              unsigned *done, const double *doff) {
+    if (doff) offset_consts(doff, fmt, k, cre, cim, offr, offi);
     double sr = 0.0, si = 0.0;
     const size_t stride = (size_t)gridDim.x * UNPACK_NT;
     for (size_t i = (size_t)blockIdx.x * UNPACK_NT + threadIdx.x; i < n; i += stride) {
@@ -185,7 +205,9 @@ __device__ __forceinline__ void load4(const void *raw, size_t q, float (&a)[4], 
 template <int FMT>
 __global__ void __launch_bounds__(UNPACK_NT)
 unpack_kernel_v4(const void *__restrict__ raw, size_t n, float2 *__restrict__ out, float cre, float cim, float k,
-                 float offr, float offi, double *__restrict__ partial, double *mean, unsigned *done) {
+                 float offr, float offi, double *__restrict__ partial, double *mean, unsigned *done,
+                 const double *doff) {
+    if (doff) offset_consts(doff, FMT, k, cre, cim, offr, offi);
     double sr = 0.0, si = 0.0;
     const size_t nq = n >> 2;
     const size_t stride = (size_t)gridDim.x * UNPACK_NT;
@@ -228,24 +250,29 @@ unpack_kernel_v4(const void *__restrict__ raw, size_t n, float2 *__restrict__ ou
  * done (with partial and mean) fuses the mean into the launch. */
 void launch_unpack(const void *raw, int fmt, size_t n, float2 *out, float cre, float cim, float k, float offr,
                    float offi, double *partial, int nb, cudaStream_t s, double *mean = nullptr,
-                   unsigned *done = nullptr) {
+                   unsigned *done = nullptr, const double *doff = nullptr) {
     const bool v4 = ((uintptr_t)raw & 15) == 0 && ((uintptr_t)out & 15) == 0 && fmt >= 0 && fmt <= 4;
     if (!v4) {
-        unpack_kernel<<<nb, UNPACK_NT, 0, s>>>(raw, fmt, n, out, cre, cim, k, offr, offi, partial, mean, done);
+        unpack_kernel<<<nb, UNPACK_NT, 0, s>>>(raw, fmt, n, out, cre, cim, k, offr, offi, partial, mean, done,
+                                               doff);
         return;
     }
     switch (fmt) {
-    case 0: unpack_kernel_v4<0><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done); break;
-    case 1: unpack_kernel_v4<1><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done); break;
-    case 2: unpack_kernel_v4<2><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done); break;
-    case 3: unpack_kernel_v4<3><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done); break;
-    default: unpack_kernel_v4<4><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done); break;
+    case 0: unpack_kernel_v4<0><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done, doff); break;
+    case 1: unpack_kernel_v4<1><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done, doff); break;
+    case 2: unpack_kernel_v4<2><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done, doff); break;
+    case 3: unpack_kernel_v4<3><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done, doff); break;
+    default: unpack_kernel_v4<4><<<nb, UNPACK_NT, 0, s>>>(raw, n, out, cre, cim, k, offr, offi, partial, mean, done, doff); break;
     }
 }
 
 __global__ void __launch_bounds__(UNPACK_NT)
 unpack_mean_kernel(const double *__restrict__ partial, int nblocks, size_t n, float offr, float offi,
-                   double *__restrict__ mean) {
+                   double *__restrict__ mean, const double *doff) {
+    if (doff) {
+        offr = __double2float_rn(__ldg(doff));
+        offi = __double2float_rn(__ldg(doff + 1));
+    }
     mean_finish(partial, nblocks, n, offr, offi, mean);
 }
 
@@ -286,28 +313,31 @@ extern "C" int atkb_unpack_partials(size_t n) {
 
 extern "C" int atkb_unpack(const void *raw, int fmt, size_t n, void *out, float cre, float cim,
                            float k, float off_re, float off_im, double *d_mean, double *d_partial,
-                           unsigned *d_done, void *stream) {
+                           unsigned *d_done, const double *d_off, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
     const int nb = atkb_unpack_partials(n);
     if (n) {
-        if (fmt == 4 && off_re == 0.0f && off_im == 0.0f && !d_mean) {
+        if (fmt == 4 && off_re == 0.0f && off_im == 0.0f && !d_mean && !d_off) {
             if (out && out != raw &&
                 cudaMemcpyAsync(out, raw, n * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
                 return ATKB_E_KERNEL;
         } else {
             launch_unpack(raw, fmt, n, (float2 *)out, cre, cim, k, off_re, off_im, d_mean ? d_partial : nullptr,
-                          nb, s, d_mean, d_mean ? d_done : nullptr);
+                          nb, s, d_mean, d_mean ? d_done : nullptr, d_off);
         }
     }
     if (d_mean) {
-        if (!n) {
+        if (!n && d_off) {
+            /* the mean of nothing is the offset: the kernel reads no partial */
+            unpack_mean_kernel<<<1, UNPACK_NT, 0, s>>>(d_partial, 0, 0, off_re, off_im, d_mean, d_off);
+        } else if (!n) {
             /* the reference: inv = 0, so the mean is the offset itself */
             const double z[2] = {(double)off_re, (double)off_im};
             if (cudaMemcpyAsync(d_mean, z, sizeof z, cudaMemcpyHostToDevice, s) != cudaSuccess)
                 return ATKB_E_KERNEL;
             if (cudaStreamSynchronize(s) != cudaSuccess) return ATKB_E_KERNEL;
         } else if (!d_done) {               /* with d_done the unpack launch computed it */
-            unpack_mean_kernel<<<1, UNPACK_NT, 0, s>>>(d_partial, nb, n, off_re, off_im, d_mean);
+            unpack_mean_kernel<<<1, UNPACK_NT, 0, s>>>(d_partial, nb, n, off_re, off_im, d_mean, d_off);
         }
     }
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
@@ -387,6 +417,6 @@ extern "C" int atkb_unpack_noalloc(const void *raw, int fmt, size_t n, void *out
         }
     }
     /* with n == 0 the mean kernel reads no partial and writes the offset */
-    if (d_mean) unpack_mean_kernel<<<1, UNPACK_NT, 0, s>>>(part, n ? nb : 0, n, off_re, off_im, d_mean);
+    if (d_mean) unpack_mean_kernel<<<1, UNPACK_NT, 0, s>>>(part, n ? nb : 0, n, off_re, off_im, d_mean, nullptr);
     return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }

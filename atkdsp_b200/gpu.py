@@ -83,7 +83,9 @@ def process_w12(p: Pfb, x: torch.Tensor, fmt="cf32", offset: complex = 0j, out: 
                 stream=None) -> torch.Tensor:
     """atkdsp_gpu_pfb_process_w12: one element's block through the filterbank
     with W1 / W2 fused into its epilogue. x: complex64 samples (fmt "cf32") or
-    int16 I/Q pairs (fmt "ci16" / "ci16q11"). Returns (1, nchan, m)."""
+    int16 I/Q pairs (fmt "ci16" / "ci16q11"). offset: a complex, or a (2,)
+    float64 CUDA tensor holding it on the device (a block_mean output: the
+    _dev entry point, no host round trip). Returns (1, nchan, m)."""
     lib = load()
     n = int(x.numel()) if x.dtype == torch.complex64 else int(x.numel()) // 2
     m = p.out_hops(n)
@@ -92,10 +94,17 @@ def process_w12(p: Pfb, x: torch.Tensor, fmt="cf32", offset: complex = 0j, out: 
     need = int(lib.atkdsp_gpu_pfb_w12_scratch_bytes(p.handle, n))
     if scratch is None or scratch.numel() * scratch.element_size() < need:
         scratch = torch.empty(max(need, 8), dtype=torch.uint8, device=x.device)
-    got = lib.atkdsp_gpu_pfb_process_w12(p.handle, _ptr(x), n, _fmt(fmt), float(offset.real), float(offset.imag),
-                                         _ptr(out), out.numel(), _ptr(gate), _ptr(R), _ptr(counts), _ptr(pwr),
-                                         _ptr(mean_pwr), _ptr(scratch), scratch.numel() * scratch.element_size(),
-                                         _stream(stream))
+    if isinstance(offset, torch.Tensor):
+        _check_offset(offset)
+        got = lib.atkdsp_gpu_pfb_process_w12_dev(p.handle, _ptr(x), n, _fmt(fmt), _ptr(offset), _ptr(out),
+                                                 out.numel(), _ptr(gate), _ptr(R), _ptr(counts), _ptr(pwr),
+                                                 _ptr(mean_pwr), _ptr(scratch),
+                                                 scratch.numel() * scratch.element_size(), _stream(stream))
+    else:
+        got = lib.atkdsp_gpu_pfb_process_w12(p.handle, _ptr(x), n, _fmt(fmt), float(offset.real),
+                                             float(offset.imag), _ptr(out), out.numel(), _ptr(gate), _ptr(R),
+                                             _ptr(counts), _ptr(pwr), _ptr(mean_pwr), _ptr(scratch),
+                                             scratch.numel() * scratch.element_size(), _stream(stream))
     _check(int(got), "gpu_pfb_process_w12")
     return out[: p.nchan * got].view(1, p.nchan, got)
 
@@ -132,13 +141,25 @@ def unpack(raw: torch.Tensor, fmt, dc_alpha: float = 0.0, dc_state: torch.Tensor
 
 def block_mean(raw: torch.Tensor, fmt, offset: complex = 0j, mean: torch.Tensor | None = None,
                stream=None) -> torch.Tensor:
-    """atkdsp_gpu_block_mean: the unpack_dc mean of a raw block, (2,) float64."""
+    """atkdsp_gpu_block_mean: the unpack_dc mean of a raw block, (2,) float64.
+    offset: a complex, or a (2,) float64 CUDA tensor (atkdsp_gpu_block_mean_dev;
+    it may be ``mean`` itself)."""
     if mean is None:
         mean = torch.empty(2, dtype=torch.float64, device=raw.device)
-    _check(int(load().atkdsp_gpu_block_mean(_ptr(raw), raw.numel() * raw.element_size(), _fmt(fmt),
-                                            float(offset.real), float(offset.imag), _ptr(mean),
-                                            _stream(stream))), "gpu_block_mean")
+    if isinstance(offset, torch.Tensor):
+        _check_offset(offset)
+        got = load().atkdsp_gpu_block_mean_dev(_ptr(raw), raw.numel() * raw.element_size(), _fmt(fmt),
+                                               _ptr(offset), _ptr(mean), _stream(stream))
+    else:
+        got = load().atkdsp_gpu_block_mean(_ptr(raw), raw.numel() * raw.element_size(), _fmt(fmt),
+                                           float(offset.real), float(offset.imag), _ptr(mean), _stream(stream))
+    _check(int(got), "gpu_block_mean")
     return mean
+
+
+def _check_offset(offset: torch.Tensor) -> None:
+    if offset.dtype != torch.float64 or offset.numel() != 2 or not offset.is_cuda or not offset.is_contiguous():
+        raise AtkDspError("a device offset is a contiguous (2,) float64 CUDA tensor (re, im)")
 
 
 def accumulate(out: torch.Tensor, nel: int, nchan: int, R: torch.Tensor | None,

@@ -102,6 +102,21 @@ ATKDSP_API ptrdiff_t   atkdsp_gpu_pfb_process_w12(atkdsp_pfb *p, const void *d_i
  * receives 2 doubles (device). Returns the sample count. */
 ATKDSP_API ptrdiff_t   atkdsp_gpu_block_mean(const void *d_raw, size_t nbytes, int fmt, float off_re,
                                              float off_im, double *d_mean, void *stream);
+/* The running DC estimate kept on the device: atkdsp_gpu_block_mean and
+ * atkdsp_gpu_pfb_process_w12 with the offset read from device memory --
+ * d_offset holds two doubles (typically the previous block's d_mean), each
+ * rounded to float on the device exactly as a host caller rounds the mean it
+ * read back, so the results equal the host-offset calls' bit for bit. No
+ * host round trip per block. block_mean_dev accepts d_offset == d_mean;
+ * process_w12_dev takes the int16 formats only. */
+ATKDSP_API ptrdiff_t   atkdsp_gpu_block_mean_dev(const void *d_raw, size_t nbytes, int fmt,
+                                                 const double *d_offset, double *d_mean, void *stream);
+ATKDSP_API ptrdiff_t   atkdsp_gpu_pfb_process_w12_dev(atkdsp_pfb *p, const void *d_in, size_t n, int fmt,
+                                                      const double *d_offset, atkdsp_cf32 *d_out,
+                                                      size_t cap, const uint8_t *d_gate,
+                                                      atkdsp_cf32 *d_R, uint32_t *d_counts,
+                                                      float *d_pwr, float *d_mean_pwr, void *d_scratch,
+                                                      size_t scratch_bytes, void *stream);
 /* atkdsp_unpack (reference include/atkdsp.h:252) on device buffers;
  * d_dc_state is one device cf32, read and updated when dc_alpha > 0. */
 ATKDSP_API ptrdiff_t   atkdsp_gpu_unpack(const void *d_raw, size_t nbytes, int fmt,
