@@ -7,7 +7,7 @@
  * Subtract and multiply are __fsub_rn / __fmul_rn so nvcc cannot fuse them:
  * the samples are bit-identical to the reference's. With 16-byte aligned
  * buffers every thread converts four samples per step with 16-byte loads and
- * stores (unpack_kernel_v4), two steps in flight. The mean of the samples
+ * stores (unpack_kernel_v4), four steps in flight, one wave of blocks. The mean of the samples
  * BEFORE the offset came out is sum(double(out)) / n + off; the double sum
  * is a two-stage deterministic reduction (per-block partials, then one
  * block), so it agrees with the reference's eight-way serial sum to ~1e-16.
@@ -26,6 +26,18 @@
 #define UNPACK_NT 256
 #define UNPACK_PER_THREAD 8
 #define UNPACK_MAX_BLOCKS 2048
+/* one wave on a B200: 148 SMs x UNPACK_MINB resident blocks of 256 threads (the v4
+ * kernel's launch bounds); more blocks would leave a partial second wave */
+#ifndef UNPACK_MINB
+#define UNPACK_MINB 4
+#endif
+#ifndef UNPACK_GRID_MAX
+#define UNPACK_GRID_MAX (148 * UNPACK_MINB)
+#endif
+/* 16-byte loads in flight per thread in the v4 kernel */
+#ifndef UNPACK_STEPS
+#define UNPACK_STEPS 4
+#endif
 
 namespace {
 
@@ -86,9 +98,11 @@ __device__ __forceinline__ double warp_sum(double v) {
 /* The mean from the blocks' partial sums, by one block of UNPACK_NT threads:
  * thread t adds partials t, t + UNPACK_NT, ... in order, then the warps and
  * the warp sums reduce in a fixed order. The loads bypass L1: in the fused
- * form the partials were written by other blocks of the same launch. */
-__device__ void mean_finish(const double *partial, int nblocks, size_t n, float offr, float offi,
-                            double *mean) {
+ * form the partials were written by other blocks of the same launch. Not
+ * inlined: its eight loads in flight would otherwise raise the register
+ * count of the whole conversion kernel. */
+__device__ __noinline__ void mean_finish(const double *partial, int nblocks, size_t n, float offr, float offi,
+                                         double *mean) {
     __shared__ double red[2][UNPACK_NT / 32];
     double sr = 0.0, si = 0.0;
     /* eight partials in flight per thread; past the last block +0.0, which
@@ -176,7 +190,7 @@ unpack_kernel(const void *__restrict__ raw, int fmt, size_t n, float2 *__restric
 }
 
 /* The same conversion and partial sums with 16-byte accesses: four samples
- * per thread and step (two steps in flight), for raw and out 16-byte
+ * per thread and step (UNPACK_STEPS steps in flight), for raw and out 16-byte
  * aligned; the last n % 4 samples by the first threads of block 0 after.
  * Each sample is converted exactly as convert_one does; only the order of
  * the per-thread double sums differs from unpack_kernel. */
@@ -203,7 +217,7 @@ __device__ __forceinline__ void load4(const void *raw, size_t q, float (&a)[4], 
 }
 
 template <int FMT>
-__global__ void __launch_bounds__(UNPACK_NT)
+__global__ void __launch_bounds__(UNPACK_NT, UNPACK_MINB)
 unpack_kernel_v4(const void *__restrict__ raw, size_t n, float2 *__restrict__ out, float cre, float cim, float k,
                  float offr, float offi, double *__restrict__ partial, double *mean, unsigned *done,
                  const double *doff) {
@@ -212,14 +226,14 @@ unpack_kernel_v4(const void *__restrict__ raw, size_t n, float2 *__restrict__ ou
     const size_t nq = n >> 2;
     const size_t stride = (size_t)gridDim.x * UNPACK_NT;
     const bool copy = FMT == 4 && offr == 0.0f && offi == 0.0f;
-    for (size_t q0 = (size_t)blockIdx.x * UNPACK_NT + threadIdx.x; q0 < nq; q0 += 2 * stride) {
-        float a[2][4], b[2][4];
-        const bool two = q0 + stride < nq;
-        load4<FMT>(raw, q0, a[0], b[0]);
-        if (two) load4<FMT>(raw, q0 + stride, a[1], b[1]);
+    for (size_t q0 = (size_t)blockIdx.x * UNPACK_NT + threadIdx.x; q0 < nq; q0 += UNPACK_STEPS * stride) {
+        float a[UNPACK_STEPS][4], b[UNPACK_STEPS][4];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            if (h == 1 && !two) break;
+        for (int h = 0; h < UNPACK_STEPS; ++h)
+            if (q0 + h * stride < nq) load4<FMT>(raw, q0 + h * stride, a[h], b[h]);
+#pragma unroll
+        for (int h = 0; h < UNPACK_STEPS; ++h) {
+            if (q0 + h * stride >= nq) break;
             float2 y[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
@@ -307,7 +321,7 @@ __global__ void dc_pole_kernel(float *__restrict__ x, size_t n, float alpha, flo
 extern "C" int atkb_unpack_partials(size_t n) {
     size_t b = (n + (size_t)UNPACK_NT * UNPACK_PER_THREAD - 1) / ((size_t)UNPACK_NT * UNPACK_PER_THREAD);
     if (b < 1) b = 1;
-    if (b > UNPACK_MAX_BLOCKS) b = UNPACK_MAX_BLOCKS;
+    if (b > UNPACK_GRID_MAX) b = UNPACK_GRID_MAX;
     return (int)b;
 }
 
