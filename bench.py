@@ -375,8 +375,27 @@ def _plain_arm(args, specs, sets, outs, torch, device, barrier, max_over_ranks):
     barrier()
     t = max_over_ranks(_timed(st, torch, step, args.steps))
     barrier()
+    # where one call per stream loses: one more pass with each call bracketed
+    # by events on its stream, grouped by the stream's length (log2 bucket)
+    evs = []
+    for p, x, o in zip(handles, sets[0][1], outs):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        gpu.process_n(p, [x], 1, out=o, stream=st)
+        e1.record(st)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    buckets: dict = {}
+    for sp, (e0, e1) in zip(specs, evs):
+        b = buckets.setdefault(int(math.log2(sp.length)), [0, 0, 0.0])
+        b[0] += 1
+        b[1] += sp.length
+        b[2] += e0.elapsed_time(e1)
+    by_len = [{"log2_length": k, "streams": v[0], "samples": v[1], "ms": round(v[2], 4),
+               "msps": round(v[1] / v[2] / 1e3, 1), "us_per_call": round(v[2] / v[0] * 1e3, 1)}
+              for k, v in sorted(buckets.items())]
     del handles
-    return t
+    return t, by_len
 
 
 def _e2e_batch_arm(args, S, sets, obuf, bstream, bstep, torch, barrier, max_over_ranks):
@@ -1203,7 +1222,7 @@ def run_ours(args, rep):
     out_bytes = 8 * sum(s.nchan * m for s, m in zip(specs, ms_list))
     extra = {}
     if "plain" in arms:
-        t_plain = _plain_arm(args, specs, sets, outs, torch, device, barrier, max_over_ranks)
+        t_plain, plain_by_len = _plain_arm(args, specs, sets, outs, torch, device, barrier, max_over_ranks)
     t_e2e_batch = None
     if "e2e" in arms:
         t_e2e_batch = _e2e_batch_arm(args, S, sets, obuf, bstream, bstep, torch, barrier, max_over_ranks)
@@ -1260,7 +1279,8 @@ def run_ours(args, rep):
         "config": dict(_config(args, world), samples_per_step_per_gpu=S),
         "plain": None if t_plain is None else {
             "value": round(total * args.steps / t_plain / 1e6, 2), "unit": "MSamples/s",
-            "what": "one device-pointer call per stream"},
+            "what": "one device-pointer call per stream",
+            "by_length": plain_by_len},
         "batched_over_plain": None if t_plain is None else round(t_plain / t_batch, 2),
         "e2e": None if t_e2e is None else {
             "value": round(total * args.steps / t_e2e[0] / 1e6, 2), "unit": "MSamples/s",
