@@ -422,7 +422,7 @@ def _e2e_batch_arm(args, S, sets, obuf, bstream, bstep, torch, barrier, max_over
     return t
 
 
-CABI_THREADS = max(1, min(8, os.cpu_count() or 1))
+CABI_THREADS = max(1, min(8, os.cpu_count() or 1))      # --cabi-threads overrides
 
 
 def _cabi_arm(specs, sets, torch, barrier, max_over_ranks, pinned: bool, steps: int, warmup: int):
@@ -1352,11 +1352,16 @@ def main():
     ap.add_argument("--arms", default="batched,plain,e2e,dropin,cpu,single_stream,front_end,coherent_array,"
                     "extractor,scale_bank,spectrum,cfar,served",
                     help="comma list of arms to run (the batched arm always runs)")
+    ap.add_argument("--cabi-threads", type=int, default=0,
+                    help="host threads for the C-ABI (e2e, drop-in) arms; 0: min(8, cores)")
     ap.add_argument("--streams", type=int, default=256)
     ap.add_argument("--min-log2", type=float, default=14.0)
     ap.add_argument("--max-log2", type=float, default=22.0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.cabi_threads > 0:
+        global CABI_THREADS
+        CABI_THREADS = args.cabi_threads
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         sys.exit(_spawn_ranks(args.gpus))
     from atkdsp_b200.replicas import Replicas
