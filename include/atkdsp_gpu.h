@@ -50,9 +50,13 @@ ATKDSP_API ptrdiff_t   atkdsp_gpu_pfb_process_n_raw(atkdsp_pfb *p, const void *c
 
 /* atkdsp_unpack_dc (reference include/atkdsp.h:270) on device buffers. When
  * d_mean is not NULL it receives the two means (re, im) as doubles on the
- * device. d_raw must be aligned to the sample's component size. Uses a
- * per-device scratch area that the library allocates on the first call on
- * each device; calls on one device must not overlap on the GPU. */
+ * device. d_raw must be aligned to the sample's component size. The mean's
+ * partial sums and the counter that lets the launch's last block finish the
+ * mean live in a scratch area of the calling thread on the current device,
+ * allocated by that thread's first such call. One thread's calls with a mean
+ * (this and atkdsp_gpu_block_mean / _dev) must not overlap on the GPU: issue
+ * them on one stream, or order them with events. Calls from different host
+ * threads never share the area. */
 ATKDSP_API ptrdiff_t   atkdsp_gpu_unpack_dc(const void *d_raw, size_t nbytes, int fmt,
                                             atkdsp_cf32 *d_out, size_t out_cap,
                                             float off_re, float off_im, double *d_mean,
@@ -99,7 +103,8 @@ ATKDSP_API ptrdiff_t   atkdsp_gpu_pfb_process_w12(atkdsp_pfb *p, const void *d_i
  * of the samples before the offset (off_re, off_im) is taken out -- without
  * writing the samples: for a caller whose filterbank reads the raw samples
  * (atkdsp_gpu_pfb_process_n_raw) and who keeps a running DC estimate. d_mean
- * receives 2 doubles (device). Returns the sample count. */
+ * receives 2 doubles (device). Returns the sample count. Uses the calling
+ * thread's scratch as atkdsp_gpu_unpack_dc does (the same ordering rule). */
 ATKDSP_API ptrdiff_t   atkdsp_gpu_block_mean(const void *d_raw, size_t nbytes, int fmt, float off_re,
                                              float off_im, double *d_mean, void *stream);
 /* The running DC estimate kept on the device: atkdsp_gpu_block_mean and
