@@ -1363,6 +1363,10 @@ pfb_tiles_kernel(const atkb_job *__restrict__ jobs, const int *__restrict__ tile
         /* the barrier at the top of the loop fences this tile's reads of sm
          * and of its slot from the next tile's writes */
     }
+    /* this CTA's tiles are done: a programmatic dependent (the W2 finish of
+     * atkdsp_gpu_pfb_process_w12) may be scheduled once every CTA is here; it
+     * waits for this grid's completion before it reads anything */
+    asm volatile("griddepcontrol.launch_dependents;");
     /* then the state carries, one job's per claim, the CTA's threads copying
      * s[from, from + len) into the other state buffer (no tile reads it) */
     __shared__ int s_carry;
@@ -1827,6 +1831,8 @@ __global__ void __launch_bounds__(32 * W2F_WARPS)
 w2_finish_kernel(const double *__restrict__ part, int tiles, int M, long long m, const uint8_t *__restrict__ gate,
                  float2 *__restrict__ R, uint32_t *__restrict__ counts, float *__restrict__ pwr,
                  float *__restrict__ mean_pwr) {
+    /* launched as a programmatic dependent of the tile kernel: wait for it */
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     __shared__ double red[W2F_STREAMS][W2F_CH];
     __shared__ double grp[W2F_STREAMS / 8][W2F_CH];
     const int c = threadIdx.x % W2F_CH, sidx = threadIdx.x / W2F_CH;
@@ -1875,7 +1881,19 @@ w2_finish_kernel(const double *__restrict__ part, int tiles, int M, long long m,
 
 extern "C" int atkb_w2_finish(const double *part, int tiles, int nchan, long long m, const uint8_t *gate, void *R,
                               uint32_t *counts, float *pwr, float *mean_pwr, void *stream) {
-    w2_finish_kernel<<<(nchan + W2F_CH - 1) / W2F_CH, 32 * W2F_WARPS, 0, (cudaStream_t)stream>>>(
-        part, tiles, nchan, m, gate, (float2 *)R, counts, pwr, mean_pwr);
-    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+    /* a programmatic dependent of the tile kernel launched just before it on
+     * the stream: its launch overlaps that kernel's last tiles and carries */
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((nchan + W2F_CH - 1) / W2F_CH));
+    cfg.blockDim = dim3(32 * W2F_WARPS);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = (cudaStream_t)stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, w2_finish_kernel, part, tiles, nchan, m, gate, (float2 *)R,
+                                             counts, pwr, mean_pwr);
+    return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
 }
