@@ -829,15 +829,24 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
         job_conv(&J[e], &C[e], cv);
     }
     T[nel] = (int)nel * tiles;
-    /* the tables as laid out for max_nel, uploaded whole (they are small) */
     void *tb = p->d_tables;
-    rc = atkb_h2d(p->d_tables, p->h_tables, p->tbl_bytes + up_extra, stream);
-    if (rc == ATKB_OK) rc = atkb_event_record(p->tbl_event, stream);
-    if (rc != ATKB_OK) return rc;
-    p->tbl_event_live = 1;
-    if (cv->doff) {                      /* the int16 offset lives on the device */
-        rc = atkb_pfb_conv_from_offset(tbl_jobs(tb), tbl_carry(tb, p->max_nel), (int)nel, stream);
+    if (cv->doff && nel == 1 && !up_extra) {
+        /* one job with its int16 offset on the device: a kernel writes the
+         * table from its launch parameters and derives the constants there
+         * (no host->device copy, and the host table is free again at once) */
+        rc = atkb_pfb_job_from_params(&J[0], &C[0], tiles, tbl_jobs(tb), tbl_carry(tb, p->max_nel),
+                                      tbl_tiles(tb, p->max_nel), stream);
         if (rc != ATKB_OK) return rc;
+    } else {
+        /* the tables as laid out for max_nel, uploaded whole (they are small) */
+        rc = atkb_h2d(p->d_tables, p->h_tables, p->tbl_bytes + up_extra, stream);
+        if (rc == ATKB_OK) rc = atkb_event_record(p->tbl_event, stream);
+        if (rc != ATKB_OK) return rc;
+        p->tbl_event_live = 1;
+        if (cv->doff) {                  /* the int16 offset lives on the device */
+            rc = atkb_pfb_conv_from_offset(tbl_jobs(tb), tbl_carry(tb, p->max_nel), (int)nel, stream);
+            if (rc != ATKB_OK) return rc;
+        }
     }
     if (big) {
         /* the hops through the separate kernels, a chunk at a time; after the

@@ -232,6 +232,11 @@ int  atkb_pfb_hops_ok(const atkb_bank *B);
 /* the int16 constants of nel device jobs and carries whose doff is set, from
  * that device-held offset (after the table upload, before the tile kernel) */
 int  atkb_pfb_conv_from_offset(atkb_job *d_jobs, atkb_carry *d_carry, int nel, void *stream);
+/* a one-job table written by a kernel from its launch parameters (the job,
+ * its carry, tile_start = {0, tiles}), constants derived as above: no
+ * host->device copy; the tile kernel follows as a programmatic dependent */
+int  atkb_pfb_job_from_params(const atkb_job *J, const atkb_carry *C, int tiles, atkb_job *d_jobs,
+                              atkb_carry *d_carry, int *d_tile_start, void *stream);
 
 int  atkb_pfb_big(const atkb_job *J, const atkb_bank *B, long long h0, int nh, void *scratch, int grid,
                   void *stream);

@@ -1770,6 +1770,33 @@ __global__ void conv_from_offset_kernel(atkb_job *jobs, atkb_carry *carries, int
     jobs[e].cim = carries[e].cim = cim;
 }
 
+/* A one-job table from the launch's own parameters (no host->device copy):
+ * the job, its carry and the tile starts, the int16 constants derived from
+ * the device-held offset when the job has one. */
+__global__ void job_from_params_kernel(const atkb_job J, const atkb_carry C, int tiles, atkb_job *jobs,
+                                       atkb_carry *carries, int *tile_start) {
+    asm volatile("griddepcontrol.launch_dependents;");
+    if (threadIdx.x != 0) return;
+    atkb_job j = J;
+    atkb_carry c = C;
+    if (j.doff) {
+        float cre, cim;
+        doff_consts(j.doff, j.kscale, cre, cim);
+        j.cre = c.cre = cre;
+        j.cim = c.cim = cim;
+    }
+    jobs[0] = j;
+    carries[0] = c;
+    tile_start[0] = 0;
+    tile_start[1] = tiles;
+}
+
+extern "C" int atkb_pfb_job_from_params(const atkb_job *J, const atkb_carry *C, int tiles, atkb_job *d_jobs,
+                                        atkb_carry *d_carry, int *d_tile_start, void *stream) {
+    job_from_params_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(*J, *C, tiles, d_jobs, d_carry, d_tile_start);
+    return cudaGetLastError() == cudaSuccess ? ATKB_OK : ATKB_E_KERNEL;
+}
+
 extern "C" int atkb_pfb_conv_from_offset(atkb_job *d_jobs, atkb_carry *d_carry, int nel, void *stream) {
     if (nel < 1 || nel > 1024) return ATKB_E_ARG;
     conv_from_offset_kernel<<<1, nel, 0, (cudaStream_t)stream>>>(d_jobs, d_carry, nel);
