@@ -830,10 +830,11 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
     }
     T[nel] = (int)nel * tiles;
     void *tb = p->d_tables;
-    if (cv->doff && nel == 1 && !up_extra) {
-        /* one job with its int16 offset on the device: a kernel writes the
-         * table from its launch parameters and derives the constants there
-         * (no host->device copy, and the host table is free again at once) */
+    const int from_params = nel == 1 && !up_extra;
+    if (from_params) {
+        /* one job: a kernel writes the table from its launch parameters (and
+         * derives the int16 constants there when the offset lives on the
+         * device): no host->device copy, and the host table is free at once */
         rc = atkb_pfb_job_from_params(&J[0], &C[0], tiles, tbl_jobs(tb), tbl_carry(tb, p->max_nel),
                                       tbl_tiles(tb, p->max_nel), stream);
         if (rc != ATKB_OK) return rc;
@@ -867,7 +868,7 @@ static int run_step_up(atkdsp_pfb *p, unsigned nel, const void *const *ins, size
         const int work = (int)nel * tiles + (int)nel;
         if (per_hop && !big)
             rc = atkb_pfb_hops(tbl_jobs(tb), tbl_carry(tb, p->max_nel), (int)nel, (int)m, p->d_counters, stream);
-        else if (cv->doff && !big)       /* right after the constants kernel */
+        else if ((from_params || cv->doff) && !big)   /* right after the table kernel */
             rc = atkb_pfb_launch_pdl(tbl_jobs(tb), tbl_tiles(tb, p->max_nel), tbl_carry(tb, p->max_nel),
                                      (int)nel, p->d_counters, p->grid < work ? p->grid : work,
                                      p->bank.smem_bytes, stream);
