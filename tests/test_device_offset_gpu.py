@@ -50,14 +50,15 @@ def test_block_mean_dev_equals_the_host_offset(fmt, n):
     assert np.array_equal(a.cpu().numpy().view(np.uint64), c.cpu().numpy().view(np.uint64))
 
 
-@pytest.mark.parametrize("fmt", ["ci16q11", "ci16"])
-def test_front_end_with_the_dc_estimate_on_the_device(fmt):
+@pytest.mark.parametrize("fmt,M,os_,K", [("ci16q11", 1024, 2, 12), ("ci16", 1024, 2, 12),
+                                          ("ci16q11", 192, 2, 6), ("ci16", 8192, 2, 4)])
+def test_front_end_with_the_dc_estimate_on_the_device(fmt, M, os_, K):
     """Five blocks: block_mean, then the filterbank with W1/W2, the offset of
     block b the mean of block b-1. The host-offset run reads each mean back;
     the device run never does. Outputs, W1, W2 and the means agree bit for
-    bit."""
+    bit: with W1/W2 in the epilogue (nchan 1024), as a separate pass (192,
+    not a power of two) and through the large-filterbank kernels (8192)."""
     from atkdsp_b200 import gpu
-    M, os_, K = 1024, 2, 12
     rng = np.random.default_rng(11)
     blocks = [_raw(fmt, int(rng.integers(40000, 90000)), rng) for _ in range(5)]
     runs = []
