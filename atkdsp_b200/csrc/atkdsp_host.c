@@ -1007,6 +1007,18 @@ ATKDSP_API ptrdiff_t atkdsp_pfb_process_n(atkdsp_pfb *p, const atkdsp_cf32 *cons
         for (e = 0; e < nel && rc == ATKB_OK; ++e)
             rc = atkb_h2d((void *)dins[e], ins[e] + pos, nc * sizeof(atkdsp_cf32), p->stream);
         if (rc != ATKB_OK) break;
+        if (nc == n) {
+            /* the whole call in one chunk: the staging takes the caller's row
+             * stride (m <= out_ld), so the outputs come back in one contiguous
+             * copy instead of one row per channel */
+            rc = run_step(p, nel, (const void *const *)dins, nc, (atkdsp_cf32 *)p->d_out_stage, mc ? mc : 1,
+                          mc, p->stream, &CONV_CF32);
+            if (rc == ATKB_OK && mc > 0)
+                rc = atkb_d2h(out, p->d_out_stage, (size_t)nel * p->nchan * mc * sizeof(atkdsp_cf32), p->stream);
+            col += mc;
+            pos += nc;
+            continue;
+        }
         rc = run_step(p, nel, (const void *const *)dins, nc, (atkdsp_cf32 *)p->d_out_stage, p->out_ld,
                       mc, p->stream, &CONV_CF32);
         if (rc != ATKB_OK) break;
