@@ -661,6 +661,16 @@ def _c2_check(raw, blk, torch, device) -> dict:
         refs.append(y)
         offs.append(complex(np.float32(mean.real), np.float32(mean.imag)))
     rdt = time.perf_counter() - t0
+    ref.lib.atkdsp_set_threads(1)                     # one block again, on one thread
+    rp1 = ref.Pfb(FS, 1024, 2, 12, 80.0, 1)
+    R1, c1 = np.zeros((1024, 1, 1), np.complex64), np.zeros(1024, np.uint32)
+    t0 = time.perf_counter()
+    x, _ = ref.unpack_dc(blocks[0].tobytes(), "ci16q11", 0j)
+    y1 = rp1.process_n([x], 1)
+    ref.pfb_cov_accumulate(y1, 1, 1024, None, R1, c1)
+    ref.pfb_channel_power(y1, 1, 1024)
+    rdt1 = time.perf_counter() - t0
+    ref.lib.atkdsp_set_threads(nth)
     # the benchmarked calls, pipelined as the timed loop issues them
     p = ak.Pfb(FS, 1024, 2, 12, 80.0, 1)
     Rg = torch.zeros((1024, 1, 1), dtype=torch.complex64, device=device)
@@ -695,6 +705,9 @@ def _c2_check(raw, blk, torch, device) -> dict:
     acc["w1_counts_equal"] = bool(np.array_equal(cg.cpu().numpy().astype(np.uint32), cnt))
     acc["offsets_equal_reference"] = bool(off_same)
     return {"accuracy": acc,
+            "cpu_baseline_1thread": {"value": round(blk / rdt1 / 1e6, 2), "unit": "MSamples/s", "cores": 1,
+                                     "kind": "reference", "sample": "one 2,000,000-sample block: unpack_dc, "
+                                                                    "filterbank, W1, W2"},
             "cpu_baseline": {"value": round(3 * blk / rdt / 1e6, 2), "unit": "MSamples/s", "cores": nth,
                              "kind": "reference", "sample": "three 2,000,000-sample blocks: unpack_dc, "
                                                             "filterbank, W1, W2"}}
@@ -772,6 +785,16 @@ def _c3_check(xs, torch, device) -> dict:
     ref.pfb_cov_accumulate(yr, nel, M, None, R, cnt)
     pr, _ = ref.pfb_channel_power(yr, nel, M)
     rdt = time.perf_counter() - t0
+    ref.lib.atkdsp_set_threads(1)                     # 2^18 samples per element, one thread
+    rp1 = ref.Pfb(FS, M, 1, 16, W.ATTEN_BETA8, nel)
+    R1, c1 = np.zeros((M, nel, nel), np.complex64), np.zeros(M, np.uint32)
+    xs1 = [x[: 1 << 18] for x in xs]
+    t0 = time.perf_counter()
+    y1 = rp1.process_n(xs1, nel)
+    ref.pfb_cov_accumulate(y1, nel, M, None, R1, c1)
+    ref.pfb_channel_power(y1, nel, M)
+    rdt1 = time.perf_counter() - t0
+    ref.lib.atkdsp_set_threads(nth)
     p = ak.Pfb(FS, M, 1, 16, W.ATTEN_BETA8, nel)
     st = torch.cuda.ExternalStream(ak.load().atkdsp_gpu_pfb_stream(p.handle), device=device)
     din = [torch.from_numpy(x).to(device) for x in xs]
@@ -789,6 +812,10 @@ def _c3_check(xs, torch, device) -> dict:
     acc["w1_max_rel"] = float(f"{float(np.max(np.abs(Rg - R)) / np.max(np.abs(R))):.3g}")
     acc["w2_power_max_rel"] = float(f"{float(np.max(np.abs(pd.cpu().numpy() - pr) / pr)):.3g}")
     return {"accuracy": acc,
+            "cpu_baseline_1thread": {"value": round(nel * (1 << 18) / rdt1 / 1e6, 2),
+                                     "unit": "MSamples/s (aggregate over elements)", "cores": 1,
+                                     "kind": "reference", "sample": "2^18 samples of each element: process_n, "
+                                                                    "W1, W2"},
             "cpu_baseline": {"value": round(nel * xs[0].size / rdt / 1e6, 2),
                              "unit": "MSamples/s (aggregate over elements)", "cores": nth, "kind": "reference",
                              "sample": "2^20 samples of each element: process_n, W1, W2"}}
@@ -1157,7 +1184,21 @@ def _served_check(torch, device) -> dict:
         h.process_n([x], 1)
         n += x.size
     rdt = time.perf_counter() - t0
+    ref.lib.atkdsp_set_threads(1)                     # the first 64 of those blocks, one thread
+    handles1 = {}
+    n1 = 0
+    t0 = time.perf_counter()
+    for sp, raw in blocks[:64]:
+        h = handles1.get(sp.nchan) or handles1.setdefault(sp.nchan, ref.Pfb(FS, sp.nchan, 2, 16, 80.0, 1))
+        x, _ = ref.unpack_dc(raw, "ci16", 0j)
+        h.process_n([x], 1)
+        n1 += x.size
+    rdt1 = time.perf_counter() - t0
+    ref.lib.atkdsp_set_threads(nth)
     return {"accuracy": acc,
+            "cpu_baseline_1thread": {"value": round(n1 / rdt1 / 1e6, 2), "unit": "MSamples/s", "cores": 1,
+                                     "kind": "reference",
+                                     "sample": "one block of each of the first 64 streams of the trace"},
             "cpu_baseline": {"value": round(n / rdt / 1e6, 2), "unit": "MSamples/s", "cores": nth,
                              "kind": "reference",
                              "sample": "one block of each of the first 512 streams of the trace (unpack_dc + "
@@ -1268,6 +1309,7 @@ def run_ours(args, rep):
             traffic_src = (f"ratio {pj['ratio_traffic_over_algorithmic']} (profiles/pfb_tiles_uneven256.json: "
                            f"{pj.get('captured', 'ncu capture')}) x this launch's algorithmic bytes")
     cpu = _cpu_reference_rate(specs) if "cpu" in arms and not args.no_cpu else None
+    cpu1 = _cpu_reference_rate(specs, budget_s=3.0, threads=1) if "cpu" in arms and not args.no_cpu else None
     acc = _batched_accuracy(specs, torch, device) if "cpu" in arms and not args.no_cpu else None
     total = S * world
     value = total * args.steps / t_batch / 1e6
@@ -1308,6 +1350,9 @@ def run_ours(args, rep):
     if cpu:
         line["cpu_baseline"] = {"value": round(cpu[0], 2), "unit": "MSamples/s", "cores": cpu[1],
                                 "kind": "reference", "sample": cpu[2]}
+    if cpu1:
+        line["cpu_baseline_1thread"] = {"value": round(cpu1[0], 2), "unit": "MSamples/s", "cores": 1,
+                                        "kind": "reference", "sample": cpu1[2]}
     print(json.dumps(line))
 
 
